@@ -1,0 +1,176 @@
+"""B200-native (sm_100a) 3-prime NTT big-integer multiplication.
+
+Python front end of the C ABI in include/fast_mul.h, loaded from the in-tree build
+fast_mul_ntt_b200/lib/libfastmul_b200.so.  The API mirrors the reference's two entry points
+(HJimmyK/fast_mul_ntt src/fast_mul.h:39,45):
+
+    abs_mul64(in1, in2) -> out      # len(out) == len(in1) + len(in2)
+    abs_sqr64(in1)      -> out      # len(out) == 2 * len(in1)
+
+over little-endian numpy uint64 limb arrays, plus device-pointer forms for torch tensors.
+There is no CPU fallback: every product runs the CUDA kernels, and a missing library or
+GPU raises.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libfastmul_b200.so")
+
+FMN_OK = 0
+_ERRNAMES = {1: "FMN_ERR_ARG", 2: "FMN_ERR_CUDA", 3: "FMN_ERR_NOMEM", 4: "FMN_ERR_DEVICE",
+             5: "FMN_ERR_TOO_LARGE"}
+
+# Every symbol include/fast_mul.h declares (checked by the tests).
+EXPORTS = ["abs_mul64", "abs_sqr64", "fmn_init", "fmn_shutdown", "fmn_last_error", "fmn_mul", "fmn_sqr",
+           "fmn_mul_device", "fmn_sqr_device", "fmn_sync", "fmn_workspace_size", "fmn_mul_device_ws",
+           "fmn_ws_status", "fmn_ntt_len"]
+
+_u64 = ctypes.c_uint64
+_u64p = ctypes.POINTER(ctypes.c_uint64)
+_vp = ctypes.c_void_p
+_lib = None
+
+
+class FastMulError(RuntimeError):
+    """A status code other than FMN_OK from the library."""
+
+    def __init__(self, code, msg):
+        super().__init__(f"{_ERRNAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+def load_library(path=None):
+    """Load (once) and return the ctypes handle of the CUDA library."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = path or LIB_PATH
+    if not os.path.exists(p):
+        raise RuntimeError(f"CUDA library not built: {p} (run python -m fast_mul_ntt_b200.build)")
+    lib = ctypes.CDLL(p)
+    lib.abs_mul64.argtypes = [_u64p, _u64, _u64p, _u64, _u64p]
+    lib.abs_mul64.restype = None
+    lib.abs_sqr64.argtypes = [_u64p, _u64, _u64p]
+    lib.abs_sqr64.restype = None
+    lib.fmn_init.argtypes = [ctypes.c_int]
+    lib.fmn_init.restype = ctypes.c_int
+    lib.fmn_shutdown.argtypes = []
+    lib.fmn_shutdown.restype = None
+    lib.fmn_last_error.argtypes = []
+    lib.fmn_last_error.restype = ctypes.c_char_p
+    lib.fmn_mul.argtypes = [_u64p, _u64, _u64p, _u64, _u64p]
+    lib.fmn_mul.restype = ctypes.c_int
+    lib.fmn_sqr.argtypes = [_u64p, _u64, _u64p]
+    lib.fmn_sqr.restype = ctypes.c_int
+    lib.fmn_mul_device.argtypes = [_vp, _u64, _vp, _u64, _vp, _vp]
+    lib.fmn_mul_device.restype = ctypes.c_int
+    lib.fmn_sqr_device.argtypes = [_vp, _u64, _vp, _vp]
+    lib.fmn_sqr_device.restype = ctypes.c_int
+    lib.fmn_sync.argtypes = [_vp]
+    lib.fmn_sync.restype = ctypes.c_int
+    lib.fmn_workspace_size.argtypes = [_u64, _u64, ctypes.c_int]
+    lib.fmn_workspace_size.restype = ctypes.c_size_t
+    lib.fmn_mul_device_ws.argtypes = [_vp, _u64, _vp, _u64, _vp, _vp, ctypes.c_size_t, _vp]
+    lib.fmn_mul_device_ws.restype = ctypes.c_int
+    lib.fmn_ws_status.argtypes = [_vp, _u64, _u64, ctypes.c_int, _vp]
+    lib.fmn_ws_status.restype = ctypes.c_int
+    lib.fmn_ntt_len.argtypes = [_u64, _u64]
+    lib.fmn_ntt_len.restype = _u64
+    if path is None:
+        _lib = lib
+    return lib
+
+
+def _check(rc):
+    if rc != FMN_OK:
+        raise FastMulError(rc, _lib.fmn_last_error().decode())
+
+
+def _limbs(x):
+    return np.ascontiguousarray(x, dtype=np.uint64)
+
+
+def _p(a):
+    return a.ctypes.data_as(_u64p)
+
+
+def init(device=0):
+    """Select ``device`` for the calling thread and upload the twiddle tables."""
+    _check(load_library().fmn_init(device))
+
+
+def abs_mul64(in1, in2, out=None):
+    """in1 * in2 as a numpy uint64 array of len(in1) + len(in2) limbs (host memory)."""
+    lib = load_library()
+    a, b = _limbs(in1), _limbs(in2)
+    if out is None:
+        out = np.empty(len(a) + len(b), dtype=np.uint64)
+    if a.size and b.size and a.ctypes.data == b.ctypes.data and len(a) != len(b):
+        b = b.copy()
+    _check(lib.fmn_mul(_p(a), len(a), _p(b), len(b), _p(out)))
+    return out
+
+
+def abs_sqr64(in1, out=None):
+    """in1 * in1 as a numpy uint64 array of 2 * len(in1) limbs (host memory)."""
+    lib = load_library()
+    a = _limbs(in1)
+    if out is None:
+        out = np.empty(2 * len(a), dtype=np.uint64)
+    _check(lib.fmn_sqr(_p(a), len(a), _p(out)))
+    return out
+
+
+def ntt_len(len1, len2):
+    """Transform length of a product (next power of two >= len1 + len2 - 1)."""
+    return int(load_library().fmn_ntt_len(len1, len2))
+
+
+def _stream_ptr(stream):
+    if stream is None:
+        import torch
+        return torch.cuda.current_stream().cuda_stream
+    return getattr(stream, "cuda_stream", stream)
+
+
+def mul_device(a, b, out, stream=None):
+    """Device product of int64/uint64 CUDA tensors holding limbs; asynchronous on ``stream``
+    (default: torch's current stream).  ``out`` must hold len(a) + len(b) limbs."""
+    lib = load_library()
+    _check(lib.fmn_mul_device(a.data_ptr(), a.numel(), b.data_ptr(), b.numel(), out.data_ptr(),
+                              _stream_ptr(stream)))
+    return out
+
+
+def sqr_device(a, out, stream=None):
+    """Device square of a CUDA limb tensor into ``out`` (2 * len(a) limbs)."""
+    lib = load_library()
+    _check(lib.fmn_sqr_device(a.data_ptr(), a.numel(), out.data_ptr(), _stream_ptr(stream)))
+    return out
+
+
+def sync(stream=None):
+    """Wait for ``stream`` and raise if a kernel reported an internal error."""
+    _check(load_library().fmn_sync(_stream_ptr(stream)))
+
+
+def workspace_size(len1, len2, sqr=False):
+    """Scratch bytes one product needs (for mul_device_ws)."""
+    return int(load_library().fmn_workspace_size(len1, len2, 1 if sqr else 0))
+
+
+def mul_device_ws(a, b, out, ws, stream=None):
+    """Device product with caller-provided scratch ``ws`` (a CUDA tensor of at least
+    workspace_size bytes, 256-byte aligned)."""
+    lib = load_library()
+    _check(lib.fmn_mul_device_ws(a.data_ptr(), a.numel(), b.data_ptr(), b.numel(), out.data_ptr(),
+                                 ws.data_ptr(), ws.numel() * ws.element_size(), _stream_ptr(stream)))
+    return out
+
+
+def ws_status(ws, stream=None):
+    """Raise if the product that used workspace ``ws`` reported a device-side error."""
+    _check(load_library().fmn_ws_status(ws.data_ptr(), 0, 0, 0, _stream_ptr(stream)))

@@ -1,0 +1,343 @@
+// fmn_api.cu -- the C ABI (include/fast_mul.h): abs_mul64 / abs_sqr64 drop-ins and the
+// fmn_* extensions.  Host code only; the kernels live in fmn_ntt.cu.
+//
+// Each device gets a context with a cached scratch workspace, a stream and an event that
+// orders uses of the workspace across streams.  Host-pointer calls copy the operands to the
+// device, run the product and copy the result back (out may alias the inputs, as in the
+// reference, because the inputs are consumed before the output is written).
+#include <cuda_runtime.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <mutex>
+#include <string>
+
+#include "../../include/fast_mul.h"
+#include "fmn_internal.h"
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int set_err(int code, const char* what, cudaError_t e = cudaSuccess) {
+    g_last_error = what;
+    if (e != cudaSuccess) {
+        g_last_error += ": ";
+        g_last_error += cudaGetErrorString(e);
+    }
+    return code;
+}
+
+constexpr int MAX_DEV = 64;
+
+struct DevCtx {
+    std::mutex mu;
+    int dev = -1;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t done = nullptr;       // last job that used `ws`
+    bool done_valid = false;
+    void* ws = nullptr;
+    size_t ws_cap = 0;
+    u64* io = nullptr;                // device staging for host-pointer calls
+    size_t io_cap = 0;
+    unsigned* h_err = nullptr;        // pinned word for reading the device error flag
+};
+
+std::mutex g_ctx_mu;
+DevCtx* g_ctx[MAX_DEV] = {nullptr};
+
+int cur_device(int* dev) {
+    cudaError_t e = cudaGetDevice(dev);
+    if (e != cudaSuccess) return set_err(FMN_ERR_CUDA, "cudaGetDevice", e);
+    if (*dev < 0 || *dev >= MAX_DEV) return set_err(FMN_ERR_ARG, "device index out of range");
+    return FMN_OK;
+}
+
+// Context of the current device, created (tables uploaded) on first use.
+int get_ctx(DevCtx** out) {
+    int dev;
+    int rc = cur_device(&dev);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> lk(g_ctx_mu);
+    if (!g_ctx[dev]) {
+        cudaError_t e = fmn::ensure_tables();
+        if (e != cudaSuccess) return set_err(FMN_ERR_CUDA, "uploading twiddle tables", e);
+        DevCtx* c = new DevCtx();
+        c->dev = dev;
+        if ((e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)) != cudaSuccess ||
+            (e = cudaEventCreateWithFlags(&c->done, cudaEventDisableTiming)) != cudaSuccess ||
+            (e = cudaMallocHost((void**)&c->h_err, sizeof(unsigned))) != cudaSuccess) {
+            delete c;
+            return set_err(FMN_ERR_CUDA, "creating device context", e);
+        }
+        g_ctx[dev] = c;
+    }
+    *out = g_ctx[dev];
+    return FMN_OK;
+}
+
+// Grow the cached workspace of `c` (caller holds c->mu).  The error word at offset 0 is
+// zeroed on allocation.
+int ensure_ws(DevCtx* c, size_t bytes) {
+    if (c->ws_cap >= bytes) return FMN_OK;
+    cudaError_t e;
+    if (c->ws) {
+        if ((e = cudaDeviceSynchronize()) != cudaSuccess) return set_err(FMN_ERR_CUDA, "sync before regrow", e);
+        cudaFree(c->ws);
+        c->ws = nullptr;
+        c->ws_cap = 0;
+    }
+    if ((e = cudaMalloc(&c->ws, bytes)) != cudaSuccess) {
+        cudaGetLastError();
+        return set_err(FMN_ERR_NOMEM, "cudaMalloc of the product workspace", e);
+    }
+    if ((e = cudaMemset(c->ws, 0, 256)) != cudaSuccess) return set_err(FMN_ERR_CUDA, "cudaMemset", e);
+    c->ws_cap = bytes;
+    return FMN_OK;
+}
+
+int ensure_io(DevCtx* c, size_t bytes) {
+    if (c->io_cap >= bytes) return FMN_OK;
+    cudaError_t e;
+    if (c->io) {
+        if ((e = cudaDeviceSynchronize()) != cudaSuccess) return set_err(FMN_ERR_CUDA, "sync before regrow", e);
+        cudaFree(c->io);
+        c->io = nullptr;
+        c->io_cap = 0;
+    }
+    if ((e = cudaMalloc((void**)&c->io, bytes)) != cudaSuccess) {
+        cudaGetLastError();
+        return set_err(FMN_ERR_NOMEM, "cudaMalloc of the operand buffers", e);
+    }
+    c->io_cap = bytes;
+    return FMN_OK;
+}
+
+// Coefficients are < min(len1, len2) * 2^128 and must stay below p0 p1 p2 (about 2^184.7);
+// transforms are limited to 2^30 points by the twiddle tables.
+int check_sizes(u64 len1, u64 len2) {
+    const u64 mn = len1 < len2 ? len1 : len2;
+    if (mn >= (1ull << 56)) return set_err(FMN_ERR_TOO_LARGE, "operand too long for the 3-prime coefficient range");
+    if (len1 + len2 - 1 > (1ull << fmn::MAX_LOG_N))
+        return set_err(FMN_ERR_TOO_LARGE, "product needs a transform longer than 2^30");
+    return FMN_OK;
+}
+
+size_t round256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+// Enqueue a product on stream s using the context workspace (caller holds c->mu).
+int run_job_ctx(DevCtx* c, const fmn::Job& j, cudaStream_t s) {
+    const size_t need = fmn::job_workspace_bytes(j.la, j.lb, j.sqr);
+    int rc = ensure_ws(c, need);
+    if (rc) return rc;
+    cudaError_t e;
+    if (c->done_valid && (e = cudaStreamWaitEvent(s, c->done, 0)) != cudaSuccess)
+        return set_err(FMN_ERR_CUDA, "cudaStreamWaitEvent", e);
+    if ((e = fmn::enqueue_job(j, c->ws, c->ws_cap, s)) != cudaSuccess) return set_err(FMN_ERR_CUDA, "kernel launch", e);
+    if ((e = cudaEventRecord(c->done, s)) != cudaSuccess) return set_err(FMN_ERR_CUDA, "cudaEventRecord", e);
+    c->done_valid = true;
+    return FMN_OK;
+}
+
+// Read and clear the device error word of a workspace after stream s has drained.
+int take_device_error(void* ws, unsigned* h_word, cudaStream_t s) {
+    cudaError_t e;
+    if ((e = cudaMemcpyAsync(h_word, ws, sizeof(unsigned), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(s)) != cudaSuccess)
+        return set_err(FMN_ERR_CUDA, "synchronising the product", e);
+    if (*h_word) {
+        cudaMemsetAsync(ws, 0, sizeof(unsigned), s);
+        cudaStreamSynchronize(s);
+        return set_err(FMN_ERR_DEVICE, "carry scan: bounded wait expired");
+    }
+    return FMN_OK;
+}
+
+int host_product(const u64* in1, u64 len1, const u64* in2, u64 len2, u64* out, int sqr) {
+    const u64 out_len = len1 + len2;
+    if (out_len == 0) return FMN_OK;
+    if (!in1 || !out || (!sqr && !in2)) return set_err(FMN_ERR_ARG, "null pointer");
+    if (len1 == 0 || len2 == 0) {
+        memset(out, 0, out_len * sizeof(u64));
+        return FMN_OK;
+    }
+    int rc = check_sizes(len1, len2);
+    if (rc) return rc;
+    DevCtx* c;
+    if ((rc = get_ctx(&c))) return rc;
+    std::lock_guard<std::mutex> lk(c->mu);
+    // device layout: [in1][in2][out], each 256-byte aligned
+    const size_t o1 = 0, o2 = round256(len1 * 8), oo = o2 + (sqr ? 0 : round256(len2 * 8));
+    if ((rc = ensure_io(c, oo + round256(out_len * 8)))) return rc;
+    char* io = (char*)c->io;
+    cudaError_t e;
+    if ((e = cudaMemcpyAsync(io + o1, in1, len1 * 8, cudaMemcpyHostToDevice, c->stream)) != cudaSuccess)
+        return set_err(FMN_ERR_CUDA, "copying in1 to the device", e);
+    if (!sqr && (e = cudaMemcpyAsync(io + o2, in2, len2 * 8, cudaMemcpyHostToDevice, c->stream)) != cudaSuccess)
+        return set_err(FMN_ERR_CUDA, "copying in2 to the device", e);
+    fmn::Job j;
+    j.a = (const u64*)(io + o1);
+    j.la = len1;
+    j.b = sqr ? j.a : (const u64*)(io + o2);
+    j.lb = len2;
+    j.out = (u64*)(io + oo);
+    j.sqr = sqr;
+    if ((rc = run_job_ctx(c, j, c->stream))) return rc;
+    if ((e = cudaMemcpyAsync(out, io + oo, out_len * 8, cudaMemcpyDeviceToHost, c->stream)) != cudaSuccess)
+        return set_err(FMN_ERR_CUDA, "copying the product to the host", e);
+    return take_device_error(c->ws, c->h_err, c->stream);
+}
+
+int device_product(const u64* d1, u64 len1, const u64* d2, u64 len2, u64* dout, int sqr, void* stream) {
+    const u64 out_len = len1 + len2;
+    if (out_len == 0) return FMN_OK;
+    if (!d1 || !dout || (!sqr && !d2)) return set_err(FMN_ERR_ARG, "null pointer");
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaError_t e;
+    if (len1 == 0 || len2 == 0) {
+        if ((e = cudaMemsetAsync(dout, 0, out_len * 8, s)) != cudaSuccess) return set_err(FMN_ERR_CUDA, "cudaMemsetAsync", e);
+        return FMN_OK;
+    }
+    int rc = check_sizes(len1, len2);
+    if (rc) return rc;
+    DevCtx* c;
+    if ((rc = get_ctx(&c))) return rc;
+    std::lock_guard<std::mutex> lk(c->mu);
+    fmn::Job j;
+    j.a = d1;
+    j.la = len1;
+    j.b = sqr ? d1 : d2;
+    j.lb = len2;
+    j.out = dout;
+    j.sqr = sqr;
+    return run_job_ctx(c, j, s);
+}
+
+void die(const char* fn) {
+    fprintf(stderr, "%s failed: %s\n", fn, g_last_error.c_str());
+    abort();
+}
+
+}  // namespace
+
+extern "C" {
+
+void abs_mul64(const u64* in1, u64 len1, const u64* in2, u64 len2, u64* out) {
+    // Same block and same length: the square (the reference requires in1 != in2,
+    // src/fast_mul.h:37; the product is the same number either way).
+    const int sq = (in1 == in2 && len1 == len2);
+    if (host_product(in1, len1, in2, len2, out, sq)) die("abs_mul64");
+}
+
+void abs_sqr64(const u64* in1, u64 len1, u64* out) {
+    if (host_product(in1, len1, in1, len1, out, 1)) die("abs_sqr64");
+}
+
+int fmn_init(int device) {
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) return set_err(FMN_ERR_CUDA, "cudaSetDevice", e);
+    DevCtx* c;
+    return get_ctx(&c);
+}
+
+void fmn_shutdown(void) {
+    std::lock_guard<std::mutex> lk(g_ctx_mu);
+    int prev = 0;
+    cudaGetDevice(&prev);
+    for (int d = 0; d < MAX_DEV; ++d) {
+        DevCtx* c = g_ctx[d];
+        if (!c) continue;
+        cudaSetDevice(d);
+        cudaDeviceSynchronize();
+        if (c->ws) cudaFree(c->ws);
+        if (c->io) cudaFree(c->io);
+        if (c->h_err) cudaFreeHost(c->h_err);
+        if (c->done) cudaEventDestroy(c->done);
+        if (c->stream) cudaStreamDestroy(c->stream);
+        delete c;
+        g_ctx[d] = nullptr;
+    }
+    cudaSetDevice(prev);
+}
+
+const char* fmn_last_error(void) { return g_last_error.c_str(); }
+
+int fmn_mul(const u64* in1, u64 len1, const u64* in2, u64 len2, u64* out) {
+    return host_product(in1, len1, in2, len2, out, (in1 == in2 && len1 == len2));
+}
+
+int fmn_sqr(const u64* in1, u64 len1, u64* out) { return host_product(in1, len1, in1, len1, out, 1); }
+
+int fmn_mul_device(const u64* d_in1, u64 len1, const u64* d_in2, u64 len2, u64* d_out, void* stream) {
+    return device_product(d_in1, len1, d_in2, len2, d_out, (d_in1 == d_in2 && len1 == len2), stream);
+}
+
+int fmn_sqr_device(const u64* d_in1, u64 len1, u64* d_out, void* stream) {
+    return device_product(d_in1, len1, d_in1, len1, d_out, 1, stream);
+}
+
+int fmn_sync(void* stream) {
+    DevCtx* c;
+    int rc = get_ctx(&c);
+    if (rc) return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaError_t e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return set_err(FMN_ERR_CUDA, "cudaStreamSynchronize", e);
+    std::lock_guard<std::mutex> lk(c->mu);
+    if (!c->ws) return FMN_OK;
+    return take_device_error(c->ws, c->h_err, c->stream);
+}
+
+size_t fmn_workspace_size(u64 len1, u64 len2, int sqr) { return fmn::job_workspace_bytes(len1, len2, sqr ? 1 : 0); }
+
+int fmn_mul_device_ws(const u64* d_in1, u64 len1, const u64* d_in2, u64 len2, u64* d_out, void* d_ws,
+                      size_t ws_bytes, void* stream) {
+    const u64 out_len = len1 + len2;
+    if (out_len == 0) return FMN_OK;
+    if (!d_in1 || !d_in2 || !d_out || !d_ws) return set_err(FMN_ERR_ARG, "null pointer");
+    if (((uintptr_t)d_ws & 255) != 0) return set_err(FMN_ERR_ARG, "workspace must be 256-byte aligned");
+    int rc = check_sizes(len1, len2);
+    if (rc) return rc;
+    const int sq = (d_in1 == d_in2 && len1 == len2);
+    if (ws_bytes < fmn::job_workspace_bytes(len1, len2, sq)) return set_err(FMN_ERR_ARG, "workspace too small");
+    fmn::Job j;
+    j.a = d_in1;
+    j.la = len1;
+    j.b = d_in2;
+    j.lb = len2;
+    j.out = d_out;
+    j.sqr = sq;
+    cudaError_t e = cudaMemsetAsync(d_ws, 0, sizeof(unsigned), (cudaStream_t)stream);   // status word
+    if (e == cudaSuccess) e = fmn::enqueue_job(j, d_ws, ws_bytes, (cudaStream_t)stream);
+    if (e != cudaSuccess) return set_err(FMN_ERR_CUDA, "kernel launch", e);
+    return FMN_OK;
+}
+
+int fmn_ws_status(const void* d_ws, u64 len1, u64 len2, int sqr, void* stream) {
+    (void)len1;
+    (void)len2;
+    (void)sqr;
+    if (!d_ws) return set_err(FMN_ERR_ARG, "null pointer");
+    unsigned word = 0;
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaError_t e;
+    if ((e = cudaMemcpyAsync(&word, d_ws, sizeof(word), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(s)) != cudaSuccess)
+        return set_err(FMN_ERR_CUDA, "reading the workspace status", e);
+    if (word) {
+        cudaMemsetAsync((void*)d_ws, 0, sizeof(unsigned), s);
+        cudaStreamSynchronize(s);
+        return set_err(FMN_ERR_DEVICE, "carry scan: bounded wait expired");
+    }
+    return FMN_OK;
+}
+
+u64 fmn_ntt_len(u64 len1, u64 len2) {
+    const u64 conv = len1 + len2 ? len1 + len2 - 1 : 0;
+    u64 n = 1;
+    while (n < conv) n <<= 1;
+    return n;
+}
+
+}  // extern "C"

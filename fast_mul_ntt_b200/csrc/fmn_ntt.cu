@@ -1,0 +1,899 @@
+// fmn_ntt.cu -- sm_100a kernels of the 3-prime NTT multiplication path and their launchers.
+//
+// Path (reference src/fast_mul.c:308-396 abs_mul64, :398-460 abs_sqr64):
+//   limbs -> Montgomery residues mod p0, p1, p2 (entry fused into the first pass)
+//   -> forward NTT of each operand (four-step, passes of <= 2^9 points per CTA)
+//   -> pointwise product fused between the last forward and first inverse pass
+//   -> inverse NTT -> CRT to a 192-bit coefficient -> carry propagation by a single-pass
+//      decoupled look-back scan (replacing the serial loop at src/fast_mul.c:378-389).
+//
+// Data layout in HBM: one product owns a workspace holding, per operand, three residue
+// arrays of N = 2^n u64 (prime-major: prime i at base + i*N).  The transform is the
+// four-step decomposition: pass p works on contiguous blocks of B_p = 2^(n - sum of earlier
+// pass bits) elements, viewed as a [2^m][B_p / 2^m] row-major matrix; each CTA takes a tile
+// of 16 adjacent columns (a 16 x 8 B = 128 B stretch of every row) and performs the 2^m-point
+// decimation-in-frequency sub-transform down each column in shared memory, then multiplies
+// by the four-step twiddle w_B^(column * frequency).  The last pass works on contiguous
+// blocks (16 blocks per tile).  Spectra are left in the permuted order that the matching
+// inverse passes consume; only final limbs are observable.
+//
+// Shared-memory tile: element (row j, column c) lives at (j << 4) | (c ^ (j & 15)); the XOR
+// swizzle keeps both the row-wise (16 columns of a row) and the column-wise (consecutive rows
+// of one column) access patterns free of bank conflicts.
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string.h>
+
+#include <mutex>
+#include <vector>
+
+#include "fmn_arith.cuh"
+#include "fmn_internal.h"
+
+namespace fmn {
+
+constexpr int NT = 256;           // threads per CTA, NTT passes
+constexpr int TC = 16;            // columns per tile
+constexpr int RT_MAXLOGL = 12;    // round tables cover sub-transforms up to 2^12 points
+constexpr int TWB = 15;           // two-level twiddle tables: w^x = HI[x >> 15] * LO[x & 0x7fff]
+static_assert(2 * TWB == MAX_LOG_N, "two-level table covers roots of order 2^30");
+
+// ------------------------------------------------------------------ round structure
+// A 2^m-point sub-transform is done in rounds of radix 2^RB held in registers.
+__host__ __device__ constexpr int rounds_count(int logl) {
+    return logl == 0 ? 0 : logl <= 4 ? 1 : logl <= 8 ? 2 : 3;
+}
+__host__ __device__ constexpr int round_bits(int logl, int idx) {
+    return logl <= 4 ? logl
+         : logl <= 8 ? (idx == 0 ? (logl + 1) / 2 : logl / 2)
+                     : (idx == 0 ? (logl + 2) / 3 : idx == 1 ? (logl + 1) / 3 : logl / 3);
+}
+__host__ __device__ constexpr int round_top(int logl, int idx) {
+    return idx == 0 ? logl - 1 : round_top(logl, idx - 1) - round_bits(logl, idx - 1);
+}
+
+// Round twiddle tables.  For a round of RB bits whose top index bit is TOP, the group with
+// low offset q (q < 2^(TOP-RB+1)) needs, for stage s (span 2^(TOP-s)) and u < 2^(RB-1-s):
+//     w_{2^(TOP-s+1)}^(q + u * 2^(TOP-RB+1))
+// stored at rt_off(RB, TOP) + q * 2^RB + (2^RB - 2^(RB-s)) + u (entry 2^RB - 1 is padding).
+__host__ __device__ constexpr int rt_base(int r) {
+    return r <= 1 ? 0 : rt_base(r - 1) + (1 << (r - 1)) * ((1 << (RT_MAXLOGL - r + 2)) - 1);
+}
+__host__ __device__ constexpr int rt_off(int r, int top) {
+    return rt_base(r) + (1 << r) * ((1 << (top - r + 1)) - 1);
+}
+constexpr int RT_SIZE = rt_base(5);
+
+__device__ __align__(16) u64 g_rt[2][3][RT_SIZE];      // [forward/inverse][prime]
+__device__ __align__(16) u64 g_tw[2][3][1 << TWB];     // [low/high level][prime]
+
+// w_{2^30}^x for x < 2^30 (Montgomery form, < 2p).
+template <int I>
+__device__ __forceinline__ u64 root30(u32 x) {
+    return mmul<I>(__ldg(&g_tw[1][I][x >> TWB]), __ldg(&g_tw[0][I][x & ((1u << TWB) - 1)]));
+}
+
+__device__ __forceinline__ int sw(int j, int c) { return (j << 4) | (c ^ (j & 15)); }
+
+// ------------------------------------------------------------------ kernel arguments
+enum { M_FWD = 0, M_FWD_LAST = 1, M_FUSED = 2, M_INV = 3 };
+
+struct PassArgs {
+    const u64* src;   // ENTRY: limbs of the operand being transformed
+    u64 len;          // ENTRY: number of limbs
+    u64* data;        // residue arrays of the operand being transformed
+    u64* other;       // M_FUSED: the other operand's spectrum; the product is written here
+    u64 N;            // transform length
+    int logB;         // log2 block length of this pass
+    int ncols;        // contiguous passes: number of blocks (columns) in a tile, <= 16
+};
+
+// ------------------------------------------------------------------ one round
+// Runs all radix-2^RB groups of one round.  `ld(j, c)` fetches element (j, c), `st(j, c, v)`
+// stores it.  QFAST maps consecutive threads to consecutive rows of one column (coalesced
+// global access of contiguous blocks); otherwise consecutive threads take consecutive columns.
+template <int I, int LOGL, int RB, int TOP, bool INV, bool QFAST, class LD, class ST>
+__device__ __forceinline__ void run_round(LD ld, ST st) {
+    constexpr int L = 1 << LOGL, R = 1 << RB, SPL = TOP - RB + 1, SP = 1 << SPL;
+    constexpr int GPC = L / R;
+    constexpr int G = GPC * TC;
+    constexpr bool LOWEST = (SPL == 0);
+    const u64* tab = &g_rt[INV ? 1 : 0][I][rt_off(RB, TOP)];
+#pragma unroll 1
+    for (int gi = threadIdx.x; gi < G; gi += NT) {
+        int c, g;
+        if (QFAST) {
+            g = gi % GPC;
+            c = gi / GPC;
+        } else {
+            c = gi & (TC - 1);
+            g = gi >> 4;
+        }
+        const int qlo = g & (SP - 1);
+        const int row0 = qlo + ((g >> SPL) << (TOP + 1));
+        u64 x[R];
+#pragma unroll
+        for (int t = 0; t < R; ++t) x[t] = ld(row0 + t * SP, c);
+        const u64* tw = tab + qlo * R;
+        if (!INV) {
+#pragma unroll
+            for (int s = 0; s < RB; ++s) {
+                const int half = R >> (s + 1);
+#pragma unroll
+                for (int t = 0; t < R; ++t) {
+                    if (t & half) continue;
+                    const int u = t & (half - 1);
+                    if (LOWEST && u == 0)
+                        bfly_dif1<I>(x[t], x[t + half]);
+                    else
+                        bfly_dif<I>(x[t], x[t + half], __ldg(tw + (R - (R >> s)) + u));
+                }
+            }
+        } else {
+#pragma unroll
+            for (int s = RB - 1; s >= 0; --s) {
+                const int half = R >> (s + 1);
+#pragma unroll
+                for (int t = 0; t < R; ++t) {
+                    if (t & half) continue;
+                    const int u = t & (half - 1);
+                    if (LOWEST && u == 0)
+                        bfly_dit1<I>(x[t], x[t + half]);
+                    else
+                        bfly_dit<I>(x[t], x[t + half], __ldg(tw + (R - (R >> s)) + u));
+                }
+            }
+        }
+#pragma unroll
+        for (int t = 0; t < R; ++t) st(row0 + t * SP, c, x[t]);
+    }
+}
+
+// Rounds IDX.. of a sub-transform.  Forward order: round 0 holds the top bits.  Inverse
+// order: inverse round k undoes forward round NR-1-k.  The first round reads with `ld0`, the
+// last writes with `stl`, the rest go through shared memory.
+template <int I, int LOGL, bool INV, bool CONTIG, int IDX, class LD0, class STL>
+__device__ __forceinline__ void rounds(u64* sm, LD0 ld0, STL stl) {
+    constexpr int NR = rounds_count(LOGL);
+    constexpr int FR = INV ? NR - 1 - IDX : IDX;
+    constexpr int RB = round_bits(LOGL, FR), TOP = round_top(LOGL, FR);
+    constexpr bool QF = CONTIG && (TOP == LOGL - 1);
+    auto lds = [sm](int j, int c) { return sm[sw(j, c)]; };
+    auto sts = [sm](int j, int c, u64 v) { sm[sw(j, c)] = v; };
+    if constexpr (NR == 1) {
+        run_round<I, LOGL, RB, TOP, INV, QF>(ld0, stl);
+    } else if constexpr (IDX == 0) {
+        run_round<I, LOGL, RB, TOP, INV, QF>(ld0, sts);
+        __syncthreads();
+        rounds<I, LOGL, INV, CONTIG, 1>(sm, ld0, stl);
+    } else if constexpr (IDX == NR - 1) {
+        run_round<I, LOGL, RB, TOP, INV, QF>(lds, stl);
+    } else {
+        run_round<I, LOGL, RB, TOP, INV, QF>(lds, sts);
+        __syncthreads();
+        rounds<I, LOGL, INV, CONTIG, IDX + 1>(sm, ld0, stl);
+    }
+}
+
+// ------------------------------------------------------------------ pass bodies
+template <int I>
+__device__ __forceinline__ u64 entry_val(const u64* __restrict__ src, u64 len, u64 g) {
+    return g < len ? mmul<I>(__ldg(src + g), PrimeX<I>::R2) : 0ull;   // limb * R mod p
+}
+
+// Forward strided pass (pass p < P-1 of a multi-pass transform).
+template <int I, int LOGL, bool ENTRY>
+__device__ __forceinline__ void body_fwd(u64* sm, const PassArgs& a, u64 tile) {
+    const int logS = a.logB - LOGL;
+    const u64 tpb_log = logS - 4;
+    const u64 blk = tile >> tpb_log;
+    const u32 col0 = (u32)((tile & ((1ull << tpb_log) - 1)) << 4);
+    const u64 gbase = (blk << a.logB) + col0;
+    u64* __restrict__ d = a.data + (u64)I * a.N;
+    const u64* __restrict__ src = a.src;
+    const u64 len = a.len;
+    auto ld0 = [=](int j, int c) -> u64 {
+        const u64 g = gbase + c + ((u64)j << logS);
+        if constexpr (ENTRY) return entry_val<I>(src, len, g);
+        else return d[g];
+    };
+    const int shift = MAX_LOG_N - a.logB;
+    auto stl = [=](int j, int c, u64 v) {
+        const u32 k = __brev((u32)j) >> (32 - LOGL);
+        const u32 e = (col0 + c) * k;                       // < B <= 2^30
+        d[gbase + c + ((u64)j << logS)] = mmul<I>(v, root30<I>(e << shift));
+    };
+    rounds<I, LOGL, false, false, 0>(sm, ld0, stl);
+}
+
+// Inverse strided pass: inverse four-step twiddle, then the inverse sub-transform.
+template <int I, int LOGL>
+__device__ __forceinline__ void body_inv(u64* sm, const PassArgs& a, u64 tile) {
+    const int logS = a.logB - LOGL;
+    const u64 tpb_log = logS - 4;
+    const u64 blk = tile >> tpb_log;
+    const u32 col0 = (u32)((tile & ((1ull << tpb_log) - 1)) << 4);
+    const u64 gbase = (blk << a.logB) + col0;
+    u64* __restrict__ d = a.data + (u64)I * a.N;
+    const int shift = MAX_LOG_N - a.logB;
+    auto ld0 = [=](int j, int c) -> u64 {
+        const u32 k = __brev((u32)j) >> (32 - LOGL);
+        const u32 e = (col0 + c) * k;
+        const u32 x = (0u - (e << shift)) & ((1u << MAX_LOG_N) - 1);   // w^-e
+        return mmul<I>(d[gbase + c + ((u64)j << logS)], red1<I>(root30<I>(x)));
+    };
+    auto stl = [=](int j, int c, u64 v) { d[gbase + c + ((u64)j << logS)] = v; };
+    rounds<I, LOGL, true, false, 0>(sm, ld0, stl);
+}
+
+// Forward last pass over contiguous blocks (operand A of a product).
+template <int I, int LOGL, bool ENTRY>
+__device__ __forceinline__ void body_fwd_last(u64* sm, const PassArgs& a, u64 tile) {
+    constexpr int L = 1 << LOGL;
+    const u64 gbase = tile << (LOGL + 4);
+    const int ncols = a.ncols;
+    u64* __restrict__ d = a.data + (u64)I * a.N;
+    const u64* __restrict__ src = a.src;
+    const u64 len = a.len;
+    auto ld0 = [=](int j, int c) -> u64 {
+        if (c >= ncols) return 0ull;
+        const u64 g = gbase + (u64)c * L + j;
+        if constexpr (ENTRY) return entry_val<I>(src, len, g);
+        else return d[g];
+    };
+    auto stl = [=](int j, int c, u64 v) {
+        if (c < ncols) d[gbase + (u64)c * L + j] = v;
+    };
+    if constexpr (LOGL == 0) {
+        if (threadIdx.x < (unsigned)ncols) stl(0, threadIdx.x, ld0(0, threadIdx.x));
+    } else {
+        rounds<I, LOGL, false, true, 0>(sm, ld0, stl);
+    }
+}
+
+// The lowest forward round, the pointwise product and the lowest inverse round of one
+// contiguous tile, all in registers.
+template <int I, int LOGL, bool SQR, class LD, class ST>
+__device__ __forceinline__ void fused_lowest(LD ld, ST st, const u64* __restrict__ oth, u64 gbase,
+                                             int ncols) {
+    constexpr int L = 1 << LOGL;
+    constexpr int NR = rounds_count(LOGL);
+    constexpr int RB = round_bits(LOGL, NR - 1);
+    constexpr int R = 1 << RB;
+    constexpr int G = (L / R) * TC;
+    const u64* tf = &g_rt[0][I][rt_off(RB, RB - 1)];
+    const u64* ti = &g_rt[1][I][rt_off(RB, RB - 1)];
+#pragma unroll 1
+    for (int gi = threadIdx.x; gi < G; gi += NT) {
+        const int c = gi & (TC - 1);
+        const int row0 = (gi >> 4) << RB;
+        u64 x[R];
+#pragma unroll
+        for (int t = 0; t < R; ++t) x[t] = ld(row0 + t, c);
+#pragma unroll
+        for (int s = 0; s < RB; ++s) {
+            const int half = R >> (s + 1);
+#pragma unroll
+            for (int t = 0; t < R; ++t) {
+                if (t & half) continue;
+                const int u = t & (half - 1);
+                if (u == 0) bfly_dif1<I>(x[t], x[t + half]);
+                else bfly_dif<I>(x[t], x[t + half], __ldg(tf + (R - (R >> s)) + u));
+            }
+        }
+        if (c < ncols) {
+            const u64* po = oth + gbase + (u64)c * L + row0;
+#pragma unroll
+            for (int t = 0; t < R; ++t) x[t] = mmul<I>(x[t], SQR ? x[t] : po[t]);
+        }
+#pragma unroll
+        for (int s = RB - 1; s >= 0; --s) {
+            const int half = R >> (s + 1);
+#pragma unroll
+            for (int t = 0; t < R; ++t) {
+                if (t & half) continue;
+                const int u = t & (half - 1);
+                if (u == 0) bfly_dit1<I>(x[t], x[t + half]);
+                else bfly_dit<I>(x[t], x[t + half], __ldg(ti + (R - (R >> s)) + u));
+            }
+        }
+#pragma unroll
+        for (int t = 0; t < R; ++t) st(row0 + t, c, x[t]);
+    }
+}
+
+// Fused last pass: forward last pass of the second operand (or of the only operand when
+// squaring), pointwise product with the first operand's spectrum, inverse last pass.
+// The result overwrites the first operand's spectrum (`other`).
+template <int I, int LOGL, bool ENTRY, bool SQR>
+__device__ __forceinline__ void body_fused(u64* sm, const PassArgs& a, u64 tile) {
+    constexpr int L = 1 << LOGL;
+    constexpr int NR = rounds_count(LOGL);
+    const u64 gbase = tile << (LOGL + 4);
+    const int ncols = a.ncols;
+    const u64* __restrict__ d = a.data + (u64)I * a.N;
+    u64* __restrict__ o = a.other + (u64)I * a.N;
+    const u64* __restrict__ src = a.src;
+    const u64 len = a.len;
+    auto ldg = [=](int j, int c) -> u64 {
+        if (c >= ncols) return 0ull;
+        const u64 g = gbase + (u64)c * L + j;
+        if constexpr (ENTRY) return entry_val<I>(src, len, g);
+        else return d[g];
+    };
+    auto stg = [=](int j, int c, u64 v) {
+        if (c < ncols) o[gbase + (u64)c * L + j] = v;
+    };
+    auto lds = [sm](int j, int c) { return sm[sw(j, c)]; };
+    auto sts = [sm](int j, int c, u64 v) { sm[sw(j, c)] = v; };
+    if constexpr (LOGL == 0) {
+        if (threadIdx.x < (unsigned)ncols) {
+            const int c = threadIdx.x;
+            const u64 x = ldg(0, c);
+            stg(0, c, mmul<I>(x, SQR ? x : o[gbase + c]));
+        }
+    } else if constexpr (NR == 1) {
+        fused_lowest<I, LOGL, SQR>(ldg, stg, o, gbase, ncols);
+    } else {
+        // forward rounds 0 .. NR-2
+        constexpr int RB0 = round_bits(LOGL, 0);
+        run_round<I, LOGL, RB0, LOGL - 1, false, true>(ldg, sts);
+        __syncthreads();
+        if constexpr (NR == 3) {
+            constexpr int RB1 = round_bits(LOGL, 1), T1 = round_top(LOGL, 1);
+            run_round<I, LOGL, RB1, T1, false, false>(lds, sts);
+            __syncthreads();
+        }
+        fused_lowest<I, LOGL, SQR>(lds, sts, o, gbase, ncols);
+        __syncthreads();
+        if constexpr (NR == 3) {
+            constexpr int RB1 = round_bits(LOGL, 1), T1 = round_top(LOGL, 1);
+            run_round<I, LOGL, RB1, T1, true, false>(lds, sts);
+            __syncthreads();
+        }
+        run_round<I, LOGL, RB0, LOGL - 1, true, true>(lds, stg);
+    }
+}
+
+// ------------------------------------------------------------------ pass kernels
+template <int MODE, int LOGL, bool ENTRY, bool SQR>
+__global__ void __launch_bounds__(NT) k_pass(PassArgs a) {
+    extern __shared__ __align__(16) u64 sm[];
+    const int prime = blockIdx.x % 3;
+    const u64 tile = blockIdx.x / 3;
+#define FMN_BODY(I)                                                        \
+    if constexpr (MODE == M_FWD) body_fwd<I, LOGL, ENTRY>(sm, a, tile);             \
+    else if constexpr (MODE == M_INV) body_inv<I, LOGL>(sm, a, tile);               \
+    else if constexpr (MODE == M_FWD_LAST) body_fwd_last<I, LOGL, ENTRY>(sm, a, tile); \
+    else body_fused<I, LOGL, ENTRY, SQR>(sm, a, tile);
+    if (prime == 0) {
+        FMN_BODY(0)
+    } else if (prime == 1) {
+        FMN_BODY(1)
+    } else {
+        FMN_BODY(2)
+    }
+#undef FMN_BODY
+}
+
+// ------------------------------------------------------------------ CRT + carry
+// crt3 (src/core.h:77-104) then carry propagation.  Coefficient c_j < p0 p1 p2 < 2^185 spans
+// three limbs; output limb j receives s_j = c_j[0] + c_{j-1}[1] + c_{j-2}[2] < 3 * 2^64
+// plus an incoming carry in [0, 3].  A span of limbs maps its incoming carry to its outgoing
+// carry by a function {0..3} -> {0..3} (packed as 4 x 2 bits); these compose associatively,
+// which gives a parallel scan: per-thread functions, a CTA scan, and a decoupled look-back
+// across CTAs in the order CTAs obtain tickets.
+constexpr int CNT = 256;           // threads per CTA
+constexpr int CE = 8;              // limbs per thread
+constexpr int CTILE = CNT * CE;    // limbs per CTA
+constexpr u32 ID_FN = 0xE4;        // identity map
+constexpr u32 ST_AGG = 1u << 8, ST_PRE = 2u << 8;
+constexpr long SPIN_LIMIT = 1l << 22;   // bounded waits: ~ seconds at most, then error flag
+
+struct CrtArgs {
+    const u64* res;     // three natural-order residue arrays (prime i at res + i*N), < 4p
+    u64 N;
+    u64 nvalid;         // coefficients that may be nonzero: min(conv_len, N)
+    u64* out;
+    u64 out_len;
+    u64 cst[3];         // M_i^-1 * N^-1 mod p_i (plain)
+    u32* state;         // per-CTA look-back words, zeroed before launch
+    u32* ticket;        // zeroed before launch
+    u32* err;
+};
+
+__host__ __device__ constexpr u64 m_lo(int i) {
+    return (u64)(i == 0 ? (unsigned __int128)Prime<1>::P * Prime<2>::P
+                 : i == 1 ? (unsigned __int128)Prime<0>::P * Prime<2>::P
+                          : (unsigned __int128)Prime<0>::P * Prime<1>::P);
+}
+__host__ __device__ constexpr u64 m_hi(int i) {
+    return (u64)((i == 0 ? (unsigned __int128)Prime<1>::P * Prime<2>::P
+                  : i == 1 ? (unsigned __int128)Prime<0>::P * Prime<2>::P
+                           : (unsigned __int128)Prime<0>::P * Prime<1>::P) >> 64);
+}
+constexpr unsigned __int128 P01 = (unsigned __int128)Prime<0>::P * Prime<1>::P;
+constexpr unsigned __int128 PL = (unsigned __int128)(u64)P01 * Prime<2>::P;
+constexpr unsigned __int128 PH = (unsigned __int128)(u64)(P01 >> 64) * Prime<2>::P;
+constexpr u64 PALL0 = (u64)PL;
+constexpr u64 PALL1 = (u64)((PL >> 64) + (u64)PH);
+constexpr u64 PALL2 = (u64)((((PL >> 64) + (u64)PH) >> 64) + (u64)(PH >> 64));
+
+__device__ __forceinline__ void acc_mul(u64 y, u64 ml, u64 mh, u64& w0, u64& w1, u64& w2) {
+    const unsigned __int128 lo = (unsigned __int128)y * ml;
+    const unsigned __int128 hi = (unsigned __int128)y * mh;
+    const unsigned __int128 s0 = (unsigned __int128)w0 + (u64)lo;
+    const unsigned __int128 s1 = (unsigned __int128)w1 + (u64)(lo >> 64) + (u64)hi + (u64)(s0 >> 64);
+    w0 = (u64)s0;
+    w1 = (u64)s1;
+    w2 = w2 + (u64)(hi >> 64) + (u64)(s1 >> 64);
+}
+
+__device__ __forceinline__ void crt_coef(const CrtArgs& a, u64 j, u64& w0, u64& w1, u64& w2) {
+    w0 = w1 = w2 = 0;
+    if (j >= a.nvalid) return;
+    const u64 y0 = red1<0>(mmul<0>(a.res[j], a.cst[0]));
+    const u64 y1 = red1<1>(mmul<1>(a.res[a.N + j], a.cst[1]));
+    const u64 y2 = red1<2>(mmul<2>(a.res[2 * a.N + j], a.cst[2]));
+    acc_mul(y0, m_lo(0), m_hi(0), w0, w1, w2);
+    acc_mul(y1, m_lo(1), m_hi(1), w0, w1, w2);
+    acc_mul(y2, m_lo(2), m_hi(2), w0, w1, w2);
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {   // sum < 3 * P: at most two subtractions
+        const bool ge = w2 != PALL2 ? w2 > PALL2 : w1 != PALL1 ? w1 > PALL1 : w0 >= PALL0;
+        if (ge) {
+            const u64 b0 = w0 < PALL0;
+            w0 -= PALL0;
+            const u64 t1 = w1 - PALL1;
+            const u64 b1 = (w1 < PALL1) | (t1 < b0);
+            w1 = t1 - b0;
+            w2 = w2 - PALL2 - b1;
+        }
+    }
+}
+
+__device__ __forceinline__ u32 fn_apply(u32 f, u32 c) { return (f >> (2 * c)) & 3u; }
+__device__ __forceinline__ u32 fn_compose(u32 later, u32 earlier) {   // later o earlier
+    u32 r = 0;
+#pragma unroll
+    for (u32 c = 0; c < 4; ++c) r |= fn_apply(later, fn_apply(earlier, c)) << (2 * c);
+    return r;
+}
+
+__global__ void __launch_bounds__(CNT) k_crt_carry(CrtArgs a) {
+    __shared__ u32 s_tile;
+    __shared__ u64 s_hi1[CNT / 32], s_hi2[CNT / 32], s_hi2b[CNT / 32];
+    __shared__ u32 s_warp[CNT / 32];
+    __shared__ u32 s_cin;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid == 0) s_tile = atomicAdd(a.ticket, 1u);
+    __syncthreads();
+    const u64 tile = s_tile;
+    const u64 j0 = tile * CTILE + (u64)tid * CE;
+
+    u64 w0[CE], w1[CE], w2[CE];
+#pragma unroll
+    for (int e = 0; e < CE; ++e) crt_coef(a, j0 + e, w0[e], w1[e], w2[e]);
+
+    // high words of the two coefficients just below j0
+    u64 p1w1 = __shfl_up_sync(0xffffffffu, w1[CE - 1], 1);
+    u64 p1w2 = __shfl_up_sync(0xffffffffu, w2[CE - 1], 1);
+    u64 p2w2 = __shfl_up_sync(0xffffffffu, w2[CE - 2], 1);
+    if (lane == 31) {
+        s_hi1[warp] = w1[CE - 1];
+        s_hi2[warp] = w2[CE - 1];
+        s_hi2b[warp] = w2[CE - 2];
+    }
+    __syncthreads();
+    if (lane == 0) {
+        if (warp > 0) {
+            p1w1 = s_hi1[warp - 1];
+            p1w2 = s_hi2[warp - 1];
+            p2w2 = s_hi2b[warp - 1];
+        } else {
+            u64 q0, q1, q2, r0, r1, r2;
+            if (j0 >= 1) crt_coef(a, j0 - 1, q0, q1, q2); else q0 = q1 = q2 = 0;
+            if (j0 >= 2) crt_coef(a, j0 - 2, r0, r1, r2); else r0 = r1 = r2 = 0;
+            p1w1 = q1;
+            p1w2 = q2;
+            p2w2 = r2;
+        }
+    }
+
+    // s_j = lo + h * 2^64
+    u64 lo[CE];
+    u32 h[CE];
+#pragma unroll
+    for (int e = 0; e < CE; ++e) {
+        const u64 x1 = e >= 1 ? w1[e - 1] : p1w1;
+        const u64 x2 = e >= 2 ? w2[e - 2] : (e == 1 ? p1w2 : p2w2);
+        const u64 t = w0[e] + x1;
+        u32 hh = t < x1;
+        const u64 t2 = t + x2;
+        hh += t2 < x2;
+        lo[e] = t2;
+        h[e] = hh;
+    }
+    // carry-transfer function of this thread's limbs
+    u32 f = 0;
+#pragma unroll
+    for (u32 cin = 0; cin < 4; ++cin) {
+        u64 c = cin;
+#pragma unroll
+        for (int e = 0; e < CE; ++e) {
+            const u64 t = lo[e] + c;
+            c = h[e] + (t < c);
+        }
+        f |= (u32)c << (2 * cin);
+    }
+    // CTA inclusive scan (Kogge-Stone in the warp, then across warps)
+    u32 inc = f;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const u32 o = __shfl_up_sync(0xffffffffu, inc, d);
+        if (lane >= d) inc = fn_compose(inc, o);
+    }
+    u32 exc = __shfl_up_sync(0xffffffffu, inc, 1);
+    if (lane == 0) exc = ID_FN;
+    if (lane == 31) s_warp[warp] = inc;
+    __syncthreads();
+    if (tid == 0) {
+        u32 agg = ID_FN;
+        for (int w = 0; w < CNT / 32; ++w) {
+            const u32 t = s_warp[w];
+            s_warp[w] = agg;                 // exclusive prefix of warp w
+            agg = fn_compose(t, agg);
+        }
+        volatile u32* st = a.state;
+        u32 cin = 0;
+        if (tile == 0) {
+            atomicExch(&a.state[0], ST_PRE | fn_apply(agg, 0));
+        } else {
+            atomicExch(&a.state[tile], ST_AGG | agg);
+            u32 acc = ID_FN;                 // composition of the aggregates seen so far
+            long p = (long)tile - 1;
+            long spins = 0;
+            while (true) {
+                const u32 v = st[p];
+                if (v & ST_PRE) {
+                    cin = fn_apply(acc, v & 0xff);
+                    break;
+                }
+                if (v & ST_AGG) {
+                    acc = fn_compose(acc, v & 0xff);
+                    if (--p < 0) {
+                        cin = fn_apply(acc, 0);
+                        break;
+                    }
+                    continue;
+                }
+                if (++spins > SPIN_LIMIT) {
+                    atomicOr(a.err, 1u);
+                    cin = 0;
+                    break;
+                }
+                __nanosleep(64);
+            }
+            atomicExch(&a.state[tile], ST_PRE | fn_apply(agg, cin));
+        }
+        s_cin = cin;
+    }
+    __syncthreads();
+    u64 c = fn_apply(exc, fn_apply(s_warp[warp], s_cin));
+#pragma unroll
+    for (int e = 0; e < CE; ++e) {
+        const u64 t = lo[e] + c;
+        c = h[e] + (t < c);
+        if (j0 + e < a.out_len) a.out[j0 + e] = t;
+    }
+}
+
+// ------------------------------------------------------------------ host: tables
+static u64 h_mulmod(u64 a, u64 b, u64 m) { return (u64)(((unsigned __int128)a * b) % m); }
+static u64 h_pow(u64 b, u64 e, u64 m) {
+    u64 r = 1;
+    b %= m;
+    while (e) {
+        if (e & 1) r = h_mulmod(r, b, m);
+        b = h_mulmod(b, b, m);
+        e >>= 1;
+    }
+    return r;
+}
+static const u64 kP[3] = {Prime<0>::P, Prime<1>::P, Prime<2>::P};
+static const u64 kG[3] = {5, 5, 3};   // primitive roots (src/data.h:69-71)
+
+struct HostTables {
+    std::vector<u64> rt;   // [2][3][RT_SIZE]
+    std::vector<u64> tw;   // [2][3][1 << TWB]
+};
+
+static const HostTables& host_tables() {
+    static HostTables T;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        T.rt.assign((size_t)2 * 3 * RT_SIZE, 0);
+        T.tw.assign((size_t)2 * 3 * (1u << TWB), 0);
+        for (int i = 0; i < 3; ++i) {
+            const u64 p = kP[i];
+            const u64 r1 = (u64)((((unsigned __int128)1) << 64) % p);
+            const u64 w = h_pow(kG[i], (p - 1) >> MAX_LOG_N, p);     // root of order 2^30
+            std::vector<u64> lo(1u << TWB), hi(1u << TWB);
+            const u64 whi = h_pow(w, 1ull << TWB, p);
+            u64 cl = 1, ch = 1;
+            for (u32 x = 0; x < (1u << TWB); ++x) {
+                lo[x] = cl;
+                hi[x] = ch;
+                cl = h_mulmod(cl, w, p);
+                ch = h_mulmod(ch, whi, p);
+            }
+            auto wpow = [&](u64 e) {   // w^e, e mod 2^30
+                e &= (1ull << MAX_LOG_N) - 1;
+                return h_mulmod(hi[e >> TWB], lo[e & ((1u << TWB) - 1)], p);
+            };
+            auto mont = [&](u64 v) { return h_mulmod(v, r1, p); };
+            for (u32 x = 0; x < (1u << TWB); ++x) {
+                T.tw[((size_t)0 * 3 + i) * (1u << TWB) + x] = mont(lo[x]);
+                T.tw[((size_t)1 * 3 + i) * (1u << TWB) + x] = mont(hi[x]);
+            }
+            for (int r = 1; r <= 4; ++r)
+                for (int top = r - 1; top < RT_MAXLOGL; ++top) {
+                    const int R = 1 << r, spl = top - r + 1;
+                    for (int q = 0; q < (1 << spl); ++q)
+                        for (int s = 0; s < r; ++s)
+                            for (int u = 0; u < (R >> (s + 1)); ++u) {
+                                // w_{2^(top-s+1)}^(q + u 2^spl) = w^((q + u 2^spl) 2^(30-(top-s+1)))
+                                const u64 e = ((u64)q + ((u64)u << spl)) << (MAX_LOG_N - (top - s + 1));
+                                const size_t at = (size_t)rt_off(r, top) + (size_t)q * R + (R - (R >> s)) + u;
+                                T.rt[((size_t)0 * 3 + i) * RT_SIZE + at] = mont(wpow(e));
+                                T.rt[((size_t)1 * 3 + i) * RT_SIZE + at] =
+                                    mont(wpow((1ull << MAX_LOG_N) - (e & ((1ull << MAX_LOG_N) - 1))));
+                            }
+                }
+        }
+    });
+    return T;
+}
+
+// ------------------------------------------------------------------ host: launch plumbing
+typedef void (*PassKernel)(PassArgs);
+
+template <int MODE, int LOGL, bool ENTRY, bool SQR>
+static PassKernel kernel_ptr() {
+    return k_pass<MODE, LOGL, ENTRY, SQR>;
+}
+
+// Table of every kernel instance: [mode-variant][logl]
+enum { V_FWD, V_FWD_E, V_LAST, V_LAST_E, V_FUSED, V_FUSED_E, V_SQR, V_SQR_E, V_INV, NV };
+
+template <int LOGL>
+static void fill_row(PassKernel (&t)[NV][MAX_PASS_BITS + 1]) {
+    t[V_FWD][LOGL] = LOGL >= 5 ? kernel_ptr<M_FWD, (LOGL >= 5 ? LOGL : 5), false, false>() : nullptr;
+    t[V_FWD_E][LOGL] = LOGL >= 5 ? kernel_ptr<M_FWD, (LOGL >= 5 ? LOGL : 5), true, false>() : nullptr;
+    t[V_INV][LOGL] = LOGL >= 5 ? kernel_ptr<M_INV, (LOGL >= 5 ? LOGL : 5), false, false>() : nullptr;
+    t[V_LAST][LOGL] = kernel_ptr<M_FWD_LAST, LOGL, false, false>();
+    t[V_LAST_E][LOGL] = kernel_ptr<M_FWD_LAST, LOGL, true, false>();
+    t[V_FUSED][LOGL] = kernel_ptr<M_FUSED, LOGL, false, false>();
+    t[V_FUSED_E][LOGL] = kernel_ptr<M_FUSED, LOGL, true, false>();
+    t[V_SQR][LOGL] = kernel_ptr<M_FUSED, LOGL, false, true>();
+    t[V_SQR_E][LOGL] = kernel_ptr<M_FUSED, LOGL, true, true>();
+}
+
+struct KernelTable {
+    PassKernel k[NV][MAX_PASS_BITS + 1];
+    KernelTable() {
+        memset(k, 0, sizeof(k));
+        fill_row<0>(k);
+        fill_row<1>(k);
+        fill_row<2>(k);
+        fill_row<3>(k);
+        fill_row<4>(k);
+        fill_row<5>(k);
+        fill_row<6>(k);
+        fill_row<7>(k);
+        fill_row<8>(k);
+        fill_row<9>(k);
+    }
+};
+static const KernelTable& ktab() {
+    static KernelTable t;
+    return t;
+}
+
+static size_t pass_smem(int logl) { return (size_t)TC * ((size_t)1 << logl) * sizeof(u64); }
+
+cudaError_t ensure_tables() {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    static std::mutex mu;
+    static std::vector<int> done;
+    std::lock_guard<std::mutex> lock(mu);
+    for (int d : done)
+        if (d == dev) return cudaSuccess;
+    const HostTables& T = host_tables();
+    e = cudaMemcpyToSymbol(g_rt, T.rt.data(), T.rt.size() * sizeof(u64));
+    if (e != cudaSuccess) return e;
+    e = cudaMemcpyToSymbol(g_tw, T.tw.data(), T.tw.size() * sizeof(u64));
+    if (e != cudaSuccess) return e;
+    const KernelTable& K = ktab();
+    for (int v = 0; v < NV; ++v)
+        for (int l = 0; l <= MAX_PASS_BITS; ++l)
+            if (K.k[v][l]) {
+                e = cudaFuncSetAttribute((const void*)K.k[v][l], cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)pass_smem(l));
+                if (e != cudaSuccess) return e;
+            }
+    done.push_back(dev);
+    return cudaSuccess;
+}
+
+Plan make_plan(int n) {
+    Plan p;
+    p.n = n;
+    if (n <= MAX_PASS_BITS) {
+        p.passes = 1;
+        p.bits[0] = n;
+        return p;
+    }
+    p.passes = (n + MAX_PASS_BITS - 1) / MAX_PASS_BITS;
+    for (int i = 0; i < p.passes; ++i) p.bits[i] = n / p.passes + (i < n % p.passes ? 1 : 0);
+    return p;
+}
+
+static u64 ceil_pow2(u64 x) {
+    u64 r = 1;
+    while (r < x) r <<= 1;
+    return r;
+}
+static int ilog2(u64 x) {
+    int r = 0;
+    while ((1ull << r) < x) ++r;
+    return r;
+}
+static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+// Workspace of one product: [error word, 256 B][A residues][B residues][ticket + state].
+// The error word sits at offset 0 of every workspace and is never cleared by a job, so a
+// caller can read (and clear) it after any number of jobs.
+struct WsLayout {
+    u64 N;
+    int n;
+    size_t a, b, ticket, state, total;
+    u64 ncta;
+};
+static WsLayout ws_layout(u64 la, u64 lb, int sqr) {
+    WsLayout w;
+    memset(&w, 0, sizeof(w));
+    const u64 out_len = la + lb;
+    if (la == 0 || lb == 0) return w;
+    w.N = ceil_pow2(out_len - 1);
+    w.n = ilog2(w.N);
+    w.ncta = (out_len + CTILE - 1) / CTILE;
+    size_t off = 256;
+    w.a = off;
+    off = align256(off + 3 * w.N * sizeof(u64));
+    w.b = off;
+    if (!sqr) off = align256(off + 3 * w.N * sizeof(u64));
+    w.ticket = off;
+    w.state = off + 16;
+    off = align256(w.state + w.ncta * sizeof(u32));
+    w.total = off;
+    return w;
+}
+
+size_t job_workspace_bytes(u64 la, u64 lb, int sqr) {
+    const size_t t = ws_layout(la, lb, sqr).total;
+    return t ? t : 256;
+}
+
+static cudaError_t launch_pass(int variant, int logl, const PassArgs& a, u64 tiles, cudaStream_t s) {
+    PassKernel k = ktab().k[variant][logl];
+    if (!k) return cudaErrorInvalidValue;
+    k<<<(unsigned)(tiles * 3), NT, pass_smem(logl), s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t enqueue_job(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s) {
+    const u64 out_len = j.la + j.lb;
+    if (out_len == 0) return cudaSuccess;
+    if (j.la == 0 || j.lb == 0) return cudaMemsetAsync(j.out, 0, out_len * sizeof(u64), s);
+    const int sqr = j.sqr ? 1 : 0;
+    const WsLayout w = ws_layout(j.la, j.lb, sqr);
+    if (ws_bytes < w.total || w.n > MAX_LOG_N) return cudaErrorInvalidValue;
+    cudaError_t e = ensure_tables();
+    if (e != cudaSuccess) return e;
+    char* base = (char*)ws;
+    u64* A = (u64*)(base + w.a);
+    u64* B = sqr ? A : (u64*)(base + w.b);
+    const Plan pl = make_plan(w.n);
+    const int P = pl.passes;
+    const u64 N = w.N;
+
+    PassArgs pa;
+    memset(&pa, 0, sizeof(pa));
+    pa.N = N;
+    pa.ncols = TC;
+    int logB[MAX_PASSES];
+    logB[0] = w.n;
+    for (int p = 1; p < P; ++p) logB[p] = logB[p - 1] - pl.bits[p - 1];
+    const int lastl = pl.bits[P - 1];
+    const u64 nblk_last = N >> lastl;
+    const u64 tiles_last = (nblk_last + TC - 1) / TC;
+    const int ncols_last = nblk_last < (u64)TC ? (int)nblk_last : TC;
+
+    // forward strided passes of one operand
+    auto fwd_strided = [&](const u64* src, u64 len, u64* data) -> cudaError_t {
+        for (int p = 0; p + 1 < P; ++p) {
+            pa.src = src;
+            pa.len = len;
+            pa.data = data;
+            pa.logB = logB[p];
+            const cudaError_t r =
+                launch_pass(p == 0 ? V_FWD_E : V_FWD, pl.bits[p], pa, N >> (pl.bits[p] + 4), s);
+            if (r != cudaSuccess) return r;
+        }
+        return cudaSuccess;
+    };
+
+    if (!sqr) {
+        if ((e = fwd_strided(j.a, j.la, A)) != cudaSuccess) return e;
+        pa.src = j.a;
+        pa.len = j.la;
+        pa.data = A;
+        pa.logB = logB[P - 1];
+        pa.ncols = ncols_last;
+        if ((e = launch_pass(P == 1 ? V_LAST_E : V_LAST, lastl, pa, tiles_last, s)) != cudaSuccess) return e;
+        pa.ncols = TC;
+        if ((e = fwd_strided(j.b, j.lb, B)) != cudaSuccess) return e;
+        pa.src = j.b;
+        pa.len = j.lb;
+        pa.data = B;
+        pa.other = A;
+        pa.logB = logB[P - 1];
+        pa.ncols = ncols_last;
+        if ((e = launch_pass(P == 1 ? V_FUSED_E : V_FUSED, lastl, pa, tiles_last, s)) != cudaSuccess) return e;
+    } else {
+        if ((e = fwd_strided(j.a, j.la, A)) != cudaSuccess) return e;
+        pa.src = j.a;
+        pa.len = j.la;
+        pa.data = A;
+        pa.other = A;
+        pa.logB = logB[P - 1];
+        pa.ncols = ncols_last;
+        if ((e = launch_pass(P == 1 ? V_SQR_E : V_SQR, lastl, pa, tiles_last, s)) != cudaSuccess) return e;
+    }
+    pa.ncols = TC;
+    pa.src = nullptr;
+    pa.other = nullptr;
+    for (int p = P - 2; p >= 0; --p) {
+        pa.data = A;
+        pa.logB = logB[p];
+        if ((e = launch_pass(V_INV, pl.bits[p], pa, N >> (pl.bits[p] + 4), s)) != cudaSuccess) return e;
+    }
+
+    // CRT constants: M_i^-1 * N^-1 mod p_i
+    CrtArgs ca;
+    memset(&ca, 0, sizeof(ca));
+    for (int i = 0; i < 3; ++i) {
+        const u64 p = kP[i];
+        const unsigned __int128 M = (unsigned __int128)kP[(i + 1) % 3] * kP[(i + 2) % 3];
+        const u64 minv = h_pow((u64)(M % p), p - 2, p);
+        const u64 ninv = h_pow(N % p, p - 2, p);
+        ca.cst[i] = h_mulmod(minv, ninv, p);
+    }
+    ca.res = A;
+    ca.N = N;
+    ca.nvalid = (out_len - 1) < N ? (out_len - 1) : N;
+    ca.out = j.out;
+    ca.out_len = out_len;
+    ca.state = (u32*)(base + w.state);
+    ca.ticket = (u32*)(base + w.ticket);
+    ca.err = (u32*)base;
+    e = cudaMemsetAsync(base + w.ticket, 0, w.total - w.ticket, s);
+    if (e != cudaSuccess) return e;
+    k_crt_carry<<<(unsigned)w.ncta, CNT, 0, s>>>(ca);
+    return cudaGetLastError();
+}
+
+}  // namespace fmn

@@ -1,0 +1,87 @@
+/*
+ * fast_mul.h -- C ABI of the B200 (sm_100a) 3-prime NTT big-integer multiplication library.
+ *
+ * Drop-in for HJimmyK/fast_mul_ntt src/fast_mul.h: the two entry points below keep the
+ * reference's names, argument meaning and error behaviour.  Numbers are little-endian
+ * arrays of 64-bit limbs (least significant limb first).  Everything else is a namespaced
+ * extension (fmn_*) for callers that want status codes, device pointers or batching.
+ *
+ * Link: -lfastmul_b200 (fast_mul_ntt_b200/lib/libfastmul_b200.so).  One CUDA device is used
+ * per calling thread (the current device, or device 0).
+ */
+#ifndef FAST_MUL_B200_H
+#define FAST_MUL_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef unsigned long long u64;
+
+/* out = in1 * in2; out has exactly len1 + len2 limbs, all written (the top limb may be 0).
+ * in1 and in2 must not be the same block (their values may be equal); out may alias either
+ * input.  Host pointers, synchronous.  On failure prints a message to stderr and calls
+ * abort(), as the reference does on allocation failure.
+ * Replaces: abs_mul64, src/fast_mul.h:39 (implementation src/fast_mul.c:308-396). */
+void abs_mul64(const u64* in1, u64 len1, const u64* in2, u64 len2, u64* out);
+
+/* out = in1 * in1; out has exactly 2 * len1 limbs.
+ * Replaces: abs_sqr64, src/fast_mul.h:45 (implementation src/fast_mul.c:398-460). */
+void abs_sqr64(const u64* in1, u64 len1, u64* out);
+
+/* ----------------------------------------------------------------- extensions */
+
+/* Status codes returned by every fmn_* call. */
+enum {
+    FMN_OK = 0,
+    FMN_ERR_ARG = 1,        /* bad argument (null pointer, length out of range, in1 == in2) */
+    FMN_ERR_CUDA = 2,       /* a CUDA runtime call failed; see fmn_last_error() */
+    FMN_ERR_NOMEM = 3,      /* device or pinned host memory could not be allocated */
+    FMN_ERR_DEVICE = 4,     /* a kernel reported an internal error (bounded wait expired) */
+    FMN_ERR_TOO_LARGE = 5   /* transform length above 2^30 or coefficient range exceeded */
+};
+
+/* Select and initialise a device for the calling thread (optional: the first call does it
+ * with the current device).  Uploads the twiddle tables.  Counterpart of
+ * fft_small_init (fft_small/fft_small.h:33). */
+int fmn_init(int device);
+/* Release cached device and pinned buffers of this process (fft_small_clear,
+ * fft_small/fft_small.h:34). */
+void fmn_shutdown(void);
+/* Text of the last error seen by the calling thread ("" if none). */
+const char* fmn_last_error(void);
+
+/* Status-returning forms of abs_mul64 / abs_sqr64 (host pointers, synchronous). */
+int fmn_mul(const u64* in1, u64 len1, const u64* in2, u64 len2, u64* out);
+int fmn_sqr(const u64* in1, u64 len1, u64* out);
+
+/* Device-pointer forms, asynchronous on `stream` (a cudaStream_t, NULL = default stream).
+ * Scratch comes from a per-device cache owned by the library; calls on one device are
+ * serialised by a lock while they are enqueued.  Internal errors of the kernels are
+ * reported by the next fmn_sync(stream). */
+int fmn_mul_device(const u64* d_in1, u64 len1, const u64* d_in2, u64 len2, u64* d_out, void* stream);
+int fmn_sqr_device(const u64* d_in1, u64 len1, u64* d_out, void* stream);
+/* Wait for `stream` and report device-side errors of earlier fmn_*_device calls. */
+int fmn_sync(void* stream);
+
+/* Scratch a product needs, for callers that manage memory themselves. */
+size_t fmn_workspace_size(u64 len1, u64 len2, int sqr);
+/* Device-pointer product with caller-provided scratch (d_ws: fmn_workspace_size bytes,
+ * 256-byte aligned, not shared by calls in flight).  No allocation, no lock.  The first
+ * word of d_ws is a status word, cleared by this call and read by fmn_ws_status. */
+int fmn_mul_device_ws(const u64* d_in1, u64 len1, const u64* d_in2, u64 len2, u64* d_out,
+                      void* d_ws, size_t ws_bytes, void* stream);
+/* After the stream has finished, read the device-side error flag of such a call. */
+int fmn_ws_status(const void* d_ws, u64 len1, u64 len2, int sqr, void* stream);
+
+/* Transform length used for a product: the next power of two >= len1 + len2 - 1
+ * (int_ceil2, src/fast_mul.c:299-312). */
+u64 fmn_ntt_len(u64 len1, u64 len2);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FAST_MUL_B200_H */
