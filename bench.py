@@ -1,0 +1,389 @@
+"""Benchmark of abs_mul64 at 10,000,000 x 10,000,000 limbs on B200 (one product per step).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints ONE JSON line (rank 0).  With N > 1 the script is launched by torchrun, one rank per
+GPU; every rank multiplies its own copy of the operands (replicas: a single product does
+not shard), and the timed region is bracketed by a barrier and a device synchronize, its
+length taken as the max over ranks.
+
+  value   products/s with operands and output resident in HBM (device API), all ranks;
+  e2e     the same metric through the C ABI abs_mul64 with pinned host buffers: each step
+          copies both operands host->device and the product device->host;
+  roofline / roofline_int
+          the dominant kernel, timed live with CUDA events inside the timed region, against
+          the measured HBM copy bandwidth (MEASURED_PEAKS.json) and against the measured
+          peak of this library's Montgomery product (microbenchmark run here);
+  cpu_baseline
+          the reference's own src/ abs_mul64 (oracle/_ref, compiled unmodified) on one host
+          core, one 10M x 10M product (rank 0, N = 1 only).
+
+--impl reference times that reference CPU implementation with all host cores (independent
+products in parallel threads) on the same workload and prints the same JSON line.
+"""
+import argparse
+import ctypes
+import hashlib
+import json
+import os
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+LEN1 = LEN2 = 10_000_000
+SEED = 0
+KIND = "uniform"
+METRIC = "abs_mul64 products/s at 10M x 10M limbs (bit-exact)"
+UNIT = "products/s"
+WORKLOAD = "abs_mul64 10,000,000 x 10,000,000 limbs (uniform u64, seed 0), NTT length 2^25 over 3 primes"
+DATA = "synthetic: splitmix64 seed 0, uniform u64 limbs, top limb nonzero (no dataset involved)"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the reference CPU timing")
+    ap.add_argument("--len", type=int, default=None, help="override operand length (profiling runs)")
+    return ap.parse_args()
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def golden_digest(op, kind, l1, l2):
+    path = os.path.join(ROOT, "tests", "golden", "golden_vectors.json")
+    with open(path) as f:
+        for c in json.load(f)["cases"]:
+            if (c["op"], c["kind"], c["len1"], c["len2"], c["seed"]) == (op, kind, l1, l2, SEED):
+                return c["sha256"]
+    return None
+
+
+def digest(x):
+    return hashlib.sha256(np.ascontiguousarray(x, dtype="<u8").tobytes()).hexdigest()
+
+
+# ----------------------------------------------------------------------------- clocks
+class ClockSampler:
+    """Samples SM clock and clock-event (throttle) reasons through NVML in a thread."""
+
+    REASONS = {0x8: "hw_slowdown", 0x40: "hw_thermal_slowdown", 0x20: "sw_thermal_slowdown",
+               0x4: "sw_power_cap", 0x80: "hw_power_brake_slowdown", 0x100: "display_clock_setting",
+               0x2: "applications_clocks_setting", 0x1: "gpu_idle", 0x10: "sync_boost"}
+
+    def __init__(self, index):
+        self.ok = False
+        self.samples = []
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(index)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+            self.ok = True
+        except Exception:
+            self.ok = False
+        self._stop = threading.Event()
+
+    def _run(self):
+        nv = self.nv
+        while not self._stop.is_set():
+            try:
+                mhz = nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)
+                try:
+                    r = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                except Exception:
+                    r = nv.nvmlDeviceGetCurrentClocksThrottleReasons(self.h)
+                self.samples.append((mhz, r))
+            except Exception:
+                pass
+            time.sleep(0.005)
+
+    def __enter__(self):
+        if self.ok:
+            self.t = threading.Thread(target=self._run, daemon=True)
+            self.t.start()
+        return self
+
+    def __exit__(self, *a):
+        if self.ok:
+            self._stop.set()
+            self.t.join()
+
+    def summary(self):
+        if not self.ok or not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": getattr(self, "max_mhz", None), "reasons": [], "samples": 0}
+        mhz = sorted(s[0] for s in self.samples)
+        bits = 0
+        for _, r in self.samples:
+            bits |= int(r)
+        reasons = sorted(name for b, name in self.REASONS.items() if bits & b and name != "gpu_idle")
+        return {"sm_mhz": mhz[len(mhz) // 2], "sm_max_mhz": self.max_mhz, "reasons": reasons,
+                "samples": len(self.samples)}
+
+
+# ----------------------------------------------------------------------------- CPU reference
+def ref_lib():
+    from oracle.oracle import RefFastMul, Oracle
+    if RefFastMul.available():
+        return RefFastMul(), "reference"
+    return Oracle(), "port"
+
+
+def cpu_baseline(a, b):
+    """One product with the reference's single-threaded src/ code on this host."""
+    lib, kind = ref_lib()
+    w1, w2 = a[:1_000_000].copy(), b[:1_000_000].copy()
+    lib.mul(w1, w2)                                    # warm-up: code and page faults
+    t0 = time.perf_counter()
+    out = lib.mul(a, b)
+    dt = time.perf_counter() - t0
+    return {"value": 1.0 / dt, "unit": UNIT, "cores": 1, "kind": kind,
+            "sample": f"one {len(a)} x {len(b)}-limb abs_mul64 (seed 0) after a 1M x 1M warm-up, "
+                      f"{dt:.2f} s, single thread (the reference has no threading)",
+            "seconds_per_product": dt}, out
+
+
+def host_threads_and_mem():
+    cores = os.cpu_count() or 1
+    try:
+        import psutil
+        avail = psutil.virtual_memory().available
+    except Exception:
+        avail = 16 << 30
+    per = 1.6 * (1 << 30)         # reference scratch (4 x 2^25 u64) + output, per product
+    return max(1, min(cores, int(avail * 0.6 / per), 64)), cores
+
+
+def run_reference(args, ws, rank):
+    if rank != 0:
+        return
+    from fast_mul_ntt_b200 import synth
+    a, b = synth.operands(KIND, LEN1, LEN2, SEED)
+    lib, kind = ref_lib()
+    threads, cores = host_threads_and_mem()
+    outs = [np.zeros(LEN1 + LEN2, np.uint64) for _ in range(threads)]
+
+    def one_round(x, y):
+        ts = [threading.Thread(target=lambda i=i: lib.mul(x, y, outs[i]) if kind == "reference"
+                               else lib.mul(x, y)) for i in range(threads)]
+        for t in ts:
+            t.start()
+        for t in ts:
+            t.join()
+
+    wa, wb = a[:1_000_000].copy(), b[:1_000_000].copy()
+    for _ in range(max(1, min(args.warmup, 3))):
+        one_round(wa, wb)                              # warm-up on a 1M x 1M sample
+    budget = 150.0
+    rounds, t_total = 0, 0.0
+    while rounds < args.steps:
+        t0 = time.perf_counter()
+        one_round(a, b)
+        t_total += time.perf_counter() - t0
+        rounds += 1
+        if t_total > budget:
+            break
+    want = golden_digest("mul", KIND, LEN1, LEN2)
+    exact = (digest(outs[0]) == want) if kind == "reference" else None
+    value = threads * rounds / t_total
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws,
+            "steps": rounds, "warmup": args.warmup, "ms_per_step": 1e3 * t_total / rounds,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": DATA,
+            "config": {"workload": WORKLOAD, "len1": LEN1, "len2": LEN2, "ntt_len": 1 << 25,
+                       "parallelism": f"{threads} independent products in parallel host threads"},
+            "bit_exact": exact,
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
+                             "sample": f"{rounds} rounds of {threads} concurrent {LEN1} x {LEN2} products "
+                                       f"(reference src/ abs_mul64, compiled unmodified, one call per "
+                                       f"thread; {cores} host cores); warm-up on 1M x 1M",
+                             "seconds_per_round": t_total / rounds},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------------------------- ours
+def run_ours(args, ws, rank, local):
+    import torch
+    import fast_mul_ntt_b200 as fmn
+    from fast_mul_ntt_b200 import synth
+
+    dist = ws > 1
+    if dist:
+        import datetime
+        import torch.distributed as tdist
+        torch.cuda.set_device(local)
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                 device_id=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    fmn.init(local)
+    l1 = args.len or LEN1
+    l2 = args.len or LEN2
+    a, b = synth.operands(KIND, l1, l2, SEED)
+    da = torch.from_numpy(a.view(np.int64)).to(dev)
+    db = torch.from_numpy(b.view(np.int64)).to(dev)
+    dout = torch.empty(l1 + l2, dtype=torch.int64, device=dev)
+    stream = torch.cuda.Stream(device=dev)
+
+    def step():
+        fmn.mul_device(da, db, dout, stream=stream)
+
+    # correctness of the timed configuration (against the reference's own output digest)
+    with torch.cuda.stream(stream):
+        step()
+    fmn.sync(stream)
+    got = dout.cpu().numpy().view(np.uint64)
+    want = golden_digest("mul", KIND, l1, l2)
+    bit_exact = (digest(got) == want) if want else None
+
+    for _ in range(args.warmup):
+        step()
+    stream.synchronize()
+
+    def barrier():
+        if dist:
+            torch.distributed.barrier()
+
+    sampler = ClockSampler(local)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    fmn.profile_enable(True)
+    fmn.profile_take()
+    barrier()
+    torch.cuda.synchronize(dev)
+    with sampler:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            step()
+        ev1.record(stream)
+        torch.cuda.synchronize(dev)
+    barrier()
+    fmn.profile_enable(False)
+    prof = fmn.profile_take()
+    fmn.sync(stream)
+    ms = ev0.elapsed_time(ev1)
+    if dist:
+        t = torch.tensor([ms], device=dev, dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    value = ws * args.steps / (ms * 1e-3)
+
+    # e2e through the reference-facing C ABI with pinned host buffers
+    lib = fmn.load_library()
+    ha = torch.from_numpy(a.view(np.int64)).pin_memory().numpy().view(np.uint64)
+    hb = torch.from_numpy(b.view(np.int64)).pin_memory().numpy().view(np.uint64)
+    hout = torch.empty(l1 + l2, dtype=torch.int64).pin_memory().numpy().view(np.uint64)
+    P = ctypes.POINTER(ctypes.c_uint64)
+    pa, pb, po = ha.ctypes.data_as(P), hb.ctypes.data_as(P), hout.ctypes.data_as(P)
+    e2e_steps = max(3, min(args.steps, 10))
+    lib.abs_mul64(pa, l1, pb, l2, po)                  # warm-up (buffers, tables)
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        lib.abs_mul64(pa, l1, pb, l2, po)
+    e2e_s = time.perf_counter() - t0
+    if dist:
+        t = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    barrier()
+    e2e_exact = bool(np.array_equal(hout, got))
+
+    result = None
+    if rank == 0:
+        peaks = {}
+        try:
+            with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+                peaks = json.load(f)
+        except Exception:
+            pass
+        hbm_peak = peaks.get("hbm_gbs")
+        hbm_src = "measured" if hbm_peak else "fallback"
+        hbm_peak = hbm_peak or 6650.0
+        mm_peak, bf_peak = fmn.bench_modmul()
+        dom = max(prof.items(), key=lambda kv: kv[1]["ms"])
+        name, st = dom
+        per_launch_ms = st["ms"] / max(1, st["launches"])
+        bytes_per_launch = st["bytes"] / max(1, st["launches"])
+        mm_per_launch = st["modmuls"] / max(1, st["launches"])
+        achieved_gbs = bytes_per_launch / (per_launch_ms * 1e-3) / 1e9
+        achieved_mm = mm_per_launch / (per_launch_ms * 1e-3)
+        traffic = None
+        tpath = os.path.join(ROOT, "profiles", "traffic.json")
+        if os.path.exists(tpath):
+            try:
+                with open(tpath) as f:
+                    traffic = json.load(f).get(name)
+            except Exception:
+                traffic = None
+        total_prof = sum(v["ms"] for v in prof.values()) or 1.0
+        all_mm = sum(v["modmuls"] for v in prof.values()) / args.steps
+        per_step_ms = ms / args.steps
+        result = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": per_step_ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": DATA,
+            "config": {"workload": WORKLOAD if l1 == LEN1 else f"abs_mul64 {l1} x {l2} limbs",
+                       "len1": l1, "len2": l2, "ntt_len": fmn.ntt_len(l1, l2),
+                       "parallelism": "replicas: one independent product per GPU" if ws > 1 else "single GPU",
+                       "l2_policy": "no flush: operands (160 MB) and residues (1.6 GB) per product exceed the 126 MB L2"},
+            "us_per_product": 1e3 * per_step_ms,
+            "limbs_per_s": (l1 + l2) * value,
+            "bit_exact": bit_exact,
+            "roofline": {"bound": "hbm", "kernel": name, "achieved": achieved_gbs, "peak": hbm_peak,
+                         "unit": "GB/s", "frac": achieved_gbs / hbm_peak, "traffic": traffic,
+                         "peak_source": f"{hbm_src} (MEASURED_PEAKS.json hbm_gbs)" if hbm_src == "measured"
+                         else "fallback 6.65 TB/s",
+                         "algorithmic_bytes_per_launch": bytes_per_launch, "ms_per_launch": per_launch_ms},
+            "roofline_int": {"bound": "imad (integer multiply pipe)", "kernel": name,
+                             "achieved": achieved_mm / 1e9, "peak": mm_peak / 1e9, "unit": "Gmodmul/s",
+                             "frac": achieved_mm / mm_peak,
+                             "peak_source": "measured: independent Montgomery-product chains on this GPU",
+                             "butterfly_peak": bf_peak / 1e9,
+                             "frac_of_butterfly_peak": achieved_mm / bf_peak,
+                             "algorithmic_modmuls_per_launch": mm_per_launch,
+                             "whole_product_frac": (all_mm / (per_step_ms * 1e-3)) / mm_peak},
+            "kernels": {k: {"ms_per_step": v["ms"] / args.steps, "launches_per_step": v["launches"] / args.steps,
+                            "share": v["ms"] / total_prof} for k, v in prof.items()},
+            "gpu_launches": fmn.launches_per_product(l1, l2) * args.steps,
+            "clocks": sampler.summary(),
+            "e2e": {"value": ws * e2e_steps / e2e_s, "unit": UNIT,
+                    "h2d_bytes_per_step": 8 * (l1 + l2), "d2h_bytes_per_step": 8 * (l1 + l2),
+                    "steps": e2e_steps, "bit_exact": e2e_exact,
+                    "path": "abs_mul64 (C ABI) on pinned host buffers, synchronous"},
+        }
+    if dist:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline and l1 == LEN1:
+        cb, cout = cpu_baseline(a, b)
+        cb["bit_exact_vs_gpu"] = bool(np.array_equal(cout, got))
+        result["cpu_baseline"] = cb
+    if rank == 0:
+        print(json.dumps(result), flush=True)
+
+
+def main():
+    args = parse()
+    ws, rank, local = dist_env()
+    if args.impl == "reference":
+        run_reference(args, ws, rank)
+    else:
+        run_ours(args, ws, rank, local)
+
+
+if __name__ == "__main__":
+    main()

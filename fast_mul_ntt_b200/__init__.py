@@ -26,7 +26,9 @@ _ERRNAMES = {1: "FMN_ERR_ARG", 2: "FMN_ERR_CUDA", 3: "FMN_ERR_NOMEM", 4: "FMN_ER
 # Every symbol include/fast_mul.h declares (checked by the tests).
 EXPORTS = ["abs_mul64", "abs_sqr64", "fmn_init", "fmn_shutdown", "fmn_last_error", "fmn_mul", "fmn_sqr",
            "fmn_mul_device", "fmn_sqr_device", "fmn_sync", "fmn_workspace_size", "fmn_mul_device_ws",
-           "fmn_ws_status", "fmn_ntt_len"]
+           "fmn_ws_status", "fmn_ntt_len", "fmn_kernel_kind_name", "fmn_profile_enable", "fmn_profile_take",
+           "fmn_launches_per_product", "fmn_bench_modmul"]
+KERNEL_KINDS = 5
 
 _u64 = ctypes.c_uint64
 _u64p = ctypes.POINTER(ctypes.c_uint64)
@@ -79,6 +81,17 @@ def load_library(path=None):
     lib.fmn_ws_status.restype = ctypes.c_int
     lib.fmn_ntt_len.argtypes = [_u64, _u64]
     lib.fmn_ntt_len.restype = _u64
+    lib.fmn_kernel_kind_name.argtypes = [ctypes.c_int]
+    lib.fmn_kernel_kind_name.restype = ctypes.c_char_p
+    lib.fmn_profile_enable.argtypes = [ctypes.c_int]
+    lib.fmn_profile_enable.restype = ctypes.c_int
+    _dp = ctypes.POINTER(ctypes.c_double)
+    lib.fmn_profile_take.argtypes = [_dp, _u64p, _dp, _dp]
+    lib.fmn_profile_take.restype = ctypes.c_int
+    lib.fmn_launches_per_product.argtypes = [_u64, _u64, ctypes.c_int]
+    lib.fmn_launches_per_product.restype = ctypes.c_int
+    lib.fmn_bench_modmul.argtypes = [_dp, _dp]
+    lib.fmn_bench_modmul.restype = ctypes.c_int
     if path is None:
         _lib = lib
     return lib
@@ -174,3 +187,30 @@ def mul_device_ws(a, b, out, ws, stream=None):
 def ws_status(ws, stream=None):
     """Raise if the product that used workspace ``ws`` reported a device-side error."""
     _check(load_library().fmn_ws_status(ws.data_ptr(), 0, 0, 0, _stream_ptr(stream)))
+
+
+def profile_enable(on=True):
+    """Record CUDA events around every kernel launch of this thread."""
+    _check(load_library().fmn_profile_enable(1 if on else 0))
+
+
+def profile_take():
+    """Per kernel kind: {name: {"ms", "launches", "bytes", "modmuls"}} since the last call."""
+    lib = load_library()
+    k = KERNEL_KINDS
+    ms, bts, mm = (ctypes.c_double * k)(), (ctypes.c_double * k)(), (ctypes.c_double * k)()
+    ln = (ctypes.c_uint64 * k)()
+    _check(lib.fmn_profile_take(ms, ln, bts, mm))
+    return {lib.fmn_kernel_kind_name(i).decode(): {"ms": ms[i], "launches": int(ln[i]), "bytes": bts[i],
+                                                    "modmuls": mm[i]} for i in range(k)}
+
+
+def launches_per_product(len1, len2, sqr=False):
+    return int(load_library().fmn_launches_per_product(len1, len2, 1 if sqr else 0))
+
+
+def bench_modmul():
+    """(modmuls/s, butterflies/s) peaks of the Montgomery arithmetic on the current device."""
+    a, b = ctypes.c_double(), ctypes.c_double()
+    _check(load_library().fmn_bench_modmul(ctypes.byref(a), ctypes.byref(b)))
+    return a.value, b.value

@@ -333,6 +333,41 @@ int fmn_ws_status(const void* d_ws, u64 len1, u64 len2, int sqr, void* stream) {
     return FMN_OK;
 }
 
+const char* fmn_kernel_kind_name(int kind) { return fmn::kernel_kind_name(kind); }
+
+int fmn_profile_enable(int on) {
+    fmn::profile_enable(on != 0);
+    return FMN_OK;
+}
+
+int fmn_profile_take(double* ms, u64* launches, double* bytes, double* modmuls) {
+    fmn::KindStats st[fmn::K_KINDS];
+    memset(st, 0, sizeof(st));
+    cudaError_t e = fmn::profile_take(st);
+    if (e != cudaSuccess) return set_err(FMN_ERR_CUDA, "reading profile events", e);
+    for (int k = 0; k < fmn::K_KINDS; ++k) {
+        if (ms) ms[k] = st[k].ms;
+        if (launches) launches[k] = st[k].launches;
+        if (bytes) bytes[k] = st[k].bytes;
+        if (modmuls) modmuls[k] = st[k].modmuls;
+    }
+    return FMN_OK;
+}
+
+int fmn_launches_per_product(u64 len1, u64 len2, int sqr) { return fmn::job_launches(len1, len2, sqr ? 1 : 0); }
+
+int fmn_bench_modmul(double* modmul_per_s, double* butterfly_per_s) {
+    DevCtx* c;
+    int rc = get_ctx(&c);
+    if (rc) return rc;
+    double a = 0, b = 0;
+    cudaError_t e = fmn::bench_modmul(&a, &b);
+    if (e != cudaSuccess) return set_err(FMN_ERR_CUDA, "modmul microbenchmark", e);
+    if (modmul_per_s) *modmul_per_s = a;
+    if (butterfly_per_s) *butterfly_per_s = b;
+    return FMN_OK;
+}
+
 u64 fmn_ntt_len(u64 len1, u64 len2) {
     const u64 conv = len1 + len2 ? len1 + len2 - 1 : 0;
     u64 n = 1;

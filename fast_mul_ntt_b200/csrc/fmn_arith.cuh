@@ -11,7 +11,12 @@
 //   * m * p = m + (c * m) << k, so the high 64 bits of m * p are
 //     (c * m + (m >> k)) >> (64 - k): two 32x32->64 multiply-adds and two shifts;
 //   * t = T_hi - (m * p)_hi lies in (-p, p) when T < p * 2^64; we return t + p in (0, 2p).
-// The 64x64->128 product itself is four 32x32->64 mad.wide operations.
+//
+// The prime is a runtime value held in uniform registers (struct PrimeRT), so one code body
+// serves all three primes: kernels are a third of the size they would be with the prime as
+// a template parameter, which keeps them inside the instruction cache.  Integer multiplies
+// issue only on the FMA-heavy pipe (wide forms at half rate); this formulation was the
+// fastest of the ones measured on B200 (64x64 product through mul.lo/mul.hi.u64).
 //
 // Lazy-reduction contract used by every kernel:
 //   mmul(a, b) needs a * b < p * 2^64; it holds for a, b < 2p, and for a < 4p with b < p
@@ -45,94 +50,80 @@ template <> struct Prime<2> {
     static constexpr int K = 57;
 };
 
-template <int I> struct PrimeX : Prime<I> {
-    using B = Prime<I>;
-    static constexpr u64 P2 = 2 * B::P;
-    static constexpr u64 R1 = rmod_c(B::P);                 // Montgomery one
-    static constexpr u64 R2 = mulmod_c(R1, R1, B::P);        // R^2 mod p (to-Montgomery factor)
-    static constexpr u32 CSH = B::C << (B::K - 32);          // c * 2^(k-32), fits 32 bits
-    static_assert((u64)B::P == (((u64)B::C) << B::K) + 1, "prime form");
-    static_assert(B::K >= 55 && B::K < 64, "shift ranges");
+// Runtime descriptor of one prime.
+struct PrimeRT {
+    u64 p;       // the prime
+    u64 p2;      // 2p
+    u64 r2;      // R^2 mod p (to-Montgomery factor)
+    u32 c;       // p = c * 2^k + 1
+    u32 csh;     // c * 2^(k-32) (fits 32 bits)
+    u32 k32;     // k - 32
+    u32 k64;     // 64 - k
 };
 
-// 64x64 -> 128 product from 32-bit pieces (mad.wide.u32 chains).
-__device__ __forceinline__ void mul_wide(u64 a, u64 b, u32& t0, u32& t1, u64& hi) {
-    const u32 a0 = (u32)a, a1 = (u32)(a >> 32), b0 = (u32)b, b1 = (u32)(b >> 32);
-    const u64 p00 = (u64)a0 * b0;
-    const u64 p01 = (u64)a0 * b1 + (p00 >> 32);
-    const u64 p10 = (u64)a1 * b0 + (u32)p01;
-    hi = (u64)a1 * b1 + (p01 >> 32) + (p10 >> 32);
-    t0 = (u32)p00;
-    t1 = (u32)p10;
-}
-
-// REDC of T = (hi : t1 : t0) for p = c*2^k+1; needs T < p * 2^64; result in (0, 2p).
 template <int I>
-__device__ __forceinline__ u64 redc(u32 t0, u32 t1, u64 hi) {
-    using Q = PrimeX<I>;
-    const u32 m1 = t1 - t0 * Q::CSH;                          // m = (m1 : t0)
-    const u32 mh = m1 >> (Q::K - 32);                         // m >> k
-    const u64 x0 = (u64)Q::C * t0 + mh;
-    const u64 y = (u64)Q::C * m1 + (x0 >> 32);
-    const u64 mphi = (y << (Q::K - 32)) | ((u32)x0 >> (64 - Q::K));   // (m * p) >> 64
-    return hi + Q::P - mphi;
+constexpr PrimeRT prime_rt() {
+    return PrimeRT{Prime<I>::P, 2 * Prime<I>::P, mulmod_c(rmod_c(Prime<I>::P), rmod_c(Prime<I>::P), Prime<I>::P),
+                   Prime<I>::C, Prime<I>::C << (Prime<I>::K - 32), (u32)(Prime<I>::K - 32),
+                   (u32)(64 - Prime<I>::K)};
 }
+static_assert(Prime<0>::P == (((u64)Prime<0>::C) << Prime<0>::K) + 1, "prime form");
+static_assert(Prime<1>::P == (((u64)Prime<1>::C) << Prime<1>::K) + 1, "prime form");
+static_assert(Prime<2>::P == (((u64)Prime<2>::C) << Prime<2>::K) + 1, "prime form");
 
 // Montgomery product a * b * 2^-64 mod p, lazily reduced to (0, 2p).
-template <int I>
-__device__ __forceinline__ u64 mmul(u64 a, u64 b) {
-    u32 t0, t1;
-    u64 hi;
-    mul_wide(a, b, t0, t1, hi);
-    return redc<I>(t0, t1, hi);
+__device__ __forceinline__ u64 mmul(u64 a, u64 b, const PrimeRT& q) {
+    const u64 lo = a * b;
+    const u64 hi = __umul64hi(a, b);
+    const u32 t0 = (u32)lo, t1 = (u32)(lo >> 32);
+    const u32 m1 = t1 - t0 * q.csh;                  // m = T_lo * p^-1 = (m1 : t0)
+    const u32 mh = m1 >> q.k32;                      // m >> k
+    const u64 x0 = (u64)q.c * t0 + mh;
+    const u64 y = (u64)q.c * m1 + (x0 >> 32);
+    const u64 mphi = (y << q.k32) | ((u32)x0 >> q.k64);   // (m * p) >> 64
+    return hi + q.p - mphi;
 }
 
 // x in [0, 4p) -> [0, 2p)
-template <int I>
-__device__ __forceinline__ u64 red2(u64 x) {
-    const u64 t = x - PrimeX<I>::P2;
+__device__ __forceinline__ u64 red2(u64 x, const PrimeRT& q) {
+    const u64 t = x - q.p2;
     return t < x ? t : x;   // x >= 2p  <=>  no wrap-around
 }
 // x in [0, 2p) -> [0, p)
-template <int I>
-__device__ __forceinline__ u64 red1(u64 x) {
-    const u64 t = x - Prime<I>::P;
+__device__ __forceinline__ u64 red1(u64 x, const PrimeRT& q) {
+    const u64 t = x - q.p;
     return t < x ? t : x;
 }
 
-// Decimation-in-frequency butterfly with twiddle w < p (or w < 2p):
+// Decimation-in-frequency butterfly with twiddle w < p:
 //   u, v in [0, 2p)  ->  u' = u + v in [0, 2p),  v' = (u - v) * w in (0, 2p).
-template <int I>
-__device__ __forceinline__ void bfly_dif(u64& u, u64& v, u64 w) {
+__device__ __forceinline__ void bfly_dif(u64& u, u64& v, u64 w, const PrimeRT& q) {
     const u64 s = u + v;
-    const u64 d = u + PrimeX<I>::P2 - v;
-    u = red2<I>(s);
-    v = mmul<I>(d, w);
+    const u64 d = u + q.p2 - v;
+    u = red2(s, q);
+    v = mmul(d, w, q);
 }
 // Same with twiddle 1.
-template <int I>
-__device__ __forceinline__ void bfly_dif1(u64& u, u64& v) {
+__device__ __forceinline__ void bfly_dif1(u64& u, u64& v, const PrimeRT& q) {
     const u64 s = u + v;
-    const u64 d = u + PrimeX<I>::P2 - v;
-    u = red2<I>(s);
-    v = red2<I>(d);
+    const u64 d = u + q.p2 - v;
+    u = red2(s, q);
+    v = red2(d, q);
 }
 // Decimation-in-time butterfly with twiddle w < p:
 //   u, v in [0, 4p)  ->  u' = u + v*w, v' = u - v*w, both in [0, 4p).
-template <int I>
-__device__ __forceinline__ void bfly_dit(u64& u, u64& v, u64 w) {
-    const u64 a = red2<I>(u);
-    const u64 b = mmul<I>(v, w);
+__device__ __forceinline__ void bfly_dit(u64& u, u64& v, u64 w, const PrimeRT& q) {
+    const u64 a = red2(u, q);
+    const u64 b = mmul(v, w, q);
     u = a + b;
-    v = a + PrimeX<I>::P2 - b;
+    v = a + q.p2 - b;
 }
 // Same with twiddle 1.
-template <int I>
-__device__ __forceinline__ void bfly_dit1(u64& u, u64& v) {
-    const u64 a = red2<I>(u);
-    const u64 b = red2<I>(v);
+__device__ __forceinline__ void bfly_dit1(u64& u, u64& v, const PrimeRT& q) {
+    const u64 a = red2(u, q);
+    const u64 b = red2(v, q);
     u = a + b;
-    v = a + PrimeX<I>::P2 - b;
+    v = a + q.p2 - b;
 }
 
 }  // namespace fmn

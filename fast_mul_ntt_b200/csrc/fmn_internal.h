@@ -43,4 +43,25 @@ cudaError_t ensure_tables();
 // when a bounded wait gives up; callers zero it once and read it after the stream is done.
 cudaError_t enqueue_job(const Job& job, void* ws, size_t ws_bytes, cudaStream_t stream);
 
+// ---- optional per-kernel timing (used by bench.py; off by default)
+// Kernel kinds of the pipeline.
+enum KernelKind { K_FWD = 0, K_FWD_LAST, K_FUSED, K_INV, K_CRT, K_KINDS };
+const char* kernel_kind_name(int k);
+struct KindStats {
+    double ms;          // summed CUDA-event time
+    u64 launches;
+    double bytes;       // algorithmic HBM bytes (operands read once, spectra read/written once per pass)
+    double modmuls;     // algorithmic Montgomery products (radix-2 butterflies, pointwise, entry, CRT)
+};
+// Enable/disable event recording around every launch of the calling thread.
+void profile_enable(bool on);
+// Wait for recorded events and add their times into out[K_KINDS]; clears the record.
+cudaError_t profile_take(KindStats* out);
+// Kernel launches one product issues.
+int job_launches(u64 la, u64 lb, int sqr);
+
+// Throughput microbenchmark of independent Montgomery products (peak of the integer pipe
+// for this arithmetic): returns products per second.
+cudaError_t bench_modmul(double* per_second, double* butterflies_per_second);
+
 }  // namespace fmn

@@ -66,11 +66,11 @@ constexpr int RT_SIZE = rt_base(5);
 
 __device__ __align__(16) u64 g_rt[2][3][RT_SIZE];      // [forward/inverse][prime]
 __device__ __align__(16) u64 g_tw[2][3][1 << TWB];     // [low/high level][prime]
+__constant__ PrimeRT c_prime[3] = {prime_rt<0>(), prime_rt<1>(), prime_rt<2>()};
 
-// w_{2^30}^x for x < 2^30 (Montgomery form, < 2p).
-template <int I>
-__device__ __forceinline__ u64 root30(u32 x) {
-    return mmul<I>(__ldg(&g_tw[1][I][x >> TWB]), __ldg(&g_tw[0][I][x & ((1u << TWB) - 1)]));
+// w_{2^30}^x for x < 2^30 (Montgomery form, < 2p), prime index pi.
+__device__ __forceinline__ u64 root30(u32 x, int pi, const PrimeRT& q) {
+    return mmul(__ldg(&g_tw[1][pi][x >> TWB]), __ldg(&g_tw[0][pi][x & ((1u << TWB) - 1)]), q);
 }
 
 __device__ __forceinline__ int sw(int j, int c) { return (j << 4) | (c ^ (j & 15)); }
@@ -92,13 +92,13 @@ struct PassArgs {
 // Runs all radix-2^RB groups of one round.  `ld(j, c)` fetches element (j, c), `st(j, c, v)`
 // stores it.  QFAST maps consecutive threads to consecutive rows of one column (coalesced
 // global access of contiguous blocks); otherwise consecutive threads take consecutive columns.
-template <int I, int LOGL, int RB, int TOP, bool INV, bool QFAST, class LD, class ST>
-__device__ __forceinline__ void run_round(LD ld, ST st) {
+template <int LOGL, int RB, int TOP, bool INV, bool QFAST, class LD, class ST>
+__device__ __forceinline__ void run_round(LD ld, ST st, int pi, const PrimeRT& q) {
     constexpr int L = 1 << LOGL, R = 1 << RB, SPL = TOP - RB + 1, SP = 1 << SPL;
     constexpr int GPC = L / R;
     constexpr int G = GPC * TC;
     constexpr bool LOWEST = (SPL == 0);
-    const u64* tab = &g_rt[INV ? 1 : 0][I][rt_off(RB, TOP)];
+    const u64* tab = &g_rt[INV ? 1 : 0][pi][rt_off(RB, TOP)];
 #pragma unroll 1
     for (int gi = threadIdx.x; gi < G; gi += NT) {
         int c, g;
@@ -124,9 +124,9 @@ __device__ __forceinline__ void run_round(LD ld, ST st) {
                     if (t & half) continue;
                     const int u = t & (half - 1);
                     if (LOWEST && u == 0)
-                        bfly_dif1<I>(x[t], x[t + half]);
+                        bfly_dif1(x[t], x[t + half], q);
                     else
-                        bfly_dif<I>(x[t], x[t + half], __ldg(tw + (R - (R >> s)) + u));
+                        bfly_dif(x[t], x[t + half], __ldg(tw + (R - (R >> s)) + u), q);
                 }
             }
         } else {
@@ -138,9 +138,9 @@ __device__ __forceinline__ void run_round(LD ld, ST st) {
                     if (t & half) continue;
                     const int u = t & (half - 1);
                     if (LOWEST && u == 0)
-                        bfly_dit1<I>(x[t], x[t + half]);
+                        bfly_dit1(x[t], x[t + half], q);
                     else
-                        bfly_dit<I>(x[t], x[t + half], __ldg(tw + (R - (R >> s)) + u));
+                        bfly_dit(x[t], x[t + half], __ldg(tw + (R - (R >> s)) + u), q);
                 }
             }
         }
@@ -152,8 +152,8 @@ __device__ __forceinline__ void run_round(LD ld, ST st) {
 // Rounds IDX.. of a sub-transform.  Forward order: round 0 holds the top bits.  Inverse
 // order: inverse round k undoes forward round NR-1-k.  The first round reads with `ld0`, the
 // last writes with `stl`, the rest go through shared memory.
-template <int I, int LOGL, bool INV, bool CONTIG, int IDX, class LD0, class STL>
-__device__ __forceinline__ void rounds(u64* sm, LD0 ld0, STL stl) {
+template <int LOGL, bool INV, bool CONTIG, int IDX, class LD0, class STL>
+__device__ __forceinline__ void rounds(u64* sm, LD0 ld0, STL stl, int pi, const PrimeRT& q) {
     constexpr int NR = rounds_count(LOGL);
     constexpr int FR = INV ? NR - 1 - IDX : IDX;
     constexpr int RB = round_bits(LOGL, FR), TOP = round_top(LOGL, FR);
@@ -161,84 +161,83 @@ __device__ __forceinline__ void rounds(u64* sm, LD0 ld0, STL stl) {
     auto lds = [sm](int j, int c) { return sm[sw(j, c)]; };
     auto sts = [sm](int j, int c, u64 v) { sm[sw(j, c)] = v; };
     if constexpr (NR == 1) {
-        run_round<I, LOGL, RB, TOP, INV, QF>(ld0, stl);
+        run_round<LOGL, RB, TOP, INV, QF>(ld0, stl, pi, q);
     } else if constexpr (IDX == 0) {
-        run_round<I, LOGL, RB, TOP, INV, QF>(ld0, sts);
+        run_round<LOGL, RB, TOP, INV, QF>(ld0, sts, pi, q);
         __syncthreads();
-        rounds<I, LOGL, INV, CONTIG, 1>(sm, ld0, stl);
+        rounds<LOGL, INV, CONTIG, 1>(sm, ld0, stl, pi, q);
     } else if constexpr (IDX == NR - 1) {
-        run_round<I, LOGL, RB, TOP, INV, QF>(lds, stl);
+        run_round<LOGL, RB, TOP, INV, QF>(lds, stl, pi, q);
     } else {
-        run_round<I, LOGL, RB, TOP, INV, QF>(lds, sts);
+        run_round<LOGL, RB, TOP, INV, QF>(lds, sts, pi, q);
         __syncthreads();
-        rounds<I, LOGL, INV, CONTIG, IDX + 1>(sm, ld0, stl);
+        rounds<LOGL, INV, CONTIG, IDX + 1>(sm, ld0, stl, pi, q);
     }
 }
 
 // ------------------------------------------------------------------ pass bodies
-template <int I>
-__device__ __forceinline__ u64 entry_val(const u64* __restrict__ src, u64 len, u64 g) {
-    return g < len ? mmul<I>(__ldg(src + g), PrimeX<I>::R2) : 0ull;   // limb * R mod p
+__device__ __forceinline__ u64 entry_val(const u64* __restrict__ src, u64 len, u64 g, const PrimeRT& q) {
+    return g < len ? mmul(__ldg(src + g), q.r2, q) : 0ull;   // limb * R mod p
 }
 
 // Forward strided pass (pass p < P-1 of a multi-pass transform).
-template <int I, int LOGL, bool ENTRY>
-__device__ __forceinline__ void body_fwd(u64* sm, const PassArgs& a, u64 tile) {
+template <int LOGL, bool ENTRY>
+__device__ __forceinline__ void body_fwd(u64* sm, const PassArgs& a, u64 tile, int pi, const PrimeRT& q) {
     const int logS = a.logB - LOGL;
     const u64 tpb_log = logS - 4;
     const u64 blk = tile >> tpb_log;
     const u32 col0 = (u32)((tile & ((1ull << tpb_log) - 1)) << 4);
     const u64 gbase = (blk << a.logB) + col0;
-    u64* __restrict__ d = a.data + (u64)I * a.N;
+    u64* __restrict__ d = a.data + (u64)pi * a.N;
     const u64* __restrict__ src = a.src;
     const u64 len = a.len;
     auto ld0 = [=](int j, int c) -> u64 {
         const u64 g = gbase + c + ((u64)j << logS);
-        if constexpr (ENTRY) return entry_val<I>(src, len, g);
+        if constexpr (ENTRY) return entry_val(src, len, g, q);
         else return d[g];
     };
     const int shift = MAX_LOG_N - a.logB;
     auto stl = [=](int j, int c, u64 v) {
         const u32 k = __brev((u32)j) >> (32 - LOGL);
         const u32 e = (col0 + c) * k;                       // < B <= 2^30
-        d[gbase + c + ((u64)j << logS)] = mmul<I>(v, root30<I>(e << shift));
+        d[gbase + c + ((u64)j << logS)] = mmul(v, root30(e << shift, pi, q), q);
     };
-    rounds<I, LOGL, false, false, 0>(sm, ld0, stl);
+    rounds<LOGL, false, false, 0>(sm, ld0, stl, pi, q);
 }
 
 // Inverse strided pass: inverse four-step twiddle, then the inverse sub-transform.
-template <int I, int LOGL>
-__device__ __forceinline__ void body_inv(u64* sm, const PassArgs& a, u64 tile) {
+template <int LOGL>
+__device__ __forceinline__ void body_inv(u64* sm, const PassArgs& a, u64 tile, int pi, const PrimeRT& q) {
     const int logS = a.logB - LOGL;
     const u64 tpb_log = logS - 4;
     const u64 blk = tile >> tpb_log;
     const u32 col0 = (u32)((tile & ((1ull << tpb_log) - 1)) << 4);
     const u64 gbase = (blk << a.logB) + col0;
-    u64* __restrict__ d = a.data + (u64)I * a.N;
+    u64* __restrict__ d = a.data + (u64)pi * a.N;
     const int shift = MAX_LOG_N - a.logB;
     auto ld0 = [=](int j, int c) -> u64 {
         const u32 k = __brev((u32)j) >> (32 - LOGL);
         const u32 e = (col0 + c) * k;
         const u32 x = (0u - (e << shift)) & ((1u << MAX_LOG_N) - 1);   // w^-e
-        return mmul<I>(d[gbase + c + ((u64)j << logS)], red1<I>(root30<I>(x)));
+        return mmul(d[gbase + c + ((u64)j << logS)], red1(root30(x, pi, q), q), q);
     };
     auto stl = [=](int j, int c, u64 v) { d[gbase + c + ((u64)j << logS)] = v; };
-    rounds<I, LOGL, true, false, 0>(sm, ld0, stl);
+    rounds<LOGL, true, false, 0>(sm, ld0, stl, pi, q);
 }
 
 // Forward last pass over contiguous blocks (operand A of a product).
-template <int I, int LOGL, bool ENTRY>
-__device__ __forceinline__ void body_fwd_last(u64* sm, const PassArgs& a, u64 tile) {
+template <int LOGL, bool ENTRY>
+__device__ __forceinline__ void body_fwd_last(u64* sm, const PassArgs& a, u64 tile, int pi, const PrimeRT& q) {
     constexpr int L = 1 << LOGL;
     const u64 gbase = tile << (LOGL + 4);
     const int ncols = a.ncols;
-    u64* __restrict__ d = a.data + (u64)I * a.N;
+    u64* __restrict__ d = a.data + (u64)pi * a.N;
     const u64* __restrict__ src = a.src;
     const u64 len = a.len;
     auto ld0 = [=](int j, int c) -> u64 {
         if (c >= ncols) return 0ull;
         const u64 g = gbase + (u64)c * L + j;
-        if constexpr (ENTRY) return entry_val<I>(src, len, g);
+        if constexpr (ENTRY) return entry_val(src, len, g, q);
         else return d[g];
     };
     auto stl = [=](int j, int c, u64 v) {
@@ -247,22 +246,22 @@ __device__ __forceinline__ void body_fwd_last(u64* sm, const PassArgs& a, u64 ti
     if constexpr (LOGL == 0) {
         if (threadIdx.x < (unsigned)ncols) stl(0, threadIdx.x, ld0(0, threadIdx.x));
     } else {
-        rounds<I, LOGL, false, true, 0>(sm, ld0, stl);
+        rounds<LOGL, false, true, 0>(sm, ld0, stl, pi, q);
     }
 }
 
 // The lowest forward round, the pointwise product and the lowest inverse round of one
 // contiguous tile, all in registers.
-template <int I, int LOGL, bool SQR, class LD, class ST>
+template <int LOGL, bool SQR, class LD, class ST>
 __device__ __forceinline__ void fused_lowest(LD ld, ST st, const u64* __restrict__ oth, u64 gbase,
-                                             int ncols) {
+                                             int ncols, int pi, const PrimeRT& q) {
     constexpr int L = 1 << LOGL;
     constexpr int NR = rounds_count(LOGL);
     constexpr int RB = round_bits(LOGL, NR - 1);
     constexpr int R = 1 << RB;
     constexpr int G = (L / R) * TC;
-    const u64* tf = &g_rt[0][I][rt_off(RB, RB - 1)];
-    const u64* ti = &g_rt[1][I][rt_off(RB, RB - 1)];
+    const u64* tf = &g_rt[0][pi][rt_off(RB, RB - 1)];
+    const u64* ti = &g_rt[1][pi][rt_off(RB, RB - 1)];
 #pragma unroll 1
     for (int gi = threadIdx.x; gi < G; gi += NT) {
         const int c = gi & (TC - 1);
@@ -277,14 +276,14 @@ __device__ __forceinline__ void fused_lowest(LD ld, ST st, const u64* __restrict
             for (int t = 0; t < R; ++t) {
                 if (t & half) continue;
                 const int u = t & (half - 1);
-                if (u == 0) bfly_dif1<I>(x[t], x[t + half]);
-                else bfly_dif<I>(x[t], x[t + half], __ldg(tf + (R - (R >> s)) + u));
+                if (u == 0) bfly_dif1(x[t], x[t + half], q);
+                else bfly_dif(x[t], x[t + half], __ldg(tf + (R - (R >> s)) + u), q);
             }
         }
         if (c < ncols) {
             const u64* po = oth + gbase + (u64)c * L + row0;
 #pragma unroll
-            for (int t = 0; t < R; ++t) x[t] = mmul<I>(x[t], SQR ? x[t] : po[t]);
+            for (int t = 0; t < R; ++t) x[t] = mmul(x[t], SQR ? x[t] : po[t], q);
         }
 #pragma unroll
         for (int s = RB - 1; s >= 0; --s) {
@@ -293,8 +292,8 @@ __device__ __forceinline__ void fused_lowest(LD ld, ST st, const u64* __restrict
             for (int t = 0; t < R; ++t) {
                 if (t & half) continue;
                 const int u = t & (half - 1);
-                if (u == 0) bfly_dit1<I>(x[t], x[t + half]);
-                else bfly_dit<I>(x[t], x[t + half], __ldg(ti + (R - (R >> s)) + u));
+                if (u == 0) bfly_dit1(x[t], x[t + half], q);
+                else bfly_dit(x[t], x[t + half], __ldg(ti + (R - (R >> s)) + u), q);
             }
         }
 #pragma unroll
@@ -305,20 +304,20 @@ __device__ __forceinline__ void fused_lowest(LD ld, ST st, const u64* __restrict
 // Fused last pass: forward last pass of the second operand (or of the only operand when
 // squaring), pointwise product with the first operand's spectrum, inverse last pass.
 // The result overwrites the first operand's spectrum (`other`).
-template <int I, int LOGL, bool ENTRY, bool SQR>
-__device__ __forceinline__ void body_fused(u64* sm, const PassArgs& a, u64 tile) {
+template <int LOGL, bool ENTRY, bool SQR>
+__device__ __forceinline__ void body_fused(u64* sm, const PassArgs& a, u64 tile, int pi, const PrimeRT& q) {
     constexpr int L = 1 << LOGL;
     constexpr int NR = rounds_count(LOGL);
     const u64 gbase = tile << (LOGL + 4);
     const int ncols = a.ncols;
-    const u64* __restrict__ d = a.data + (u64)I * a.N;
-    u64* __restrict__ o = a.other + (u64)I * a.N;
+    const u64* __restrict__ d = a.data + (u64)pi * a.N;
+    u64* __restrict__ o = a.other + (u64)pi * a.N;
     const u64* __restrict__ src = a.src;
     const u64 len = a.len;
     auto ldg = [=](int j, int c) -> u64 {
         if (c >= ncols) return 0ull;
         const u64 g = gbase + (u64)c * L + j;
-        if constexpr (ENTRY) return entry_val<I>(src, len, g);
+        if constexpr (ENTRY) return entry_val(src, len, g, q);
         else return d[g];
     };
     auto stg = [=](int j, int c, u64 v) {
@@ -330,28 +329,28 @@ __device__ __forceinline__ void body_fused(u64* sm, const PassArgs& a, u64 tile)
         if (threadIdx.x < (unsigned)ncols) {
             const int c = threadIdx.x;
             const u64 x = ldg(0, c);
-            stg(0, c, mmul<I>(x, SQR ? x : o[gbase + c]));
+            stg(0, c, mmul(x, SQR ? x : o[gbase + c], q));
         }
     } else if constexpr (NR == 1) {
-        fused_lowest<I, LOGL, SQR>(ldg, stg, o, gbase, ncols);
+        fused_lowest<LOGL, SQR>(ldg, stg, o, gbase, ncols, pi, q);
     } else {
         // forward rounds 0 .. NR-2
         constexpr int RB0 = round_bits(LOGL, 0);
-        run_round<I, LOGL, RB0, LOGL - 1, false, true>(ldg, sts);
+        run_round<LOGL, RB0, LOGL - 1, false, true>(ldg, sts, pi, q);
         __syncthreads();
         if constexpr (NR == 3) {
             constexpr int RB1 = round_bits(LOGL, 1), T1 = round_top(LOGL, 1);
-            run_round<I, LOGL, RB1, T1, false, false>(lds, sts);
+            run_round<LOGL, RB1, T1, false, false>(lds, sts, pi, q);
             __syncthreads();
         }
-        fused_lowest<I, LOGL, SQR>(lds, sts, o, gbase, ncols);
+        fused_lowest<LOGL, SQR>(lds, sts, o, gbase, ncols, pi, q);
         __syncthreads();
         if constexpr (NR == 3) {
             constexpr int RB1 = round_bits(LOGL, 1), T1 = round_top(LOGL, 1);
-            run_round<I, LOGL, RB1, T1, true, false>(lds, sts);
+            run_round<LOGL, RB1, T1, true, false>(lds, sts, pi, q);
             __syncthreads();
         }
-        run_round<I, LOGL, RB0, LOGL - 1, true, true>(lds, stg);
+        run_round<LOGL, RB0, LOGL - 1, true, true>(lds, stg, pi, q);
     }
 }
 
@@ -359,21 +358,13 @@ __device__ __forceinline__ void body_fused(u64* sm, const PassArgs& a, u64 tile)
 template <int MODE, int LOGL, bool ENTRY, bool SQR>
 __global__ void __launch_bounds__(NT) k_pass(PassArgs a) {
     extern __shared__ __align__(16) u64 sm[];
-    const int prime = blockIdx.x % 3;
-    const u64 tile = blockIdx.x / 3;
-#define FMN_BODY(I)                                                        \
-    if constexpr (MODE == M_FWD) body_fwd<I, LOGL, ENTRY>(sm, a, tile);             \
-    else if constexpr (MODE == M_INV) body_inv<I, LOGL>(sm, a, tile);               \
-    else if constexpr (MODE == M_FWD_LAST) body_fwd_last<I, LOGL, ENTRY>(sm, a, tile); \
-    else body_fused<I, LOGL, ENTRY, SQR>(sm, a, tile);
-    if (prime == 0) {
-        FMN_BODY(0)
-    } else if (prime == 1) {
-        FMN_BODY(1)
-    } else {
-        FMN_BODY(2)
-    }
-#undef FMN_BODY
+    const int pi = blockIdx.x % 3;          // prime varies fastest: the three CTAs of a tile
+    const u64 tile = blockIdx.x / 3;        // read the same limbs at the same time (L2 reuse)
+    const PrimeRT q = c_prime[pi];
+    if constexpr (MODE == M_FWD) body_fwd<LOGL, ENTRY>(sm, a, tile, pi, q);
+    else if constexpr (MODE == M_INV) body_inv<LOGL>(sm, a, tile, pi, q);
+    else if constexpr (MODE == M_FWD_LAST) body_fwd_last<LOGL, ENTRY>(sm, a, tile, pi, q);
+    else body_fused<LOGL, ENTRY, SQR>(sm, a, tile, pi, q);
 }
 
 // ------------------------------------------------------------------ CRT + carry
@@ -429,12 +420,13 @@ __device__ __forceinline__ void acc_mul(u64 y, u64 ml, u64 mh, u64& w0, u64& w1,
     w2 = w2 + (u64)(hi >> 64) + (u64)(s1 >> 64);
 }
 
-__device__ __forceinline__ void crt_coef(const CrtArgs& a, u64 j, u64& w0, u64& w1, u64& w2) {
+__device__ __forceinline__ void crt_coef(const CrtArgs& a, u64 j, u64& w0, u64& w1, u64& w2,
+                                         const PrimeRT& q0, const PrimeRT& q1, const PrimeRT& q2) {
     w0 = w1 = w2 = 0;
     if (j >= a.nvalid) return;
-    const u64 y0 = red1<0>(mmul<0>(a.res[j], a.cst[0]));
-    const u64 y1 = red1<1>(mmul<1>(a.res[a.N + j], a.cst[1]));
-    const u64 y2 = red1<2>(mmul<2>(a.res[2 * a.N + j], a.cst[2]));
+    const u64 y0 = red1(mmul(a.res[j], a.cst[0], q0), q0);
+    const u64 y1 = red1(mmul(a.res[a.N + j], a.cst[1], q1), q1);
+    const u64 y2 = red1(mmul(a.res[2 * a.N + j], a.cst[2], q2), q2);
     acc_mul(y0, m_lo(0), m_hi(0), w0, w1, w2);
     acc_mul(y1, m_lo(1), m_hi(1), w0, w1, w2);
     acc_mul(y2, m_lo(2), m_hi(2), w0, w1, w2);
@@ -466,6 +458,7 @@ __global__ void __launch_bounds__(CNT) k_crt_carry(CrtArgs a) {
     __shared__ u32 s_warp[CNT / 32];
     __shared__ u32 s_cin;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const PrimeRT q0 = c_prime[0], q1 = c_prime[1], q2 = c_prime[2];
     if (tid == 0) s_tile = atomicAdd(a.ticket, 1u);
     __syncthreads();
     const u64 tile = s_tile;
@@ -473,7 +466,7 @@ __global__ void __launch_bounds__(CNT) k_crt_carry(CrtArgs a) {
 
     u64 w0[CE], w1[CE], w2[CE];
 #pragma unroll
-    for (int e = 0; e < CE; ++e) crt_coef(a, j0 + e, w0[e], w1[e], w2[e]);
+    for (int e = 0; e < CE; ++e) crt_coef(a, j0 + e, w0[e], w1[e], w2[e], q0, q1, q2);
 
     // high words of the two coefficients just below j0
     u64 p1w1 = __shfl_up_sync(0xffffffffu, w1[CE - 1], 1);
@@ -491,11 +484,11 @@ __global__ void __launch_bounds__(CNT) k_crt_carry(CrtArgs a) {
             p1w2 = s_hi2[warp - 1];
             p2w2 = s_hi2b[warp - 1];
         } else {
-            u64 q0, q1, q2, r0, r1, r2;
-            if (j0 >= 1) crt_coef(a, j0 - 1, q0, q1, q2); else q0 = q1 = q2 = 0;
-            if (j0 >= 2) crt_coef(a, j0 - 2, r0, r1, r2); else r0 = r1 = r2 = 0;
-            p1w1 = q1;
-            p1w2 = q2;
+            u64 u0, u1, u2, r0, r1, r2;
+            if (j0 >= 1) crt_coef(a, j0 - 1, u0, u1, u2, q0, q1, q2); else u0 = u1 = u2 = 0;
+            if (j0 >= 2) crt_coef(a, j0 - 2, r0, r1, r2, q0, q1, q2); else r0 = r1 = r2 = 0;
+            p1w1 = u1;
+            p1w2 = u2;
             p2w2 = r2;
         }
     }
@@ -723,6 +716,9 @@ cudaError_t ensure_tables() {
                 e = cudaFuncSetAttribute((const void*)K.k[v][l], cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)pass_smem(l));
                 if (e != cudaSuccess) return e;
+                e = cudaFuncSetAttribute((const void*)K.k[v][l], cudaFuncAttributePreferredSharedMemoryCarveout,
+                                         (int)cudaSharedmemCarveoutMaxShared);
+                if (e != cudaSuccess) return e;
             }
     done.push_back(dev);
     return cudaSuccess;
@@ -787,11 +783,112 @@ size_t job_workspace_bytes(u64 la, u64 lb, int sqr) {
     return t ? t : 256;
 }
 
+// ------------------------------------------------------------------ host: profiling
+const char* kernel_kind_name(int k) {
+    static const char* names[K_KINDS] = {"fwd_pass", "fwd_last_pass", "fused_pointwise_pass", "inv_pass",
+                                         "crt_carry"};
+    return (k >= 0 && k < K_KINDS) ? names[k] : "?";
+}
+
+namespace {
+struct ProfRec {
+    int kind;
+    cudaEvent_t a, b;
+    double bytes, modmuls;
+};
+struct ProfState {
+    bool on = false;
+    std::vector<ProfRec> recs;
+    std::vector<cudaEvent_t> pool;
+    cudaEvent_t get() {
+        if (!pool.empty()) {
+            cudaEvent_t e = pool.back();
+            pool.pop_back();
+            return e;
+        }
+        cudaEvent_t e = nullptr;
+        cudaEventCreate(&e);
+        return e;
+    }
+};
+thread_local ProfState g_prof;
+}  // namespace
+
+void profile_enable(bool on) { g_prof.on = on; }
+
+cudaError_t profile_take(KindStats* out) {
+    for (ProfRec& r : g_prof.recs) {
+        cudaError_t e = cudaEventSynchronize(r.b);
+        if (e != cudaSuccess) return e;
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, r.a, r.b);
+        out[r.kind].ms += ms;
+        out[r.kind].launches += 1;
+        out[r.kind].bytes += r.bytes;
+        out[r.kind].modmuls += r.modmuls;
+        g_prof.pool.push_back(r.a);
+        g_prof.pool.push_back(r.b);
+    }
+    g_prof.recs.clear();
+    return cudaSuccess;
+}
+
+// Launch wrapper: records events around the launch when profiling is on.
+template <class F>
+static cudaError_t timed_launch(int kind, double bytes, double modmuls, cudaStream_t s, F&& launch) {
+    ProfRec r{kind, nullptr, nullptr, bytes, modmuls};
+    if (g_prof.on) {
+        r.a = g_prof.get();
+        r.b = g_prof.get();
+        cudaEventRecord(r.a, s);
+    }
+    launch();
+    cudaError_t e = cudaGetLastError();
+    if (g_prof.on) {
+        cudaEventRecord(r.b, s);
+        g_prof.recs.push_back(r);
+    }
+    return e;
+}
+
+static int variant_kind(int v) {
+    switch (v) {
+        case V_FWD: case V_FWD_E: return K_FWD;
+        case V_LAST: case V_LAST_E: return K_FWD_LAST;
+        case V_INV: return K_INV;
+        default: return K_FUSED;
+    }
+}
+
 static cudaError_t launch_pass(int variant, int logl, const PassArgs& a, u64 tiles, cudaStream_t s) {
     PassKernel k = ktab().k[variant][logl];
     if (!k) return cudaErrorInvalidValue;
-    k<<<(unsigned)(tiles * 3), NT, pass_smem(logl), s>>>(a);
-    return cudaGetLastError();
+    // algorithmic work of the launch (3 primes)
+    const double N = (double)a.N, vec = 3.0 * N * 8.0;
+    const double bfly = 3.0 * (N / 2.0) * logl;
+    double bytes = 2.0 * vec, mm = bfly;
+    const bool entry = (variant == V_FWD_E || variant == V_LAST_E || variant == V_FUSED_E || variant == V_SQR_E);
+    if (entry) {
+        bytes = (double)a.len * 8.0 + vec;
+        mm += 3.0 * (double)a.len;
+    }
+    if (variant == V_FUSED || variant == V_FUSED_E) {
+        bytes += vec;                 // reads the other operand's spectrum too
+        mm = 2.0 * bfly + 3.0 * N + (entry ? 3.0 * (double)a.len : 0.0);
+    } else if (variant == V_SQR || variant == V_SQR_E) {
+        mm = 2.0 * bfly + 3.0 * N + (entry ? 3.0 * (double)a.len : 0.0);
+    }
+    return timed_launch(variant_kind(variant), bytes, mm, s,
+                        [&] { k<<<(unsigned)(tiles * 3), NT, pass_smem(logl), s>>>(a); });
+}
+
+int job_launches(u64 la, u64 lb, int sqr) {
+    if (la == 0 || lb == 0) return 0;
+    const WsLayout w = ws_layout(la, lb, sqr);
+    const Plan pl = make_plan(w.n);
+    const int P = pl.passes;
+    // forward strided passes (A, and B unless squaring) + A's last pass + fused + inverse + crt
+    return sqr ? (P - 1) + 1 + (P - 1) + 1 : 2 * (P - 1) + 1 + 1 + (P - 1) + 1;
 }
 
 cudaError_t enqueue_job(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s) {
@@ -892,8 +989,80 @@ cudaError_t enqueue_job(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s)
     ca.err = (u32*)base;
     e = cudaMemsetAsync(base + w.ticket, 0, w.total - w.ticket, s);
     if (e != cudaSuccess) return e;
-    k_crt_carry<<<(unsigned)w.ncta, CNT, 0, s>>>(ca);
-    return cudaGetLastError();
+    const double crt_bytes = 3.0 * (double)ca.nvalid * 8.0 + (double)out_len * 8.0;
+    return timed_launch(K_CRT, crt_bytes, 3.0 * (double)ca.nvalid, s,
+                        [&] { k_crt_carry<<<(unsigned)w.ncta, CNT, 0, s>>>(ca); });
+}
+
+// ------------------------------------------------------------------ modmul microbenchmark
+constexpr int MB_CHAINS = 8, MB_ITERS = 2048;
+__global__ void __launch_bounds__(256) k_bench_modmul(u64* sink, u64 y) {
+    const PrimeRT q = c_prime[2];
+    u64 x[MB_CHAINS];
+#pragma unroll
+    for (int i = 0; i < MB_CHAINS; ++i) x[i] = (u64)(blockIdx.x * 256 + threadIdx.x) * 0x9E3779B97F4A7C15ull + i;
+#pragma unroll 1
+    for (int it = 0; it < MB_ITERS; ++it) {
+#pragma unroll
+        for (int i = 0; i < MB_CHAINS; ++i) x[i] = mmul(x[i], y, q);   // any x < 2^64 with y < p
+    }
+    u64 acc = 0;
+#pragma unroll
+    for (int i = 0; i < MB_CHAINS; ++i) acc ^= x[i];
+    if (acc == 0x123456789ull) sink[0] = acc;
+}
+__global__ void __launch_bounds__(256) k_bench_bfly(u64* sink, u64 w) {
+    const PrimeRT q = c_prime[2];
+    u64 x[2 * MB_CHAINS];
+#pragma unroll
+    for (int i = 0; i < 2 * MB_CHAINS; ++i) x[i] = ((u64)(blockIdx.x * 256 + threadIdx.x) * 0x9E3779B97F4A7C15ull + i) >> 3;
+#pragma unroll 1
+    for (int it = 0; it < MB_ITERS; ++it) {
+#pragma unroll
+        for (int i = 0; i < MB_CHAINS; ++i) bfly_dif(x[i], x[i + MB_CHAINS], w, q);
+    }
+    u64 acc = 0;
+#pragma unroll
+    for (int i = 0; i < 2 * MB_CHAINS; ++i) acc ^= x[i];
+    if (acc == 0x123456789ull) sink[0] = acc;
+}
+
+cudaError_t bench_modmul(double* per_second, double* bfly_per_second) {
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    u64* sink = nullptr;
+    cudaError_t e = cudaMalloc(&sink, 64);
+    if (e != cudaSuccess) return e;
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    const unsigned grid = (unsigned)sms * 8;
+    const u64 y = 1234567890123456789ull % Prime<2>::P, w = 987654321987654321ull % Prime<2>::P;
+    float best = 1e30f, bestb = 1e30f;
+    for (int rep = 0; rep < 4; ++rep) {
+        cudaEventRecord(a);
+        k_bench_modmul<<<grid, 256>>>(sink, y);
+        cudaEventRecord(b);
+        cudaEventSynchronize(b);
+        float ms;
+        cudaEventElapsedTime(&ms, a, b);
+        if (rep && ms < best) best = ms;
+        cudaEventRecord(a);
+        k_bench_bfly<<<grid, 256>>>(sink, w);
+        cudaEventRecord(b);
+        cudaEventSynchronize(b);
+        cudaEventElapsedTime(&ms, a, b);
+        if (rep && ms < bestb) bestb = ms;
+    }
+    e = cudaGetLastError();
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaFree(sink);
+    const double n = (double)grid * 256.0 * MB_CHAINS * MB_ITERS;
+    *per_second = n / (best * 1e-3);
+    *bfly_per_second = n / (bestb * 1e-3);
+    return e;
 }
 
 }  // namespace fmn

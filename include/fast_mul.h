@@ -76,6 +76,25 @@ int fmn_mul_device_ws(const u64* d_in1, u64 len1, const u64* d_in2, u64 len2, u6
 /* After the stream has finished, read the device-side error flag of such a call. */
 int fmn_ws_status(const void* d_ws, u64 len1, u64 len2, int sqr, void* stream);
 
+/* ----------------------------------------------------------------- measurement hooks
+ * (no counterpart in the reference; used by bench.py) */
+
+/* Kernel kinds of the pipeline, in this order: forward pass, forward last pass, fused
+ * pointwise pass, inverse pass, CRT + carry. */
+#define FMN_KERNEL_KINDS 5
+const char* fmn_kernel_kind_name(int kind);
+/* Record CUDA events around every kernel launch of the calling thread (on = 1) or stop. */
+int fmn_profile_enable(int on);
+/* Wait for the recorded launches and return, per kernel kind, summed device milliseconds,
+ * launch count, algorithmic HBM bytes and algorithmic Montgomery products; clears the
+ * record.  Each array has FMN_KERNEL_KINDS entries. */
+int fmn_profile_take(double* ms, u64* launches, double* bytes, double* modmuls);
+/* Number of kernel launches one product issues. */
+int fmn_launches_per_product(u64 len1, u64 len2, int sqr);
+/* Peak of this library's Montgomery product on the current device: a microbenchmark of
+ * independent modmul chains and of decimation-in-frequency butterflies (per second). */
+int fmn_bench_modmul(double* modmul_per_s, double* butterfly_per_s);
+
 /* Transform length used for a product: the next power of two >= len1 + len2 - 1
  * (int_ceil2, src/fast_mul.c:299-312). */
 u64 fmn_ntt_len(u64 len1, u64 len2);
