@@ -27,7 +27,7 @@ _ERRNAMES = {1: "FMN_ERR_ARG", 2: "FMN_ERR_CUDA", 3: "FMN_ERR_NOMEM", 4: "FMN_ER
 EXPORTS = ["abs_mul64", "abs_sqr64", "fmn_init", "fmn_shutdown", "fmn_last_error", "fmn_mul", "fmn_sqr",
            "fmn_mul_device", "fmn_sqr_device", "fmn_sync", "fmn_workspace_size", "fmn_mul_device_ws",
            "fmn_ws_status", "fmn_ntt_len", "fmn_kernel_kind_name", "fmn_profile_enable", "fmn_profile_take",
-           "fmn_launches_per_product", "fmn_bench_modmul"]
+           "fmn_launches_per_product", "fmn_bench_modmul", "fmn_mul_device_noalloc"]
 KERNEL_KINDS = 5
 
 _u64 = ctypes.c_uint64
@@ -92,6 +92,8 @@ def load_library(path=None):
     lib.fmn_launches_per_product.restype = ctypes.c_int
     lib.fmn_bench_modmul.argtypes = [_dp, _dp]
     lib.fmn_bench_modmul.restype = ctypes.c_int
+    lib.fmn_mul_device_noalloc.argtypes = [_vp, _u64, _vp, _u64, _vp, _vp]
+    lib.fmn_mul_device_noalloc.restype = ctypes.c_int
     if path is None:
         _lib = lib
     return lib
@@ -187,6 +189,16 @@ def mul_device_ws(a, b, out, ws, stream=None):
 def ws_status(ws, stream=None):
     """Raise if the product that used workspace ``ws`` reported a device-side error."""
     _check(load_library().fmn_ws_status(ws.data_ptr(), 0, 0, 0, _stream_ptr(stream)))
+
+
+def mul_device_noalloc(a, b, out, stream=None):
+    """Device product that allocates no memory (fixed ~3 MB scratch array; len(a) + len(b)
+    <= 65537).  For callers that cannot allocate device memory while they run; waits for
+    ``stream``.  Calls overlapping on the GPU share the array and race."""
+    lib = load_library()
+    _check(lib.fmn_mul_device_noalloc(a.data_ptr(), a.numel(), b.data_ptr(), b.numel(), out.data_ptr(),
+                                      _stream_ptr(stream)))
+    return out
 
 
 def profile_enable(on=True):

@@ -214,6 +214,15 @@ int device_product(const u64* d1, u64 len1, const u64* d2, u64 len2, u64* dout, 
     return run_job_ctx(c, j, s);
 }
 
+}  // namespace
+
+namespace fmn {
+// Record an error for fmn_last_error() from other translation units of the library.
+int api_set_error(int code, const char* what, cudaError_t e) { return set_err(code, what, e); }
+}  // namespace fmn
+
+namespace {
+
 void die(const char* fn) {
     fprintf(stderr, "%s failed: %s\n", fn, g_last_error.c_str());
     abort();

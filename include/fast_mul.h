@@ -76,6 +76,19 @@ int fmn_mul_device_ws(const u64* d_in1, u64 len1, const u64* d_in2, u64 len2, u6
 /* After the stream has finished, read the device-side error flag of such a call. */
 int fmn_ws_status(const void* d_ws, u64 len1, u64 len2, int sqr, void* stream);
 
+/* Device-pointer product that allocates nothing, for callers that cannot call cudaMalloc
+ * while they run (a plugin inside an application whose allocator owns the device memory, a
+ * latency-critical loop that must not stall on allocation, a process with a fixed memory
+ * plan).  Its scratch is one fixed array of about 3 MB in device memory, present on every
+ * GPU that loads the library until exit, so it takes products with len1 + len2 <= 65537
+ * limbs (transforms up to 2^16 points) and rejects larger ones with FMN_ERR_TOO_LARGE.
+ * The first call on each device looks up the array's device address and uploads the
+ * twiddle tables; make it before any stream capture.  Calls share the array: they are
+ * serialised with respect to `stream` (the call waits for it), and calls whose work
+ * overlaps on the GPU from other streams or threads race on it.
+ * No counterpart in the reference (which allocates its scratch per call). */
+int fmn_mul_device_noalloc(const u64* d_in1, u64 len1, const u64* d_in2, u64 len2, u64* d_out, void* stream);
+
 /* ----------------------------------------------------------------- measurement hooks
  * (no counterpart in the reference; used by bench.py) */
 
