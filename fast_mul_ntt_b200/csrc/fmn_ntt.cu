@@ -92,7 +92,7 @@ struct PassArgs {
 // Runs all radix-2^RB groups of one round.  `ld(j, c)` fetches element (j, c), `st(j, c, v)`
 // stores it.  QFAST maps consecutive threads to consecutive rows of one column (coalesced
 // global access of contiguous blocks); otherwise consecutive threads take consecutive columns.
-template <int LOGL, int RB, int TOP, bool INV, bool QFAST, class LD, class ST>
+template <int LOGL, int RB, int TOP, bool INV, bool QFAST, bool GST = false, bool GLD = false, class LD, class ST>
 __device__ __forceinline__ void run_round(LD ld, ST st, int pi, const PrimeRT& q) {
     constexpr int L = 1 << LOGL, R = 1 << RB, SPL = TOP - RB + 1, SP = 1 << SPL;
     constexpr int GPC = L / R;
@@ -112,8 +112,12 @@ __device__ __forceinline__ void run_round(LD ld, ST st, int pi, const PrimeRT& q
         const int qlo = g & (SP - 1);
         const int row0 = qlo + ((g >> SPL) << (TOP + 1));
         u64 x[R];
+        if constexpr (GLD) {
+            ld(row0, c, x);      // whole group at once
+        } else {
 #pragma unroll
-        for (int t = 0; t < R; ++t) x[t] = ld(row0 + t * SP, c);
+            for (int t = 0; t < R; ++t) x[t] = ld(row0 + t * SP, c);
+        }
         const u64* tw = tab + qlo * R;
         if (!INV) {
 #pragma unroll
@@ -144,15 +148,44 @@ __device__ __forceinline__ void run_round(LD ld, ST st, int pi, const PrimeRT& q
                 }
             }
         }
+        if constexpr (GST) {
+            st(row0, c, x);      // whole group at once (consecutive rows: vector stores)
+        } else {
 #pragma unroll
-        for (int t = 0; t < R; ++t) st(row0 + t * SP, c, x[t]);
+            for (int t = 0; t < R; ++t) st(row0 + t * SP, c, x[t]);
+        }
+    }
+}
+
+// Store R consecutive u64 (16-byte aligned when R >= 2) with 16-byte vector stores.
+template <int R>
+__device__ __forceinline__ void st_vec(u64* p, const u64 (&x)[R]) {
+    if constexpr (R == 1) {
+        p[0] = x[0];
+    } else {
+#pragma unroll
+        for (int t = 0; t < R; t += 2) *reinterpret_cast<ulonglong2*>(p + t) = make_ulonglong2(x[t], x[t + 1]);
+    }
+}
+// Load R consecutive u64 with 16-byte vector loads.
+template <int R>
+__device__ __forceinline__ void ld_vec(const u64* p, u64 (&x)[R]) {
+    if constexpr (R == 1) {
+        x[0] = p[0];
+    } else {
+#pragma unroll
+        for (int t = 0; t < R; t += 2) {
+            const ulonglong2 v = *reinterpret_cast<const ulonglong2*>(p + t);
+            x[t] = v.x;
+            x[t + 1] = v.y;
+        }
     }
 }
 
 // Rounds IDX.. of a sub-transform.  Forward order: round 0 holds the top bits.  Inverse
 // order: inverse round k undoes forward round NR-1-k.  The first round reads with `ld0`, the
 // last writes with `stl`, the rest go through shared memory.
-template <int LOGL, bool INV, bool CONTIG, int IDX, class LD0, class STL>
+template <int LOGL, bool INV, bool CONTIG, int IDX, bool GST = false, bool GLD = false, class LD0, class STL>
 __device__ __forceinline__ void rounds(u64* sm, LD0 ld0, STL stl, int pi, const PrimeRT& q) {
     constexpr int NR = rounds_count(LOGL);
     constexpr int FR = INV ? NR - 1 - IDX : IDX;
@@ -161,17 +194,17 @@ __device__ __forceinline__ void rounds(u64* sm, LD0 ld0, STL stl, int pi, const 
     auto lds = [sm](int j, int c) { return sm[sw(j, c)]; };
     auto sts = [sm](int j, int c, u64 v) { sm[sw(j, c)] = v; };
     if constexpr (NR == 1) {
-        run_round<LOGL, RB, TOP, INV, QF>(ld0, stl, pi, q);
+        run_round<LOGL, RB, TOP, INV, QF, GST, GLD>(ld0, stl, pi, q);
     } else if constexpr (IDX == 0) {
-        run_round<LOGL, RB, TOP, INV, QF>(ld0, sts, pi, q);
+        run_round<LOGL, RB, TOP, INV, QF, false, GLD>(ld0, sts, pi, q);
         __syncthreads();
-        rounds<LOGL, INV, CONTIG, 1>(sm, ld0, stl, pi, q);
+        rounds<LOGL, INV, CONTIG, 1, GST>(sm, ld0, stl, pi, q);
     } else if constexpr (IDX == NR - 1) {
-        run_round<LOGL, RB, TOP, INV, QF>(lds, stl, pi, q);
+        run_round<LOGL, RB, TOP, INV, QF, GST>(lds, stl, pi, q);
     } else {
         run_round<LOGL, RB, TOP, INV, QF>(lds, sts, pi, q);
         __syncthreads();
-        rounds<LOGL, INV, CONTIG, IDX + 1>(sm, ld0, stl, pi, q);
+        rounds<LOGL, INV, CONTIG, IDX + 1, GST>(sm, ld0, stl, pi, q);
     }
 }
 
@@ -180,9 +213,37 @@ __device__ __forceinline__ u64 entry_val(const u64* __restrict__ src, u64 len, u
     return g < len ? mmul(__ldg(src + g), q.r2, q) : 0ull;   // limb * R mod p
 }
 
+// Four-step twiddles of a strided pass.  After the sub-transform, element (row j, column c)
+// holds frequency k = bitrev(j) and is multiplied by w_B^(i k), i = col0 + c.  The lowest
+// round's group covers rows j = qhi*R + t, whose frequencies are k = kq + t' (L/R) with
+// kq = bitrev(qhi) and t' = bitrev(t), so
+//     w_B^(i k) = w_B^(i kq) * w_B^(i t' L/R) = alpha(group) * beta[c][t'].
+// Each CTA fills beta (16 x R values) in shared memory once; each group needs one alpha.
+// The inverse uses the conjugate roots.
+template <int LOGL, bool INV>
+__device__ __forceinline__ void fill_beta(u64* beta, u32 col0, int shift, int pi, const PrimeRT& q) {
+    constexpr int RB = round_bits(LOGL, rounds_count(LOGL) - 1), R = 1 << RB;
+    for (int e = threadIdx.x; e < TC * R; e += NT) {
+        const u32 c = e >> RB, tp = e & (R - 1);
+        u32 x = ((col0 + c) * (tp << (LOGL - RB))) << shift;
+        if (INV) x = (0u - x) & ((1u << MAX_LOG_N) - 1);
+        beta[e] = red1(root30(x, pi, q), q);
+    }
+}
+template <int LOGL, bool INV>
+__device__ __forceinline__ u64 group_alpha(u32 i, int row0, int shift, int pi, const PrimeRT& q) {
+    constexpr int RB = round_bits(LOGL, rounds_count(LOGL) - 1);
+    const u32 kq = LOGL > RB ? __brev((u32)(row0 >> RB)) >> (32 - (LOGL - RB)) : 0u;
+    u32 x = (i * kq) << shift;
+    if (INV) x = (0u - x) & ((1u << MAX_LOG_N) - 1);
+    return red1(root30(x, pi, q), q);
+}
+
 // Forward strided pass (pass p < P-1 of a multi-pass transform).
 template <int LOGL, bool ENTRY>
 __device__ __forceinline__ void body_fwd(u64* sm, const PassArgs& a, u64 tile, int pi, const PrimeRT& q) {
+    constexpr int L = 1 << LOGL;
+    constexpr int RB = round_bits(LOGL, rounds_count(LOGL) - 1), R = 1 << RB;
     const int logS = a.logB - LOGL;
     const u64 tpb_log = logS - 4;
     const u64 blk = tile >> tpb_log;
@@ -191,23 +252,31 @@ __device__ __forceinline__ void body_fwd(u64* sm, const PassArgs& a, u64 tile, i
     u64* __restrict__ d = a.data + (u64)pi * a.N;
     const u64* __restrict__ src = a.src;
     const u64 len = a.len;
+    const int shift = MAX_LOG_N - a.logB;
+    u64* beta = sm + TC * L;
+    fill_beta<LOGL, false>(beta, col0, shift, pi, q);     // read after the first round's barrier
     auto ld0 = [=](int j, int c) -> u64 {
         const u64 g = gbase + c + ((u64)j << logS);
         if constexpr (ENTRY) return entry_val(src, len, g, q);
         else return d[g];
     };
-    const int shift = MAX_LOG_N - a.logB;
-    auto stl = [=](int j, int c, u64 v) {
-        const u32 k = __brev((u32)j) >> (32 - LOGL);
-        const u32 e = (col0 + c) * k;                       // < B <= 2^30
-        d[gbase + c + ((u64)j << logS)] = mmul(v, root30(e << shift, pi, q), q);
+    auto stl = [=](int row0, int c, const auto& x) {
+        const u64 al = group_alpha<LOGL, false>(col0 + c, row0, shift, pi, q);
+        const u64* bc = beta + c * R;
+#pragma unroll
+        for (int t = 0; t < R; ++t) {
+            const int tp = RB ? (int)(__brev((u32)t) >> (32 - RB)) : 0;
+            d[gbase + c + ((u64)(row0 + t) << logS)] = mmul(x[t], mmul(al, bc[tp], q), q);
+        }
     };
-    rounds<LOGL, false, false, 0>(sm, ld0, stl, pi, q);
+    rounds<LOGL, false, false, 0, true>(sm, ld0, stl, pi, q);
 }
 
 // Inverse strided pass: inverse four-step twiddle, then the inverse sub-transform.
 template <int LOGL>
 __device__ __forceinline__ void body_inv(u64* sm, const PassArgs& a, u64 tile, int pi, const PrimeRT& q) {
+    constexpr int L = 1 << LOGL;
+    constexpr int RB = round_bits(LOGL, rounds_count(LOGL) - 1), R = 1 << RB;
     const int logS = a.logB - LOGL;
     const u64 tpb_log = logS - 4;
     const u64 blk = tile >> tpb_log;
@@ -215,14 +284,22 @@ __device__ __forceinline__ void body_inv(u64* sm, const PassArgs& a, u64 tile, i
     const u64 gbase = (blk << a.logB) + col0;
     u64* __restrict__ d = a.data + (u64)pi * a.N;
     const int shift = MAX_LOG_N - a.logB;
-    auto ld0 = [=](int j, int c) -> u64 {
-        const u32 k = __brev((u32)j) >> (32 - LOGL);
-        const u32 e = (col0 + c) * k;
-        const u32 x = (0u - (e << shift)) & ((1u << MAX_LOG_N) - 1);   // w^-e
-        return mmul(d[gbase + c + ((u64)j << logS)], red1(root30(x, pi, q), q), q);
+    u64* beta = sm + TC * L;
+    fill_beta<LOGL, true>(beta, col0, shift, pi, q);
+    __syncthreads();
+    auto ld0 = [=](int row0, int c, auto& x) {
+        const u64 al = group_alpha<LOGL, true>(col0 + c, row0, shift, pi, q);
+        const u64* bc = beta + c * R;
+#pragma unroll
+        for (int t = 0; t < R; ++t) x[t] = d[gbase + c + ((u64)(row0 + t) << logS)];
+#pragma unroll
+        for (int t = 0; t < R; ++t) {
+            const int tp = RB ? (int)(__brev((u32)t) >> (32 - RB)) : 0;
+            x[t] = mmul(x[t], red1(mmul(al, bc[tp], q), q), q);
+        }
     };
     auto stl = [=](int j, int c, u64 v) { d[gbase + c + ((u64)j << logS)] = v; };
-    rounds<LOGL, true, false, 0>(sm, ld0, stl, pi, q);
+    rounds<LOGL, true, false, 0, false, true>(sm, ld0, stl, pi, q);
 }
 
 // Forward last pass over contiguous blocks (operand A of a product).
@@ -240,13 +317,14 @@ __device__ __forceinline__ void body_fwd_last(u64* sm, const PassArgs& a, u64 ti
         if constexpr (ENTRY) return entry_val(src, len, g, q);
         else return d[g];
     };
-    auto stl = [=](int j, int c, u64 v) {
-        if (c < ncols) d[gbase + (u64)c * L + j] = v;
-    };
     if constexpr (LOGL == 0) {
-        if (threadIdx.x < (unsigned)ncols) stl(0, threadIdx.x, ld0(0, threadIdx.x));
+        if (threadIdx.x < (unsigned)ncols) d[gbase + threadIdx.x] = ld0(0, threadIdx.x);
     } else {
-        rounds<LOGL, false, true, 0>(sm, ld0, stl, pi, q);
+        // the lowest round holds consecutive rows of one block: 16-byte vector stores
+        auto stl = [=](int row0, int c, const auto& x) {
+            if (c < ncols) st_vec(d + gbase + (u64)c * L + row0, x);
+        };
+        rounds<LOGL, false, true, 0, true>(sm, ld0, stl, pi, q);
     }
 }
 
@@ -281,9 +359,15 @@ __device__ __forceinline__ void fused_lowest(LD ld, ST st, const u64* __restrict
             }
         }
         if (c < ncols) {
-            const u64* po = oth + gbase + (u64)c * L + row0;
+            if constexpr (SQR) {
 #pragma unroll
-            for (int t = 0; t < R; ++t) x[t] = mmul(x[t], SQR ? x[t] : po[t], q);
+                for (int t = 0; t < R; ++t) x[t] = mmul(x[t], x[t], q);
+            } else {
+                u64 y[R];
+                ld_vec(oth + gbase + (u64)c * L + row0, y);
+#pragma unroll
+                for (int t = 0; t < R; ++t) x[t] = mmul(x[t], y[t], q);
+            }
         }
 #pragma unroll
         for (int s = RB - 1; s >= 0; --s) {
@@ -356,7 +440,7 @@ __device__ __forceinline__ void body_fused(u64* sm, const PassArgs& a, u64 tile,
 
 // ------------------------------------------------------------------ pass kernels
 template <int MODE, int LOGL, bool ENTRY, bool SQR>
-__global__ void __launch_bounds__(NT) k_pass(PassArgs a) {
+__global__ void __launch_bounds__(NT, 4) k_pass(PassArgs a) {
     extern __shared__ __align__(16) u64 sm[];
     const int pi = blockIdx.x % 3;          // prime varies fastest: the three CTAs of a tile
     const u64 tile = blockIdx.x / 3;        // read the same limbs at the same time (L2 reuse)
@@ -693,7 +777,8 @@ static const KernelTable& ktab() {
     return t;
 }
 
-static size_t pass_smem(int logl) { return (size_t)TC * ((size_t)1 << logl) * sizeof(u64); }
+// tile + the 16 x 16 four-step twiddle factors of strided passes
+static size_t pass_smem(int logl) { return ((size_t)TC * ((size_t)1 << logl) + TC * 16) * sizeof(u64); }
 
 cudaError_t ensure_tables() {
     int dev = 0;
