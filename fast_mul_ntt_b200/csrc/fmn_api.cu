@@ -12,6 +12,7 @@
 
 #include <mutex>
 #include <string>
+#include <vector>
 
 #include "../../include/fast_mul.h"
 #include "fmn_internal.h"
@@ -42,6 +43,15 @@ struct DevCtx {
     u64* io = nullptr;                // device staging for host-pointer calls
     size_t io_cap = 0;
     unsigned* h_err = nullptr;        // pinned word for reading the device error flag
+    // precomputed four-step twiddles, one set per transform length, least recently used evicted
+    struct Tw {
+        fmn::TwiddleSet set;
+        void* buf;
+        size_t bytes;
+        u64 last_use;
+    };
+    std::vector<Tw> tw;
+    u64 tick = 0;
 };
 
 std::mutex g_ctx_mu;
@@ -126,6 +136,58 @@ int check_sizes(u64 len1, u64 len2) {
 
 size_t round256(size_t x) { return (x + 255) & ~(size_t)255; }
 
+// Twiddle tables for transforms of 2^log_n points, built on stream s on first use (caller
+// holds c->mu and has ordered s after the context's previous work).  Returns null when the
+// transform has one pass or memory is short; the kernels then generate the twiddles.
+const fmn::TwiddleSet* get_twiddles(DevCtx* c, int log_n, cudaStream_t s) {
+    const size_t bytes = fmn::twiddle_table_bytes(log_n);
+    if (bytes == 0) return nullptr;
+    for (auto& t : c->tw)
+        if (t.set.log_n == log_n) {
+            t.last_use = ++c->tick;
+            return &t.set;
+        }
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    const size_t cap = total_b / 4;          // tables never take more than a quarter of the GPU
+    size_t held = 0;
+    for (auto& t : c->tw) held += t.bytes;
+    while (!c->tw.empty() && (held + bytes > cap || c->tw.size() >= 8)) {
+        size_t lru = 0;
+        for (size_t k = 1; k < c->tw.size(); ++k)
+            if (c->tw[k].last_use < c->tw[lru].last_use) lru = k;
+        cudaFree(c->tw[lru].buf);             // synchronises the device: no job still reads it
+        held -= c->tw[lru].bytes;
+        c->tw.erase(c->tw.begin() + lru);
+    }
+    if (held + bytes > cap || bytes + (size_t)(1ull << 30) > free_b) return nullptr;
+    void* buf = nullptr;
+    if (cudaMalloc(&buf, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    DevCtx::Tw t;
+    t.buf = buf;
+    t.bytes = bytes;
+    t.last_use = ++c->tick;
+    if (fmn::build_twiddle_tables(log_n, (u64*)buf, &t.set, s) != cudaSuccess) {
+        cudaGetLastError();
+        cudaFree(buf);
+        return nullptr;
+    }
+    c->tw.push_back(t);
+    return &c->tw.back().set;
+}
+
+int ilog2_ceil(u64 x) {
+    int r = 0;
+    while ((1ull << r) < x) ++r;
+    return r;
+}
+
 // Enqueue a product on stream s using the context workspace (caller holds c->mu).
 int run_job_ctx(DevCtx* c, const fmn::Job& j, cudaStream_t s) {
     const size_t need = fmn::job_workspace_bytes(j.la, j.lb, j.sqr);
@@ -134,7 +196,8 @@ int run_job_ctx(DevCtx* c, const fmn::Job& j, cudaStream_t s) {
     cudaError_t e;
     if (c->done_valid && (e = cudaStreamWaitEvent(s, c->done, 0)) != cudaSuccess)
         return set_err(FMN_ERR_CUDA, "cudaStreamWaitEvent", e);
-    if ((e = fmn::enqueue_job(j, c->ws, c->ws_cap, s)) != cudaSuccess) return set_err(FMN_ERR_CUDA, "kernel launch", e);
+    const fmn::TwiddleSet* tws = get_twiddles(c, ilog2_ceil(j.la + j.lb - 1), s);
+    if ((e = fmn::enqueue_job(j, c->ws, c->ws_cap, s, tws)) != cudaSuccess) return set_err(FMN_ERR_CUDA, "kernel launch", e);
     if ((e = cudaEventRecord(c->done, s)) != cudaSuccess) return set_err(FMN_ERR_CUDA, "cudaEventRecord", e);
     c->done_valid = true;
     return FMN_OK;
@@ -262,6 +325,7 @@ void fmn_shutdown(void) {
         if (c->ws) cudaFree(c->ws);
         if (c->io) cudaFree(c->io);
         if (c->h_err) cudaFreeHost(c->h_err);
+        for (auto& t : c->tw) cudaFree(t.buf);
         if (c->done) cudaEventDestroy(c->done);
         if (c->stream) cudaStreamDestroy(c->stream);
         delete c;

@@ -38,10 +38,24 @@ size_t job_workspace_bytes(u64 la, u64 lb, int sqr);
 // Upload twiddle tables to the current device (idempotent per device).
 cudaError_t ensure_tables();
 
+// Precomputed four-step twiddles of every strided pass of one transform length.
+struct TwiddleSet {
+    int log_n;
+    const u64* fwd[MAX_PASSES];
+    const u64* inv[MAX_PASSES];
+};
+// Device bytes the tables of a length-2^log_n transform need (0 when it has one pass).
+size_t twiddle_table_bytes(int log_n);
+// Fill `buf` (twiddle_table_bytes(log_n) bytes) on `stream` and describe it in `out`.
+cudaError_t build_twiddle_tables(int log_n, u64* buf, TwiddleSet* out, cudaStream_t stream);
+
 // Enqueue one product on `stream` using `ws` (job_workspace_bytes(...) bytes, 256-byte
 // aligned).  The first u32 of ws is an error word that the carry scan sets (never clears)
 // when a bounded wait gives up; callers zero it once and read it after the stream is done.
-cudaError_t enqueue_job(const Job& job, void* ws, size_t ws_bytes, cudaStream_t stream);
+// `tw` (optional) holds precomputed four-step twiddles for this transform length; without
+// it the kernels generate them.
+cudaError_t enqueue_job(const Job& job, void* ws, size_t ws_bytes, cudaStream_t stream,
+                        const TwiddleSet* tw = nullptr);
 
 // ---- optional per-kernel timing (used by bench.py; off by default)
 // Kernel kinds of the pipeline.

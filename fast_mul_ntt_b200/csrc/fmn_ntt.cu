@@ -86,6 +86,9 @@ struct PassArgs {
     u64 N;            // transform length
     int logB;         // log2 block length of this pass
     int ncols;        // contiguous passes: number of blocks (columns) in a tile, <= 16
+    const u64* tw;    // strided passes: precomputed four-step twiddles of this pass
+                      // (prime i at tw + i * 2^logB, entry j * S + column), or null to
+                      // generate them on the fly
 };
 
 // ------------------------------------------------------------------ one round
@@ -254,19 +257,28 @@ __device__ __forceinline__ void body_fwd(u64* sm, const PassArgs& a, u64 tile, i
     const u64 len = a.len;
     const int shift = MAX_LOG_N - a.logB;
     u64* beta = sm + TC * L;
-    fill_beta<LOGL, false>(beta, col0, shift, pi, q);     // read after the first round's barrier
+    const u64* __restrict__ tw = a.tw ? a.tw + ((u64)pi << a.logB) + col0 : nullptr;
+    if (!tw) fill_beta<LOGL, false>(beta, col0, shift, pi, q);     // read after the first round's barrier
     auto ld0 = [=](int j, int c) -> u64 {
         const u64 g = gbase + c + ((u64)j << logS);
         if constexpr (ENTRY) return entry_val(src, len, g, q);
         else return d[g];
     };
     auto stl = [=](int row0, int c, const auto& x) {
-        const u64 al = group_alpha<LOGL, false>(col0 + c, row0, shift, pi, q);
-        const u64* bc = beta + c * R;
+        if (tw) {
 #pragma unroll
-        for (int t = 0; t < R; ++t) {
-            const int tp = RB ? (int)(__brev((u32)t) >> (32 - RB)) : 0;
-            d[gbase + c + ((u64)(row0 + t) << logS)] = mmul(x[t], mmul(al, bc[tp], q), q);
+            for (int t = 0; t < R; ++t) {
+                const u64 off = c + ((u64)(row0 + t) << logS);
+                d[gbase + off] = mmul(x[t], __ldg(tw + off), q);
+            }
+        } else {
+            const u64 al = group_alpha<LOGL, false>(col0 + c, row0, shift, pi, q);
+            const u64* bc = beta + c * R;
+#pragma unroll
+            for (int t = 0; t < R; ++t) {
+                const int tp = RB ? (int)(__brev((u32)t) >> (32 - RB)) : 0;
+                d[gbase + c + ((u64)(row0 + t) << logS)] = mmul(x[t], mmul(al, bc[tp], q), q);
+            }
         }
     };
     rounds<LOGL, false, false, 0, true>(sm, ld0, stl, pi, q);
@@ -285,17 +297,25 @@ __device__ __forceinline__ void body_inv(u64* sm, const PassArgs& a, u64 tile, i
     u64* __restrict__ d = a.data + (u64)pi * a.N;
     const int shift = MAX_LOG_N - a.logB;
     u64* beta = sm + TC * L;
-    fill_beta<LOGL, true>(beta, col0, shift, pi, q);
-    __syncthreads();
+    const u64* __restrict__ tw = a.tw ? a.tw + ((u64)pi << a.logB) + col0 : nullptr;
+    if (!tw) {
+        fill_beta<LOGL, true>(beta, col0, shift, pi, q);
+        __syncthreads();
+    }
     auto ld0 = [=](int row0, int c, auto& x) {
-        const u64 al = group_alpha<LOGL, true>(col0 + c, row0, shift, pi, q);
-        const u64* bc = beta + c * R;
 #pragma unroll
         for (int t = 0; t < R; ++t) x[t] = d[gbase + c + ((u64)(row0 + t) << logS)];
+        if (tw) {
 #pragma unroll
-        for (int t = 0; t < R; ++t) {
-            const int tp = RB ? (int)(__brev((u32)t) >> (32 - RB)) : 0;
-            x[t] = mmul(x[t], red1(mmul(al, bc[tp], q), q), q);
+            for (int t = 0; t < R; ++t) x[t] = mmul(x[t], __ldg(tw + c + ((u64)(row0 + t) << logS)), q);
+        } else {
+            const u64 al = group_alpha<LOGL, true>(col0 + c, row0, shift, pi, q);
+            const u64* bc = beta + c * R;
+#pragma unroll
+            for (int t = 0; t < R; ++t) {
+                const int tp = RB ? (int)(__brev((u32)t) >> (32 - RB)) : 0;
+                x[t] = mmul(x[t], red1(mmul(al, bc[tp], q), q), q);
+            }
         }
     };
     auto stl = [=](int j, int c, u64 v) { d[gbase + c + ((u64)j << logS)] = v; };
@@ -449,6 +469,54 @@ __global__ void __launch_bounds__(NT, 4) k_pass(PassArgs a) {
     else if constexpr (MODE == M_INV) body_inv<LOGL>(sm, a, tile, pi, q);
     else if constexpr (MODE == M_FWD_LAST) body_fwd_last<LOGL, ENTRY>(sm, a, tile, pi, q);
     else body_fused<LOGL, ENTRY, SQR>(sm, a, tile, pi, q);
+}
+
+// ------------------------------------------------------------------ four-step twiddle tables
+// Entry j * S + i of pass (logB, logl): w_B^(i * bitrev(j)) (forward) and its inverse, both
+// fully reduced, for the three primes (prime-major).
+__global__ void __launch_bounds__(256) k_tw_table(u64* tf, u64* ti, int logB, int logl) {
+    const u64 B = 1ull << logB;
+    const int shift = MAX_LOG_N - logB, logS = logB - logl;
+    for (u64 idx = blockIdx.x * 256ull + threadIdx.x; idx < 3 * B; idx += (u64)gridDim.x * 256) {
+        const int pi = (int)(idx >> logB);
+        const u64 r = idx & (B - 1);
+        const u32 j = (u32)(r >> logS), i = (u32)(r & ((1ull << logS) - 1));
+        const u32 k = __brev(j) >> (32 - logl);
+        const u32 x = (i * k) << shift;
+        const PrimeRT q = c_prime[pi];
+        tf[idx] = red1(root30(x, pi, q), q);
+        ti[idx] = red1(root30((0u - x) & ((1u << MAX_LOG_N) - 1), pi, q), q);
+    }
+}
+
+size_t twiddle_table_bytes(int log_n) {
+    const Plan pl = make_plan(log_n);
+    size_t b = 0, logB = log_n;
+    for (int p = 0; p + 1 < pl.passes; ++p) {
+        b += 2 * 3 * ((size_t)1 << logB) * sizeof(u64);
+        logB -= pl.bits[p];
+    }
+    return b;
+}
+
+cudaError_t build_twiddle_tables(int log_n, u64* buf, TwiddleSet* out, cudaStream_t s) {
+    const Plan pl = make_plan(log_n);
+    memset(out, 0, sizeof(*out));
+    out->log_n = log_n;
+    int logB = log_n;
+    u64* p = buf;
+    for (int k = 0; k + 1 < pl.passes; ++k) {
+        const u64 B = 1ull << logB;
+        out->fwd[k] = p;
+        out->inv[k] = p + 3 * B;
+        const unsigned grid = (unsigned)((3 * B + 255) / 256 < 148 * 16 ? (3 * B + 255) / 256 : 148 * 16);
+        k_tw_table<<<grid, 256, 0, s>>>(p, p + 3 * B, logB, pl.bits[k]);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+        p += 6 * B;
+        logB -= pl.bits[k];
+    }
+    return cudaSuccess;
 }
 
 // ------------------------------------------------------------------ CRT + carry
@@ -976,7 +1044,7 @@ int job_launches(u64 la, u64 lb, int sqr) {
     return sqr ? (P - 1) + 1 + (P - 1) + 1 : 2 * (P - 1) + 1 + 1 + (P - 1) + 1;
 }
 
-cudaError_t enqueue_job(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s) {
+cudaError_t enqueue_job(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s, const TwiddleSet* tws) {
     const u64 out_len = j.la + j.lb;
     if (out_len == 0) return cudaSuccess;
     if (j.la == 0 || j.lb == 0) return cudaMemsetAsync(j.out, 0, out_len * sizeof(u64), s);
@@ -992,6 +1060,7 @@ cudaError_t enqueue_job(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s)
     const int P = pl.passes;
     const u64 N = w.N;
 
+    if (tws && tws->log_n != w.n) tws = nullptr;
     PassArgs pa;
     memset(&pa, 0, sizeof(pa));
     pa.N = N;
@@ -1011,6 +1080,7 @@ cudaError_t enqueue_job(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s)
             pa.len = len;
             pa.data = data;
             pa.logB = logB[p];
+            pa.tw = tws ? tws->fwd[p] : nullptr;
             const cudaError_t r =
                 launch_pass(p == 0 ? V_FWD_E : V_FWD, pl.bits[p], pa, N >> (pl.bits[p] + 4), s);
             if (r != cudaSuccess) return r;
@@ -1020,6 +1090,7 @@ cudaError_t enqueue_job(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s)
 
     if (!sqr) {
         if ((e = fwd_strided(j.a, j.la, A)) != cudaSuccess) return e;
+        pa.tw = nullptr;
         pa.src = j.a;
         pa.len = j.la;
         pa.data = A;
@@ -1028,6 +1099,7 @@ cudaError_t enqueue_job(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s)
         if ((e = launch_pass(P == 1 ? V_LAST_E : V_LAST, lastl, pa, tiles_last, s)) != cudaSuccess) return e;
         pa.ncols = TC;
         if ((e = fwd_strided(j.b, j.lb, B)) != cudaSuccess) return e;
+        pa.tw = nullptr;
         pa.src = j.b;
         pa.len = j.lb;
         pa.data = B;
@@ -1037,6 +1109,7 @@ cudaError_t enqueue_job(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s)
         if ((e = launch_pass(P == 1 ? V_FUSED_E : V_FUSED, lastl, pa, tiles_last, s)) != cudaSuccess) return e;
     } else {
         if ((e = fwd_strided(j.a, j.la, A)) != cudaSuccess) return e;
+        pa.tw = nullptr;
         pa.src = j.a;
         pa.len = j.la;
         pa.data = A;
@@ -1051,6 +1124,7 @@ cudaError_t enqueue_job(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s)
     for (int p = P - 2; p >= 0; --p) {
         pa.data = A;
         pa.logB = logB[p];
+        pa.tw = tws ? tws->inv[p] : nullptr;
         if ((e = launch_pass(V_INV, pl.bits[p], pa, N >> (pl.bits[p] + 4), s)) != cudaSuccess) return e;
     }
 
