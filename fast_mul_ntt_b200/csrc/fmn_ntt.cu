@@ -76,7 +76,7 @@ __device__ __forceinline__ u64 root30(u32 x, int pi, const PrimeRT& q) {
 __device__ __forceinline__ int sw(int j, int c) { return (j << 4) | (c ^ (j & 15)); }
 
 // ------------------------------------------------------------------ kernel arguments
-enum { M_FWD = 0, M_FWD_LAST = 1, M_FUSED = 2, M_INV = 3 };
+enum { M_FWD = 0, M_FWD_LAST = 1, M_FUSED = 2, M_INV = 3, M_FUSED2 = 4 };
 
 struct PassArgs {
     const u64* src;   // ENTRY: limbs of the operand being transformed
@@ -350,7 +350,7 @@ __device__ __forceinline__ void body_fwd_last(u64* sm, const PassArgs& a, u64 ti
 
 // The lowest forward round, the pointwise product and the lowest inverse round of one
 // contiguous tile, all in registers.
-template <int LOGL, bool SQR, class LD, class ST>
+template <int LOGL, bool SQR, bool OTH_SMEM = false, class LD, class ST>
 __device__ __forceinline__ void fused_lowest(LD ld, ST st, const u64* __restrict__ oth, u64 gbase,
                                              int ncols, int pi, const PrimeRT& q) {
     constexpr int L = 1 << LOGL;
@@ -382,6 +382,9 @@ __device__ __forceinline__ void fused_lowest(LD ld, ST st, const u64* __restrict
             if constexpr (SQR) {
 #pragma unroll
                 for (int t = 0; t < R; ++t) x[t] = mmul(x[t], x[t], q);
+            } else if constexpr (OTH_SMEM) {
+#pragma unroll
+                for (int t = 0; t < R; ++t) x[t] = mmul(x[t], oth[sw(row0 + t, c)], q);
             } else {
                 u64 y[R];
                 ld_vec(oth + gbase + (u64)c * L + row0, y);
@@ -458,6 +461,45 @@ __device__ __forceinline__ void body_fused(u64* sm, const PassArgs& a, u64 tile,
     }
 }
 
+// Both operands' last forward pass, pointwise product and first inverse pass in one CTA:
+// the first operand's tile (read from `other`) is transformed into a second shared-memory
+// tile and never written back; the product overwrites `other`.  Multi-pass products only.
+template <int LOGL>
+__device__ __forceinline__ void body_fused2(u64* sm, const PassArgs& a, u64 tile, int pi, const PrimeRT& q) {
+    constexpr int L = 1 << LOGL;
+    constexpr int NR = rounds_count(LOGL);
+    static_assert(NR >= 2, "multi-round sub-transforms only");
+    const u64 gbase = tile << (LOGL + 4);
+    const u64* __restrict__ d = a.data + (u64)pi * a.N;
+    u64* __restrict__ o = a.other + (u64)pi * a.N;
+    u64* smA = sm + TC * L;
+    // first operand: full forward sub-transform into smA
+    auto ldA = [=](int j, int c) -> u64 { return o[gbase + (u64)c * L + j]; };
+    auto stA = [smA](int j, int c, u64 v) { smA[sw(j, c)] = v; };
+    rounds<LOGL, false, true, 0>(smA, ldA, stA, pi, q);
+    // second operand: forward rounds 0 .. NR-2 in sm
+    auto ldg = [=](int j, int c) -> u64 { return d[gbase + (u64)c * L + j]; };
+    auto stg = [=](int j, int c, u64 v) { o[gbase + (u64)c * L + j] = v; };
+    auto lds = [sm](int j, int c) { return sm[sw(j, c)]; };
+    auto sts = [sm](int j, int c, u64 v) { sm[sw(j, c)] = v; };
+    constexpr int RB0 = round_bits(LOGL, 0);
+    run_round<LOGL, RB0, LOGL - 1, false, true>(ldg, sts, pi, q);
+    __syncthreads();                                   // also publishes smA
+    if constexpr (NR == 3) {
+        constexpr int RB1 = round_bits(LOGL, 1), T1 = round_top(LOGL, 1);
+        run_round<LOGL, RB1, T1, false, false>(lds, sts, pi, q);
+        __syncthreads();
+    }
+    fused_lowest<LOGL, false, true>(lds, sts, smA, gbase, TC, pi, q);
+    __syncthreads();
+    if constexpr (NR == 3) {
+        constexpr int RB1 = round_bits(LOGL, 1), T1 = round_top(LOGL, 1);
+        run_round<LOGL, RB1, T1, true, false>(lds, sts, pi, q);
+        __syncthreads();
+    }
+    run_round<LOGL, RB0, LOGL - 1, true, true>(lds, stg, pi, q);
+}
+
 // ------------------------------------------------------------------ pass kernels
 template <int MODE, int LOGL, bool ENTRY, bool SQR>
 __global__ void __launch_bounds__(NT, 4) k_pass(PassArgs a) {
@@ -468,6 +510,7 @@ __global__ void __launch_bounds__(NT, 4) k_pass(PassArgs a) {
     if constexpr (MODE == M_FWD) body_fwd<LOGL, ENTRY>(sm, a, tile, pi, q);
     else if constexpr (MODE == M_INV) body_inv<LOGL>(sm, a, tile, pi, q);
     else if constexpr (MODE == M_FWD_LAST) body_fwd_last<LOGL, ENTRY>(sm, a, tile, pi, q);
+    else if constexpr (MODE == M_FUSED2) body_fused2<(LOGL >= 5 ? LOGL : 5)>(sm, a, tile, pi, q);
     else body_fused<LOGL, ENTRY, SQR>(sm, a, tile, pi, q);
 }
 
@@ -527,7 +570,7 @@ cudaError_t build_twiddle_tables(int log_n, u64* buf, TwiddleSet* out, cudaStrea
 // which gives a parallel scan: per-thread functions, a CTA scan, and a decoupled look-back
 // across CTAs in the order CTAs obtain tickets.
 constexpr int CNT = 256;           // threads per CTA
-constexpr int CE = 8;              // limbs per thread
+constexpr int CE = 16;             // limbs per thread
 constexpr int CTILE = CNT * CE;    // limbs per CTA
 constexpr u32 ID_FN = 0xE4;        // identity map
 constexpr u32 ST_AGG = 1u << 8, ST_PRE = 2u << 8;
@@ -572,13 +615,13 @@ __device__ __forceinline__ void acc_mul(u64 y, u64 ml, u64 mh, u64& w0, u64& w1,
     w2 = w2 + (u64)(hi >> 64) + (u64)(s1 >> 64);
 }
 
-__device__ __forceinline__ void crt_coef(const CrtArgs& a, u64 j, u64& w0, u64& w1, u64& w2,
-                                         const PrimeRT& q0, const PrimeRT& q1, const PrimeRT& q2) {
+// crt3 of one coefficient from its three residues r0, r1, r2 (< 4p_i).
+__device__ __forceinline__ void crt_of(u64 r0, u64 r1, u64 r2, const u64 (&cst)[3], u64& w0, u64& w1, u64& w2,
+                                       const PrimeRT& q0, const PrimeRT& q1, const PrimeRT& q2) {
+    const u64 y0 = red1(mmul(r0, cst[0], q0), q0);
+    const u64 y1 = red1(mmul(r1, cst[1], q1), q1);
+    const u64 y2 = red1(mmul(r2, cst[2], q2), q2);
     w0 = w1 = w2 = 0;
-    if (j >= a.nvalid) return;
-    const u64 y0 = red1(mmul(a.res[j], a.cst[0], q0), q0);
-    const u64 y1 = red1(mmul(a.res[a.N + j], a.cst[1], q1), q1);
-    const u64 y2 = red1(mmul(a.res[2 * a.N + j], a.cst[2], q2), q2);
     acc_mul(y0, m_lo(0), m_hi(0), w0, w1, w2);
     acc_mul(y1, m_lo(1), m_hi(1), w0, w1, w2);
     acc_mul(y2, m_lo(2), m_hi(2), w0, w1, w2);
@@ -596,6 +639,13 @@ __device__ __forceinline__ void crt_coef(const CrtArgs& a, u64 j, u64& w0, u64& 
     }
 }
 
+__device__ __forceinline__ void crt_coef(const CrtArgs& a, u64 j, u64& w0, u64& w1, u64& w2,
+                                         const PrimeRT& q0, const PrimeRT& q1, const PrimeRT& q2) {
+    w0 = w1 = w2 = 0;
+    if (j >= a.nvalid) return;
+    crt_of(a.res[j], a.res[a.N + j], a.res[2 * a.N + j], a.cst, w0, w1, w2, q0, q1, q2);
+}
+
 __device__ __forceinline__ u32 fn_apply(u32 f, u32 c) { return (f >> (2 * c)) & 3u; }
 __device__ __forceinline__ u32 fn_compose(u32 later, u32 earlier) {   // later o earlier
     u32 r = 0;
@@ -604,9 +654,15 @@ __device__ __forceinline__ u32 fn_compose(u32 later, u32 earlier) {   // later o
     return r;
 }
 
+// Adds x to the limb sum (lo, h): lo += x, carry into the 2-bit high part.
+__device__ __forceinline__ void add_to(u64& lo, u32& h, u64 x) {
+    lo += x;
+    h += lo < x;
+}
+
 __global__ void __launch_bounds__(CNT) k_crt_carry(CrtArgs a) {
     __shared__ u32 s_tile;
-    __shared__ u64 s_hi1[CNT / 32], s_hi2[CNT / 32], s_hi2b[CNT / 32];
+    __shared__ u64 s_hw[CNT / 32][3];
     __shared__ u32 s_warp[CNT / 32];
     __shared__ u32 s_cin;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -616,49 +672,66 @@ __global__ void __launch_bounds__(CNT) k_crt_carry(CrtArgs a) {
     const u64 tile = s_tile;
     const u64 j0 = tile * CTILE + (u64)tid * CE;
 
-    u64 w0[CE], w1[CE], w2[CE];
+    // coefficients j0 .. j0+15, folded into limb sums s_j = c_j[0] + c_{j-1}[1] + c_{j-2}[2]
+    // (the two contributions from the previous thread's coefficients are added below)
+    u64 lo[CE];
+    u32 h[CE];
+    u64 pw1 = 0, pw2 = 0, ppw2 = 0;          // c_{j-1}[1], c_{j-1}[2], c_{j-2}[2]
+    const bool full = j0 + CE <= a.nvalid;
 #pragma unroll
-    for (int e = 0; e < CE; ++e) crt_coef(a, j0 + e, w0[e], w1[e], w2[e], q0, q1, q2);
-
-    // high words of the two coefficients just below j0
-    u64 p1w1 = __shfl_up_sync(0xffffffffu, w1[CE - 1], 1);
-    u64 p1w2 = __shfl_up_sync(0xffffffffu, w2[CE - 1], 1);
-    u64 p2w2 = __shfl_up_sync(0xffffffffu, w2[CE - 2], 1);
+    for (int e2 = 0; e2 < CE; e2 += 2) {
+        u64 r0[2], r1[2], r2[2];
+        if (full) {
+            const ulonglong2 v0 = *reinterpret_cast<const ulonglong2*>(a.res + j0 + e2);
+            const ulonglong2 v1 = *reinterpret_cast<const ulonglong2*>(a.res + a.N + j0 + e2);
+            const ulonglong2 v2 = *reinterpret_cast<const ulonglong2*>(a.res + 2 * a.N + j0 + e2);
+            r0[0] = v0.x, r0[1] = v0.y, r1[0] = v1.x, r1[1] = v1.y, r2[0] = v2.x, r2[1] = v2.y;
+        }
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+            const int e = e2 + u;
+            u64 w0, w1, w2;
+            if (full) crt_of(r0[u], r1[u], r2[u], a.cst, w0, w1, w2, q0, q1, q2);
+            else crt_coef(a, j0 + e, w0, w1, w2, q0, q1, q2);
+            u64 l = w0;
+            u32 hh = 0;
+            add_to(l, hh, pw1);
+            add_to(l, hh, ppw2);
+            lo[e] = l;
+            h[e] = hh;
+            ppw2 = pw2;
+            pw1 = w1;
+            pw2 = w2;
+        }
+    }
+    // contributions of the two coefficients just below j0 (previous thread / previous CTA)
+    u64 n1 = __shfl_up_sync(0xffffffffu, pw1, 1);   // c_{j0-1}[1]
+    u64 n2 = __shfl_up_sync(0xffffffffu, pw2, 1);   // c_{j0-1}[2]
+    u64 n3 = __shfl_up_sync(0xffffffffu, ppw2, 1);  // c_{j0-2}[2]
     if (lane == 31) {
-        s_hi1[warp] = w1[CE - 1];
-        s_hi2[warp] = w2[CE - 1];
-        s_hi2b[warp] = w2[CE - 2];
+        s_hw[warp][0] = pw1;
+        s_hw[warp][1] = pw2;
+        s_hw[warp][2] = ppw2;
     }
     __syncthreads();
     if (lane == 0) {
         if (warp > 0) {
-            p1w1 = s_hi1[warp - 1];
-            p1w2 = s_hi2[warp - 1];
-            p2w2 = s_hi2b[warp - 1];
+            n1 = s_hw[warp - 1][0];
+            n2 = s_hw[warp - 1][1];
+            n3 = s_hw[warp - 1][2];
         } else {
-            u64 u0, u1, u2, r0, r1, r2;
+            u64 u0, u1, u2, v0, v1, v2;
             if (j0 >= 1) crt_coef(a, j0 - 1, u0, u1, u2, q0, q1, q2); else u0 = u1 = u2 = 0;
-            if (j0 >= 2) crt_coef(a, j0 - 2, r0, r1, r2, q0, q1, q2); else r0 = r1 = r2 = 0;
-            p1w1 = u1;
-            p1w2 = u2;
-            p2w2 = r2;
+            if (j0 >= 2) crt_coef(a, j0 - 2, v0, v1, v2, q0, q1, q2); else v0 = v1 = v2 = 0;
+            n1 = u1;
+            n2 = u2;
+            n3 = v2;
         }
     }
+    add_to(lo[0], h[0], n1);
+    add_to(lo[0], h[0], n3);
+    add_to(lo[1], h[1], n2);
 
-    // s_j = lo + h * 2^64
-    u64 lo[CE];
-    u32 h[CE];
-#pragma unroll
-    for (int e = 0; e < CE; ++e) {
-        const u64 x1 = e >= 1 ? w1[e - 1] : p1w1;
-        const u64 x2 = e >= 2 ? w2[e - 2] : (e == 1 ? p1w2 : p2w2);
-        const u64 t = w0[e] + x1;
-        u32 hh = t < x1;
-        const u64 t2 = t + x2;
-        hh += t2 < x2;
-        lo[e] = t2;
-        h[e] = hh;
-    }
     // carry-transfer function of this thread's limbs
     u32 f = 0;
 #pragma unroll
@@ -671,7 +744,7 @@ __global__ void __launch_bounds__(CNT) k_crt_carry(CrtArgs a) {
         }
         f |= (u32)c << (2 * cin);
     }
-    // CTA inclusive scan (Kogge-Stone in the warp, then across warps)
+    // CTA scan: Kogge-Stone in each warp, then over the warps in warp 0
     u32 inc = f;
 #pragma unroll
     for (int d = 1; d < 32; d <<= 1) {
@@ -682,54 +755,83 @@ __global__ void __launch_bounds__(CNT) k_crt_carry(CrtArgs a) {
     if (lane == 0) exc = ID_FN;
     if (lane == 31) s_warp[warp] = inc;
     __syncthreads();
-    if (tid == 0) {
-        u32 agg = ID_FN;
-        for (int w = 0; w < CNT / 32; ++w) {
-            const u32 t = s_warp[w];
-            s_warp[w] = agg;                 // exclusive prefix of warp w
-            agg = fn_compose(t, agg);
+    if (warp == 0) {
+        u32 wt = lane < CNT / 32 ? s_warp[lane] : ID_FN;
+#pragma unroll
+        for (int d = 1; d < CNT / 32; d <<= 1) {
+            const u32 o = __shfl_up_sync(0xffffffffu, wt, d);
+            if (lane >= d) wt = fn_compose(wt, o);
         }
-        volatile u32* st = a.state;
+        u32 wex = __shfl_up_sync(0xffffffffu, wt, 1);
+        if (lane == 0) wex = ID_FN;
+        const u32 agg = __shfl_sync(0xffffffffu, wt, CNT / 32 - 1);
+        if (lane < CNT / 32) s_warp[lane] = wex;       // exclusive prefix of each warp
         u32 cin = 0;
         if (tile == 0) {
-            atomicExch(&a.state[0], ST_PRE | fn_apply(agg, 0));
+            if (lane == 0) atomicExch(&a.state[0], ST_PRE | fn_apply(agg, 0));
         } else {
-            atomicExch(&a.state[tile], ST_AGG | agg);
-            u32 acc = ID_FN;                 // composition of the aggregates seen so far
-            long p = (long)tile - 1;
-            long spins = 0;
+            if (lane == 0) atomicExch(&a.state[tile], ST_AGG | agg);
+            // warp-parallel look-back over the 32 nearest predecessors at a time
+            volatile u32* st = a.state;
+            u32 acc = ID_FN;
+            long base = (long)tile - 1;
+            bool failed = false;
             while (true) {
-                const u32 v = st[p];
-                if (v & ST_PRE) {
-                    cin = fn_apply(acc, v & 0xff);
-                    break;
-                }
-                if (v & ST_AGG) {
-                    acc = fn_compose(acc, v & 0xff);
-                    if (--p < 0) {
-                        cin = fn_apply(acc, 0);
-                        break;
+                const long p = base - lane;
+                u32 v = ST_PRE;                         // before the first CTA: carry 0
+                if (p >= 0) {
+                    long spins = 0;
+                    v = st[p];
+                    while (v == 0) {
+                        if (++spins > SPIN_LIMIT) {
+                            failed = true;
+                            v = ST_PRE;
+                            break;
+                        }
+                        __nanosleep(64);
+                        v = st[p];
                     }
-                    continue;
                 }
-                if (++spins > SPIN_LIMIT) {
-                    atomicOr(a.err, 1u);
-                    cin = 0;
+                const unsigned pre = __ballot_sync(0xffffffffu, (v & ST_PRE) != 0);
+                const int first = pre ? __ffs(pre) - 1 : 32;
+                // compose the aggregates of lanes 0 .. first-1 (nearest first)
+                u32 fl = (lane < first) ? (v & 0xff) : ID_FN;
+#pragma unroll
+                for (int d = 1; d < 32; d <<= 1) {
+                    const u32 o = __shfl_down_sync(0xffffffffu, fl, d);
+                    if ((lane & (2 * d - 1)) == 0 && lane + d < 32) fl = fn_compose(fl, o);
+                }
+                fl = __shfl_sync(0xffffffffu, fl, 0);
+                acc = fn_compose(acc, fl);
+                if (pre) {
+                    const u32 pv = __shfl_sync(0xffffffffu, v, first) & 0xff;
+                    cin = fn_apply(acc, pv);
                     break;
                 }
-                __nanosleep(64);
+                base -= 32;
             }
-            atomicExch(&a.state[tile], ST_PRE | fn_apply(agg, cin));
+            if (__any_sync(0xffffffffu, failed) && lane == 0) atomicOr(a.err, 1u);
+            if (lane == 0) atomicExch(&a.state[tile], ST_PRE | fn_apply(agg, cin));
         }
-        s_cin = cin;
+        if (lane == 0) s_cin = cin;
     }
     __syncthreads();
     u64 c = fn_apply(exc, fn_apply(s_warp[warp], s_cin));
+    u64 outv[CE];
 #pragma unroll
     for (int e = 0; e < CE; ++e) {
         const u64 t = lo[e] + c;
         c = h[e] + (t < c);
-        if (j0 + e < a.out_len) a.out[j0 + e] = t;
+        outv[e] = t;
+    }
+    if (j0 + CE <= a.out_len && ((reinterpret_cast<uintptr_t>(a.out) & 15) == 0)) {
+#pragma unroll
+        for (int e = 0; e < CE; e += 2)
+            *reinterpret_cast<ulonglong2*>(a.out + j0 + e) = make_ulonglong2(outv[e], outv[e + 1]);
+    } else {
+#pragma unroll
+        for (int e = 0; e < CE; ++e)
+            if (j0 + e < a.out_len) a.out[j0 + e] = outv[e];
     }
 }
 
@@ -809,13 +911,15 @@ static PassKernel kernel_ptr() {
 }
 
 // Table of every kernel instance: [mode-variant][logl]
-enum { V_FWD, V_FWD_E, V_LAST, V_LAST_E, V_FUSED, V_FUSED_E, V_SQR, V_SQR_E, V_INV, NV };
+enum { V_FWD, V_FWD_E, V_LAST, V_LAST_E, V_FUSED, V_FUSED_E, V_SQR, V_SQR_E, V_INV, V_FUSED2, NV };
 
 template <int LOGL>
 static void fill_row(PassKernel (&t)[NV][MAX_PASS_BITS + 1]) {
     t[V_FWD][LOGL] = LOGL >= 5 ? kernel_ptr<M_FWD, (LOGL >= 5 ? LOGL : 5), false, false>() : nullptr;
     t[V_FWD_E][LOGL] = LOGL >= 5 ? kernel_ptr<M_FWD, (LOGL >= 5 ? LOGL : 5), true, false>() : nullptr;
     t[V_INV][LOGL] = LOGL >= 5 ? kernel_ptr<M_INV, (LOGL >= 5 ? LOGL : 5), false, false>() : nullptr;
+    t[V_FUSED2][LOGL] = (LOGL >= 5 && LOGL <= 8) ? kernel_ptr<M_FUSED2, (LOGL >= 5 && LOGL <= 8 ? LOGL : 5), false, false>()
+                                                   : nullptr;
     t[V_LAST][LOGL] = kernel_ptr<M_FWD_LAST, LOGL, false, false>();
     t[V_LAST_E][LOGL] = kernel_ptr<M_FWD_LAST, LOGL, true, false>();
     t[V_FUSED][LOGL] = kernel_ptr<M_FUSED, LOGL, false, false>();
@@ -845,8 +949,11 @@ static const KernelTable& ktab() {
     return t;
 }
 
-// tile + the 16 x 16 four-step twiddle factors of strided passes
-static size_t pass_smem(int logl) { return ((size_t)TC * ((size_t)1 << logl) + TC * 16) * sizeof(u64); }
+// tile + the 16 x 16 four-step twiddle factors of strided passes; two tiles for V_FUSED2
+static size_t pass_smem(int logl, int variant = -1) {
+    const size_t tile = (size_t)TC * ((size_t)1 << logl);
+    return (variant == V_FUSED2 ? 2 * tile : tile + TC * 16) * sizeof(u64);
+}
 
 cudaError_t ensure_tables() {
     int dev = 0;
@@ -867,7 +974,7 @@ cudaError_t ensure_tables() {
         for (int l = 0; l <= MAX_PASS_BITS; ++l)
             if (K.k[v][l]) {
                 e = cudaFuncSetAttribute((const void*)K.k[v][l], cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)pass_smem(l));
+                                         (int)pass_smem(l, v));
                 if (e != cudaSuccess) return e;
                 e = cudaFuncSetAttribute((const void*)K.k[v][l], cudaFuncAttributePreferredSharedMemoryCarveout,
                                          (int)cudaSharedmemCarveoutMaxShared);
@@ -1006,6 +1113,7 @@ static cudaError_t timed_launch(int kind, double bytes, double modmuls, cudaStre
 
 static int variant_kind(int v) {
     switch (v) {
+        case V_FUSED2: return K_FUSED;
         case V_FWD: case V_FWD_E: return K_FWD;
         case V_LAST: case V_LAST_E: return K_FWD_LAST;
         case V_INV: return K_INV;
@@ -1025,14 +1133,17 @@ static cudaError_t launch_pass(int variant, int logl, const PassArgs& a, u64 til
         bytes = (double)a.len * 8.0 + vec;
         mm += 3.0 * (double)a.len;
     }
-    if (variant == V_FUSED || variant == V_FUSED_E) {
+    if (variant == V_FUSED2) {
+        bytes += vec;                 // reads both operands, writes the product
+        mm = 3.0 * bfly + 3.0 * N;
+    } else if (variant == V_FUSED || variant == V_FUSED_E) {
         bytes += vec;                 // reads the other operand's spectrum too
         mm = 2.0 * bfly + 3.0 * N + (entry ? 3.0 * (double)a.len : 0.0);
     } else if (variant == V_SQR || variant == V_SQR_E) {
         mm = 2.0 * bfly + 3.0 * N + (entry ? 3.0 * (double)a.len : 0.0);
     }
     return timed_launch(variant_kind(variant), bytes, mm, s,
-                        [&] { k<<<(unsigned)(tiles * 3), NT, pass_smem(logl), s>>>(a); });
+                        [&] { k<<<(unsigned)(tiles * 3), NT, pass_smem(logl, variant), s>>>(a); });
 }
 
 int job_launches(u64 la, u64 lb, int sqr) {
@@ -1041,6 +1152,7 @@ int job_launches(u64 la, u64 lb, int sqr) {
     const Plan pl = make_plan(w.n);
     const int P = pl.passes;
     // forward strided passes (A, and B unless squaring) + A's last pass + fused + inverse + crt
+    if (!sqr && P >= 2 && pl.bits[P - 1] <= 8) return 2 * (P - 1) + 1 + (P - 1) + 1;   // merged last pass
     return sqr ? (P - 1) + 1 + (P - 1) + 1 : 2 * (P - 1) + 1 + 1 + (P - 1) + 1;
 }
 
@@ -1088,7 +1200,18 @@ cudaError_t enqueue_job(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s,
         return cudaSuccess;
     };
 
-    if (!sqr) {
+    const bool merged = !sqr && P >= 2 && lastl <= 8;
+    if (merged) {
+        if ((e = fwd_strided(j.a, j.la, A)) != cudaSuccess) return e;
+        if ((e = fwd_strided(j.b, j.lb, B)) != cudaSuccess) return e;
+        pa.tw = nullptr;
+        pa.src = nullptr;
+        pa.data = B;
+        pa.other = A;
+        pa.logB = logB[P - 1];
+        pa.ncols = TC;
+        if ((e = launch_pass(V_FUSED2, lastl, pa, tiles_last, s)) != cudaSuccess) return e;
+    } else if (!sqr) {
         if ((e = fwd_strided(j.a, j.la, A)) != cudaSuccess) return e;
         pa.tw = nullptr;
         pa.src = j.a;
