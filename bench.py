@@ -52,6 +52,9 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the reference CPU timing")
     ap.add_argument("--len", type=int, default=None, help="override operand length (profiling runs)")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched-stream comparison")
+    ap.add_argument("--batch-only", action="store_true", help="only the batched-stream comparison")
+    ap.add_argument("--batch-count", type=int, default=4096)
     return ap.parse_args()
 
 
@@ -214,6 +217,67 @@ def run_reference(args, ws, rank):
     print(json.dumps(line), flush=True)
 
 
+# ----------------------------------------------------------------------------- batched stream
+def batch_compare(fmn, torch, dev, count, repeats=3):
+    """The mixed-size stream (each side log-uniform in [1000, 100000] limbs, 20% squares,
+    seeded): plain per-call device products in a loop vs one batched call vs a CUDA-graph
+    replay of the batch.  Operands resident in HBM; every output compared bit for bit."""
+    from fast_mul_ntt_b200 import synth
+    mix = synth.batch_mix(count, seed=0)
+    jobs_pc, jobs_b, limbs = [], [], 0
+    for op, l1, l2, seed in mix:
+        a, b = synth.operands("uniform", l1, l2, seed)
+        da = torch.from_numpy(a.view(np.int64)).to(dev)
+        db = da if op == "sqr" else torch.from_numpy(b.view(np.int64)).to(dev)
+        jobs_pc.append((op, da, db, torch.empty(l1 + l2, dtype=torch.int64, device=dev)))
+        jobs_b.append((da, db, torch.empty(l1 + l2, dtype=torch.int64, device=dev)))
+        limbs += l1 + l2
+    stream = torch.cuda.Stream(device=dev)
+
+    def per_call():
+        for op, da, db, out in jobs_pc:
+            if op == "sqr":
+                fmn.sqr_device(da, out, stream=stream)
+            else:
+                fmn.mul_device(da, db, out, stream=stream)
+
+    def timed(fn, reps):
+        fn()
+        stream.synchronize()
+        ts = []
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            e1.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        return sorted(ts)[len(ts) // 2]
+
+    t_pc = timed(per_call, repeats)
+    t_b = timed(lambda: fmn.mul_batch_device(jobs_b, stream=stream), repeats)
+    fmn.sync(stream)
+    exact_b = all(torch.equal(x[3], y[2]) for x, y in zip(jobs_pc, jobs_b))
+    for _, _, o in jobs_b:
+        o.zero_()
+    g = fmn.BatchGraph(jobs_b)
+    t_g = timed(lambda: g.launch(stream), repeats)
+    g.sync(stream)
+    exact_g = all(torch.equal(x[3], y[2]) for x, y in zip(jobs_pc, jobs_b))
+    g.close()
+    ns = sorted({fmn.ntt_len(l1, l2) for _, l1, l2, _ in mix})
+    res = {"workload": f"{count} products, each side log-uniform in [1000, 100000] limbs, 20% squares "
+                       f"(seed 0), transform lengths {ns[0]}..{ns[-1]}",
+           "limbs_total": limbs,
+           "per_call": {"products_per_s": count / (t_pc * 1e-3), "ms": t_pc},
+           "batched": {"products_per_s": count / (t_b * 1e-3), "ms": t_b, "bit_exact_vs_per_call": exact_b},
+           "graph": {"products_per_s": count / (t_g * 1e-3), "ms": t_g, "bit_exact_vs_per_call": exact_g},
+           "speedup_batched_vs_per_call": t_pc / t_b, "speedup_graph_vs_per_call": t_pc / t_g}
+    del jobs_pc, jobs_b
+    torch.cuda.empty_cache()
+    return res
+
+
 # ----------------------------------------------------------------------------- ours
 def run_ours(args, ws, rank, local):
     import torch
@@ -231,6 +295,9 @@ def run_ours(args, ws, rank, local):
         torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     fmn.init(local)
+    if args.batch_only:
+        print(json.dumps(batch_compare(fmn, torch, dev, args.batch_count)), flush=True)
+        return
     l1 = args.len or LEN1
     l2 = args.len or LEN2
     a, b = synth.operands(KIND, l1, l2, SEED)
@@ -368,6 +435,10 @@ def run_ours(args, ws, rank, local):
     if dist:
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
+    if rank == 0 and not args.no_batch and l1 == LEN1:
+        del da, db, dout
+        torch.cuda.empty_cache()
+        result["batch"] = batch_compare(fmn, torch, dev, args.batch_count)
     if rank == 0 and ws == 1 and not args.no_cpu_baseline and l1 == LEN1:
         cb, cout = cpu_baseline(a, b)
         cb["bit_exact_vs_gpu"] = bool(np.array_equal(cout, got))

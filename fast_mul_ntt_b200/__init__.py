@@ -27,7 +27,14 @@ _ERRNAMES = {1: "FMN_ERR_ARG", 2: "FMN_ERR_CUDA", 3: "FMN_ERR_NOMEM", 4: "FMN_ER
 EXPORTS = ["abs_mul64", "abs_sqr64", "fmn_init", "fmn_shutdown", "fmn_last_error", "fmn_mul", "fmn_sqr",
            "fmn_mul_device", "fmn_sqr_device", "fmn_sync", "fmn_workspace_size", "fmn_mul_device_ws",
            "fmn_ws_status", "fmn_ntt_len", "fmn_kernel_kind_name", "fmn_profile_enable", "fmn_profile_take",
-           "fmn_launches_per_product", "fmn_bench_modmul", "fmn_mul_device_noalloc"]
+           "fmn_launches_per_product", "fmn_bench_modmul", "fmn_mul_device_noalloc", "fmn_mul_batch_device",
+           "fmn_batch_graph_create", "fmn_batch_graph_launch", "fmn_batch_graph_sync", "fmn_batch_graph_destroy"]
+
+
+class FmnJob(ctypes.Structure):
+    """fmn_job of include/fast_mul.h (device pointers)."""
+    _fields_ = [("in1", ctypes.c_void_p), ("len1", ctypes.c_uint64), ("in2", ctypes.c_void_p),
+                ("len2", ctypes.c_uint64), ("out", ctypes.c_void_p)]
 KERNEL_KINDS = 5
 
 _u64 = ctypes.c_uint64
@@ -94,6 +101,17 @@ def load_library(path=None):
     lib.fmn_bench_modmul.restype = ctypes.c_int
     lib.fmn_mul_device_noalloc.argtypes = [_vp, _u64, _vp, _u64, _vp, _vp]
     lib.fmn_mul_device_noalloc.restype = ctypes.c_int
+    _jp = ctypes.POINTER(FmnJob)
+    lib.fmn_mul_batch_device.argtypes = [_jp, ctypes.c_int, _vp]
+    lib.fmn_mul_batch_device.restype = ctypes.c_int
+    lib.fmn_batch_graph_create.argtypes = [_jp, ctypes.c_int, ctypes.POINTER(_vp)]
+    lib.fmn_batch_graph_create.restype = ctypes.c_int
+    lib.fmn_batch_graph_launch.argtypes = [_vp, _vp]
+    lib.fmn_batch_graph_launch.restype = ctypes.c_int
+    lib.fmn_batch_graph_sync.argtypes = [_vp, _vp]
+    lib.fmn_batch_graph_sync.restype = ctypes.c_int
+    lib.fmn_batch_graph_destroy.argtypes = [_vp]
+    lib.fmn_batch_graph_destroy.restype = None
     if path is None:
         _lib = lib
     return lib
@@ -226,3 +244,51 @@ def bench_modmul():
     a, b = ctypes.c_double(), ctypes.c_double()
     _check(load_library().fmn_bench_modmul(ctypes.byref(a), ctypes.byref(b)))
     return a.value, b.value
+
+
+def _job_array(jobs):
+    """[(a, b, out), ...] of CUDA tensors -> ctypes array of FmnJob (a is b: square)."""
+    arr = (FmnJob * len(jobs))()
+    for i, (a, b, out) in enumerate(jobs):
+        arr[i].in1, arr[i].len1 = a.data_ptr(), a.numel()
+        arr[i].in2, arr[i].len2 = b.data_ptr(), b.numel()
+        arr[i].out = out.data_ptr()
+    return arr
+
+
+def mul_batch_device(jobs, stream=None):
+    """All products of ``jobs`` ([(a, b, out)], CUDA limb tensors; ``a is b`` squares) in
+    batched launches, asynchronously on ``stream``."""
+    lib = load_library()
+    arr = _job_array(jobs)
+    _check(lib.fmn_mul_batch_device(arr, len(jobs), _stream_ptr(stream)))
+
+
+class BatchGraph:
+    """A batch captured once in a CUDA graph; ``launch()`` recomputes every product from the
+    current contents of the same input tensors into the same outputs."""
+
+    def __init__(self, jobs):
+        lib = load_library()
+        self._jobs = jobs            # keep the tensors alive
+        arr = _job_array(jobs)
+        h = ctypes.c_void_p()
+        _check(lib.fmn_batch_graph_create(arr, len(jobs), ctypes.byref(h)))
+        self.handle = h
+
+    def launch(self, stream=None):
+        _check(load_library().fmn_batch_graph_launch(self.handle, _stream_ptr(stream)))
+
+    def sync(self, stream=None):
+        _check(load_library().fmn_batch_graph_sync(self.handle, _stream_ptr(stream)))
+
+    def close(self):
+        if self.handle:
+            load_library().fmn_batch_graph_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -52,6 +52,14 @@ struct DevCtx {
     };
     std::vector<Tw> tw;
     u64 tick = 0;
+    // batches: worker streams, fork/join events, pinned descriptor staging
+    static constexpr int NSTREAM = 4;
+    cudaStream_t wstream[NSTREAM] = {nullptr};
+    cudaEvent_t wevent[NSTREAM + 1] = {nullptr};
+    void* stage = nullptr;
+    size_t stage_cap = 0;
+    cudaEvent_t stage_free = nullptr;   // the last batch's descriptor copy has completed
+    bool stage_pending = false;
 };
 
 std::mutex g_ctx_mu;
@@ -80,6 +88,15 @@ int get_ctx(DevCtx** out) {
             (e = cudaMallocHost((void**)&c->h_err, sizeof(unsigned))) != cudaSuccess) {
             delete c;
             return set_err(FMN_ERR_CUDA, "creating device context", e);
+        }
+        for (int k = 0; k < DevCtx::NSTREAM && e == cudaSuccess; ++k)
+            e = cudaStreamCreateWithFlags(&c->wstream[k], cudaStreamNonBlocking);
+        for (int k = 0; k <= DevCtx::NSTREAM && e == cudaSuccess; ++k)
+            e = cudaEventCreateWithFlags(&c->wevent[k], cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->stage_free, cudaEventDisableTiming);
+        if (e != cudaSuccess) {
+            delete c;
+            return set_err(FMN_ERR_CUDA, "creating device context streams", e);
         }
         g_ctx[dev] = c;
     }
@@ -180,6 +197,11 @@ const fmn::TwiddleSet* get_twiddles(DevCtx* c, int log_n, cudaStream_t s) {
     }
     c->tw.push_back(t);
     return &c->tw.back().set;
+}
+
+const fmn::TwiddleSet* ctx_twiddles(void* ctx, int log_n) {
+    DevCtx* c = (DevCtx*)ctx;
+    return get_twiddles(c, log_n, c->stream);
 }
 
 int ilog2_ceil(u64 x) {
@@ -286,6 +308,45 @@ int api_set_error(int code, const char* what, cudaError_t e) { return set_err(co
 
 namespace {
 
+int to_jobs(const fmn_job* jobs, int count, std::vector<fmn::Job>& v) {
+    if (count < 0 || (count > 0 && !jobs)) return set_err(FMN_ERR_ARG, "bad job array");
+    v.resize(count);
+    for (int i = 0; i < count; ++i) {
+        const fmn_job& j = jobs[i];
+        if (j.len1 + j.len2 > 0 && (!j.out || (j.len1 && !j.in1) || (j.len2 && !j.in2)))
+            return set_err(FMN_ERR_ARG, "null pointer in a batch job");
+        if (j.len1 && j.len2) {
+            int rc = check_sizes(j.len1, j.len2);
+            if (rc) return rc;
+        }
+        v[i].a = j.in1;
+        v[i].la = j.len1;
+        v[i].b = j.in2;
+        v[i].lb = j.len2;
+        v[i].out = j.out;
+        v[i].sqr = (j.in1 == j.in2 && j.len1 == j.len2) ? 1 : 0;
+    }
+    return FMN_OK;
+}
+
+int ensure_stage(DevCtx* c, size_t bytes) {
+    cudaError_t e;
+    if (c->stage_pending) {                 // the previous batch's copy must have read it
+        if ((e = cudaEventSynchronize(c->stage_free)) != cudaSuccess) return set_err(FMN_ERR_CUDA, "staging", e);
+        c->stage_pending = false;
+    }
+    if (c->stage_cap >= bytes) return FMN_OK;
+    if (c->stage) cudaFreeHost(c->stage);
+    c->stage = nullptr;
+    c->stage_cap = 0;
+    if ((e = cudaMallocHost(&c->stage, bytes)) != cudaSuccess) {
+        cudaGetLastError();
+        return set_err(FMN_ERR_NOMEM, "pinned staging for batch descriptors", e);
+    }
+    c->stage_cap = bytes;
+    return FMN_OK;
+}
+
 void die(const char* fn) {
     fprintf(stderr, "%s failed: %s\n", fn, g_last_error.c_str());
     abort();
@@ -326,6 +387,12 @@ void fmn_shutdown(void) {
         if (c->io) cudaFree(c->io);
         if (c->h_err) cudaFreeHost(c->h_err);
         for (auto& t : c->tw) cudaFree(t.buf);
+        if (c->stage) cudaFreeHost(c->stage);
+        for (int k = 0; k < DevCtx::NSTREAM; ++k)
+            if (c->wstream[k]) cudaStreamDestroy(c->wstream[k]);
+        for (int k = 0; k <= DevCtx::NSTREAM; ++k)
+            if (c->wevent[k]) cudaEventDestroy(c->wevent[k]);
+        if (c->stage_free) cudaEventDestroy(c->stage_free);
         if (c->done) cudaEventDestroy(c->done);
         if (c->stream) cudaStreamDestroy(c->stream);
         delete c;
@@ -404,6 +471,152 @@ int fmn_ws_status(const void* d_ws, u64 len1, u64 len2, int sqr, void* stream) {
         return set_err(FMN_ERR_DEVICE, "carry scan: bounded wait expired");
     }
     return FMN_OK;
+}
+
+int fmn_mul_batch_device(const fmn_job* jobs, int count, void* stream) {
+    std::vector<fmn::Job> v;
+    int rc = to_jobs(jobs, count, v);
+    if (rc || count == 0) return rc;
+    DevCtx* c;
+    if ((rc = get_ctx(&c))) return rc;
+    std::lock_guard<std::mutex> lk(c->mu);
+    cudaStream_t s = (cudaStream_t)stream;
+    const size_t wsb = fmn::batch_workspace_bytes(v.data(), count);
+    if ((rc = ensure_ws(c, wsb))) return rc;
+    if ((rc = ensure_stage(c, fmn::batch_stage_bytes(v.data(), count)))) return rc;
+    cudaError_t e;
+    if (c->done_valid && (e = cudaStreamWaitEvent(s, c->done, 0)) != cudaSuccess)
+        return set_err(FMN_ERR_CUDA, "cudaStreamWaitEvent", e);
+    // twiddle tables are built on the context stream: order s after it
+    for (const auto& j : v)
+        if (j.la && j.lb) ctx_twiddles(c, ilog2_ceil(j.la + j.lb - 1));
+    if ((e = cudaEventRecord(c->wevent[0], c->stream)) != cudaSuccess ||
+        (e = cudaStreamWaitEvent(s, c->wevent[0], 0)) != cudaSuccess)
+        return set_err(FMN_ERR_CUDA, "ordering after twiddle tables", e);
+    e = fmn::enqueue_batch(v.data(), count, c->ws, c->ws_cap, c->stage, c->stage_cap, s, c->wstream, c->wevent,
+                           DevCtx::NSTREAM, ctx_twiddles, c);
+    if (e != cudaSuccess) return set_err(FMN_ERR_CUDA, "batch launch", e);
+    if ((e = cudaEventRecord(c->stage_free, s)) != cudaSuccess) return set_err(FMN_ERR_CUDA, "cudaEventRecord", e);
+    c->stage_pending = true;
+    if ((e = cudaEventRecord(c->done, s)) != cudaSuccess) return set_err(FMN_ERR_CUDA, "cudaEventRecord", e);
+    c->done_valid = true;
+    return FMN_OK;
+}
+
+struct fmn_batch_graph {
+    int dev;
+    void* ws;
+    size_t ws_bytes;
+    void* stage;
+    size_t stage_bytes;
+    cudaStream_t cap;                      // capture origin
+    cudaStream_t wstream[4];
+    cudaEvent_t wevent[5];
+    std::vector<void*> tw_bufs;
+    std::vector<fmn::TwiddleSet> tw_sets;
+    cudaGraph_t graph;
+    cudaGraphExec_t exec;
+    unsigned* h_err;
+};
+
+static const fmn::TwiddleSet* graph_twiddles(void* ctx, int log_n) {
+    fmn_batch_graph* g = (fmn_batch_graph*)ctx;
+    for (auto& t : g->tw_sets)
+        if (t.log_n == log_n) return &t;
+    return nullptr;
+}
+
+void fmn_batch_graph_destroy(fmn_batch_graph* g) {
+    if (!g) return;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(g->dev);
+    cudaDeviceSynchronize();
+    if (g->exec) cudaGraphExecDestroy(g->exec);
+    if (g->graph) cudaGraphDestroy(g->graph);
+    for (void* b : g->tw_bufs) cudaFree(b);
+    if (g->ws) cudaFree(g->ws);
+    if (g->stage) cudaFreeHost(g->stage);
+    if (g->h_err) cudaFreeHost(g->h_err);
+    for (int k = 0; k < 4; ++k)
+        if (g->wstream[k]) cudaStreamDestroy(g->wstream[k]);
+    for (int k = 0; k < 5; ++k)
+        if (g->wevent[k]) cudaEventDestroy(g->wevent[k]);
+    if (g->cap) cudaStreamDestroy(g->cap);
+    delete g;
+    cudaSetDevice(prev);
+}
+
+int fmn_batch_graph_create(const fmn_job* jobs, int count, fmn_batch_graph** out) {
+    if (!out) return set_err(FMN_ERR_ARG, "null pointer");
+    *out = nullptr;
+    std::vector<fmn::Job> v;
+    int rc = to_jobs(jobs, count, v);
+    if (rc) return rc;
+    DevCtx* c;
+    if ((rc = get_ctx(&c))) return rc;
+    cudaError_t e = fmn::prepare_batch();
+    if (e != cudaSuccess) return set_err(FMN_ERR_CUDA, "preparing batch kernels", e);
+    fmn_batch_graph* g = new fmn_batch_graph();   // value-initialised: null handles, empty vectors
+    g->dev = c->dev;
+    auto fail = [&](int code, const char* what, cudaError_t err) {
+        cudaGetLastError();
+        fmn_batch_graph_destroy(g);
+        return set_err(code, what, err);
+    };
+    g->ws_bytes = fmn::batch_workspace_bytes(v.data(), count);
+    g->stage_bytes = fmn::batch_stage_bytes(v.data(), count);
+    if ((e = cudaMalloc(&g->ws, g->ws_bytes)) != cudaSuccess) return fail(FMN_ERR_NOMEM, "graph workspace", e);
+    if ((e = cudaMemset(g->ws, 0, 256)) != cudaSuccess) return fail(FMN_ERR_CUDA, "graph workspace", e);
+    if ((e = cudaMallocHost(&g->stage, g->stage_bytes)) != cudaSuccess) return fail(FMN_ERR_NOMEM, "graph staging", e);
+    if ((e = cudaMallocHost((void**)&g->h_err, sizeof(unsigned))) != cudaSuccess) return fail(FMN_ERR_NOMEM, "graph status", e);
+    if ((e = cudaStreamCreateWithFlags(&g->cap, cudaStreamNonBlocking)) != cudaSuccess) return fail(FMN_ERR_CUDA, "stream", e);
+    for (int k = 0; k < 4; ++k)
+        if ((e = cudaStreamCreateWithFlags(&g->wstream[k], cudaStreamNonBlocking)) != cudaSuccess)
+            return fail(FMN_ERR_CUDA, "stream", e);
+    for (int k = 0; k < 5; ++k)
+        if ((e = cudaEventCreateWithFlags(&g->wevent[k], cudaEventDisableTiming)) != cudaSuccess)
+            return fail(FMN_ERR_CUDA, "event", e);
+    // the graph's own twiddle tables, one set per transform length in the batch
+    for (const auto& j : v) {
+        if (!j.la || !j.lb) continue;
+        const int n = ilog2_ceil(j.la + j.lb - 1);
+        const size_t bytes = fmn::twiddle_table_bytes(n);
+        bool have = false;
+        for (auto& t : g->tw_sets) have |= (t.log_n == n);
+        if (have || !bytes) continue;
+        void* buf = nullptr;
+        if ((e = cudaMalloc(&buf, bytes)) != cudaSuccess) return fail(FMN_ERR_NOMEM, "graph twiddle tables", e);
+        g->tw_bufs.push_back(buf);
+        fmn::TwiddleSet ts;
+        if ((e = fmn::build_twiddle_tables(n, (u64*)buf, &ts, g->cap)) != cudaSuccess)
+            return fail(FMN_ERR_CUDA, "graph twiddle tables", e);
+        g->tw_sets.push_back(ts);
+    }
+    if ((e = cudaStreamSynchronize(g->cap)) != cudaSuccess) return fail(FMN_ERR_CUDA, "graph twiddle tables", e);
+    if ((e = cudaStreamBeginCapture(g->cap, cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
+        return fail(FMN_ERR_CUDA, "cudaStreamBeginCapture", e);
+    e = fmn::enqueue_batch(v.data(), count, g->ws, g->ws_bytes, g->stage, g->stage_bytes, g->cap, g->wstream,
+                           g->wevent, 4, graph_twiddles, g);
+    cudaError_t e2 = cudaStreamEndCapture(g->cap, &g->graph);
+    if (e != cudaSuccess) return fail(FMN_ERR_CUDA, "capturing the batch", e);
+    if (e2 != cudaSuccess) return fail(FMN_ERR_CUDA, "cudaStreamEndCapture", e2);
+    if ((e = cudaGraphInstantiate(&g->exec, g->graph, 0)) != cudaSuccess)
+        return fail(FMN_ERR_CUDA, "cudaGraphInstantiate", e);
+    *out = g;
+    return FMN_OK;
+}
+
+int fmn_batch_graph_launch(fmn_batch_graph* g, void* stream) {
+    if (!g) return set_err(FMN_ERR_ARG, "null graph");
+    cudaError_t e = cudaGraphLaunch(g->exec, (cudaStream_t)stream);
+    if (e != cudaSuccess) return set_err(FMN_ERR_CUDA, "cudaGraphLaunch", e);
+    return FMN_OK;
+}
+
+int fmn_batch_graph_sync(fmn_batch_graph* g, void* stream) {
+    if (!g) return set_err(FMN_ERR_ARG, "null graph");
+    return take_device_error(g->ws, g->h_err, (cudaStream_t)stream);
 }
 
 const char* fmn_kernel_kind_name(int kind) { return fmn::kernel_kind_name(kind); }

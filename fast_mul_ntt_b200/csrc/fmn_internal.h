@@ -44,6 +44,8 @@ struct TwiddleSet {
     const u64* fwd[MAX_PASSES];
     const u64* inv[MAX_PASSES];
 };
+typedef const TwiddleSet* (*TwiddleLookup)(void* ctx, int log_n);
+
 // Device bytes the tables of a length-2^log_n transform need (0 when it has one pass).
 size_t twiddle_table_bytes(int log_n);
 // Fill `buf` (twiddle_table_bytes(log_n) bytes) on `stream` and describe it in `out`.
@@ -56,6 +58,22 @@ cudaError_t build_twiddle_tables(int log_n, u64* buf, TwiddleSet* out, cudaStrea
 // it the kernels generate them.
 cudaError_t enqueue_job(const Job& job, void* ws, size_t ws_bytes, cudaStream_t stream,
                         const TwiddleSet* tw = nullptr);
+
+// ---- batches of products
+// Workspace bytes for a batch (device) and host staging bytes for its launch descriptors.
+size_t batch_workspace_bytes(const Job* jobs, int count);
+size_t batch_stage_bytes(const Job* jobs, int count);
+// Enqueue a batch on `s`.  Products are grouped by transform length and kind; every group
+// runs its stages as batched launches on one of `streams` (forked from and joined into s
+// with `events`, which needs nstreams + 1 events).  `h_stage` is pinned host memory of
+// batch_stage_bytes bytes that must stay untouched until the stream has consumed it.
+// `tw_lookup` (optional) returns cached twiddle tables per transform length.
+cudaError_t enqueue_batch(const Job* jobs, int count, void* ws, size_t ws_bytes, void* h_stage,
+                          size_t stage_bytes, cudaStream_t s, const cudaStream_t* streams,
+                          const cudaEvent_t* events, int nstreams, TwiddleLookup tw_lookup, void* tw_ctx);
+
+// Make sure every batched kernel is configured (call before capturing a batch in a graph).
+cudaError_t prepare_batch();
 
 // ---- optional per-kernel timing (used by bench.py; off by default)
 // Kernel kinds of the pipeline.

@@ -660,7 +660,7 @@ __device__ __forceinline__ void add_to(u64& lo, u32& h, u64 x) {
     h += lo < x;
 }
 
-__global__ void __launch_bounds__(CNT) k_crt_carry(CrtArgs a) {
+__device__ __forceinline__ void crt_carry_body(const CrtArgs& a, u32 ncta) {
     __shared__ u32 s_tile;
     __shared__ u64 s_hw[CNT / 32][3];
     __shared__ u32 s_warp[CNT / 32];
@@ -670,6 +670,7 @@ __global__ void __launch_bounds__(CNT) k_crt_carry(CrtArgs a) {
     if (tid == 0) s_tile = atomicAdd(a.ticket, 1u);
     __syncthreads();
     const u64 tile = s_tile;
+    if (tile >= ncta) return;                   // batch launches cover the largest product
     const u64 j0 = tile * CTILE + (u64)tid * CE;
 
     // coefficients j0 .. j0+15, folded into limb sums s_j = c_j[0] + c_{j-1}[1] + c_{j-2}[2]
@@ -834,6 +835,8 @@ __global__ void __launch_bounds__(CNT) k_crt_carry(CrtArgs a) {
             if (j0 + e < a.out_len) a.out[j0 + e] = outv[e];
     }
 }
+
+__global__ void __launch_bounds__(CNT) k_crt_carry(CrtArgs a) { crt_carry_body(a, 0xffffffffu); }
 
 // ------------------------------------------------------------------ host: tables
 static u64 h_mulmod(u64 a, u64 b, u64 m) { return (u64)(((unsigned __int128)a * b) % m); }
@@ -1156,23 +1159,46 @@ int job_launches(u64 la, u64 lb, int sqr) {
     return sqr ? (P - 1) + 1 + (P - 1) + 1 : 2 * (P - 1) + 1 + 1 + (P - 1) + 1;
 }
 
-cudaError_t enqueue_job(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s, const TwiddleSet* tws) {
+// Every launch one product needs, in order, with its arguments (no launch happens here).
+struct LaunchRec {
+    int variant, logl;
+    PassArgs pa;
+    u64 tiles;
+};
+struct JobLaunches {
+    int count;
+    LaunchRec rec[3 * MAX_PASSES + 2];
+    CrtArgs crt;
+    u64 ncta;
+};
+
+// Scratch pointers of one product: residue arrays and carry-scan state.
+struct JobScratch {
+    u64* A;
+    u64* B;
+    u32* ticket;
+    u32* state;
+    u32* err;
+};
+
+static void plan_job(const Job& j, const JobScratch& sc, const TwiddleSet* tws, JobLaunches* out) {
     const u64 out_len = j.la + j.lb;
-    if (out_len == 0) return cudaSuccess;
-    if (j.la == 0 || j.lb == 0) return cudaMemsetAsync(j.out, 0, out_len * sizeof(u64), s);
     const int sqr = j.sqr ? 1 : 0;
     const WsLayout w = ws_layout(j.la, j.lb, sqr);
-    if (ws_bytes < w.total || w.n > MAX_LOG_N) return cudaErrorInvalidValue;
-    cudaError_t e = ensure_tables();
-    if (e != cudaSuccess) return e;
-    char* base = (char*)ws;
-    u64* A = (u64*)(base + w.a);
-    u64* B = sqr ? A : (u64*)(base + w.b);
+    u64* A = sc.A;
+    u64* B = sqr ? A : sc.B;
     const Plan pl = make_plan(w.n);
     const int P = pl.passes;
     const u64 N = w.N;
-
     if (tws && tws->log_n != w.n) tws = nullptr;
+    out->count = 0;
+    auto add = [&](int variant, int logl, const PassArgs& pa, u64 tiles) {
+        LaunchRec& r = out->rec[out->count++];
+        r.variant = variant;
+        r.logl = logl;
+        r.pa = pa;
+        r.tiles = tiles;
+    };
     PassArgs pa;
     memset(&pa, 0, sizeof(pa));
     pa.N = N;
@@ -1184,44 +1210,40 @@ cudaError_t enqueue_job(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s,
     const u64 nblk_last = N >> lastl;
     const u64 tiles_last = (nblk_last + TC - 1) / TC;
     const int ncols_last = nblk_last < (u64)TC ? (int)nblk_last : TC;
-
-    // forward strided passes of one operand
-    auto fwd_strided = [&](const u64* src, u64 len, u64* data) -> cudaError_t {
+    auto fwd_strided = [&](const u64* src, u64 len, u64* data) {
         for (int p = 0; p + 1 < P; ++p) {
             pa.src = src;
             pa.len = len;
             pa.data = data;
             pa.logB = logB[p];
             pa.tw = tws ? tws->fwd[p] : nullptr;
-            const cudaError_t r =
-                launch_pass(p == 0 ? V_FWD_E : V_FWD, pl.bits[p], pa, N >> (pl.bits[p] + 4), s);
-            if (r != cudaSuccess) return r;
+            add(p == 0 ? V_FWD_E : V_FWD, pl.bits[p], pa, N >> (pl.bits[p] + 4));
         }
-        return cudaSuccess;
     };
-
     const bool merged = !sqr && P >= 2 && lastl <= 8;
     if (merged) {
-        if ((e = fwd_strided(j.a, j.la, A)) != cudaSuccess) return e;
-        if ((e = fwd_strided(j.b, j.lb, B)) != cudaSuccess) return e;
+        fwd_strided(j.a, j.la, A);
+        fwd_strided(j.b, j.lb, B);
         pa.tw = nullptr;
         pa.src = nullptr;
+        pa.len = 0;
         pa.data = B;
         pa.other = A;
         pa.logB = logB[P - 1];
         pa.ncols = TC;
-        if ((e = launch_pass(V_FUSED2, lastl, pa, tiles_last, s)) != cudaSuccess) return e;
+        add(V_FUSED2, lastl, pa, tiles_last);
     } else if (!sqr) {
-        if ((e = fwd_strided(j.a, j.la, A)) != cudaSuccess) return e;
+        fwd_strided(j.a, j.la, A);
         pa.tw = nullptr;
         pa.src = j.a;
         pa.len = j.la;
         pa.data = A;
+        pa.other = nullptr;
         pa.logB = logB[P - 1];
         pa.ncols = ncols_last;
-        if ((e = launch_pass(P == 1 ? V_LAST_E : V_LAST, lastl, pa, tiles_last, s)) != cudaSuccess) return e;
+        add(P == 1 ? V_LAST_E : V_LAST, lastl, pa, tiles_last);
         pa.ncols = TC;
-        if ((e = fwd_strided(j.b, j.lb, B)) != cudaSuccess) return e;
+        fwd_strided(j.b, j.lb, B);
         pa.tw = nullptr;
         pa.src = j.b;
         pa.len = j.lb;
@@ -1229,9 +1251,9 @@ cudaError_t enqueue_job(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s,
         pa.other = A;
         pa.logB = logB[P - 1];
         pa.ncols = ncols_last;
-        if ((e = launch_pass(P == 1 ? V_FUSED_E : V_FUSED, lastl, pa, tiles_last, s)) != cudaSuccess) return e;
+        add(P == 1 ? V_FUSED_E : V_FUSED, lastl, pa, tiles_last);
     } else {
-        if ((e = fwd_strided(j.a, j.la, A)) != cudaSuccess) return e;
+        fwd_strided(j.a, j.la, A);
         pa.tw = nullptr;
         pa.src = j.a;
         pa.len = j.la;
@@ -1239,20 +1261,20 @@ cudaError_t enqueue_job(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s,
         pa.other = A;
         pa.logB = logB[P - 1];
         pa.ncols = ncols_last;
-        if ((e = launch_pass(P == 1 ? V_SQR_E : V_SQR, lastl, pa, tiles_last, s)) != cudaSuccess) return e;
+        add(P == 1 ? V_SQR_E : V_SQR, lastl, pa, tiles_last);
     }
     pa.ncols = TC;
     pa.src = nullptr;
+    pa.len = 0;
     pa.other = nullptr;
     for (int p = P - 2; p >= 0; --p) {
         pa.data = A;
         pa.logB = logB[p];
         pa.tw = tws ? tws->inv[p] : nullptr;
-        if ((e = launch_pass(V_INV, pl.bits[p], pa, N >> (pl.bits[p] + 4), s)) != cudaSuccess) return e;
+        add(V_INV, pl.bits[p], pa, N >> (pl.bits[p] + 4));
     }
-
     // CRT constants: M_i^-1 * N^-1 mod p_i
-    CrtArgs ca;
+    CrtArgs& ca = out->crt;
     memset(&ca, 0, sizeof(ca));
     for (int i = 0; i < 3; ++i) {
         const u64 p = kP[i];
@@ -1266,14 +1288,314 @@ cudaError_t enqueue_job(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s,
     ca.nvalid = (out_len - 1) < N ? (out_len - 1) : N;
     ca.out = j.out;
     ca.out_len = out_len;
-    ca.state = (u32*)(base + w.state);
-    ca.ticket = (u32*)(base + w.ticket);
-    ca.err = (u32*)base;
-    e = cudaMemsetAsync(base + w.ticket, 0, w.total - w.ticket, s);
-    if (e != cudaSuccess) return e;
-    const double crt_bytes = 3.0 * (double)ca.nvalid * 8.0 + (double)out_len * 8.0;
+    ca.state = sc.state;
+    ca.ticket = sc.ticket;
+    ca.err = sc.err;
+    out->ncta = w.ncta;
+}
+
+static cudaError_t launch_crt(const CrtArgs& ca, u64 ncta, cudaStream_t s) {
+    const double crt_bytes = 3.0 * (double)ca.nvalid * 8.0 + (double)ca.out_len * 8.0;
     return timed_launch(K_CRT, crt_bytes, 3.0 * (double)ca.nvalid, s,
-                        [&] { k_crt_carry<<<(unsigned)w.ncta, CNT, 0, s>>>(ca); });
+                        [&] { k_crt_carry<<<(unsigned)ncta, CNT, 0, s>>>(ca); });
+}
+
+cudaError_t enqueue_job(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s, const TwiddleSet* tws) {
+    const u64 out_len = j.la + j.lb;
+    if (out_len == 0) return cudaSuccess;
+    if (j.la == 0 || j.lb == 0) return cudaMemsetAsync(j.out, 0, out_len * sizeof(u64), s);
+    const int sqr = j.sqr ? 1 : 0;
+    const WsLayout w = ws_layout(j.la, j.lb, sqr);
+    if (ws_bytes < w.total || w.n > MAX_LOG_N) return cudaErrorInvalidValue;
+    cudaError_t e = ensure_tables();
+    if (e != cudaSuccess) return e;
+    char* base = (char*)ws;
+    JobScratch sc{(u64*)(base + w.a), (u64*)(base + w.b), (u32*)(base + w.ticket), (u32*)(base + w.state),
+                  (u32*)base};
+    JobLaunches L;
+    plan_job(j, sc, tws, &L);
+    for (int k = 0; k < L.count; ++k) {
+        const LaunchRec& r = L.rec[k];
+        if ((e = launch_pass(r.variant, r.logl, r.pa, r.tiles, s)) != cudaSuccess) return e;
+    }
+    if ((e = cudaMemsetAsync(base + w.ticket, 0, w.total - w.ticket, s)) != cudaSuccess) return e;
+    return launch_crt(L.crt, L.ncta, s);
+}
+
+// ------------------------------------------------------------------ batches
+// Batched kernels: products with the same transform length and kind share every launch.
+// CTA b works on product b / (3 * tiles), tile (b / 3) % tiles, prime b % 3.
+template <int MODE, int LOGL, bool ENTRY, bool SQR>
+__global__ void __launch_bounds__(NT, 4) k_pass_batch(const PassArgs* __restrict__ args, u32 tiles) {
+    extern __shared__ __align__(16) u64 sm[];
+    const int pi = blockIdx.x % 3;
+    const u32 rest = blockIdx.x / 3;
+    const PassArgs a = args[rest / tiles];
+    const u64 tile = rest % tiles;
+    const PrimeRT q = c_prime[pi];
+    if constexpr (MODE == M_FWD) body_fwd<LOGL, ENTRY>(sm, a, tile, pi, q);
+    else if constexpr (MODE == M_INV) body_inv<LOGL>(sm, a, tile, pi, q);
+    else if constexpr (MODE == M_FWD_LAST) body_fwd_last<LOGL, ENTRY>(sm, a, tile, pi, q);
+    else if constexpr (MODE == M_FUSED2) body_fused2<(LOGL >= 5 ? LOGL : 5)>(sm, a, tile, pi, q);
+    else body_fused<LOGL, ENTRY, SQR>(sm, a, tile, pi, q);
+}
+
+// CRT + carry of many products: CTAs take per-product tickets; tickets beyond a product's
+// tile count exit at once.
+__global__ void __launch_bounds__(CNT) k_crt_carry_batch(const CrtArgs* __restrict__ args, u32 ctas_per_job,
+                                                         const u32* __restrict__ ncta) {
+    const u32 job = blockIdx.x / ctas_per_job;
+    crt_carry_body(args[job], ncta[job]);
+}
+
+typedef void (*BatchKernel)(const PassArgs*, u32);
+template <int MODE, int LOGL, bool ENTRY, bool SQR>
+static BatchKernel bkernel_ptr() {
+    return k_pass_batch<MODE, LOGL, ENTRY, SQR>;
+}
+template <int LOGL>
+static void fill_brow(BatchKernel (&t)[NV][MAX_PASS_BITS + 1]) {
+    constexpr int LS = LOGL >= 5 ? LOGL : 5;
+    t[V_FWD][LOGL] = LOGL >= 5 ? bkernel_ptr<M_FWD, LS, false, false>() : nullptr;
+    t[V_FWD_E][LOGL] = LOGL >= 5 ? bkernel_ptr<M_FWD, LS, true, false>() : nullptr;
+    t[V_INV][LOGL] = LOGL >= 5 ? bkernel_ptr<M_INV, LS, false, false>() : nullptr;
+    t[V_FUSED2][LOGL] = (LOGL >= 5 && LOGL <= 8) ? bkernel_ptr<M_FUSED2, (LOGL <= 8 ? LS : 5), false, false>() : nullptr;
+    t[V_LAST][LOGL] = bkernel_ptr<M_FWD_LAST, LOGL, false, false>();
+    t[V_LAST_E][LOGL] = bkernel_ptr<M_FWD_LAST, LOGL, true, false>();
+    t[V_FUSED][LOGL] = bkernel_ptr<M_FUSED, LOGL, false, false>();
+    t[V_FUSED_E][LOGL] = bkernel_ptr<M_FUSED, LOGL, true, false>();
+    t[V_SQR][LOGL] = bkernel_ptr<M_FUSED, LOGL, false, true>();
+    t[V_SQR_E][LOGL] = bkernel_ptr<M_FUSED, LOGL, true, true>();
+}
+struct BatchKernelTable {
+    BatchKernel k[NV][MAX_PASS_BITS + 1];
+    BatchKernelTable() {
+        memset(k, 0, sizeof(k));
+        fill_brow<0>(k);
+        fill_brow<1>(k);
+        fill_brow<2>(k);
+        fill_brow<3>(k);
+        fill_brow<4>(k);
+        fill_brow<5>(k);
+        fill_brow<6>(k);
+        fill_brow<7>(k);
+        fill_brow<8>(k);
+        fill_brow<9>(k);
+    }
+};
+static const BatchKernelTable& bktab() {
+    static BatchKernelTable t;
+    return t;
+}
+
+static cudaError_t set_batch_attrs() {
+    const BatchKernelTable& K = bktab();
+    for (int v = 0; v < NV; ++v)
+        for (int l = 0; l <= MAX_PASS_BITS; ++l)
+            if (K.k[v][l]) {
+                cudaError_t e = cudaFuncSetAttribute((const void*)K.k[v][l],
+                                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pass_smem(l, v));
+                if (e != cudaSuccess) return e;
+                e = cudaFuncSetAttribute((const void*)K.k[v][l], cudaFuncAttributePreferredSharedMemoryCarveout,
+                                         (int)cudaSharedmemCarveoutMaxShared);
+                if (e != cudaSuccess) return e;
+            }
+    return cudaSuccess;
+}
+
+// Batch layout inside one workspace:
+//   [status word, 256 B][per-product residues][per-product ticket+state][launch descriptors]
+// Products are grouped by (transform length, square); each group's launches run on one of
+// the streams in `streams` (round robin), forked from and joined back into `s`.
+struct BatchGroup {
+    int n, sqr;
+    std::vector<int> idx;
+};
+
+static void batch_groups(const Job* jobs, int count, std::vector<BatchGroup>& groups) {
+    groups.clear();
+    for (int i = 0; i < count; ++i) {
+        const Job& j = jobs[i];
+        if (j.la == 0 || j.lb == 0) continue;
+        const int n = ws_layout(j.la, j.lb, j.sqr).n;
+        const int sq = j.sqr ? 1 : 0;
+        BatchGroup* g = nullptr;
+        for (auto& x : groups)
+            if (x.n == n && x.sqr == sq) g = &x;
+        if (!g) {
+            groups.push_back(BatchGroup{n, sq, {}});
+            g = &groups.back();
+        }
+        g->idx.push_back(i);
+    }
+}
+
+size_t batch_stage_bytes(const Job* jobs, int count);
+
+size_t batch_workspace_bytes(const Job* jobs, int count) {
+    size_t res = 0, st = 0;
+    for (int i = 0; i < count; ++i) {
+        const Job& j = jobs[i];
+        if (j.la == 0 || j.lb == 0) continue;
+        const WsLayout w = ws_layout(j.la, j.lb, j.sqr);
+        res += align256(3 * w.N * sizeof(u64)) * (j.sqr ? 1 : 2);
+        st += 16 + ((w.ncta * sizeof(u32) + 15) & ~(size_t)15);
+    }
+    return 256 + align256(res) + align256(st) + align256(batch_stage_bytes(jobs, count));
+}
+
+cudaError_t enqueue_batch(const Job* jobs, int count, void* ws, size_t ws_bytes, void* h_stage, size_t stage_bytes,
+                          cudaStream_t s, const cudaStream_t* streams, const cudaEvent_t* events, int nstreams,
+                          TwiddleLookup tw_lookup, void* tw_ctx) {
+    if (count <= 0) return cudaSuccess;
+    const size_t need = batch_workspace_bytes(jobs, count);
+    if (ws_bytes < need) return cudaErrorInvalidValue;
+    cudaError_t e = prepare_batch();
+    if (e != cudaSuccess) return e;
+    std::vector<BatchGroup> groups;
+    batch_groups(jobs, count, groups);
+    // zero-length products: the product is zero
+    for (int i = 0; i < count; ++i)
+        if ((jobs[i].la == 0 || jobs[i].lb == 0) && jobs[i].la + jobs[i].lb > 0)
+            if ((e = cudaMemsetAsync(jobs[i].out, 0, (jobs[i].la + jobs[i].lb) * sizeof(u64), s)) != cudaSuccess)
+                return e;
+    // carve the workspace
+    char* base = (char*)ws;
+    size_t res = 0, st = 0;
+    for (int i = 0; i < count; ++i) {
+        const Job& j = jobs[i];
+        if (j.la == 0 || j.lb == 0) continue;
+        const WsLayout w = ws_layout(j.la, j.lb, j.sqr);
+        res += align256(3 * w.N * sizeof(u64)) * (j.sqr ? 1 : 2);
+        st += 16 + ((w.ncta * sizeof(u32) + 15) & ~(size_t)15);
+    }
+    char* res_base = base + 256;
+    char* st_base = res_base + align256(res);
+    char* desc_base = st_base + align256(st);
+    // descriptors are built in pinned host staging memory, then copied in one transfer
+    char* hp = (char*)h_stage;
+    size_t hoff = 0;
+    auto hreserve = [&](size_t bytes) -> size_t {
+        const size_t o = hoff;
+        hoff = (hoff + bytes + 15) & ~(size_t)15;
+        return o;
+    };
+    struct GroupLaunch {
+        int count;
+        int variant[3 * MAX_PASSES + 2], logl[3 * MAX_PASSES + 2];
+        u64 tiles[3 * MAX_PASSES + 2];
+        size_t args_off[3 * MAX_PASSES + 2];
+        size_t crt_off, ncta_off;
+        u32 max_ncta;
+        int m;
+        char* st_lo;
+        size_t st_bytes;
+    };
+    std::vector<GroupLaunch> gl(groups.size());
+    size_t roff = 0, soff = 0;
+    std::vector<JobLaunches> jl;
+    for (size_t g = 0; g < groups.size(); ++g) {
+        const BatchGroup& G = groups[g];
+        const int m = (int)G.idx.size();
+        const TwiddleSet* tws = tw_lookup ? tw_lookup(tw_ctx, G.n) : nullptr;
+        jl.assign(m, JobLaunches());
+        GroupLaunch& L = gl[g];
+        L.m = m;
+        L.st_lo = st_base + soff;
+        u32 maxc = 0;
+        for (int t = 0; t < m; ++t) {
+            const Job& j = jobs[G.idx[t]];
+            const WsLayout w = ws_layout(j.la, j.lb, j.sqr);
+            JobScratch sc;
+            sc.A = (u64*)(res_base + roff);
+            roff += align256(3 * w.N * sizeof(u64));
+            sc.B = sc.A;
+            if (!j.sqr) {
+                sc.B = (u64*)(res_base + roff);
+                roff += align256(3 * w.N * sizeof(u64));
+            }
+            sc.ticket = (u32*)(st_base + soff);
+            sc.state = sc.ticket + 4;
+            soff += 16 + ((w.ncta * sizeof(u32) + 15) & ~(size_t)15);
+            sc.err = (u32*)base;
+            plan_job(j, sc, tws, &jl[t]);
+            if (jl[t].ncta > maxc) maxc = (u32)jl[t].ncta;
+        }
+        L.st_bytes = (size_t)(st_base + soff - L.st_lo);
+        L.max_ncta = maxc;
+        L.count = jl[0].count;
+        for (int k = 0; k < L.count; ++k) {
+            L.variant[k] = jl[0].rec[k].variant;
+            L.logl[k] = jl[0].rec[k].logl;
+            L.tiles[k] = jl[0].rec[k].tiles;
+            L.args_off[k] = hreserve((size_t)m * sizeof(PassArgs));
+            if (hoff > stage_bytes) return cudaErrorInvalidValue;
+            PassArgs* dst = (PassArgs*)(hp + L.args_off[k]);
+            for (int t = 0; t < m; ++t) dst[t] = jl[t].rec[k].pa;
+        }
+        L.crt_off = hreserve((size_t)m * sizeof(CrtArgs));
+        L.ncta_off = hreserve((size_t)m * sizeof(u32));
+        if (hoff > stage_bytes) return cudaErrorInvalidValue;
+        CrtArgs* cd = (CrtArgs*)(hp + L.crt_off);
+        u32* nc = (u32*)(hp + L.ncta_off);
+        for (int t = 0; t < m; ++t) {
+            cd[t] = jl[t].crt;
+            nc[t] = (u32)jl[t].ncta;
+        }
+    }
+    if (hoff > (size_t)((base + need) - desc_base)) return cudaErrorInvalidValue;
+    if ((e = cudaMemcpyAsync(desc_base, hp, hoff, cudaMemcpyHostToDevice, s)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(st_base, 0, align256(st), s)) != cudaSuccess) return e;
+    // fork: every worker stream waits for the descriptors (and any twiddle tables built on s)
+    if (nstreams > 0) {
+        if ((e = cudaEventRecord(events[0], s)) != cudaSuccess) return e;
+        for (int k = 0; k < nstreams; ++k)
+            if ((e = cudaStreamWaitEvent(streams[k], events[0], 0)) != cudaSuccess) return e;
+    }
+    const BatchKernelTable& BK = bktab();
+    for (size_t g = 0; g < groups.size(); ++g) {
+        const GroupLaunch& L = gl[g];
+        cudaStream_t gs = nstreams > 0 ? streams[g % nstreams] : s;
+        for (int k = 0; k < L.count; ++k) {
+            BatchKernel kk = BK.k[L.variant[k]][L.logl[k]];
+            if (!kk) return cudaErrorInvalidValue;
+            const PassArgs* d_args = (const PassArgs*)(desc_base + L.args_off[k]);
+            const unsigned grid = (unsigned)((u64)L.m * L.tiles[k] * 3);
+            kk<<<grid, NT, pass_smem(L.logl[k], L.variant[k]), gs>>>(d_args, (u32)L.tiles[k]);
+            if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        }
+        k_crt_carry_batch<<<(unsigned)(L.m * L.max_ncta), CNT, 0, gs>>>(
+            (const CrtArgs*)(desc_base + L.crt_off), L.max_ncta, (const u32*)(desc_base + L.ncta_off));
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
+    // join
+    for (int k = 0; k < nstreams; ++k) {
+        if ((e = cudaEventRecord(events[1 + k], streams[k])) != cudaSuccess) return e;
+        if ((e = cudaStreamWaitEvent(s, events[1 + k], 0)) != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+cudaError_t prepare_batch() {
+    cudaError_t e = ensure_tables();
+    if (e != cudaSuccess) return e;
+    int dev = 0;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+    static std::mutex mu;
+    static std::vector<int> done;
+    std::lock_guard<std::mutex> lk(mu);
+    for (int d : done)
+        if (d == dev) return cudaSuccess;
+    if ((e = set_batch_attrs()) != cudaSuccess) return e;
+    done.push_back(dev);
+    return cudaSuccess;
+}
+
+size_t batch_stage_bytes(const Job* jobs, int count) {
+    size_t desc = 0;
+    for (int i = 0; i < count; ++i)
+        desc += (3 * MAX_PASSES + 2) * (sizeof(PassArgs) + 16) + sizeof(CrtArgs) + sizeof(u32) + 32;
+    return desc + 4096;
 }
 
 // ------------------------------------------------------------------ modmul microbenchmark

@@ -89,6 +89,33 @@ int fmn_ws_status(const void* d_ws, u64 len1, u64 len2, int sqr, void* stream);
  * No counterpart in the reference (which allocates its scratch per call). */
 int fmn_mul_device_noalloc(const u64* d_in1, u64 len1, const u64* d_in2, u64 len2, u64* d_out, void* stream);
 
+/* ----------------------------------------------------------------- batches
+ * Many independent products in a few launches: products are grouped by transform length
+ * and kind (multiply / square) and each stage of a group runs as one batched launch, groups
+ * running concurrently on internal streams.  No counterpart in the reference (which has
+ * one product per call). */
+typedef struct {
+    const u64* in1;   /* device pointers; in1 == in2 with len1 == len2 is a square */
+    u64 len1;
+    const u64* in2;
+    u64 len2;
+    u64* out;         /* len1 + len2 limbs */
+} fmn_job;
+
+/* All products of `jobs` on `stream`, asynchronously; scratch from the library's cache.
+ * Device-side errors are reported by the next fmn_sync(stream). */
+int fmn_mul_batch_device(const fmn_job* jobs, int count, void* stream);
+
+/* A batch captured once in a CUDA graph that owns its scratch; launching it recomputes all
+ * products from the (possibly updated) contents of the same input buffers into the same
+ * outputs, with one graph launch. */
+typedef struct fmn_batch_graph fmn_batch_graph;
+int fmn_batch_graph_create(const fmn_job* jobs, int count, fmn_batch_graph** out);
+int fmn_batch_graph_launch(fmn_batch_graph* g, void* stream);
+/* Wait for `stream` and report device-side errors of the graph's products. */
+int fmn_batch_graph_sync(fmn_batch_graph* g, void* stream);
+void fmn_batch_graph_destroy(fmn_batch_graph* g);
+
 /* ----------------------------------------------------------------- measurement hooks
  * (no counterpart in the reference; used by bench.py) */
 
