@@ -28,7 +28,26 @@ EXPORTS = ["abs_mul64", "abs_sqr64", "fmn_init", "fmn_shutdown", "fmn_last_error
            "fmn_mul_device", "fmn_sqr_device", "fmn_sync", "fmn_workspace_size", "fmn_mul_device_ws",
            "fmn_ws_status", "fmn_ntt_len", "fmn_kernel_kind_name", "fmn_profile_enable", "fmn_profile_take",
            "fmn_launches_per_product", "fmn_bench_modmul", "fmn_mul_device_noalloc", "fmn_mul_batch_device",
-           "fmn_batch_graph_create", "fmn_batch_graph_launch", "fmn_batch_graph_sync", "fmn_batch_graph_destroy"]
+           "fmn_batch_graph_create", "fmn_batch_graph_launch", "fmn_batch_graph_sync", "fmn_batch_graph_destroy",
+           "fmn_operand_create", "fmn_operand_destroy", "fmn_operand_len", "fmn_mul_operand_device",
+           "fmn_operand_workspace_size", "fmn_mul_operand_ws", "fmn_server_create", "fmn_server_submit",
+           "fmn_server_wait", "fmn_server_take", "fmn_server_get_stats", "fmn_server_replay", "fmn_server_destroy"]
+
+FMN_OP_MUL, FMN_OP_SQR, FMN_OP_MUL_OPERAND = 0, 1, 2
+
+
+class FmnRequest(ctypes.Structure):
+    """fmn_request of include/fast_mul.h."""
+    _fields_ = [("op", ctypes.c_int), ("in1", ctypes.c_void_p), ("len1", ctypes.c_uint64),
+                ("in2", ctypes.c_void_p), ("len2", ctypes.c_uint64), ("operand", ctypes.c_void_p),
+                ("out", ctypes.c_void_p), ("check", ctypes.c_void_p), ("tag", ctypes.c_uint64)]
+
+
+class FmnServerStats(ctypes.Structure):
+    """fmn_server_stats of include/fast_mul.h."""
+    _fields_ = [("submitted", ctypes.c_uint64), ("completed", ctypes.c_uint64), ("rejected", ctypes.c_uint64),
+                ("failed", ctypes.c_uint64), ("batches", ctypes.c_uint64), ("mismatches", ctypes.c_uint64),
+                ("device_errors", ctypes.c_uint64), ("peak_bytes", ctypes.c_size_t)]
 
 
 class FmnJob(ctypes.Structure):
@@ -112,6 +131,32 @@ def load_library(path=None):
     lib.fmn_batch_graph_sync.restype = ctypes.c_int
     lib.fmn_batch_graph_destroy.argtypes = [_vp]
     lib.fmn_batch_graph_destroy.restype = None
+    lib.fmn_operand_create.argtypes = [_vp, _u64, _u64, _vp, ctypes.POINTER(_vp)]
+    lib.fmn_operand_create.restype = ctypes.c_int
+    lib.fmn_operand_destroy.argtypes = [_vp]
+    lib.fmn_operand_destroy.restype = None
+    lib.fmn_operand_len.argtypes = [_vp]
+    lib.fmn_operand_len.restype = _u64
+    lib.fmn_mul_operand_device.argtypes = [_vp, _vp, _u64, _vp, _vp]
+    lib.fmn_mul_operand_device.restype = ctypes.c_int
+    lib.fmn_operand_workspace_size.argtypes = [_vp, _u64]
+    lib.fmn_operand_workspace_size.restype = ctypes.c_size_t
+    lib.fmn_mul_operand_ws.argtypes = [_vp, _vp, _u64, _vp, _vp, ctypes.c_size_t, _vp]
+    lib.fmn_mul_operand_ws.restype = ctypes.c_int
+    lib.fmn_server_create.argtypes = [ctypes.c_int, ctypes.c_size_t, ctypes.c_int, ctypes.c_int, ctypes.POINTER(_vp)]
+    lib.fmn_server_create.restype = ctypes.c_int
+    lib.fmn_server_submit.argtypes = [_vp, ctypes.POINTER(FmnRequest)]
+    lib.fmn_server_submit.restype = ctypes.c_int
+    lib.fmn_server_wait.argtypes = [_vp]
+    lib.fmn_server_wait.restype = ctypes.c_int
+    lib.fmn_server_take.argtypes = [_vp, _u64p, _dp, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
+    lib.fmn_server_take.restype = ctypes.c_int
+    lib.fmn_server_get_stats.argtypes = [_vp, ctypes.POINTER(FmnServerStats)]
+    lib.fmn_server_get_stats.restype = ctypes.c_int
+    lib.fmn_server_replay.argtypes = [_vp, ctypes.POINTER(FmnRequest), _dp, ctypes.c_int, _dp, _dp]
+    lib.fmn_server_replay.restype = ctypes.c_int
+    lib.fmn_server_destroy.argtypes = [_vp]
+    lib.fmn_server_destroy.restype = None
     if path is None:
         _lib = lib
     return lib
@@ -285,6 +330,87 @@ class BatchGraph:
     def close(self):
         if self.handle:
             load_library().fmn_batch_graph_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Operand:
+    """A resident operand: its forward transform stays in device memory, so products with it
+    transform only the partner (``mul``).  ``limbs`` (a CUDA tensor) must outlive it."""
+
+    def __init__(self, limbs, max_partner_len, stream=None):
+        lib = load_library()
+        self.limbs = limbs
+        h = ctypes.c_void_p()
+        _check(lib.fmn_operand_create(limbs.data_ptr(), limbs.numel(), max_partner_len, _stream_ptr(stream),
+                                      ctypes.byref(h)))
+        self.handle = h
+        self.len = limbs.numel()
+
+    def mul(self, b, out, stream=None):
+        _check(load_library().fmn_mul_operand_device(self.handle, b.data_ptr(), b.numel(), out.data_ptr(),
+                                                      _stream_ptr(stream)))
+        return out
+
+    def close(self):
+        if getattr(self, "handle", None):
+            load_library().fmn_operand_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """The product server (continuous batching with an HBM budget); ``batching=False`` gives
+    the plain per-call path on one stream."""
+
+    def __init__(self, device=0, hbm_budget=120 << 30, max_batch=512, batching=True):
+        lib = load_library()
+        h = ctypes.c_void_p()
+        _check(lib.fmn_server_create(device, hbm_budget, max_batch, 1 if batching else 0, ctypes.byref(h)))
+        self.handle = h
+
+    def submit(self, req):
+        _check(load_library().fmn_server_submit(self.handle, ctypes.byref(req)))
+
+    def wait(self):
+        _check(load_library().fmn_server_wait(self.handle))
+
+    def take(self, max_n=1 << 16):
+        tags = (ctypes.c_uint64 * max_n)()
+        lat = (ctypes.c_double * max_n)()
+        n = ctypes.c_int()
+        _check(load_library().fmn_server_take(self.handle, tags, lat, max_n, ctypes.byref(n)))
+        return [(int(tags[i]), lat[i]) for i in range(n.value)]
+
+    def stats(self):
+        st = FmnServerStats()
+        _check(load_library().fmn_server_get_stats(self.handle, ctypes.byref(st)))
+        return {k: int(getattr(st, k)) for k, _ in FmnServerStats._fields_}
+
+    def replay(self, requests, arrivals):
+        """Open-loop replay of a request array at the given arrival times (seconds); returns
+        (latencies in ms per request, wall seconds)."""
+        n = len(requests)
+        arr = (FmnRequest * n)(*requests)
+        at = (ctypes.c_double * n)(*arrivals)
+        lat = (ctypes.c_double * n)()
+        wall = ctypes.c_double()
+        _check(load_library().fmn_server_replay(self.handle, arr, at, n, lat, ctypes.byref(wall)))
+        return list(lat), wall.value
+
+    def close(self):
+        if getattr(self, "handle", None):
+            load_library().fmn_server_destroy(self.handle)
             self.handle = None
 
     def __del__(self):

@@ -212,13 +212,13 @@ int ilog2_ceil(u64 x) {
 
 // Enqueue a product on stream s using the context workspace (caller holds c->mu).
 int run_job_ctx(DevCtx* c, const fmn::Job& j, cudaStream_t s) {
-    const size_t need = fmn::job_workspace_bytes(j.la, j.lb, j.sqr);
+    const size_t need = fmn::job_workspace_bytes(j);
     int rc = ensure_ws(c, need);
     if (rc) return rc;
     cudaError_t e;
     if (c->done_valid && (e = cudaStreamWaitEvent(s, c->done, 0)) != cudaSuccess)
         return set_err(FMN_ERR_CUDA, "cudaStreamWaitEvent", e);
-    const fmn::TwiddleSet* tws = get_twiddles(c, ilog2_ceil(j.la + j.lb - 1), s);
+    const fmn::TwiddleSet* tws = get_twiddles(c, j.spectrum ? j.log_n : ilog2_ceil(j.la + j.lb - 1), s);
     if ((e = fmn::enqueue_job(j, c->ws, c->ws_cap, s, tws)) != cudaSuccess) return set_err(FMN_ERR_CUDA, "kernel launch", e);
     if ((e = cudaEventRecord(c->done, s)) != cudaSuccess) return set_err(FMN_ERR_CUDA, "cudaEventRecord", e);
     c->done_valid = true;
@@ -617,6 +617,30 @@ int fmn_batch_graph_launch(fmn_batch_graph* g, void* stream) {
 int fmn_batch_graph_sync(fmn_batch_graph* g, void* stream) {
     if (!g) return set_err(FMN_ERR_ARG, "null graph");
     return take_device_error(g->ws, g->h_err, (cudaStream_t)stream);
+}
+
+int fmn_mul_operand_device(const fmn_operand* op, const u64* d_in2, u64 len2, u64* d_out, void* stream) {
+    if (!op || !d_out || (len2 && !d_in2)) return set_err(FMN_ERR_ARG, "null pointer");
+    if (len2 > op->max_partner) return set_err(FMN_ERR_ARG, "partner longer than the operand allows");
+    cudaStream_t s = (cudaStream_t)stream;
+    if (len2 == 0) {
+        cudaError_t e = cudaMemsetAsync(d_out, 0, op->len * sizeof(u64), s);
+        return e == cudaSuccess ? FMN_OK : set_err(FMN_ERR_CUDA, "cudaMemsetAsync", e);
+    }
+    DevCtx* c;
+    int rc = get_ctx(&c);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> lk(c->mu);
+    fmn::Job j;
+    j.a = nullptr;
+    j.la = op->len;
+    j.b = d_in2;
+    j.lb = len2;
+    j.out = d_out;
+    j.sqr = 0;
+    j.spectrum = op->spec;
+    j.log_n = op->log_n;
+    return run_job_ctx(c, j, s);
 }
 
 const char* fmn_kernel_kind_name(int kind) { return fmn::kernel_kind_name(kind); }

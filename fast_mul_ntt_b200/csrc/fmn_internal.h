@@ -24,22 +24,33 @@ Plan make_plan(int log_n);
 
 // One product on the device.  All pointers are device pointers.
 struct Job {
-    const u64* a;      // in1 limbs
+    const u64* a;      // in1 limbs (unused when `spectrum` is set)
     u64 la;
     const u64* b;      // in2 limbs (ignored when sqr)
     u64 lb;
     u64* out;          // la + lb limbs
     int sqr;
+    // Resident first operand (conv_single reuse): its forward spectrum, computed by
+    // spectrum_enqueue for a transform of 2^log_n points; la is its length.  Null otherwise.
+    const u64* spectrum = nullptr;
+    int log_n = 0;
 };
+
+// Forward transform of `len` limbs at `src` into `spec` (3 * 2^log_n u64): the spectrum a
+// resident operand keeps for products of up to 2^log_n - len + 1 partner limbs.
+cudaError_t spectrum_enqueue(const u64* src, u64 len, int log_n, u64* spec, cudaStream_t s,
+                             const struct TwiddleSet* tw);
 
 // Scratch needed by one product: residue arrays + carry-scan state.
 size_t job_workspace_bytes(u64 la, u64 lb, int sqr);
+size_t job_workspace_bytes(const Job& j);
 
 // Upload twiddle tables to the current device (idempotent per device).
 cudaError_t ensure_tables();
 
 // Precomputed four-step twiddles of every strided pass of one transform length.
 struct TwiddleSet {
+    TwiddleSet() : log_n(0), fwd{}, inv{} {}
     int log_n;
     const u64* fwd[MAX_PASSES];
     const u64* inv[MAX_PASSES];
@@ -97,3 +108,13 @@ int job_launches(u64 la, u64 lb, int sqr);
 cudaError_t bench_modmul(double* per_second, double* butterflies_per_second);
 
 }  // namespace fmn
+
+// A resident operand (include/fast_mul.h): its forward spectrum stays in device memory.
+struct fmn_operand {
+    int dev;
+    const u64* src;      // the caller's limbs (used by the plain per-call path)
+    u64 len;
+    int log_n;           // transform length of its products
+    u64 max_partner;     // longest partner it was sized for
+    u64* spec;           // 3 * 2^log_n residues, forward-transformed
+};

@@ -89,6 +89,8 @@ struct PassArgs {
     const u64* tw;    // strided passes: precomputed four-step twiddles of this pass
                       // (prime i at tw + i * 2^logB, entry j * S + column), or null to
                       // generate them on the fly
+    u64* dst;         // M_FUSED: where the product goes when `other` must stay intact
+                      // (a resident spectrum); null writes it over `other`
 };
 
 // ------------------------------------------------------------------ one round
@@ -419,6 +421,7 @@ __device__ __forceinline__ void body_fused(u64* sm, const PassArgs& a, u64 tile,
     const int ncols = a.ncols;
     const u64* __restrict__ d = a.data + (u64)pi * a.N;
     u64* __restrict__ o = a.other + (u64)pi * a.N;
+    u64* __restrict__ dd = (a.dst ? a.dst : a.other) + (u64)pi * a.N;
     const u64* __restrict__ src = a.src;
     const u64 len = a.len;
     auto ldg = [=](int j, int c) -> u64 {
@@ -428,7 +431,7 @@ __device__ __forceinline__ void body_fused(u64* sm, const PassArgs& a, u64 tile,
         else return d[g];
     };
     auto stg = [=](int j, int c, u64 v) {
-        if (c < ncols) o[gbase + (u64)c * L + j] = v;
+        if (c < ncols) dd[gbase + (u64)c * L + j] = v;
     };
     auto lds = [sm](int j, int c) { return sm[sw(j, c)]; };
     auto sts = [sm](int j, int c, u64 v) { sm[sw(j, c)] = v; };
@@ -436,7 +439,8 @@ __device__ __forceinline__ void body_fused(u64* sm, const PassArgs& a, u64 tile,
         if (threadIdx.x < (unsigned)ncols) {
             const int c = threadIdx.x;
             const u64 x = ldg(0, c);
-            stg(0, c, mmul(x, SQR ? x : o[gbase + c], q));
+            const u64 y = SQR ? x : o[gbase + c];
+            stg(0, c, mmul(x, y, q));
         }
     } else if constexpr (NR == 1) {
         fused_lowest<LOGL, SQR>(ldg, stg, o, gbase, ncols, pi, q);
@@ -1021,12 +1025,13 @@ struct WsLayout {
     size_t a, b, ticket, state, total;
     u64 ncta;
 };
-static WsLayout ws_layout(u64 la, u64 lb, int sqr) {
+static WsLayout ws_layout(u64 la, u64 lb, int sqr, int force_n = 0) {
     WsLayout w;
     memset(&w, 0, sizeof(w));
     const u64 out_len = la + lb;
     if (la == 0 || lb == 0) return w;
     w.N = ceil_pow2(out_len - 1);
+    if (force_n > 0 && (1ull << force_n) > w.N) w.N = 1ull << force_n;
     w.n = ilog2(w.N);
     w.ncta = (out_len + CTILE - 1) / CTILE;
     size_t off = 256;
@@ -1044,6 +1049,43 @@ static WsLayout ws_layout(u64 la, u64 lb, int sqr) {
 size_t job_workspace_bytes(u64 la, u64 lb, int sqr) {
     const size_t t = ws_layout(la, lb, sqr).total;
     return t ? t : 256;
+}
+
+size_t job_workspace_bytes(const Job& j) {
+    const size_t t = ws_layout(j.la, j.lb, j.sqr, j.spectrum ? j.log_n : 0).total;
+    return t ? t : 256;
+}
+
+static cudaError_t launch_pass(int variant, int logl, const PassArgs& a, u64 tiles, cudaStream_t s);
+
+cudaError_t spectrum_enqueue(const u64* src, u64 len, int log_n, u64* spec, cudaStream_t s, const TwiddleSet* tws) {
+    cudaError_t e = ensure_tables();
+    if (e != cudaSuccess) return e;
+    if (tws && tws->log_n != log_n) tws = nullptr;
+    const Plan pl = make_plan(log_n);
+    const int P = pl.passes;
+    const u64 N = 1ull << log_n;
+    PassArgs pa;
+    memset(&pa, 0, sizeof(pa));
+    pa.N = N;
+    pa.ncols = TC;
+    pa.src = src;
+    pa.len = len;
+    pa.data = spec;
+    int logB = log_n;
+    for (int p = 0; p + 1 < P; ++p) {
+        pa.logB = logB;
+        pa.tw = tws ? tws->fwd[p] : nullptr;
+        if ((e = launch_pass(p == 0 ? V_FWD_E : V_FWD, pl.bits[p], pa, N >> (pl.bits[p] + 4), s)) != cudaSuccess)
+            return e;
+        logB -= pl.bits[p];
+    }
+    const int lastl = pl.bits[P - 1];
+    const u64 nblk = N >> lastl;
+    pa.tw = nullptr;
+    pa.logB = logB;
+    pa.ncols = nblk < (u64)TC ? (int)nblk : TC;
+    return launch_pass(P == 1 ? V_LAST_E : V_LAST, lastl, pa, (nblk + TC - 1) / TC, s);
 }
 
 // ------------------------------------------------------------------ host: profiling
@@ -1184,7 +1226,7 @@ struct JobScratch {
 static void plan_job(const Job& j, const JobScratch& sc, const TwiddleSet* tws, JobLaunches* out) {
     const u64 out_len = j.la + j.lb;
     const int sqr = j.sqr ? 1 : 0;
-    const WsLayout w = ws_layout(j.la, j.lb, sqr);
+    const WsLayout w = ws_layout(j.la, j.lb, sqr, j.spectrum ? j.log_n : 0);
     u64* A = sc.A;
     u64* B = sqr ? A : sc.B;
     const Plan pl = make_plan(w.n);
@@ -1220,8 +1262,22 @@ static void plan_job(const Job& j, const JobScratch& sc, const TwiddleSet* tws, 
             add(p == 0 ? V_FWD_E : V_FWD, pl.bits[p], pa, N >> (pl.bits[p] + 4));
         }
     };
-    const bool merged = !sqr && P >= 2 && lastl <= 8;
-    if (merged) {
+    const bool merged = !sqr && !j.spectrum && P >= 2 && lastl <= 8;
+    if (j.spectrum) {
+        // resident first operand (conv_single, src/fast_mul.c:135-212): only the second
+        // operand is transformed; the product lands in A, the spectrum stays intact
+        fwd_strided(j.b, j.lb, B);
+        pa.tw = nullptr;
+        pa.src = j.b;
+        pa.len = j.lb;
+        pa.data = B;
+        pa.other = (u64*)j.spectrum;
+        pa.dst = A;
+        pa.logB = logB[P - 1];
+        pa.ncols = ncols_last;
+        add(P == 1 ? V_FUSED_E : V_FUSED, lastl, pa, tiles_last);
+        pa.dst = nullptr;
+    } else if (merged) {
         fwd_strided(j.a, j.la, A);
         fwd_strided(j.b, j.lb, B);
         pa.tw = nullptr;
@@ -1305,7 +1361,7 @@ cudaError_t enqueue_job(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s,
     if (out_len == 0) return cudaSuccess;
     if (j.la == 0 || j.lb == 0) return cudaMemsetAsync(j.out, 0, out_len * sizeof(u64), s);
     const int sqr = j.sqr ? 1 : 0;
-    const WsLayout w = ws_layout(j.la, j.lb, sqr);
+    const WsLayout w = ws_layout(j.la, j.lb, sqr, j.spectrum ? j.log_n : 0);
     if (ws_bytes < w.total || w.n > MAX_LOG_N) return cudaErrorInvalidValue;
     cudaError_t e = ensure_tables();
     if (e != cudaSuccess) return e;
@@ -1408,20 +1464,21 @@ static cudaError_t set_batch_attrs() {
 // Products are grouped by (transform length, square); each group's launches run on one of
 // the streams in `streams` (round robin), forked from and joined back into `s`.
 struct BatchGroup {
-    int n, sqr;
+    int n, kind;          // kind: 0 multiply, 1 square, 2 resident first operand
     std::vector<int> idx;
 };
+static int job_kind(const Job& j) { return j.spectrum ? 2 : (j.sqr ? 1 : 0); }
 
 static void batch_groups(const Job* jobs, int count, std::vector<BatchGroup>& groups) {
     groups.clear();
     for (int i = 0; i < count; ++i) {
         const Job& j = jobs[i];
         if (j.la == 0 || j.lb == 0) continue;
-        const int n = ws_layout(j.la, j.lb, j.sqr).n;
-        const int sq = j.sqr ? 1 : 0;
+        const int n = ws_layout(j.la, j.lb, j.sqr, j.spectrum ? j.log_n : 0).n;
+        const int sq = job_kind(j);
         BatchGroup* g = nullptr;
         for (auto& x : groups)
-            if (x.n == n && x.sqr == sq) g = &x;
+            if (x.n == n && x.kind == sq) g = &x;
         if (!g) {
             groups.push_back(BatchGroup{n, sq, {}});
             g = &groups.back();
@@ -1437,7 +1494,7 @@ size_t batch_workspace_bytes(const Job* jobs, int count) {
     for (int i = 0; i < count; ++i) {
         const Job& j = jobs[i];
         if (j.la == 0 || j.lb == 0) continue;
-        const WsLayout w = ws_layout(j.la, j.lb, j.sqr);
+        const WsLayout w = ws_layout(j.la, j.lb, j.sqr, j.spectrum ? j.log_n : 0);
         res += align256(3 * w.N * sizeof(u64)) * (j.sqr ? 1 : 2);
         st += 16 + ((w.ncta * sizeof(u32) + 15) & ~(size_t)15);
     }
@@ -1465,7 +1522,7 @@ cudaError_t enqueue_batch(const Job* jobs, int count, void* ws, size_t ws_bytes,
     for (int i = 0; i < count; ++i) {
         const Job& j = jobs[i];
         if (j.la == 0 || j.lb == 0) continue;
-        const WsLayout w = ws_layout(j.la, j.lb, j.sqr);
+        const WsLayout w = ws_layout(j.la, j.lb, j.sqr, j.spectrum ? j.log_n : 0);
         res += align256(3 * w.N * sizeof(u64)) * (j.sqr ? 1 : 2);
         st += 16 + ((w.ncta * sizeof(u32) + 15) & ~(size_t)15);
     }
@@ -1505,7 +1562,7 @@ cudaError_t enqueue_batch(const Job* jobs, int count, void* ws, size_t ws_bytes,
         u32 maxc = 0;
         for (int t = 0; t < m; ++t) {
             const Job& j = jobs[G.idx[t]];
-            const WsLayout w = ws_layout(j.la, j.lb, j.sqr);
+            const WsLayout w = ws_layout(j.la, j.lb, j.sqr, j.spectrum ? j.log_n : 0);
             JobScratch sc;
             sc.A = (u64*)(res_base + roff);
             roff += align256(3 * w.N * sizeof(u64));

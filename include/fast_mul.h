@@ -116,6 +116,65 @@ int fmn_batch_graph_launch(fmn_batch_graph* g, void* stream);
 int fmn_batch_graph_sync(fmn_batch_graph* g, void* stream);
 void fmn_batch_graph_destroy(fmn_batch_graph* g);
 
+/* ----------------------------------------------------------------- resident operands
+ * A number whose forward transform is computed once and kept in device memory; products
+ * with it transform only the partner.  Counterpart of the reference's conv_single
+ * (src/fast_mul.c:135-212), which multiplies by an already-transformed operand but which
+ * the reference's driver never calls. */
+typedef struct fmn_operand fmn_operand;
+/* Transform `len` limbs at device pointer d_in for products with partners of up to
+ * max_partner_len limbs (synchronous on `stream`).  d_in must stay valid while the operand
+ * is used by a plain (non-batching) server. */
+int fmn_operand_create(const u64* d_in, u64 len, u64 max_partner_len, void* stream, fmn_operand** out);
+void fmn_operand_destroy(fmn_operand* op);
+u64 fmn_operand_len(const fmn_operand* op);
+/* d_out (len(op) + len2 limbs) = op * d_in2, asynchronously on `stream`. */
+int fmn_mul_operand_device(const fmn_operand* op, const u64* d_in2, u64 len2, u64* d_out, void* stream);
+/* Same with caller-provided scratch of fmn_operand_workspace_size bytes. */
+size_t fmn_operand_workspace_size(const fmn_operand* op, u64 len2);
+int fmn_mul_operand_ws(const fmn_operand* op, const u64* d_in2, u64 len2, u64* d_out, void* d_ws,
+                       size_t ws_bytes, void* stream);
+
+/* ----------------------------------------------------------------- product server
+ * Continuous batching: requests submitted from any thread are admitted in arrival order
+ * while their scratch fits the HBM budget and a slot (CUDA stream) is free; admitted
+ * requests run as one batch, batches overlap on the device, and requests arriving meanwhile
+ * join the next batch as slots and memory free up.  With batching = 0 the server is the
+ * plain per-call path: one product per launch sequence, in arrival order, on one stream,
+ * without resident-operand reuse.  No counterpart in the reference. */
+enum { FMN_OP_MUL = 0, FMN_OP_SQR = 1, FMN_OP_MUL_OPERAND = 2 };
+typedef struct {
+    int op;                      /* FMN_OP_* */
+    const u64* in1;              /* device pointers (in1 only for squares) */
+    u64 len1;
+    const u64* in2;              /* FMN_OP_MUL and FMN_OP_MUL_OPERAND */
+    u64 len2;
+    const fmn_operand* operand;  /* FMN_OP_MUL_OPERAND */
+    u64* out;                    /* product; NULL: the server computes it into scratch and discards it */
+    const u64* check;            /* optional expected product (device); mismatches are counted */
+    u64 tag;                     /* returned by fmn_server_take */
+} fmn_request;
+typedef struct {
+    u64 submitted, completed, rejected, failed, batches;
+    u64 mismatches;              /* requests whose product differed from `check` */
+    u64 device_errors;           /* batches whose carry scan reported a bounded-wait expiry */
+    size_t peak_bytes;           /* highest scratch in use */
+} fmn_server_stats;
+typedef struct fmn_server fmn_server;
+int fmn_server_create(int device, size_t hbm_budget_bytes, int max_batch, int batching, fmn_server** out);
+int fmn_server_submit(fmn_server* s, const fmn_request* req);
+/* Wait until every submitted request has completed. */
+int fmn_server_wait(fmn_server* s);
+/* Completed requests since the last call, in completion order: tags and latency
+ * (completion - submission, milliseconds). */
+int fmn_server_take(fmn_server* s, u64* tags, double* latency_ms, int max, int* n);
+int fmn_server_get_stats(fmn_server* s, fmn_server_stats* st);
+/* Open-loop replay: request i is submitted arrival_s[i] seconds after the start regardless
+ * of the server's state; waits for all; latency_ms[i] = completion - scheduled arrival. */
+int fmn_server_replay(fmn_server* s, const fmn_request* reqs, const double* arrival_s, int count,
+                      double* latency_ms, double* wall_s);
+void fmn_server_destroy(fmn_server* s);
+
 /* ----------------------------------------------------------------- measurement hooks
  * (no counterpart in the reference; used by bench.py) */
 
