@@ -55,6 +55,10 @@ def parse():
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-stream comparison")
     ap.add_argument("--batch-only", action="store_true", help="only the batched-stream comparison")
     ap.add_argument("--batch-count", type=int, default=4096)
+    ap.add_argument("--no-serve", action="store_true", help="skip the served-stream comparison")
+    ap.add_argument("--serve-only", action="store_true", help="only the served-stream comparison")
+    ap.add_argument("--serve-requests", type=int, default=5000)
+    ap.add_argument("--serve-rate", type=float, default=1500.0, help="offered requests per second")
     return ap.parse_args()
 
 
@@ -278,6 +282,101 @@ def batch_compare(fmn, torch, dev, count, repeats=3):
     return res
 
 
+# ----------------------------------------------------------------------------- served stream
+def serve_compare(fmn, torch, dev, n_requests, rate, seed=0, templates=256, residents=8):
+    """Open-loop Poisson stream at `rate` requests/s: 70% multiplies, 30% squares, operand
+    lengths log-uniform in [256, 4,000,000] limbs, 25% of the multiplies by a resident
+    (already transformed) operand; HBM admission budget 120 GB.  The same stream through the
+    continuous-batching server and through the plain per-call path (one product at a time
+    on one stream, no reuse).  Every output is compared on the device with its expected
+    product, computed beforehand by the per-call path."""
+    rng = np.random.default_rng(seed)
+    lo, hi = 256, 4_000_000
+
+    def loglen():
+        return int(np.exp(rng.uniform(np.log(lo), np.log(hi))))
+
+    hold = []
+    res_ops = []
+    for k in range(residents):
+        a = synth_limbs("uniform", loglen(), 500_000 + k)
+        da = torch.from_numpy(a.view(np.int64)).to(dev)
+        hold.append(da)
+        res_ops.append(fmn.Operand(da, max_partner_len=hi))
+    tmpl = []
+    stream = torch.cuda.Stream(device=dev)
+    for t in range(templates):
+        r = fmn.FmnRequest()
+        u = rng.uniform()
+        if u < 0.30:                                   # square
+            l1 = loglen()
+            da = torch.from_numpy(synth_limbs("uniform", l1, 600_000 + t).view(np.int64)).to(dev)
+            hold.append(da)
+            want = torch.empty(2 * l1, dtype=torch.int64, device=dev)
+            fmn.sqr_device(da, want, stream=stream)
+            r.op, r.in1, r.len1 = fmn.FMN_OP_SQR, da.data_ptr(), l1
+        elif u < 0.30 + 0.70 * 0.25:                   # multiply by a resident operand
+            op = res_ops[t % residents]
+            l2 = loglen()
+            db = torch.from_numpy(synth_limbs("uniform", l2, 700_000 + t).view(np.int64)).to(dev)
+            hold.append(db)
+            want = torch.empty(op.len + l2, dtype=torch.int64, device=dev)
+            fmn.mul_device(op.limbs, db, want, stream=stream)
+            r.op, r.operand, r.in2, r.len2 = fmn.FMN_OP_MUL_OPERAND, op.handle.value, db.data_ptr(), l2
+        else:                                          # multiply
+            l1, l2 = loglen(), loglen()
+            da = torch.from_numpy(synth_limbs("uniform", l1, 800_000 + t).view(np.int64)).to(dev)
+            db = torch.from_numpy(synth_limbs("uniform", l2, 900_000 + t).view(np.int64)).to(dev)
+            hold += [da, db]
+            want = torch.empty(l1 + l2, dtype=torch.int64, device=dev)
+            fmn.mul_device(da, db, want, stream=stream)
+            r.op, r.in1, r.len1, r.in2, r.len2 = fmn.FMN_OP_MUL, da.data_ptr(), l1, db.data_ptr(), l2
+        hold.append(want)
+        r.check = want.data_ptr()
+        r.out = None
+        tmpl.append(r)
+    fmn.sync(stream)
+    pick = rng.integers(0, templates, n_requests)
+    reqs = []
+    for i, t in enumerate(pick):
+        r = fmn.FmnRequest()
+        ctypes.pointer(r)[0] = tmpl[t]
+        r.tag = i
+        reqs.append(r)
+    arrivals = list(np.cumsum(rng.exponential(1.0 / rate, n_requests)))
+    ops = [tmpl[t].op for t in pick]
+    out = {"workload": f"{n_requests} requests, open-loop Poisson at {rate:g}/s; 70% multiply / 30% square, "
+                       f"25% of the multiplies by one of {residents} resident operands; lengths log-uniform in "
+                       f"[{lo}, {hi}] limbs ({templates} request templates, seed {seed}); HBM budget 120 GB",
+           "mix": {"mul": ops.count(fmn.FMN_OP_MUL), "sqr": ops.count(fmn.FMN_OP_SQR),
+                   "mul_resident": ops.count(fmn.FMN_OP_MUL_OPERAND)}}
+    for name, batching in (("served", True), ("per_call", False)):
+        srv = fmn.Server(device=dev.index or 0, hbm_budget=120 << 30, max_batch=256, batching=batching)
+        try:
+            lat, wall = srv.replay(reqs, arrivals)
+            st = srv.stats()
+        finally:
+            srv.close()
+        lat = np.sort(np.array(lat))
+        out[name] = {"products_per_s": st["completed"] / wall, "wall_s": wall,
+                     "p50_ms": float(lat[len(lat) // 2]), "p99_ms": float(lat[min(len(lat) - 1, int(0.99 * len(lat)))]),
+                     "mean_ms": float(lat.mean()), "batches": st["batches"], "peak_scratch_gb": st["peak_bytes"] / 2**30,
+                     "mismatches": st["mismatches"], "rejected": st["rejected"], "device_errors": st["device_errors"],
+                     "bit_exact": st["mismatches"] == 0 and st["device_errors"] == 0 and st["rejected"] == 0}
+    out["throughput_ratio_served_vs_per_call"] = out["served"]["products_per_s"] / out["per_call"]["products_per_s"]
+    out["p99_ratio_per_call_vs_served"] = out["per_call"]["p99_ms"] / out["served"]["p99_ms"]
+    for op in res_ops:
+        op.close()
+    del hold
+    torch.cuda.empty_cache()
+    return out
+
+
+def synth_limbs(kind, n, seed):
+    from fast_mul_ntt_b200 import synth
+    return synth.limbs(kind, n, seed)
+
+
 # ----------------------------------------------------------------------------- ours
 def run_ours(args, ws, rank, local):
     import torch
@@ -297,6 +396,9 @@ def run_ours(args, ws, rank, local):
     fmn.init(local)
     if args.batch_only:
         print(json.dumps(batch_compare(fmn, torch, dev, args.batch_count)), flush=True)
+        return
+    if args.serve_only:
+        print(json.dumps(serve_compare(fmn, torch, dev, args.serve_requests, args.serve_rate)), flush=True)
         return
     l1 = args.len or LEN1
     l2 = args.len or LEN2
@@ -439,6 +541,9 @@ def run_ours(args, ws, rank, local):
         del da, db, dout
         torch.cuda.empty_cache()
         result["batch"] = batch_compare(fmn, torch, dev, args.batch_count)
+    if rank == 0 and not args.no_serve and l1 == LEN1:
+        torch.cuda.empty_cache()
+        result["serve"] = serve_compare(fmn, torch, dev, args.serve_requests, args.serve_rate)
     if rank == 0 and ws == 1 and not args.no_cpu_baseline and l1 == LEN1:
         cb, cout = cpu_baseline(a, b)
         cb["bit_exact_vs_gpu"] = bool(np.array_equal(cout, got))

@@ -98,7 +98,8 @@ struct fmn_server {
     std::vector<std::pair<void*, fmn::TwiddleSet>> tw;   // per transform length
     std::mutex mu;
     std::condition_variable cv;
-    std::deque<size_t> pending;
+    std::deque<size_t> pending;           // plain mode: one queue
+    std::deque<size_t> big;               // batching mode: large products (lane 0, one at a time)
     std::vector<Req> log;                 // every request ever submitted, by index
     std::vector<size_t> completed_order;  // indices in completion order
     size_t taken = 0;                     // completions handed out by fmn_server_take
@@ -170,6 +171,18 @@ u64 out_len_of(const fmn_request& r) {
 
 size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
+// Transform length (log2) of a request's product.
+int request_log_n(const fmn_request& r, bool reuse) {
+    if (r.op == FMN_OP_MUL_OPERAND && reuse) return r.operand->log_n;
+    const u64 ol = out_len_of(r);
+    return ol > 1 ? ilog2c(ol - 1) : 0;
+}
+
+// Products this large run alone with the single-product kernels (they fill the GPU by
+// themselves); smaller ones are batched, up to kBatchPoints transform points per batch.
+constexpr int kAloneLogN = 20;
+constexpr u64 kBatchPoints = 1ull << 22;
+
 // Scratch a request is charged: its product workspace (as one batch of one, an upper
 // bound of its share of a batch) plus a server-owned output when it has none.
 size_t request_bytes(const fmn_request& r, bool reuse) {
@@ -190,8 +203,8 @@ bool launch_batch(fmn_server* s, Slot* sl, const std::vector<size_t>& idx) {
         jobs[k] = to_job(r, reuse, r.out);
     }
     // outputs owned by the server live after the batch workspace
-    size_t ws_bytes = s->batching ? fmn::batch_workspace_bytes(jobs.data(), (int)jobs.size())
-                                  : fmn::job_workspace_bytes(jobs[0]);
+    const bool single = jobs.size() == 1;
+    size_t ws_bytes = single ? fmn::job_workspace_bytes(jobs[0]) : fmn::batch_workspace_bytes(jobs.data(), (int)jobs.size());
     ws_bytes = align256(ws_bytes);
     const size_t total = ws_bytes + out_bytes;
     void* mem = nullptr;
@@ -213,7 +226,7 @@ bool launch_batch(fmn_server* s, Slot* sl, const std::vector<size_t>& idx) {
     }
     cudaError_t e = cudaMemsetAsync(mem, 0, 256, sl->stream);     // status word
     if (e == cudaSuccess) {
-        if (s->batching) {
+        if (!single) {
             const size_t sb = fmn::batch_stage_bytes(jobs.data(), (int)jobs.size());
             if (sl->stage_cap < sb) {
                 if (sl->stage) cudaFreeHost(sl->stage);
@@ -225,7 +238,8 @@ bool launch_batch(fmn_server* s, Slot* sl, const std::vector<size_t>& idx) {
                                                sl->stream, nullptr, nullptr, 0, server_twiddles, s)
                           : cudaErrorMemoryAllocation;
         } else {
-            const int n = jobs[0].la && jobs[0].lb ? ilog2c(jobs[0].la + jobs[0].lb - 1) : 0;
+            const int n = jobs[0].spectrum ? jobs[0].log_n
+                          : (jobs[0].la && jobs[0].lb ? ilog2c(jobs[0].la + jobs[0].lb - 1) : 0);
             e = fmn::enqueue_job(jobs[0], mem, ws_bytes, sl->stream, server_twiddles(s, n));
         }
     }
@@ -283,46 +297,67 @@ void dispatcher(fmn_server* s) {
                 progress = true;
             }
         if (progress) s->cv.notify_all();
-        // admission: in arrival order, while budget and a slot allow
-        while (!s->pending.empty()) {
-            Slot* free_slot = nullptr;
-            for (Slot* sl : s->slots)
-                if (!sl->busy) {
-                    free_slot = sl;
-                    break;
-                }
-            if (!free_slot) break;
-            std::vector<size_t> take;
-            size_t bytes = 0;
-            const bool reuse = s->batching != 0;
-            while (!s->pending.empty() && (int)take.size() < s->max_batch) {
-                const size_t i = s->pending.front();
-                const size_t b = request_bytes(s->log[i].r, reuse);
-                if (b > s->budget) {               // can never fit: reject
-                    s->pending.pop_front();
-                    s->log[i].done = clk::now();
-                    s->log[i].bytes = 0;
-                    ++s->rejected;
-                    s->completed_order.push_back(i);
-                    continue;
-                }
-                if (s->in_use + bytes + b > s->budget) break;
-                bytes += b;
-                take.push_back(i);
-                s->pending.pop_front();
+        // admission, each queue in arrival order, while budget and a slot allow.  Batching
+        // mode: slot 0 takes large products one at a time (each fills the GPU), the other
+        // slots take batches of small ones, so small requests never queue behind large ones.
+        auto reject_if_too_big = [&](std::deque<size_t>& q) {
+            while (!q.empty() && request_bytes(s->log[q.front()].r, s->batching != 0) > s->budget) {
+                const size_t i = q.front();
+                q.pop_front();
+                s->log[i].done = clk::now();
+                ++s->rejected;
+                s->completed_order.push_back(i);
             }
-            if (take.empty()) break;
-            if (!launch_batch(s, free_slot, take)) {
+        };
+        auto launch_or_fail = [&](Slot* sl, const std::vector<size_t>& take) {
+            if (!launch_batch(s, sl, take))
                 for (size_t i : take) {                // could not launch: fail these requests
                     s->log[i].done = clk::now();
                     ++s->failures;
                     s->completed_order.push_back(i);
                 }
-            }
             progress = true;
+        };
+        if (s->batching) {
+            reject_if_too_big(s->big);
+            if (!s->big.empty() && !s->slots[0]->busy) {
+                const size_t i = s->big.front();
+                if (s->in_use + request_bytes(s->log[i].r, true) <= s->budget) {
+                    s->big.pop_front();
+                    launch_or_fail(s->slots[0], std::vector<size_t>{i});
+                }
+            }
+        }
+        while (true) {
+            reject_if_too_big(s->pending);
+            if (s->pending.empty()) break;
+            Slot* free_slot = nullptr;
+            for (size_t k = s->batching ? 1 : 0; k < s->slots.size(); ++k)
+                if (!s->slots[k]->busy) {
+                    free_slot = s->slots[k];
+                    break;
+                }
+            if (!free_slot) break;
+            std::vector<size_t> take;
+            size_t bytes = 0;
+            u64 points = 0;
+            const bool reuse = s->batching != 0;
+            while (!s->pending.empty() && (int)take.size() < s->max_batch) {
+                const size_t i = s->pending.front();
+                const size_t b = request_bytes(s->log[i].r, reuse);
+                const int n = request_log_n(s->log[i].r, reuse);
+                if (!take.empty() && points + (1ull << n) > kBatchPoints) break;
+                if (s->in_use + bytes + b > s->budget) break;
+                bytes += b;
+                points += 1ull << n;
+                take.push_back(i);
+                s->pending.pop_front();
+            }
+            if (take.empty()) break;
+            launch_or_fail(free_slot, take);
         }
         if (s->completed_order.size() != done_before) s->cv.notify_all();
-        if (s->stop && s->pending.empty()) {
+        if (s->stop && s->pending.empty() && s->big.empty()) {
             bool busy = false;
             for (Slot* sl : s->slots) busy |= sl->busy;
             if (!busy) break;
@@ -479,7 +514,9 @@ static int submit_at(fmn_server* s, const fmn_request* r, clk::time_point arriva
         q.done = clk::time_point();
         q.bytes = 0;
         s->log.push_back(q);
-        s->pending.push_back(s->log.size() - 1);
+        const size_t i = s->log.size() - 1;
+        if (s->batching && request_log_n(*r, true) >= kAloneLogN) s->big.push_back(i);
+        else s->pending.push_back(i);
     }
     s->cv.notify_all();
     return FMN_OK;
