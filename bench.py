@@ -82,6 +82,24 @@ def digest(x):
     return hashlib.sha256(np.ascontiguousarray(x, dtype="<u8").tobytes()).hexdigest()
 
 
+# ----------------------------------------------------------------------------- ranks
+def max_over_ranks(x, device=None):
+    """Max of a per-rank float over all ranks of the default process group (the timing rule:
+    the slowest rank bounds the whole job); returns x itself without a process group."""
+    import torch
+    import torch.distributed as tdist
+    if not (tdist.is_available() and tdist.is_initialized()) or tdist.get_world_size() == 1:
+        return float(x)
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_throughput(world_size, steps, max_seconds):
+    """Whole-job products/s of replicated products: every rank completed `steps` products."""
+    return world_size * steps / max_seconds
+
+
 # ----------------------------------------------------------------------------- clocks
 class ClockSampler:
     """Samples SM clock and clock-event (throttle) reasons through NVML in a thread."""
@@ -443,12 +461,8 @@ def run_ours(args, ws, rank, local):
     fmn.profile_enable(False)
     prof = fmn.profile_take()
     fmn.sync(stream)
-    ms = ev0.elapsed_time(ev1)
-    if dist:
-        t = torch.tensor([ms], device=dev, dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
-    value = ws * args.steps / (ms * 1e-3)
+    ms = max_over_ranks(ev0.elapsed_time(ev1), dev)
+    value = job_throughput(ws, args.steps, ms * 1e-3)
 
     # e2e through the reference-facing C ABI with pinned host buffers
     lib = fmn.load_library()
@@ -463,11 +477,7 @@ def run_ours(args, ws, rank, local):
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
         lib.abs_mul64(pa, l1, pb, l2, po)
-    e2e_s = time.perf_counter() - t0
-    if dist:
-        t = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks(time.perf_counter() - t0, dev)
     barrier()
     e2e_exact = bool(np.array_equal(hout, got))
 
