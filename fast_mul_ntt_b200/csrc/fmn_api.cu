@@ -60,6 +60,7 @@ struct DevCtx {
     size_t stage_cap = 0;
     cudaEvent_t stage_free = nullptr;   // the last batch's descriptor copy has completed
     bool stage_pending = false;
+    cudaEvent_t cb_event[4] = {nullptr};   // chunked copy-back of host products
 };
 
 std::mutex g_ctx_mu;
@@ -94,6 +95,7 @@ int get_ctx(DevCtx** out) {
         for (int k = 0; k <= DevCtx::NSTREAM && e == cudaSuccess; ++k)
             e = cudaEventCreateWithFlags(&c->wevent[k], cudaEventDisableTiming);
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->stage_free, cudaEventDisableTiming);
+        for (int k = 0; k < 4 && e == cudaSuccess; ++k) e = cudaEventCreateWithFlags(&c->cb_event[k], cudaEventDisableTiming);
         if (e != cudaSuccess) {
             delete c;
             return set_err(FMN_ERR_CUDA, "creating device context streams", e);
@@ -239,6 +241,84 @@ int take_device_error(void* ws, unsigned* h_word, cudaStream_t s) {
     return FMN_OK;
 }
 
+bool is_pinned(const void* p) {
+    cudaPointerAttributes at;
+    if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return at.type == cudaMemoryTypeHost;
+}
+
+struct CopyBack {
+    cudaStream_t main, copy;
+    cudaEvent_t ev[4];
+    int used;
+    u64* dst;
+    const u64* src;
+};
+
+cudaError_t copy_back_chunk(void* p, u64 lo, u64 hi) {
+    CopyBack* cb = (CopyBack*)p;
+    cudaEvent_t ev = cb->ev[cb->used++ % 4];
+    cudaError_t e = cudaEventRecord(ev, cb->main);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(cb->copy, ev, 0);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(cb->dst + lo, cb->src + lo, (hi - lo) * sizeof(u64), cudaMemcpyDeviceToHost, cb->copy);
+    return e;
+}
+
+// Host product on pinned buffers: in2 is copied on a second stream while in1's forward
+// passes run, and the output comes back in chunks as the carry scan finishes them.
+int host_product_pinned(DevCtx* c, const u64* in1, u64 len1, const u64* in2, u64 len2, u64* out, int sqr) {
+    const u64 out_len = len1 + len2;
+    const size_t o1 = 0, o2 = round256(len1 * 8), oo = o2 + (sqr ? 0 : round256(len2 * 8));
+    int rc;
+    if ((rc = ensure_io(c, oo + round256(out_len * 8)))) return rc;
+    char* io = (char*)c->io;
+    cudaStream_t s = c->stream, cs = c->wstream[0];
+    cudaError_t e;
+    fmn::Job j;
+    j.a = (const u64*)(io + o1);
+    j.la = len1;
+    j.b = sqr ? j.a : (const u64*)(io + o2);
+    j.lb = len2;
+    j.out = (u64*)(io + oo);
+    j.sqr = sqr;
+    const size_t need = fmn::job_workspace_bytes(j);
+    if ((rc = ensure_ws(c, need))) return rc;
+    if (c->done_valid && ((e = cudaStreamWaitEvent(s, c->done, 0)) != cudaSuccess ||
+                          (e = cudaStreamWaitEvent(cs, c->done, 0)) != cudaSuccess))
+        return set_err(FMN_ERR_CUDA, "cudaStreamWaitEvent", e);
+    const fmn::TwiddleSet* tws = get_twiddles(c, ilog2_ceil(out_len - 1), s);
+    if ((e = cudaMemcpyAsync(io + o1, in1, len1 * 8, cudaMemcpyHostToDevice, s)) != cudaSuccess)
+        return set_err(FMN_ERR_CUDA, "copying in1 to the device", e);
+    cudaEvent_t b_ready = nullptr;
+    if (!sqr) {
+        if ((e = cudaMemcpyAsync(io + o2, in2, len2 * 8, cudaMemcpyHostToDevice, cs)) != cudaSuccess ||
+            (e = cudaEventRecord(c->wevent[1], cs)) != cudaSuccess)
+            return set_err(FMN_ERR_CUDA, "copying in2 to the device", e);
+        b_ready = c->wevent[1];
+    }
+    CopyBack cb;
+    cb.main = s;
+    cb.copy = cs;
+    cb.used = 0;
+    cb.dst = out;
+    cb.src = j.out;
+    for (int k = 0; k < 4; ++k) cb.ev[k] = c->cb_event[k];
+    const int chunks = out_len >= (1u << 20) ? 4 : 1;
+    if ((e = fmn::enqueue_job_overlapped(j, c->ws, c->ws_cap, s, tws, b_ready, chunks, copy_back_chunk, &cb)) !=
+        cudaSuccess)
+        return set_err(FMN_ERR_CUDA, "kernel launch", e);
+    // the copy stream ends after the last chunk; order the main stream (and later jobs) after it
+    if ((e = cudaEventRecord(c->wevent[2], cs)) != cudaSuccess || (e = cudaStreamWaitEvent(s, c->wevent[2], 0)) != cudaSuccess)
+        return set_err(FMN_ERR_CUDA, "joining the copy stream", e);
+    if ((e = cudaEventRecord(c->done, s)) != cudaSuccess) return set_err(FMN_ERR_CUDA, "cudaEventRecord", e);
+    c->done_valid = true;
+    return take_device_error(c->ws, c->h_err, s);
+}
+
 int host_product(const u64* in1, u64 len1, const u64* in2, u64 len2, u64* out, int sqr) {
     const u64 out_len = len1 + len2;
     if (out_len == 0) return FMN_OK;
@@ -252,6 +332,11 @@ int host_product(const u64* in1, u64 len1, const u64* in2, u64 len2, u64* out, i
     DevCtx* c;
     if ((rc = get_ctx(&c))) return rc;
     std::lock_guard<std::mutex> lk(c->mu);
+    // pinned buffers that do not overlap each other: overlapped copies
+    if (is_pinned(in1) && (sqr || is_pinned(in2)) && is_pinned(out) &&
+        ((const char*)out + (len1 + len2) * 8 <= (const char*)in1 || (const char*)out >= (const char*)(in1 + len1)) &&
+        (sqr || (const char*)out + (len1 + len2) * 8 <= (const char*)in2 || (const char*)out >= (const char*)(in2 + len2)))
+        return host_product_pinned(c, in1, len1, in2, len2, out, sqr);
     // device layout: [in1][in2][out], each 256-byte aligned
     const size_t o1 = 0, o2 = round256(len1 * 8), oo = o2 + (sqr ? 0 : round256(len2 * 8));
     if ((rc = ensure_io(c, oo + round256(out_len * 8)))) return rc;
@@ -393,6 +478,8 @@ void fmn_shutdown(void) {
         for (int k = 0; k <= DevCtx::NSTREAM; ++k)
             if (c->wevent[k]) cudaEventDestroy(c->wevent[k]);
         if (c->stage_free) cudaEventDestroy(c->stage_free);
+        for (int k = 0; k < 4; ++k)
+            if (c->cb_event[k]) cudaEventDestroy(c->cb_event[k]);
         if (c->done) cudaEventDestroy(c->done);
         if (c->stream) cudaStreamDestroy(c->stream);
         delete c;

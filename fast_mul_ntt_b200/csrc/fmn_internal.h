@@ -70,6 +70,14 @@ cudaError_t build_twiddle_tables(int log_n, u64* buf, TwiddleSet* out, cudaStrea
 cudaError_t enqueue_job(const Job& job, void* ws, size_t ws_bytes, cudaStream_t stream,
                         const TwiddleSet* tw = nullptr);
 
+// A product with copy overlap: launches that read the second operand wait for `b_ready`
+// (its host-to-device copy on another stream), and the carry scan runs in `crt_chunks`
+// launches; after each, `after_chunk(ctx, first_limb, end_limb)` is called so the caller can
+// copy those final limbs back while the next chunk computes.
+typedef cudaError_t (*ChunkDone)(void* ctx, u64 first_limb, u64 end_limb);
+cudaError_t enqueue_job_overlapped(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s, const TwiddleSet* tw,
+                                   cudaEvent_t b_ready, int crt_chunks, ChunkDone after_chunk, void* ctx);
+
 // ---- batches of products
 // Workspace bytes for a batch (device) and host staging bytes for its launch descriptors.
 size_t batch_workspace_bytes(const Job* jobs, int count);

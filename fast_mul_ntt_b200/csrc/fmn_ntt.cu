@@ -1206,6 +1206,7 @@ struct LaunchRec {
     int variant, logl;
     PassArgs pa;
     u64 tiles;
+    bool needs_b;     // reads the second operand's limbs
 };
 struct JobLaunches {
     int count;
@@ -1240,6 +1241,7 @@ static void plan_job(const Job& j, const JobScratch& sc, const TwiddleSet* tws, 
         r.logl = logl;
         r.pa = pa;
         r.tiles = tiles;
+        r.needs_b = !sqr && j.b && pa.src == j.b;
     };
     PassArgs pa;
     memset(&pa, 0, sizeof(pa));
@@ -1376,6 +1378,43 @@ cudaError_t enqueue_job(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s,
     }
     if ((e = cudaMemsetAsync(base + w.ticket, 0, w.total - w.ticket, s)) != cudaSuccess) return e;
     return launch_crt(L.crt, L.ncta, s);
+}
+
+cudaError_t enqueue_job_overlapped(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s, const TwiddleSet* tws,
+                                   cudaEvent_t b_ready, int crt_chunks, ChunkDone after_chunk, void* ctx) {
+    const u64 out_len = j.la + j.lb;
+    if (j.la == 0 || j.lb == 0 || out_len == 0) return cudaErrorInvalidValue;
+    const int sqr = j.sqr ? 1 : 0;
+    const WsLayout w = ws_layout(j.la, j.lb, sqr, j.spectrum ? j.log_n : 0);
+    if (ws_bytes < w.total || w.n > MAX_LOG_N) return cudaErrorInvalidValue;
+    cudaError_t e = ensure_tables();
+    if (e != cudaSuccess) return e;
+    char* base = (char*)ws;
+    JobScratch sc{(u64*)(base + w.a), (u64*)(base + w.b), (u32*)(base + w.ticket), (u32*)(base + w.state),
+                  (u32*)base};
+    JobLaunches L;
+    plan_job(j, sc, tws, &L);
+    bool waited = false;
+    for (int k = 0; k < L.count; ++k) {
+        const LaunchRec& r = L.rec[k];
+        if (r.needs_b && !waited && b_ready) {          // second operand copied meanwhile
+            if ((e = cudaStreamWaitEvent(s, b_ready, 0)) != cudaSuccess) return e;
+            waited = true;
+        }
+        if ((e = launch_pass(r.variant, r.logl, r.pa, r.tiles, s)) != cudaSuccess) return e;
+    }
+    if ((e = cudaMemsetAsync(base + w.ticket, 0, w.total - w.ticket, s)) != cudaSuccess) return e;
+    // carry scan in chunks of CTAs: tickets continue across launches, each chunk's limbs are
+    // final once its launch completes
+    if (crt_chunks < 1) crt_chunks = 1;
+    const u64 per = (L.ncta + crt_chunks - 1) / crt_chunks;
+    for (u64 t0 = 0; t0 < L.ncta; t0 += per) {
+        const u64 n = t0 + per <= L.ncta ? per : L.ncta - t0;
+        if ((e = launch_crt(L.crt, n, s)) != cudaSuccess) return e;
+        const u64 lo = t0 * CTILE, hi = (t0 + n) * CTILE < out_len ? (t0 + n) * CTILE : out_len;
+        if (after_chunk && (e = after_chunk(ctx, lo, hi)) != cudaSuccess) return e;
+    }
+    return cudaSuccess;
 }
 
 // ------------------------------------------------------------------ batches

@@ -97,6 +97,24 @@ def test_same_block_is_square(fmn, oracle):
     assert np.array_equal(out, oracle.sqr(a))
 
 
+def test_pinned_host_buffers(fmn, oracle):
+    """abs_mul64 / abs_sqr64 on pinned host memory take the overlapped path (second operand
+    copied while the first is transformed, output copied back in chunks)."""
+    import torch
+    lib = fmn.load_library()
+    P = ctypes.POINTER(ctypes.c_uint64)
+    for la, lb in [(600000, 700001), (5, 3), (1 << 19, 1 << 19)]:
+        a, b = synth.operands("uniform", la, lb, 31)
+        ha = torch.from_numpy(a.view(np.int64)).pin_memory().numpy().view(np.uint64)
+        hb = torch.from_numpy(b.view(np.int64)).pin_memory().numpy().view(np.uint64)
+        ho = torch.zeros(la + lb, dtype=torch.int64).pin_memory().numpy().view(np.uint64)
+        lib.abs_mul64(ha.ctypes.data_as(P), la, hb.ctypes.data_as(P), lb, ho.ctypes.data_as(P))
+        assert np.array_equal(ho, oracle.mul(a, b)), (la, lb)
+        hs = torch.zeros(2 * la, dtype=torch.int64).pin_memory().numpy().view(np.uint64)
+        lib.abs_sqr64(ha.ctypes.data_as(P), la, hs.ctypes.data_as(P))
+        assert np.array_equal(hs, oracle.sqr(a)), la
+
+
 def test_device_api_and_caller_workspace(fmn, oracle):
     import torch
     a, b = synth.operands("uniform", 70000, 50000, 21)
