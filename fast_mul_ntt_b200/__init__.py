@@ -31,7 +31,8 @@ EXPORTS = ["abs_mul64", "abs_sqr64", "fmn_init", "fmn_shutdown", "fmn_last_error
            "fmn_batch_graph_create", "fmn_batch_graph_launch", "fmn_batch_graph_sync", "fmn_batch_graph_destroy",
            "fmn_operand_create", "fmn_operand_destroy", "fmn_operand_len", "fmn_mul_operand_device",
            "fmn_operand_workspace_size", "fmn_mul_operand_ws", "fmn_server_create", "fmn_server_submit",
-           "fmn_server_wait", "fmn_server_take", "fmn_server_get_stats", "fmn_server_replay", "fmn_server_destroy"]
+           "fmn_server_wait", "fmn_server_take", "fmn_server_get_stats", "fmn_server_replay", "fmn_server_destroy",
+           "fmn_get_plan", "fmn_set_plan", "fmn_autotune", "fmn_load_plans", "fmn_load_default_plans"]
 
 FMN_OP_MUL, FMN_OP_SQR, FMN_OP_MUL_OPERAND = 0, 1, 2
 
@@ -157,6 +158,17 @@ def load_library(path=None):
     lib.fmn_server_replay.restype = ctypes.c_int
     lib.fmn_server_destroy.argtypes = [_vp]
     lib.fmn_server_destroy.restype = None
+    _ip = ctypes.POINTER(ctypes.c_int)
+    lib.fmn_get_plan.argtypes = [ctypes.c_int, _ip, ctypes.c_int]
+    lib.fmn_get_plan.restype = ctypes.c_int
+    lib.fmn_set_plan.argtypes = [ctypes.c_int, _ip, ctypes.c_int]
+    lib.fmn_set_plan.restype = ctypes.c_int
+    lib.fmn_autotune.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_char_p]
+    lib.fmn_autotune.restype = ctypes.c_int
+    lib.fmn_load_plans.argtypes = [ctypes.c_char_p]
+    lib.fmn_load_plans.restype = ctypes.c_int
+    lib.fmn_load_default_plans.argtypes = []
+    lib.fmn_load_default_plans.restype = ctypes.c_int
     if path is None:
         _lib = lib
     return lib
@@ -418,3 +430,28 @@ class Server:
             self.close()
         except Exception:
             pass
+
+
+PLAN_DIR = os.path.join(HERE, "tune")
+
+
+def get_plan(log_n):
+    """Pass bits of the plan in effect for 2^log_n points."""
+    bits = (ctypes.c_int * 4)()
+    p = load_library().fmn_get_plan(log_n, bits, 4)
+    if p < 0:
+        raise FastMulError(-p, "bad length")
+    return [bits[i] for i in range(p)]
+
+
+def set_plan(log_n, bits=None):
+    """Replace the plan of 2^log_n points (None restores the default)."""
+    bits = list(bits or [])
+    arr = (ctypes.c_int * max(1, len(bits)))(*bits)
+    _check(load_library().fmn_set_plan(log_n, arr, len(bits)))
+
+
+def autotune(n_lo=10, n_hi=27, save_path=None):
+    """Time every valid plan for 2^n_lo .. 2^n_hi points on the current GPU and keep the
+    fastest; optionally write a plan file."""
+    _check(load_library().fmn_autotune(n_lo, n_hi, save_path.encode() if save_path else None))

@@ -14,7 +14,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIBDIR, "libfastmul_b200.so")
-SOURCES = ["fmn_ntt.cu", "fmn_api.cu", "fmn_noalloc.cu", "fmn_server.cu"]
+SOURCES = ["fmn_ntt.cu", "fmn_api.cu", "fmn_noalloc.cu", "fmn_server.cu", "fmn_tune.cu"]
 HEADERS = ["fmn_arith.cuh", "fmn_internal.h"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
@@ -47,7 +47,7 @@ def build(force=False, verbose=False):
         objs.append(obj)
     tmp = LIB + ".tmp"
     subprocess.run([NVCC, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-o", tmp] + objs +
-                   ["-lcudart"], check=True)
+                   ["-lcudart", "-ldl"], check=True)
     os.replace(tmp, LIB)
     return LIB
 

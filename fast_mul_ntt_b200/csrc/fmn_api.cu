@@ -101,6 +101,7 @@ int get_ctx(DevCtx** out) {
             return set_err(FMN_ERR_CUDA, "creating device context streams", e);
         }
         g_ctx[dev] = c;
+        fmn_load_default_plans();              // tuned plans for this GPU, if a plan file matches
     }
     *out = g_ctx[dev];
     return FMN_OK;
@@ -161,11 +162,18 @@ size_t round256(size_t x) { return (x + 255) & ~(size_t)255; }
 const fmn::TwiddleSet* get_twiddles(DevCtx* c, int log_n, cudaStream_t s) {
     const size_t bytes = fmn::twiddle_table_bytes(log_n);
     if (bytes == 0) return nullptr;
-    for (auto& t : c->tw)
-        if (t.set.log_n == log_n) {
+    const fmn::Plan cur = fmn::make_plan(log_n);
+    for (size_t k = 0; k < c->tw.size(); ++k) {
+        auto& t = c->tw[k];
+        if (t.set.log_n != log_n) continue;
+        if (fmn::same_plan(t.set.plan, cur)) {
             t.last_use = ++c->tick;
             return &t.set;
         }
+        cudaFree(t.buf);                       // built for a plan no longer in effect
+        c->tw.erase(c->tw.begin() + k);
+        break;
+    }
     size_t free_b = 0, total_b = 0;
     if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
         cudaGetLastError();
@@ -221,7 +229,10 @@ int run_job_ctx(DevCtx* c, const fmn::Job& j, cudaStream_t s) {
     if (c->done_valid && (e = cudaStreamWaitEvent(s, c->done, 0)) != cudaSuccess)
         return set_err(FMN_ERR_CUDA, "cudaStreamWaitEvent", e);
     const fmn::TwiddleSet* tws = get_twiddles(c, j.spectrum ? j.log_n : ilog2_ceil(j.la + j.lb - 1), s);
-    if ((e = fmn::enqueue_job(j, c->ws, c->ws_cap, s, tws)) != cudaSuccess) return set_err(FMN_ERR_CUDA, "kernel launch", e);
+    if ((e = fmn::enqueue_job(j, c->ws, c->ws_cap, s, tws)) != cudaSuccess) {
+        std::string m = std::string("kernel launch (") + fmn::launch_diag() + ")";
+        return set_err(FMN_ERR_CUDA, m.c_str(), e);
+    }
     if ((e = cudaEventRecord(c->done, s)) != cudaSuccess) return set_err(FMN_ERR_CUDA, "cudaEventRecord", e);
     c->done_valid = true;
     return FMN_OK;

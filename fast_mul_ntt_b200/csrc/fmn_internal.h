@@ -5,6 +5,8 @@
 #include <stddef.h>
 #include <stdint.h>
 
+#include <vector>
+
 typedef unsigned long long u64;
 
 namespace fmn {
@@ -20,7 +22,13 @@ struct Plan {
     int passes;               // number of passes
     int bits[MAX_PASSES];     // index bits handled by each pass (sum = n)
 };
-Plan make_plan(int log_n);
+Plan make_plan(int log_n);          // the plan in effect (tuned or default)
+Plan default_plan(int log_n);
+bool valid_plan(const Plan& p);
+bool same_plan(const Plan& a, const Plan& b);
+bool set_plan(const Plan& p);       // replaces the plan of p.n; false if invalid
+void clear_plan(int log_n);         // back to the default
+std::vector<Plan> candidate_plans(int log_n);
 
 // One product on the device.  All pointers are device pointers.
 struct Job {
@@ -50,8 +58,9 @@ cudaError_t ensure_tables();
 
 // Precomputed four-step twiddles of every strided pass of one transform length.
 struct TwiddleSet {
-    TwiddleSet() : log_n(0), fwd{}, inv{} {}
+    TwiddleSet() : log_n(0), plan{}, fwd{}, inv{} {}
     int log_n;
+    Plan plan;             // the pass plan the tables were built for
     const u64* fwd[MAX_PASSES];
     const u64* inv[MAX_PASSES];
 };
@@ -94,6 +103,9 @@ cudaError_t enqueue_batch(const Job* jobs, int count, void* ws, size_t ws_bytes,
 // Make sure every batched kernel is configured (call before capturing a batch in a graph).
 cudaError_t prepare_batch();
 
+// Description of the most recent pass launch of this thread (for error messages).
+const char* launch_diag();
+
 // ---- optional per-kernel timing (used by bench.py; off by default)
 // Kernel kinds of the pipeline.
 enum KernelKind { K_FWD = 0, K_FWD_LAST, K_FUSED, K_INV, K_CRT, K_KINDS };
@@ -110,6 +122,9 @@ void profile_enable(bool on);
 cudaError_t profile_take(KindStats* out);
 // Kernel launches one product issues.
 int job_launches(u64 la, u64 lb, int sqr);
+
+// splitmix64 limbs on the device (tuning runs).
+cudaError_t fill_limbs(u64* p, u64 n, u64 seed, cudaStream_t s);
 
 // Throughput microbenchmark of independent Montgomery products (peak of the integer pipe
 // for this arithmetic): returns products per second.

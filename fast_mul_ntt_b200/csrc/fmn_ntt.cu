@@ -22,6 +22,7 @@
 // of one column) access patterns free of bank conflicts.
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <stdio.h>
 #include <string.h>
 
 #include <mutex>
@@ -550,6 +551,7 @@ cudaError_t build_twiddle_tables(int log_n, u64* buf, TwiddleSet* out, cudaStrea
     const Plan pl = make_plan(log_n);
     memset(out, 0, sizeof(*out));
     out->log_n = log_n;
+    out->plan = pl;
     int logB = log_n;
     u64* p = buf;
     for (int k = 0; k + 1 < pl.passes; ++k) {
@@ -991,8 +993,11 @@ cudaError_t ensure_tables() {
     return cudaSuccess;
 }
 
-Plan make_plan(int n) {
+// Pass plans.  The default splits n bits into ceil(n/9) nearly equal passes (larger first);
+// the autotuner (fmn_autotune) or a tuning file may replace the plan of any length.
+Plan default_plan(int n) {
     Plan p;
+    memset(&p, 0, sizeof(p));
     p.n = n;
     if (n <= MAX_PASS_BITS) {
         p.passes = 1;
@@ -1002,6 +1007,92 @@ Plan make_plan(int n) {
     p.passes = (n + MAX_PASS_BITS - 1) / MAX_PASS_BITS;
     for (int i = 0; i < p.passes; ++i) p.bits[i] = n / p.passes + (i < n % p.passes ? 1 : 0);
     return p;
+}
+
+// A plan is valid when its bits add up to n, every strided pass has 5..9 bits and at least
+// 16 columns (4 bits) after it, and the last pass has at most 9 bits.
+bool valid_plan(const Plan& p) {
+    if (p.n < 0 || p.n > MAX_LOG_N || p.passes < 1 || p.passes > MAX_PASSES) return false;
+    int sum = 0;
+    for (int i = 0; i < p.passes; ++i) {
+        if (p.bits[i] < 0 || p.bits[i] > MAX_PASS_BITS) return false;
+        sum += p.bits[i];
+    }
+    if (sum != p.n) return false;
+    if (p.passes == 1) return p.n <= MAX_PASS_BITS;
+    int rest = p.n;
+    for (int i = 0; i + 1 < p.passes; ++i) {
+        rest -= p.bits[i];
+        if (p.bits[i] < 5 || rest < 4) return false;
+    }
+    return p.bits[p.passes - 1] >= 1;
+}
+
+bool same_plan(const Plan& a, const Plan& b) {
+    if (a.n != b.n || a.passes != b.passes) return false;
+    for (int i = 0; i < a.passes; ++i)
+        if (a.bits[i] != b.bits[i]) return false;
+    return true;
+}
+
+static std::mutex g_plan_mu;
+static Plan g_plan_tab[MAX_LOG_N + 1];
+static bool g_plan_set[MAX_LOG_N + 1] = {false};
+
+Plan make_plan(int n) {
+    if (n >= 0 && n <= MAX_LOG_N) {
+        std::lock_guard<std::mutex> lk(g_plan_mu);
+        if (g_plan_set[n]) return g_plan_tab[n];
+    }
+    return default_plan(n);
+}
+
+bool set_plan(const Plan& p) {
+    if (!valid_plan(p)) return false;
+    std::lock_guard<std::mutex> lk(g_plan_mu);
+    g_plan_tab[p.n] = p;
+    g_plan_set[p.n] = true;
+    return true;
+}
+
+void clear_plan(int n) {
+    if (n < 0 || n > MAX_LOG_N) return;
+    std::lock_guard<std::mutex> lk(g_plan_mu);
+    g_plan_set[n] = false;
+}
+
+// Every valid plan of n bits with the default pass count or one more.
+std::vector<Plan> candidate_plans(int n) {
+    std::vector<Plan> out;
+    if (n <= MAX_PASS_BITS) {
+        out.push_back(default_plan(n));
+        return out;
+    }
+    const int p0 = (n + MAX_PASS_BITS - 1) / MAX_PASS_BITS;
+    for (int P = p0; P <= p0 + 1 && P <= MAX_PASSES; ++P) {
+        int b[MAX_PASSES] = {0};
+        // enumerate compositions with each part in [1, 9]
+        std::vector<int> stack;
+        auto rec = [&](auto&& self, int i, int left) -> void {
+            if (i == P - 1) {
+                if (left < 1 || left > MAX_PASS_BITS) return;
+                b[i] = left;
+                Plan p;
+                memset(&p, 0, sizeof(p));
+                p.n = n;
+                p.passes = P;
+                for (int k = 0; k < P; ++k) p.bits[k] = b[k];
+                if (valid_plan(p)) out.push_back(p);
+                return;
+            }
+            for (int m = 5; m <= MAX_PASS_BITS; ++m) {
+                b[i] = m;
+                self(self, i + 1, left - m);
+            }
+        };
+        rec(rec, 0, n);
+    }
+    return out;
 }
 
 static u64 ceil_pow2(u64 x) {
@@ -1061,8 +1152,8 @@ static cudaError_t launch_pass(int variant, int logl, const PassArgs& a, u64 til
 cudaError_t spectrum_enqueue(const u64* src, u64 len, int log_n, u64* spec, cudaStream_t s, const TwiddleSet* tws) {
     cudaError_t e = ensure_tables();
     if (e != cudaSuccess) return e;
-    if (tws && tws->log_n != log_n) tws = nullptr;
     const Plan pl = make_plan(log_n);
+    if (tws && (tws->log_n != log_n || !same_plan(tws->plan, pl))) tws = nullptr;
     const int P = pl.passes;
     const u64 N = 1ull << log_n;
     PassArgs pa;
@@ -1166,8 +1257,13 @@ static int variant_kind(int v) {
     }
 }
 
+static thread_local char g_launch_diag[128];
+const char* launch_diag() { return g_launch_diag; }
+
 static cudaError_t launch_pass(int variant, int logl, const PassArgs& a, u64 tiles, cudaStream_t s) {
     PassKernel k = ktab().k[variant][logl];
+    snprintf(g_launch_diag, sizeof(g_launch_diag), "pass variant %d, %d bits, %llu tiles", variant, logl,
+             (unsigned long long)tiles);
     if (!k) return cudaErrorInvalidValue;
     // algorithmic work of the launch (3 primes)
     const double N = (double)a.N, vec = 3.0 * N * 8.0;
@@ -1197,7 +1293,7 @@ int job_launches(u64 la, u64 lb, int sqr) {
     const Plan pl = make_plan(w.n);
     const int P = pl.passes;
     // forward strided passes (A, and B unless squaring) + A's last pass + fused + inverse + crt
-    if (!sqr && P >= 2 && pl.bits[P - 1] <= 8) return 2 * (P - 1) + 1 + (P - 1) + 1;   // merged last pass
+    if (!sqr && P >= 2 && pl.bits[P - 1] >= 5 && pl.bits[P - 1] <= 8) return 2 * (P - 1) + 1 + (P - 1) + 1;   // merged
     return sqr ? (P - 1) + 1 + (P - 1) + 1 : 2 * (P - 1) + 1 + 1 + (P - 1) + 1;
 }
 
@@ -1233,7 +1329,7 @@ static void plan_job(const Job& j, const JobScratch& sc, const TwiddleSet* tws, 
     const Plan pl = make_plan(w.n);
     const int P = pl.passes;
     const u64 N = w.N;
-    if (tws && tws->log_n != w.n) tws = nullptr;
+    if (tws && (tws->log_n != w.n || !same_plan(tws->plan, pl))) tws = nullptr;
     out->count = 0;
     auto add = [&](int variant, int logl, const PassArgs& pa, u64 tiles) {
         LaunchRec& r = out->rec[out->count++];
@@ -1264,7 +1360,7 @@ static void plan_job(const Job& j, const JobScratch& sc, const TwiddleSet* tws, 
             add(p == 0 ? V_FWD_E : V_FWD, pl.bits[p], pa, N >> (pl.bits[p] + 4));
         }
     };
-    const bool merged = !sqr && !j.spectrum && P >= 2 && lastl <= 8;
+    const bool merged = !sqr && !j.spectrum && P >= 2 && lastl >= 5 && lastl <= 8;   // two tiles fit
     if (j.spectrum) {
         // resident first operand (conv_single, src/fast_mul.c:135-212): only the second
         // operand is transformed; the product lands in A, the spectrum stays intact
@@ -1692,6 +1788,21 @@ size_t batch_stage_bytes(const Job* jobs, int count) {
     for (int i = 0; i < count; ++i)
         desc += (3 * MAX_PASSES + 2) * (sizeof(PassArgs) + 16) + sizeof(CrtArgs) + sizeof(u32) + 32;
     return desc + 4096;
+}
+
+// ------------------------------------------------------------------ synthetic limbs (tuning)
+__global__ void k_fill(u64* p, u64 n, u64 seed) {
+    for (u64 i = blockIdx.x * (u64)blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x) {
+        u64 z = seed + (i + 1) * 0x9E3779B97F4A7C15ull;       // splitmix64
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        p[i] = z ^ (z >> 31);
+    }
+}
+
+cudaError_t fill_limbs(u64* p, u64 n, u64 seed, cudaStream_t s) {
+    k_fill<<<148 * 8, 256, 0, s>>>(p, n, seed);
+    return cudaGetLastError();
 }
 
 // ------------------------------------------------------------------ modmul microbenchmark

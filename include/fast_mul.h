@@ -175,6 +175,23 @@ int fmn_server_replay(fmn_server* s, const fmn_request* reqs, const double* arri
                       double* latency_ms, double* wall_s);
 void fmn_server_destroy(fmn_server* s);
 
+/* ----------------------------------------------------------------- pass plans and tuning
+ * A 2^n-point transform runs as passes of <= 9 index bits each; the split is a plan (e.g.
+ * 2^25: 9+8+8).  Plans come from the default split, from fmn_set_plan, or from a plan file
+ * written by fmn_autotune (which times every valid plan of each length on the current GPU
+ * and keeps the fastest).  The library loads <lib dir>/../tune/plans-<gpu name>.txt (or the
+ * file named by FMN_PLAN_FILE) when a device context is first created, if the file's GPU
+ * name and driver version match.  No counterpart in the reference (its split is fixed). */
+/* Passes of the plan in effect for 2^log_n points, bits written to bits[0..]; < 0 on error. */
+int fmn_get_plan(int log_n, int* bits, int max_passes);
+/* Replace the plan of 2^log_n points (passes == 0 restores the default). */
+int fmn_set_plan(int log_n, const int* bits, int passes);
+/* Time every valid plan for 2^n_lo .. 2^n_hi points and keep the fastest; save to
+ * save_path (if not NULL) as a plan file. */
+int fmn_autotune(int n_lo, int n_hi, const char* save_path);
+int fmn_load_plans(const char* path);
+int fmn_load_default_plans(void);
+
 /* ----------------------------------------------------------------- measurement hooks
  * (no counterpart in the reference; used by bench.py) */
 

@@ -1,0 +1,85 @@
+"""Pass plans: the host-side rules (CPU) and products under non-default plans (GPU)."""
+import numpy as np
+import pytest
+
+import fast_mul_ntt_b200 as fmn
+from fast_mul_ntt_b200 import synth
+
+
+def test_default_plans():
+    for n in (0, 9, 15, 25, 27):
+        fmn.set_plan(n, None)                 # drop any tuned plan loaded by an earlier test
+    assert fmn.get_plan(0) == [0]
+    assert fmn.get_plan(9) == [9]
+    assert fmn.get_plan(15) == [8, 7]
+    assert fmn.get_plan(25) == [9, 8, 8]
+    assert fmn.get_plan(27) == [9, 9, 9]
+    for n in range(0, 31):
+        bits = fmn.get_plan(n)
+        assert sum(bits) == n and all(0 <= b <= 9 for b in bits)
+
+
+def test_committed_plan_file_is_valid():
+    """The B200 plan file shipped beside the library parses into valid plans for 2^10..2^27."""
+    import os
+    path = os.path.join(fmn.PLAN_DIR, "plans-NVIDIA_B200.txt")
+    lines = [l.split("#")[0].split() for l in open(path) if l[0].isdigit()]
+    head = open(path).read()
+    assert "gpu NVIDIA B200" in head and "\ndriver " in head
+    seen = set()
+    for f in lines:
+        n, p, bits = int(f[0]), int(f[1]), [int(x) for x in f[2:2 + int(f[1])]]
+        assert sum(bits) == n and len(bits) == p and all(1 <= b <= 9 for b in bits)
+        assert all(b >= 5 for b in bits[:-1])
+        seen.add(n)
+    assert seen == set(range(10, 28))
+
+
+def test_set_plan_validates_and_restores():
+    with pytest.raises(fmn.FastMulError):
+        fmn.set_plan(25, [10, 8, 7])          # a pass above 9 bits
+    with pytest.raises(fmn.FastMulError):
+        fmn.set_plan(25, [9, 8, 7])           # bits do not add up
+    with pytest.raises(fmn.FastMulError):
+        fmn.set_plan(15, [12, 3])             # strided pass too wide
+    fmn.set_plan(25, [8, 9, 8])
+    try:
+        assert fmn.get_plan(25) == [8, 9, 8]
+    finally:
+        fmn.set_plan(25, None)
+    assert fmn.get_plan(25) == [9, 8, 8]
+
+
+@pytest.mark.gpu
+def test_products_under_every_plan_shape(fmn, oracle):
+    """Alternative splits (2 and 3 passes, last pass 9 bits or fewer) give the same numbers."""
+    import torch
+    cases = {15: [[7, 8], [5, 5, 5], [9, 6]], 18: [[9, 9], [6, 6, 6], [5, 9, 4]], 21: [[9, 6, 6], [5, 8, 8], [7, 7, 7]]}
+    try:
+        for n, plans in cases.items():
+            half = 1 << (n - 1)
+            a, b = synth.operands("uniform", half, half - 3, n)
+            want = oracle.mul(a, b)
+            for bits in plans:
+                fmn.set_plan(n, bits)
+                assert np.array_equal(fmn.abs_mul64(a, b), want), (n, bits)
+                assert np.array_equal(fmn.abs_sqr64(a), oracle.sqr(a)), (n, bits)
+        # a large length against the default plan's (golden-pinned) result
+        n = 24
+        half = 1 << (n - 1)
+        a, b = synth.operands("uniform", half, half, 5)
+        da = torch.from_numpy(a.view(np.int64)).cuda()
+        db = torch.from_numpy(b.view(np.int64)).cuda()
+        ref = torch.empty(2 * half, dtype=torch.int64, device="cuda")
+        fmn.set_plan(n, None)
+        fmn.mul_device(da, db, ref)
+        fmn.sync()
+        for bits in ([8, 8, 8], [9, 7, 8], [7, 8, 9], [6, 6, 6, 6]):
+            fmn.set_plan(n, bits)
+            out = torch.empty_like(ref)
+            fmn.mul_device(da, db, out)
+            fmn.sync()
+            assert torch.equal(out, ref), bits
+    finally:
+        for n in (15, 18, 21, 24):
+            fmn.set_plan(n, None)
