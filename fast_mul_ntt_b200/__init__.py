@@ -32,7 +32,10 @@ EXPORTS = ["abs_mul64", "abs_sqr64", "fmn_init", "fmn_shutdown", "fmn_last_error
            "fmn_operand_create", "fmn_operand_destroy", "fmn_operand_len", "fmn_mul_operand_device",
            "fmn_operand_workspace_size", "fmn_mul_operand_ws", "fmn_server_create", "fmn_server_submit",
            "fmn_server_wait", "fmn_server_take", "fmn_server_get_stats", "fmn_server_replay", "fmn_server_destroy",
-           "fmn_get_plan", "fmn_set_plan", "fmn_autotune", "fmn_load_plans", "fmn_load_default_plans"]
+           "fmn_get_plan", "fmn_set_plan", "fmn_autotune", "fmn_load_plans", "fmn_load_default_plans",
+           "fmn_set_engine", "fmn_get_engine", "fmn_engine_for"]
+
+ENGINE_AUTO, ENGINE_64, ENGINE_32 = 0, 1, 2
 
 FMN_OP_MUL, FMN_OP_SQR, FMN_OP_MUL_OPERAND = 0, 1, 2
 
@@ -169,6 +172,12 @@ def load_library(path=None):
     lib.fmn_load_plans.restype = ctypes.c_int
     lib.fmn_load_default_plans.argtypes = []
     lib.fmn_load_default_plans.restype = ctypes.c_int
+    lib.fmn_set_engine.argtypes = [ctypes.c_int]
+    lib.fmn_set_engine.restype = ctypes.c_int
+    lib.fmn_get_engine.argtypes = []
+    lib.fmn_get_engine.restype = ctypes.c_int
+    lib.fmn_engine_for.argtypes = [_u64, _u64, ctypes.c_int]
+    lib.fmn_engine_for.restype = ctypes.c_int
     if path is None:
         _lib = lib
     return lib
@@ -449,6 +458,21 @@ def set_plan(log_n, bits=None):
     bits = list(bits or [])
     arr = (ctypes.c_int * max(1, len(bits)))(*bits)
     _check(load_library().fmn_set_plan(log_n, arr, len(bits)))
+
+
+def set_engine(engine):
+    """Process-wide residue engine for single products: ENGINE_AUTO (default), ENGINE_64 (the
+    reference's 62-bit primes) or ENGINE_32 (32-bit digits, products up to 2^25 limbs)."""
+    _check(load_library().fmn_set_engine(engine))
+
+
+def get_engine():
+    return load_library().fmn_get_engine()
+
+
+def engine_for(len1, len2, sqr=False):
+    """The engine (ENGINE_64 or ENGINE_32) a product of these lengths runs on."""
+    return load_library().fmn_engine_for(len1, len2, 1 if sqr else 0)
 
 
 def autotune(n_lo=10, n_hi=27, save_path=None):

@@ -228,7 +228,8 @@ int run_job_ctx(DevCtx* c, const fmn::Job& j, cudaStream_t s) {
     cudaError_t e;
     if (c->done_valid && (e = cudaStreamWaitEvent(s, c->done, 0)) != cudaSuccess)
         return set_err(FMN_ERR_CUDA, "cudaStreamWaitEvent", e);
-    const fmn::TwiddleSet* tws = get_twiddles(c, j.spectrum ? j.log_n : ilog2_ceil(j.la + j.lb - 1), s);
+    const fmn::TwiddleSet* tws = fmn::job_engine(j) != fmn::ENGINE_64 ? nullptr
+                                 : get_twiddles(c, j.spectrum ? j.log_n : ilog2_ceil(j.la + j.lb - 1), s);
     if ((e = fmn::enqueue_job(j, c->ws, c->ws_cap, s, tws)) != cudaSuccess) {
         std::string m = std::string("kernel launch (") + fmn::launch_diag() + ")";
         return set_err(FMN_ERR_CUDA, m.c_str(), e);
@@ -301,7 +302,7 @@ int host_product_pinned(DevCtx* c, const u64* in1, u64 len1, const u64* in2, u64
     if (c->done_valid && ((e = cudaStreamWaitEvent(s, c->done, 0)) != cudaSuccess ||
                           (e = cudaStreamWaitEvent(cs, c->done, 0)) != cudaSuccess))
         return set_err(FMN_ERR_CUDA, "cudaStreamWaitEvent", e);
-    const fmn::TwiddleSet* tws = get_twiddles(c, ilog2_ceil(out_len - 1), s);
+    const fmn::TwiddleSet* tws = fmn::job_engine(j) != fmn::ENGINE_64 ? nullptr : get_twiddles(c, ilog2_ceil(out_len - 1), s);
     if ((e = cudaMemcpyAsync(io + o1, in1, len1 * 8, cudaMemcpyHostToDevice, s)) != cudaSuccess)
         return set_err(FMN_ERR_CUDA, "copying in1 to the device", e);
     cudaEvent_t b_ready = nullptr;
@@ -528,6 +529,25 @@ int fmn_sync(void* stream) {
 }
 
 size_t fmn_workspace_size(u64 len1, u64 len2, int sqr) { return fmn::job_workspace_bytes(len1, len2, sqr ? 1 : 0); }
+
+int fmn_set_engine(int engine) {
+    if (engine != FMN_ENGINE_AUTO && engine != FMN_ENGINE_64 && engine != FMN_ENGINE_32)
+        return set_err(FMN_ERR_ARG, "engine must be FMN_ENGINE_AUTO, FMN_ENGINE_64 or FMN_ENGINE_32");
+    fmn::set_default_engine(engine);
+    return FMN_OK;
+}
+
+int fmn_get_engine(void) { return fmn::default_engine(); }
+
+int fmn_engine_for(u64 len1, u64 len2, int sqr) {
+    fmn::Job j;
+    j.a = j.b = nullptr;
+    j.out = nullptr;
+    j.la = len1;
+    j.lb = len2;
+    j.sqr = sqr ? 1 : 0;
+    return fmn::job_engine(j);
+}
 
 int fmn_mul_device_ws(const u64* d_in1, u64 len1, const u64* d_in2, u64 len2, u64* d_out, void* d_ws,
                       size_t ws_bytes, void* stream) {

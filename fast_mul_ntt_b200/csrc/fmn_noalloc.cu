@@ -54,7 +54,15 @@ extern "C" int fmn_mul_device_noalloc(const u64* d_in1, u64 len1, const u64* d_i
         return FMN_OK;
     }
     const int sq = (d_in1 == d_in2 && len1 == len2);
-    const size_t need = fmn::job_workspace_bytes(len1, len2, sq);
+    fmn::Job j;
+    j.a = d_in1;
+    j.la = len1;
+    j.b = d_in2;
+    j.lb = len2;
+    j.out = d_out;
+    j.sqr = sq;
+    j.engine = fmn::ENGINE_64;      // the scratch array is sized for this engine's layout
+    const size_t need = fmn::job_workspace_bytes(j);
     if (out_len - 1 > kNoallocMaxNtt || need > sizeof(g_noalloc_scratch))
         return fmn::api_set_error(FMN_ERR_TOO_LARGE,
                                   "fmn_mul_device_noalloc: product needs a transform above 65536 points "
@@ -76,13 +84,6 @@ extern "C" int fmn_mul_device_noalloc(const u64* d_in1, u64 len1, const u64* d_i
         }
         scratch = g_noalloc_addr[dev];
     }
-    fmn::Job j;
-    j.a = d_in1;
-    j.la = len1;
-    j.b = d_in2;
-    j.lb = len2;
-    j.out = d_out;
-    j.sqr = sq;
     if ((e = cudaMemsetAsync(scratch, 0, sizeof(unsigned), s)) != cudaSuccess)   // status word
         return fmn::api_set_error(FMN_ERR_CUDA, "clearing the status word", e);
     if ((e = fmn::enqueue_job(j, scratch, sizeof(g_noalloc_scratch), s)) != cudaSuccess)

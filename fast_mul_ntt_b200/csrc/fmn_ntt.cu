@@ -25,47 +25,23 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <atomic>
 #include <mutex>
 #include <vector>
 
 #include "fmn_arith.cuh"
+#include "fmn_carry.cuh"
 #include "fmn_internal.h"
+#include "fmn_rounds.cuh"
 
 namespace fmn {
 
 constexpr int NT = 256;           // threads per CTA, NTT passes
 constexpr int TC = 16;            // columns per tile
-constexpr int RT_MAXLOGL = 12;    // round tables cover sub-transforms up to 2^12 points
 constexpr int TWB = 15;           // two-level twiddle tables: w^x = HI[x >> 15] * LO[x & 0x7fff]
 static_assert(2 * TWB == MAX_LOG_N, "two-level table covers roots of order 2^30");
 
-// ------------------------------------------------------------------ round structure
-// A 2^m-point sub-transform is done in rounds of radix 2^RB held in registers.
-__host__ __device__ constexpr int rounds_count(int logl) {
-    return logl == 0 ? 0 : logl <= 4 ? 1 : logl <= 8 ? 2 : 3;
-}
-__host__ __device__ constexpr int round_bits(int logl, int idx) {
-    return logl <= 4 ? logl
-         : logl <= 8 ? (idx == 0 ? (logl + 1) / 2 : logl / 2)
-                     : (idx == 0 ? (logl + 2) / 3 : idx == 1 ? (logl + 1) / 3 : logl / 3);
-}
-__host__ __device__ constexpr int round_top(int logl, int idx) {
-    return idx == 0 ? logl - 1 : round_top(logl, idx - 1) - round_bits(logl, idx - 1);
-}
-
-// Round twiddle tables.  For a round of RB bits whose top index bit is TOP, the group with
-// low offset q (q < 2^(TOP-RB+1)) needs, for stage s (span 2^(TOP-s)) and u < 2^(RB-1-s):
-//     w_{2^(TOP-s+1)}^(q + u * 2^(TOP-RB+1))
-// stored at rt_off(RB, TOP) + q * 2^RB + (2^RB - 2^(RB-s)) + u (entry 2^RB - 1 is padding).
-__host__ __device__ constexpr int rt_base(int r) {
-    return r <= 1 ? 0 : rt_base(r - 1) + (1 << (r - 1)) * ((1 << (RT_MAXLOGL - r + 2)) - 1);
-}
-__host__ __device__ constexpr int rt_off(int r, int top) {
-    return rt_base(r) + (1 << r) * ((1 << (top - r + 1)) - 1);
-}
-constexpr int RT_SIZE = rt_base(5);
-
-__device__ __align__(16) u64 g_rt[2][3][RT_SIZE];      // [forward/inverse][prime]
+__device__ __align__(16) ulonglong2 g_rt[2][3][RT_SIZE];   // [forward/inverse][prime]: (w, w') Shoup pairs
 __device__ __align__(16) u64 g_tw[2][3][1 << TWB];     // [low/high level][prime]
 __constant__ PrimeRT c_prime[3] = {prime_rt<0>(), prime_rt<1>(), prime_rt<2>()};
 
@@ -104,7 +80,7 @@ __device__ __forceinline__ void run_round(LD ld, ST st, int pi, const PrimeRT& q
     constexpr int GPC = L / R;
     constexpr int G = GPC * TC;
     constexpr bool LOWEST = (SPL == 0);
-    const u64* tab = &g_rt[INV ? 1 : 0][pi][rt_off(RB, TOP)];
+    const ulonglong2* tab = &g_rt[INV ? 1 : 0][pi][rt_off(RB, TOP)];
 #pragma unroll 1
     for (int gi = threadIdx.x; gi < G; gi += NT) {
         int c, g;
@@ -124,7 +100,7 @@ __device__ __forceinline__ void run_round(LD ld, ST st, int pi, const PrimeRT& q
 #pragma unroll
             for (int t = 0; t < R; ++t) x[t] = ld(row0 + t * SP, c);
         }
-        const u64* tw = tab + qlo * R;
+        const ulonglong2* tw = tab + qlo * R;
         if (!INV) {
 #pragma unroll
             for (int s = 0; s < RB; ++s) {
@@ -216,7 +192,7 @@ __device__ __forceinline__ void rounds(u64* sm, LD0 ld0, STL stl, int pi, const 
 
 // ------------------------------------------------------------------ pass bodies
 __device__ __forceinline__ u64 entry_val(const u64* __restrict__ src, u64 len, u64 g, const PrimeRT& q) {
-    return g < len ? mmul(__ldg(src + g), q.r2, q) : 0ull;   // limb * R mod p
+    return g < len ? smul(__ldg(src + g), 1ull, q.r64, q) : 0ull;   // limb mod p, in [0, 2p)
 }
 
 // Four-step twiddles of a strided pass.  After the sub-transform, element (row j, column c)
@@ -361,8 +337,8 @@ __device__ __forceinline__ void fused_lowest(LD ld, ST st, const u64* __restrict
     constexpr int RB = round_bits(LOGL, NR - 1);
     constexpr int R = 1 << RB;
     constexpr int G = (L / R) * TC;
-    const u64* tf = &g_rt[0][pi][rt_off(RB, RB - 1)];
-    const u64* ti = &g_rt[1][pi][rt_off(RB, RB - 1)];
+    const ulonglong2* tf = &g_rt[0][pi][rt_off(RB, RB - 1)];
+    const ulonglong2* ti = &g_rt[1][pi][rt_off(RB, RB - 1)];
 #pragma unroll 1
     for (int gi = threadIdx.x; gi < G; gi += NT) {
         const int c = gi & (TC - 1);
@@ -575,12 +551,6 @@ cudaError_t build_twiddle_tables(int log_n, u64* buf, TwiddleSet* out, cudaStrea
 // carry by a function {0..3} -> {0..3} (packed as 4 x 2 bits); these compose associatively,
 // which gives a parallel scan: per-thread functions, a CTA scan, and a decoupled look-back
 // across CTAs in the order CTAs obtain tickets.
-constexpr int CNT = 256;           // threads per CTA
-constexpr int CE = 16;             // limbs per thread
-constexpr int CTILE = CNT * CE;    // limbs per CTA
-constexpr u32 ID_FN = 0xE4;        // identity map
-constexpr u32 ST_AGG = 1u << 8, ST_PRE = 2u << 8;
-constexpr long SPIN_LIMIT = 1l << 22;   // bounded waits: ~ seconds at most, then error flag
 
 struct CrtArgs {
     const u64* res;     // three natural-order residue arrays (prime i at res + i*N), < 4p
@@ -588,7 +558,7 @@ struct CrtArgs {
     u64 nvalid;         // coefficients that may be nonzero: min(conv_len, N)
     u64* out;
     u64 out_len;
-    u64 cst[3];         // M_i^-1 * N^-1 mod p_i (plain)
+    u64 cst[3];         // M_i^-1 * N^-1 * 2^128 mod p_i (undoes the two Montgomery products)
     u32* state;         // per-CTA look-back words, zeroed before launch
     u32* ticket;        // zeroed before launch
     u32* err;
@@ -652,30 +622,11 @@ __device__ __forceinline__ void crt_coef(const CrtArgs& a, u64 j, u64& w0, u64& 
     crt_of(a.res[j], a.res[a.N + j], a.res[2 * a.N + j], a.cst, w0, w1, w2, q0, q1, q2);
 }
 
-__device__ __forceinline__ u32 fn_apply(u32 f, u32 c) { return (f >> (2 * c)) & 3u; }
-__device__ __forceinline__ u32 fn_compose(u32 later, u32 earlier) {   // later o earlier
-    u32 r = 0;
-#pragma unroll
-    for (u32 c = 0; c < 4; ++c) r |= fn_apply(later, fn_apply(earlier, c)) << (2 * c);
-    return r;
-}
-
-// Adds x to the limb sum (lo, h): lo += x, carry into the 2-bit high part.
-__device__ __forceinline__ void add_to(u64& lo, u32& h, u64 x) {
-    lo += x;
-    h += lo < x;
-}
-
 __device__ __forceinline__ void crt_carry_body(const CrtArgs& a, u32 ncta) {
-    __shared__ u32 s_tile;
     __shared__ u64 s_hw[CNT / 32][3];
-    __shared__ u32 s_warp[CNT / 32];
-    __shared__ u32 s_cin;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const PrimeRT q0 = c_prime[0], q1 = c_prime[1], q2 = c_prime[2];
-    if (tid == 0) s_tile = atomicAdd(a.ticket, 1u);
-    __syncthreads();
-    const u64 tile = s_tile;
+    const u64 tile = carry_ticket(a.ticket);
     if (tile >= ncta) return;                   // batch launches cover the largest product
     const u64 j0 = tile * CTILE + (u64)tid * CE;
 
@@ -739,107 +690,7 @@ __device__ __forceinline__ void crt_carry_body(const CrtArgs& a, u32 ncta) {
     add_to(lo[0], h[0], n3);
     add_to(lo[1], h[1], n2);
 
-    // carry-transfer function of this thread's limbs
-    u32 f = 0;
-#pragma unroll
-    for (u32 cin = 0; cin < 4; ++cin) {
-        u64 c = cin;
-#pragma unroll
-        for (int e = 0; e < CE; ++e) {
-            const u64 t = lo[e] + c;
-            c = h[e] + (t < c);
-        }
-        f |= (u32)c << (2 * cin);
-    }
-    // CTA scan: Kogge-Stone in each warp, then over the warps in warp 0
-    u32 inc = f;
-#pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-        const u32 o = __shfl_up_sync(0xffffffffu, inc, d);
-        if (lane >= d) inc = fn_compose(inc, o);
-    }
-    u32 exc = __shfl_up_sync(0xffffffffu, inc, 1);
-    if (lane == 0) exc = ID_FN;
-    if (lane == 31) s_warp[warp] = inc;
-    __syncthreads();
-    if (warp == 0) {
-        u32 wt = lane < CNT / 32 ? s_warp[lane] : ID_FN;
-#pragma unroll
-        for (int d = 1; d < CNT / 32; d <<= 1) {
-            const u32 o = __shfl_up_sync(0xffffffffu, wt, d);
-            if (lane >= d) wt = fn_compose(wt, o);
-        }
-        u32 wex = __shfl_up_sync(0xffffffffu, wt, 1);
-        if (lane == 0) wex = ID_FN;
-        const u32 agg = __shfl_sync(0xffffffffu, wt, CNT / 32 - 1);
-        if (lane < CNT / 32) s_warp[lane] = wex;       // exclusive prefix of each warp
-        u32 cin = 0;
-        if (tile == 0) {
-            if (lane == 0) atomicExch(&a.state[0], ST_PRE | fn_apply(agg, 0));
-        } else {
-            if (lane == 0) atomicExch(&a.state[tile], ST_AGG | agg);
-            // warp-parallel look-back over the 32 nearest predecessors at a time
-            volatile u32* st = a.state;
-            u32 acc = ID_FN;
-            long base = (long)tile - 1;
-            bool failed = false;
-            while (true) {
-                const long p = base - lane;
-                u32 v = ST_PRE;                         // before the first CTA: carry 0
-                if (p >= 0) {
-                    long spins = 0;
-                    v = st[p];
-                    while (v == 0) {
-                        if (++spins > SPIN_LIMIT) {
-                            failed = true;
-                            v = ST_PRE;
-                            break;
-                        }
-                        __nanosleep(64);
-                        v = st[p];
-                    }
-                }
-                const unsigned pre = __ballot_sync(0xffffffffu, (v & ST_PRE) != 0);
-                const int first = pre ? __ffs(pre) - 1 : 32;
-                // compose the aggregates of lanes 0 .. first-1 (nearest first)
-                u32 fl = (lane < first) ? (v & 0xff) : ID_FN;
-#pragma unroll
-                for (int d = 1; d < 32; d <<= 1) {
-                    const u32 o = __shfl_down_sync(0xffffffffu, fl, d);
-                    if ((lane & (2 * d - 1)) == 0 && lane + d < 32) fl = fn_compose(fl, o);
-                }
-                fl = __shfl_sync(0xffffffffu, fl, 0);
-                acc = fn_compose(acc, fl);
-                if (pre) {
-                    const u32 pv = __shfl_sync(0xffffffffu, v, first) & 0xff;
-                    cin = fn_apply(acc, pv);
-                    break;
-                }
-                base -= 32;
-            }
-            if (__any_sync(0xffffffffu, failed) && lane == 0) atomicOr(a.err, 1u);
-            if (lane == 0) atomicExch(&a.state[tile], ST_PRE | fn_apply(agg, cin));
-        }
-        if (lane == 0) s_cin = cin;
-    }
-    __syncthreads();
-    u64 c = fn_apply(exc, fn_apply(s_warp[warp], s_cin));
-    u64 outv[CE];
-#pragma unroll
-    for (int e = 0; e < CE; ++e) {
-        const u64 t = lo[e] + c;
-        c = h[e] + (t < c);
-        outv[e] = t;
-    }
-    if (j0 + CE <= a.out_len && ((reinterpret_cast<uintptr_t>(a.out) & 15) == 0)) {
-#pragma unroll
-        for (int e = 0; e < CE; e += 2)
-            *reinterpret_cast<ulonglong2*>(a.out + j0 + e) = make_ulonglong2(outv[e], outv[e + 1]);
-    } else {
-#pragma unroll
-        for (int e = 0; e < CE; ++e)
-            if (j0 + e < a.out_len) a.out[j0 + e] = outv[e];
-    }
+    carry_finish(lo, h, tile, j0, a.state, a.err, a.out, a.out_len);
 }
 
 __global__ void __launch_bounds__(CNT) k_crt_carry(CrtArgs a) { crt_carry_body(a, 0xffffffffu); }
@@ -860,7 +711,7 @@ static const u64 kP[3] = {Prime<0>::P, Prime<1>::P, Prime<2>::P};
 static const u64 kG[3] = {5, 5, 3};   // primitive roots (src/data.h:69-71)
 
 struct HostTables {
-    std::vector<u64> rt;   // [2][3][RT_SIZE]
+    std::vector<u64> rt;   // [2][3][RT_SIZE][2]: (w, floor(w 2^64 / p)) plain Shoup pairs
     std::vector<u64> tw;   // [2][3][1 << TWB]
 };
 
@@ -868,7 +719,7 @@ static const HostTables& host_tables() {
     static HostTables T;
     static std::once_flag once;
     std::call_once(once, [] {
-        T.rt.assign((size_t)2 * 3 * RT_SIZE, 0);
+        T.rt.assign((size_t)2 * 3 * RT_SIZE * 2, 0);
         T.tw.assign((size_t)2 * 3 * (1u << TWB), 0);
         for (int i = 0; i < 3; ++i) {
             const u64 p = kP[i];
@@ -901,9 +752,14 @@ static const HostTables& host_tables() {
                                 // w_{2^(top-s+1)}^(q + u 2^spl) = w^((q + u 2^spl) 2^(30-(top-s+1)))
                                 const u64 e = ((u64)q + ((u64)u << spl)) << (MAX_LOG_N - (top - s + 1));
                                 const size_t at = (size_t)rt_off(r, top) + (size_t)q * R + (R - (R >> s)) + u;
-                                T.rt[((size_t)0 * 3 + i) * RT_SIZE + at] = mont(wpow(e));
-                                T.rt[((size_t)1 * 3 + i) * RT_SIZE + at] =
-                                    mont(wpow((1ull << MAX_LOG_N) - (e & ((1ull << MAX_LOG_N) - 1))));
+                                const u64 wf = wpow(e);
+                                const u64 wi = wpow((1ull << MAX_LOG_N) - (e & ((1ull << MAX_LOG_N) - 1)));
+                                const size_t f0 = (((size_t)0 * 3 + i) * RT_SIZE + at) * 2;
+                                const size_t i0 = (((size_t)1 * 3 + i) * RT_SIZE + at) * 2;
+                                T.rt[f0] = wf;
+                                T.rt[f0 + 1] = (u64)((((unsigned __int128)wf) << 64) / p);
+                                T.rt[i0] = wi;
+                                T.rt[i0 + 1] = (u64)((((unsigned __int128)wi) << 64) / p);
                             }
                 }
         }
@@ -1137,15 +993,33 @@ static WsLayout ws_layout(u64 la, u64 lb, int sqr, int force_n = 0) {
     return w;
 }
 
-size_t job_workspace_bytes(u64 la, u64 lb, int sqr) {
-    const size_t t = ws_layout(la, lb, sqr).total;
-    return t ? t : 256;
+static std::atomic<int> g_engine{ENGINE_AUTO};
+void set_default_engine(int engine) { g_engine.store(engine); }
+int default_engine() { return g_engine.load(); }
+
+int job_engine(const Job& j) {
+    if (j.spectrum) return ENGINE_64;
+    const int e = j.engine ? j.engine : default_engine();
+    if (e == ENGINE_64) return ENGINE_64;
+    return q32_fits(j.la, j.lb) ? ENGINE_32 : ENGINE_64;
+}
+
+static Job plain_job(u64 la, u64 lb, int sqr) {
+    Job j;
+    memset(&j, 0, sizeof(j));
+    j.la = la;
+    j.lb = lb;
+    j.sqr = sqr;
+    return j;
 }
 
 size_t job_workspace_bytes(const Job& j) {
+    if (job_engine(j) == ENGINE_32) return q32_workspace_bytes(j.la, j.lb, j.sqr ? 1 : 0);
     const size_t t = ws_layout(j.la, j.lb, j.sqr, j.spectrum ? j.log_n : 0).total;
     return t ? t : 256;
 }
+
+size_t job_workspace_bytes(u64 la, u64 lb, int sqr) { return job_workspace_bytes(plain_job(la, lb, sqr)); }
 
 static cudaError_t launch_pass(int variant, int logl, const PassArgs& a, u64 tiles, cudaStream_t s);
 
@@ -1229,21 +1103,29 @@ cudaError_t profile_take(KindStats* out) {
     return cudaSuccess;
 }
 
+ProfMark prof_begin(int kind, double bytes, double modmuls, cudaStream_t s) {
+    ProfMark m{kind, nullptr, bytes, modmuls};
+    if (g_prof.on) {
+        m.a = g_prof.get();
+        cudaEventRecord(m.a, s);
+    }
+    return m;
+}
+
+void prof_end(const ProfMark& m, cudaStream_t s) {
+    if (!g_prof.on || !m.a) return;
+    ProfRec r{m.kind, m.a, g_prof.get(), m.bytes, m.modmuls};
+    cudaEventRecord(r.b, s);
+    g_prof.recs.push_back(r);
+}
+
 // Launch wrapper: records events around the launch when profiling is on.
 template <class F>
 static cudaError_t timed_launch(int kind, double bytes, double modmuls, cudaStream_t s, F&& launch) {
-    ProfRec r{kind, nullptr, nullptr, bytes, modmuls};
-    if (g_prof.on) {
-        r.a = g_prof.get();
-        r.b = g_prof.get();
-        cudaEventRecord(r.a, s);
-    }
+    const ProfMark m = prof_begin(kind, bytes, modmuls, s);
     launch();
     cudaError_t e = cudaGetLastError();
-    if (g_prof.on) {
-        cudaEventRecord(r.b, s);
-        g_prof.recs.push_back(r);
-    }
+    prof_end(m, s);
     return e;
 }
 
@@ -1289,6 +1171,7 @@ static cudaError_t launch_pass(int variant, int logl, const PassArgs& a, u64 til
 
 int job_launches(u64 la, u64 lb, int sqr) {
     if (la == 0 || lb == 0) return 0;
+    if (job_engine(plain_job(la, lb, sqr)) == ENGINE_32) return q32_launches(la, lb, sqr);
     const WsLayout w = ws_layout(la, lb, sqr);
     const Plan pl = make_plan(w.n);
     const int P = pl.passes;
@@ -1427,7 +1310,7 @@ static void plan_job(const Job& j, const JobScratch& sc, const TwiddleSet* tws, 
         pa.tw = tws ? tws->inv[p] : nullptr;
         add(V_INV, pl.bits[p], pa, N >> (pl.bits[p] + 4));
     }
-    // CRT constants: M_i^-1 * N^-1 mod p_i
+    // CRT constants: M_i^-1 * N^-1 * 2^128 mod p_i
     CrtArgs& ca = out->crt;
     memset(&ca, 0, sizeof(ca));
     for (int i = 0; i < 3; ++i) {
@@ -1435,7 +1318,9 @@ static void plan_job(const Job& j, const JobScratch& sc, const TwiddleSet* tws, 
         const unsigned __int128 M = (unsigned __int128)kP[(i + 1) % 3] * kP[(i + 2) % 3];
         const u64 minv = h_pow((u64)(M % p), p - 2, p);
         const u64 ninv = h_pow(N % p, p - 2, p);
-        ca.cst[i] = h_mulmod(minv, ninv, p);
+        const u64 r1 = (u64)((((unsigned __int128)1) << 64) % p);
+        // y = r * cst * 2^-64 with r = N * conv * 2^-64 (the pointwise Montgomery product)
+        ca.cst[i] = h_mulmod(h_mulmod(minv, ninv, p), h_mulmod(r1, r1, p), p);
     }
     ca.res = A;
     ca.N = N;
@@ -1458,6 +1343,7 @@ cudaError_t enqueue_job(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s,
     const u64 out_len = j.la + j.lb;
     if (out_len == 0) return cudaSuccess;
     if (j.la == 0 || j.lb == 0) return cudaMemsetAsync(j.out, 0, out_len * sizeof(u64), s);
+    if (job_engine(j) == ENGINE_32) return q32_enqueue(j, ws, ws_bytes, s, nullptr, 1, nullptr, nullptr);
     const int sqr = j.sqr ? 1 : 0;
     const WsLayout w = ws_layout(j.la, j.lb, sqr, j.spectrum ? j.log_n : 0);
     if (ws_bytes < w.total || w.n > MAX_LOG_N) return cudaErrorInvalidValue;
@@ -1480,6 +1366,7 @@ cudaError_t enqueue_job_overlapped(const Job& j, void* ws, size_t ws_bytes, cuda
                                    cudaEvent_t b_ready, int crt_chunks, ChunkDone after_chunk, void* ctx) {
     const u64 out_len = j.la + j.lb;
     if (j.la == 0 || j.lb == 0 || out_len == 0) return cudaErrorInvalidValue;
+    if (job_engine(j) == ENGINE_32) return q32_enqueue(j, ws, ws_bytes, s, b_ready, crt_chunks, after_chunk, ctx);
     const int sqr = j.sqr ? 1 : 0;
     const WsLayout w = ws_layout(j.la, j.lb, sqr, j.spectrum ? j.log_n : 0);
     if (ws_bytes < w.total || w.n > MAX_LOG_N) return cudaErrorInvalidValue;
@@ -1822,7 +1709,7 @@ __global__ void __launch_bounds__(256) k_bench_modmul(u64* sink, u64 y) {
     for (int i = 0; i < MB_CHAINS; ++i) acc ^= x[i];
     if (acc == 0x123456789ull) sink[0] = acc;
 }
-__global__ void __launch_bounds__(256) k_bench_bfly(u64* sink, u64 w) {
+__global__ void __launch_bounds__(256) k_bench_bfly(u64* sink, ulonglong2 w) {
     const PrimeRT q = c_prime[2];
     u64 x[2 * MB_CHAINS];
 #pragma unroll
@@ -1849,7 +1736,8 @@ cudaError_t bench_modmul(double* per_second, double* bfly_per_second) {
     cudaEventCreate(&a);
     cudaEventCreate(&b);
     const unsigned grid = (unsigned)sms * 8;
-    const u64 y = 1234567890123456789ull % Prime<2>::P, w = 987654321987654321ull % Prime<2>::P;
+    const u64 y = 1234567890123456789ull % Prime<2>::P, w0 = 987654321987654321ull % Prime<2>::P;
+    const ulonglong2 w = make_ulonglong2(w0, (u64)((((unsigned __int128)w0) << 64) / Prime<2>::P));
     float best = 1e30f, bestb = 1e30f;
     for (int rep = 0; rep < 4; ++rep) {
         cudaEventRecord(a);

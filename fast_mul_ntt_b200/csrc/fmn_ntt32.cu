@@ -1,0 +1,987 @@
+// fmn_ntt32.cu -- the 32-bit residue engine: sm_100a kernels and launchers for products
+// whose transform over 32-bit digits has at most 2^26 points (up to 2^25 output limbs).
+//
+// The pipeline is the one of the 64-bit engine (fmn_ntt.cu, reference src/fast_mul.c:308-460):
+// entry fused into the first forward pass, four-step passes of <= 2^9 points per CTA, the
+// pointwise product fused between the last forward and the first inverse pass, CRT fused
+// with the carry scan.  What differs is the residue arithmetic (fmn_arith32.cuh): each
+// 64-bit limb enters as two 32-bit digits (little-endian, digit g is 32-bit word g of the
+// limb array) and residues are u32 modulo three primes below 2^31, whose products are
+// single 32 x 32-bit multiplies instead of 64-bit chains.  The integer product that comes
+// out is the same, limb for limb.
+//
+// Data layout: per operand three residue arrays of N u32 (prime-major).  A strided pass
+// views a block of B = 2^logB digits as a [2^m][B / 2^m] row-major matrix; a CTA takes 32
+// adjacent columns (a 128-byte stretch of each row) and transforms every column in shared
+// memory.  The tile stores element (row j, column c) at j * 33 + c: one padding word per row
+// keeps row-wise and column-wise access free of bank conflicts, and the offsets of a group's
+// elements are compile-time steps from one base (no per-element address arithmetic).
+// Indices within one prime's residue array are 32-bit (N <= 2^26).
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <mutex>
+#include <vector>
+
+#include "fmn_arith32.cuh"
+#include "fmn_carry.cuh"
+#include "fmn_internal.h"
+#include "fmn_rounds.cuh"
+
+namespace fmn {
+namespace q32 {
+
+constexpr int NT = 256;                 // threads per CTA, NTT passes
+constexpr int LOG_TC = 5;
+constexpr int TC = 1 << LOG_TC;         // columns per tile
+constexpr int QTWB = 13;                // two-level root tables: w^x = HI[x >> 13] * LO[x & 8191]
+constexpr u32 MASK_N = (1u << Q32_MAX_LOG_N) - 1;
+static_assert(2 * QTWB == Q32_MAX_LOG_N, "two-level table covers roots of order 2^26");
+
+__device__ __align__(16) uint2 g_qrt[2][3][RT_SIZE];   // [forward/inverse][prime]: (w, w') Shoup pairs
+__device__ __align__(16) u32 g_qtw[2][3][1 << QTWB];   // [low/high level][prime], Montgomery form
+__constant__ PrimeQ c_q[3] = {prime_q(Q32_P0), prime_q(Q32_P1), prime_q(Q32_P2)};
+
+// Montgomery product a * b * 2^-32 mod p left in (0, 2p) (a, b < p); the result may be the
+// second factor of qmont, whose bound a * b < p * 2^32 still holds.
+__device__ __forceinline__ u32 qmont_lazy(u32 a, u32 b, const PrimeQ& q) {
+    const u64 t = (u64)a * b;
+    const u32 m = (u32)t * q.pinv;
+    return (u32)(t >> 32) + q.p - __umulhi(m, q.p);
+}
+
+// Montgomery form of w_{2^26}^x, prime index pi.
+__device__ __forceinline__ u32 qroot(u32 x, int pi, const PrimeQ& q) {
+    return qmont(__ldg(&g_qtw[1][pi][x >> QTWB]), __ldg(&g_qtw[0][pi][x & ((1u << QTWB) - 1)]), q);
+}
+
+constexpr int TP = TC + 1;              // padded row pitch of a shared-memory tile (words)
+__device__ __forceinline__ int tix(int j, int c) { return j * TP + c; }
+
+enum { M_FWD = 0, M_FWD_LAST = 1, M_FUSED = 2, M_INV = 3, M_FUSED2 = 4 };
+
+struct QArgs {
+    const u64* src;   // ENTRY: limbs of the operand being transformed
+    u64 len;          // ENTRY: number of limbs (2 * len digits)
+    u32* data;        // residue arrays of the operand being transformed
+    u32* other;       // M_FUSED / M_FUSED2: the other operand's spectrum; the product goes here
+    u64 N;            // transform length (digits)
+    int logB;         // log2 block length of this pass
+    int ncols;        // contiguous passes: number of blocks (columns) in a tile, <= 32
+};
+
+// ------------------------------------------------------------------ one round
+// Runs all radix-2^RB groups of one round; see fmn_ntt.cu for the index scheme (identical).
+template <int LOGL, int RB, int TOP, bool INV, bool QFAST, bool GST = false, bool GLD = false, class LD, class ST>
+__device__ __forceinline__ void run_round(LD ld, ST st, int pi, const PrimeQ& q) {
+    constexpr int L = 1 << LOGL, R = 1 << RB, SPL = TOP - RB + 1, SP = 1 << SPL;
+    constexpr int GPC = L / R;
+    constexpr int G = GPC * TC;
+    constexpr bool LOWEST = (SPL == 0);
+    const uint2* tab = &g_qrt[INV ? 1 : 0][pi][rt_off(RB, TOP)];
+#pragma unroll 1
+    for (int gi = threadIdx.x; gi < G; gi += NT) {
+        int c, g;
+        if (QFAST) {
+            g = gi % GPC;
+            c = gi / GPC;
+        } else {
+            c = gi & (TC - 1);
+            g = gi >> LOG_TC;
+        }
+        const int qlo = g & (SP - 1);
+        const int row0 = qlo + ((g >> SPL) << (TOP + 1));
+        u32 x[R];
+        if constexpr (GLD) {
+            ld(row0, c, x);
+        } else {
+#pragma unroll
+            for (int t = 0; t < R; ++t) x[t] = ld(row0 + t * SP, c);
+        }
+        const uint2* tw = tab + qlo * R;
+        if (!INV) {
+#pragma unroll
+            for (int s = 0; s < RB; ++s) {
+                const int half = R >> (s + 1);
+#pragma unroll
+                for (int t = 0; t < R; ++t) {
+                    if (t & half) continue;
+                    const int u = t & (half - 1);
+                    if (LOWEST && u == 0)
+                        qbfly_dif1(x[t], x[t + half], q);
+                    else
+                        qbfly_dif(x[t], x[t + half], __ldg(tw + (R - (R >> s)) + u), q);
+                }
+            }
+        } else {
+#pragma unroll
+            for (int s = RB - 1; s >= 0; --s) {
+                const int half = R >> (s + 1);
+#pragma unroll
+                for (int t = 0; t < R; ++t) {
+                    if (t & half) continue;
+                    const int u = t & (half - 1);
+                    if (LOWEST && u == 0)
+                        qbfly_dit1(x[t], x[t + half], q);
+                    else
+                        qbfly_dit(x[t], x[t + half], __ldg(tw + (R - (R >> s)) + u), q);
+                }
+            }
+        }
+        if constexpr (GST) {
+            st(row0, c, x);
+        } else {
+#pragma unroll
+            for (int t = 0; t < R; ++t) st(row0 + t * SP, c, x[t]);
+        }
+    }
+}
+
+// R consecutive u32 (aligned to 4R bytes) with vector stores / loads.
+template <int R>
+__device__ __forceinline__ void st_vec(u32* p, const u32 (&x)[R]) {
+    if constexpr (R == 1) {
+        p[0] = x[0];
+    } else if constexpr (R == 2) {
+        *reinterpret_cast<uint2*>(p) = make_uint2(x[0], x[1]);
+    } else {
+#pragma unroll
+        for (int t = 0; t < R; t += 4) *reinterpret_cast<uint4*>(p + t) = make_uint4(x[t], x[t + 1], x[t + 2], x[t + 3]);
+    }
+}
+template <int R>
+__device__ __forceinline__ void ld_vec(const u32* p, u32 (&x)[R]) {
+    if constexpr (R == 1) {
+        x[0] = p[0];
+    } else if constexpr (R == 2) {
+        const uint2 v = *reinterpret_cast<const uint2*>(p);
+        x[0] = v.x;
+        x[1] = v.y;
+    } else {
+#pragma unroll
+        for (int t = 0; t < R; t += 4) {
+            const uint4 v = *reinterpret_cast<const uint4*>(p + t);
+            x[t] = v.x;
+            x[t + 1] = v.y;
+            x[t + 2] = v.z;
+            x[t + 3] = v.w;
+        }
+    }
+}
+
+// Rounds IDX.. of a sub-transform (forward: round 0 holds the top bits; inverse round k
+// undoes forward round NR-1-k).  The first round reads with `ld0`, the last writes with
+// `stl`, the rest go through shared memory.
+template <int LOGL, bool INV, bool CONTIG, int IDX, bool GST = false, bool GLD = false, class LD0, class STL>
+__device__ __forceinline__ void rounds(u32* sm, LD0 ld0, STL stl, int pi, const PrimeQ& q) {
+    constexpr int NR = rounds_count(LOGL);
+    constexpr int FR = INV ? NR - 1 - IDX : IDX;
+    constexpr int RB = round_bits(LOGL, FR), TOP = round_top(LOGL, FR);
+    constexpr bool QF = CONTIG && (TOP == LOGL - 1);
+    auto lds = [sm](int j, int c) { return sm[tix(j, c)]; };
+    auto sts = [sm](int j, int c, u32 v) { sm[tix(j, c)] = v; };
+    if constexpr (NR == 1) {
+        run_round<LOGL, RB, TOP, INV, QF, GST, GLD>(ld0, stl, pi, q);
+    } else if constexpr (IDX == 0) {
+        run_round<LOGL, RB, TOP, INV, QF, false, GLD>(ld0, sts, pi, q);
+        __syncthreads();
+        rounds<LOGL, INV, CONTIG, 1, GST>(sm, ld0, stl, pi, q);
+    } else if constexpr (IDX == NR - 1) {
+        run_round<LOGL, RB, TOP, INV, QF, GST>(lds, stl, pi, q);
+    } else {
+        run_round<LOGL, RB, TOP, INV, QF>(lds, sts, pi, q);
+        __syncthreads();
+        rounds<LOGL, INV, CONTIG, IDX + 1, GST>(sm, ld0, stl, pi, q);
+    }
+}
+
+// ------------------------------------------------------------------ pass bodies
+// Digit g of the operand (32-bit word g of its limbs) reduced mod q, zero past the end.
+__device__ __forceinline__ u32 entry_val(const u64* __restrict__ src, u64 len, u32 g, const PrimeQ& q) {
+    return (g >> 1) < len ? qsmul(__ldg(reinterpret_cast<const u32*>(src) + g), 1u, q.one, q) : 0u;
+}
+
+// Four-step twiddles of a strided pass: element (row j, column c) holds frequency
+// k = bitrev(j) and is multiplied by w_B^(i k), i = col0 + c, factored per lowest-round group
+// as alpha(group) * beta[c][t'] (see fmn_ntt.cu).  Both factors are in Montgomery form.
+template <int LOGL, bool INV>
+__device__ __forceinline__ void fill_beta(u32* beta, u32 col0, int shift, int pi, const PrimeQ& q) {
+    constexpr int RB = round_bits(LOGL, rounds_count(LOGL) - 1), R = 1 << RB;
+    for (int e = threadIdx.x; e < TC * R; e += NT) {   // beta[tp * TC + c]: conflict-free reads
+        const u32 c = e & (TC - 1), tp = e >> LOG_TC;
+        u32 x = ((col0 + c) * (tp << (LOGL - RB))) << shift;
+        if (INV) x = (0u - x) & MASK_N;
+        beta[e] = qroot(x, pi, q);
+    }
+}
+template <int LOGL, bool INV>
+__device__ __forceinline__ u32 group_alpha(u32 i, int row0, int shift, int pi, const PrimeQ& q) {
+    constexpr int RB = round_bits(LOGL, rounds_count(LOGL) - 1);
+    const u32 kq = LOGL > RB ? __brev((u32)(row0 >> RB)) >> (32 - (LOGL - RB)) : 0u;
+    u32 x = (i * kq) << shift;
+    if (INV) x = (0u - x) & MASK_N;
+    return qroot(x, pi, q);
+}
+
+// Forward strided pass (pass p < P-1 of a multi-pass transform).
+template <int LOGL, bool ENTRY>
+__device__ __forceinline__ void body_fwd(u32* sm, const QArgs& a, u64 tile, int pi, const PrimeQ& q) {
+    constexpr int L = 1 << LOGL;
+    constexpr int RB = round_bits(LOGL, rounds_count(LOGL) - 1), R = 1 << RB;
+    const int logS = a.logB - LOGL;
+    const int tpb_log = logS - LOG_TC;
+    const u32 blk = (u32)(tile >> tpb_log);
+    const u32 col0 = (u32)((tile & ((1ull << tpb_log) - 1)) << LOG_TC);
+    const u32 gbase = (blk << a.logB) + col0;
+    u32* __restrict__ d = a.data + (u64)pi * a.N;
+    const u64* __restrict__ src = a.src;
+    const u64 len = a.len;
+    const int shift = Q32_MAX_LOG_N - a.logB;
+    u32* beta = sm + TP * L;
+    fill_beta<LOGL, false>(beta, col0, shift, pi, q);     // read after the first round's barrier
+    auto ld0 = [=](int j, int c) -> u32 {
+        const u32 g = gbase + c + ((u32)j << logS);
+        if constexpr (ENTRY) return entry_val(src, len, g, q);
+        else return d[g];
+    };
+    auto stl = [=](int row0, int c, const auto& x) {
+        const u32 al = group_alpha<LOGL, false>(col0 + c, row0, shift, pi, q);
+        const u32 o = gbase + c + ((u32)row0 << logS);
+#pragma unroll
+        for (int t = 0; t < R; ++t) {
+            const int tp = RB ? (int)(__brev((u32)t) >> (32 - RB)) : 0;
+            d[o + ((u32)t << logS)] = qmont(x[t], qmont_lazy(al, beta[tp * TC + c], q), q);
+        }
+    };
+    rounds<LOGL, false, false, 0, true>(sm, ld0, stl, pi, q);
+}
+
+// Inverse strided pass: inverse four-step twiddle, then the inverse sub-transform.
+template <int LOGL>
+__device__ __forceinline__ void body_inv(u32* sm, const QArgs& a, u64 tile, int pi, const PrimeQ& q) {
+    constexpr int L = 1 << LOGL;
+    constexpr int RB = round_bits(LOGL, rounds_count(LOGL) - 1), R = 1 << RB;
+    const int logS = a.logB - LOGL;
+    const int tpb_log = logS - LOG_TC;
+    const u32 blk = (u32)(tile >> tpb_log);
+    const u32 col0 = (u32)((tile & ((1ull << tpb_log) - 1)) << LOG_TC);
+    const u32 gbase = (blk << a.logB) + col0;
+    u32* __restrict__ d = a.data + (u64)pi * a.N;
+    const int shift = Q32_MAX_LOG_N - a.logB;
+    u32* beta = sm + TP * L;
+    fill_beta<LOGL, true>(beta, col0, shift, pi, q);
+    __syncthreads();
+    auto ld0 = [=](int row0, int c, auto& x) {
+        const u32 o = gbase + c + ((u32)row0 << logS);
+#pragma unroll
+        for (int t = 0; t < R; ++t) x[t] = d[o + ((u32)t << logS)];
+        const u32 al = group_alpha<LOGL, true>(col0 + c, row0, shift, pi, q);
+#pragma unroll
+        for (int t = 0; t < R; ++t) {
+            const int tp = RB ? (int)(__brev((u32)t) >> (32 - RB)) : 0;
+            x[t] = qmont(x[t], qmont_lazy(al, beta[tp * TC + c], q), q);
+        }
+    };
+    auto stl = [=](int j, int c, u32 v) { d[gbase + c + ((u32)j << logS)] = v; };
+    rounds<LOGL, true, false, 0, false, true>(sm, ld0, stl, pi, q);
+}
+
+// Forward last pass over contiguous blocks (first operand of a product).
+template <int LOGL, bool ENTRY>
+__device__ __forceinline__ void body_fwd_last(u32* sm, const QArgs& a, u64 tile, int pi, const PrimeQ& q) {
+    constexpr int L = 1 << LOGL;
+    const u32 gbase = (u32)tile << (LOGL + LOG_TC);
+    const int ncols = a.ncols;
+    u32* __restrict__ d = a.data + (u64)pi * a.N;
+    const u64* __restrict__ src = a.src;
+    const u64 len = a.len;
+    auto ld0 = [=](int j, int c) -> u32 {
+        if (c >= ncols) return 0u;
+        const u32 g = gbase + (u32)c * L + j;
+        if constexpr (ENTRY) return entry_val(src, len, g, q);
+        else return d[g];
+    };
+    if constexpr (LOGL == 0) {
+        if (threadIdx.x < (unsigned)ncols) d[gbase + threadIdx.x] = ld0(0, threadIdx.x);
+    } else {
+        auto stl = [=](int row0, int c, const auto& x) {
+            if (c < ncols) st_vec(d + gbase + (u32)c * L + row0, x);
+        };
+        rounds<LOGL, false, true, 0, true>(sm, ld0, stl, pi, q);
+    }
+}
+
+// The lowest forward round, the pointwise product and the lowest inverse round of one
+// contiguous tile, all in registers.
+template <int LOGL, bool SQR, bool OTH_SMEM = false, class LD, class ST>
+__device__ __forceinline__ void fused_lowest(LD ld, ST st, const u32* __restrict__ oth, u32 gbase, int ncols, int pi,
+                                             const PrimeQ& q) {
+    constexpr int L = 1 << LOGL;
+    constexpr int NR = rounds_count(LOGL);
+    constexpr int RB = round_bits(LOGL, NR - 1);
+    constexpr int R = 1 << RB;
+    constexpr int G = (L / R) * TC;
+    const uint2* tf = &g_qrt[0][pi][rt_off(RB, RB - 1)];
+    const uint2* ti = &g_qrt[1][pi][rt_off(RB, RB - 1)];
+#pragma unroll 1
+    for (int gi = threadIdx.x; gi < G; gi += NT) {
+        const int c = gi & (TC - 1);
+        const int row0 = (gi >> LOG_TC) << RB;
+        u32 x[R];
+#pragma unroll
+        for (int t = 0; t < R; ++t) x[t] = ld(row0 + t, c);
+#pragma unroll
+        for (int s = 0; s < RB; ++s) {
+            const int half = R >> (s + 1);
+#pragma unroll
+            for (int t = 0; t < R; ++t) {
+                if (t & half) continue;
+                const int u = t & (half - 1);
+                if (u == 0) qbfly_dif1(x[t], x[t + half], q);
+                else qbfly_dif(x[t], x[t + half], __ldg(tf + (R - (R >> s)) + u), q);
+            }
+        }
+        if (c < ncols) {
+            if constexpr (SQR) {
+#pragma unroll
+                for (int t = 0; t < R; ++t) x[t] = qmont(x[t], x[t], q);
+            } else if constexpr (OTH_SMEM) {
+#pragma unroll
+                for (int t = 0; t < R; ++t) x[t] = qmont(x[t], oth[tix(row0 + t, c)], q);
+            } else {
+                u32 y[R];
+                ld_vec(oth + gbase + (u32)c * L + row0, y);
+#pragma unroll
+                for (int t = 0; t < R; ++t) x[t] = qmont(x[t], y[t], q);
+            }
+        }
+#pragma unroll
+        for (int s = RB - 1; s >= 0; --s) {
+            const int half = R >> (s + 1);
+#pragma unroll
+            for (int t = 0; t < R; ++t) {
+                if (t & half) continue;
+                const int u = t & (half - 1);
+                if (u == 0) qbfly_dit1(x[t], x[t + half], q);
+                else qbfly_dit(x[t], x[t + half], __ldg(ti + (R - (R >> s)) + u), q);
+            }
+        }
+#pragma unroll
+        for (int t = 0; t < R; ++t) st(row0 + t, c, x[t]);
+    }
+}
+
+// Last forward pass of the second operand (or of the only one when squaring), pointwise
+// product with the first operand's spectrum, first inverse pass; overwrites `other`.
+template <int LOGL, bool ENTRY, bool SQR>
+__device__ __forceinline__ void body_fused(u32* sm, const QArgs& a, u64 tile, int pi, const PrimeQ& q) {
+    constexpr int L = 1 << LOGL;
+    constexpr int NR = rounds_count(LOGL);
+    const u32 gbase = (u32)tile << (LOGL + LOG_TC);
+    const int ncols = a.ncols;
+    const u32* __restrict__ d = a.data + (u64)pi * a.N;
+    u32* __restrict__ o = a.other + (u64)pi * a.N;
+    const u64* __restrict__ src = a.src;
+    const u64 len = a.len;
+    auto ldg = [=](int j, int c) -> u32 {
+        if (c >= ncols) return 0u;
+        const u32 g = gbase + (u32)c * L + j;
+        if constexpr (ENTRY) return entry_val(src, len, g, q);
+        else return d[g];
+    };
+    auto stg = [=](int j, int c, u32 v) {
+        if (c < ncols) o[gbase + (u32)c * L + j] = v;
+    };
+    auto lds = [sm](int j, int c) { return sm[tix(j, c)]; };
+    auto sts = [sm](int j, int c, u32 v) { sm[tix(j, c)] = v; };
+    if constexpr (LOGL == 0) {
+        if (threadIdx.x < (unsigned)ncols) {
+            const int c = threadIdx.x;
+            const u32 x = ldg(0, c);
+            const u32 y = SQR ? x : o[gbase + c];
+            stg(0, c, qmont(x, y, q));
+        }
+    } else if constexpr (NR == 1) {
+        fused_lowest<LOGL, SQR>(ldg, stg, o, gbase, ncols, pi, q);
+    } else {
+        constexpr int RB0 = round_bits(LOGL, 0);
+        run_round<LOGL, RB0, LOGL - 1, false, true>(ldg, sts, pi, q);
+        __syncthreads();
+        if constexpr (NR == 3) {
+            constexpr int RB1 = round_bits(LOGL, 1), T1 = round_top(LOGL, 1);
+            run_round<LOGL, RB1, T1, false, false>(lds, sts, pi, q);
+            __syncthreads();
+        }
+        fused_lowest<LOGL, SQR>(lds, sts, o, gbase, ncols, pi, q);
+        __syncthreads();
+        if constexpr (NR == 3) {
+            constexpr int RB1 = round_bits(LOGL, 1), T1 = round_top(LOGL, 1);
+            run_round<LOGL, RB1, T1, true, false>(lds, sts, pi, q);
+            __syncthreads();
+        }
+        run_round<LOGL, RB0, LOGL - 1, true, true>(lds, stg, pi, q);
+    }
+}
+
+// Both operands' last forward pass, the pointwise product and the first inverse pass: the
+// first operand's tile (from `other`) is transformed into a second shared-memory tile and
+// never written back; the product overwrites `other`.  Multi-pass products only.
+template <int LOGL>
+__device__ __forceinline__ void body_fused2(u32* sm, const QArgs& a, u64 tile, int pi, const PrimeQ& q) {
+    constexpr int L = 1 << LOGL;
+    constexpr int NR = rounds_count(LOGL);
+    static_assert(NR >= 2, "multi-round sub-transforms only");
+    const u32 gbase = (u32)tile << (LOGL + LOG_TC);
+    const u32* __restrict__ d = a.data + (u64)pi * a.N;
+    u32* __restrict__ o = a.other + (u64)pi * a.N;
+    u32* smA = sm + TP * L;
+    auto ldA = [=](int j, int c) -> u32 { return o[gbase + (u32)c * L + j]; };
+    auto stA = [smA](int j, int c, u32 v) { smA[tix(j, c)] = v; };
+    rounds<LOGL, false, true, 0>(smA, ldA, stA, pi, q);
+    auto ldg = [=](int j, int c) -> u32 { return d[gbase + (u32)c * L + j]; };
+    auto stg = [=](int j, int c, u32 v) { o[gbase + (u32)c * L + j] = v; };
+    auto lds = [sm](int j, int c) { return sm[tix(j, c)]; };
+    auto sts = [sm](int j, int c, u32 v) { sm[tix(j, c)] = v; };
+    constexpr int RB0 = round_bits(LOGL, 0);
+    run_round<LOGL, RB0, LOGL - 1, false, true>(ldg, sts, pi, q);
+    __syncthreads();                                   // also publishes smA
+    if constexpr (NR == 3) {
+        constexpr int RB1 = round_bits(LOGL, 1), T1 = round_top(LOGL, 1);
+        run_round<LOGL, RB1, T1, false, false>(lds, sts, pi, q);
+        __syncthreads();
+    }
+    fused_lowest<LOGL, false, true>(lds, sts, smA, gbase, TC, pi, q);
+    __syncthreads();
+    if constexpr (NR == 3) {
+        constexpr int RB1 = round_bits(LOGL, 1), T1 = round_top(LOGL, 1);
+        run_round<LOGL, RB1, T1, true, false>(lds, sts, pi, q);
+        __syncthreads();
+    }
+    run_round<LOGL, RB0, LOGL - 1, true, true>(lds, stg, pi, q);
+}
+
+template <int MODE, int LOGL, bool ENTRY, bool SQR>
+__global__ void __launch_bounds__(NT, (MODE == M_FWD || MODE == M_INV) && LOGL >= 9 ? 3 : 4) k_qpass(QArgs a) {
+    extern __shared__ __align__(16) u32 qsm[];
+    const int pi = blockIdx.x % 3;          // the three CTAs of a tile read the same limbs together
+    const u64 tile = blockIdx.x / 3;
+    const PrimeQ q = c_q[pi];
+    if constexpr (MODE == M_FWD) body_fwd<LOGL, ENTRY>(qsm, a, tile, pi, q);
+    else if constexpr (MODE == M_INV) body_inv<LOGL>(qsm, a, tile, pi, q);
+    else if constexpr (MODE == M_FWD_LAST) body_fwd_last<LOGL, ENTRY>(qsm, a, tile, pi, q);
+    else if constexpr (MODE == M_FUSED2) body_fused2<(LOGL >= 5 ? LOGL : 5)>(qsm, a, tile, pi, q);
+    else body_fused<LOGL, ENTRY, SQR>(qsm, a, tile, pi, q);
+}
+
+// ------------------------------------------------------------------ CRT + carry
+// Digit coefficient k of the product, c_k < Q = q0 q1 q2 < 2^91, from its residues by
+// c_k = sum_i y_i M_i mod Q with y_i = r_i * M_i^-1 (M_i = Q / q_i; the CRT of
+// src/core.h:77-104 for these primes).  Output limb j collects the 128-bit pair
+// C_j = c_{2j} + c_{2j+1} 2^32 < 2^124: s_j = C_j.lo + C_{j-1}.hi, then the carry scan.
+struct QCrtArgs {
+    const u32* res;     // three natural-order residue arrays (prime i at res + i*N), in [0, q)
+    u64 N;
+    u64 nvalid;         // digit coefficients that may be nonzero
+    u64* out;
+    u64 out_len;
+    u32 cst[3];         // M_i^-1 * N^-1 * 2^64 mod q_i (undoes the two Montgomery products)
+    u32* state;
+    u32* ticket;
+    u32* err;
+};
+
+typedef unsigned __int128 u128;
+constexpr u64 QM0 = (u64)Q32_P1 * Q32_P2, QM1 = (u64)Q32_P0 * Q32_P2, QM2 = (u64)Q32_P0 * Q32_P1;
+constexpr u128 QALL = (u128)QM2 * Q32_P2;
+
+__device__ __forceinline__ u128 qcrt(u32 r0, u32 r1, u32 r2, const QCrtArgs& a, const PrimeQ& q0, const PrimeQ& q1,
+                                     const PrimeQ& q2) {
+    const u64 y0 = qmont(r0, a.cst[0], q0), y1 = qmont(r1, a.cst[1], q1), y2 = qmont(r2, a.cst[2], q2);
+    u128 s = (u128)y0 * QM0 + (u128)y1 * QM1 + (u128)y2 * QM2;   // < 3 Q
+    if (s >= QALL) s -= QALL;
+    if (s >= QALL) s -= QALL;
+    return s;
+}
+__device__ __forceinline__ u128 qcoef(const QCrtArgs& a, u64 k, const PrimeQ& q0, const PrimeQ& q1, const PrimeQ& q2) {
+    if (k >= a.nvalid) return 0;
+    return qcrt(a.res[k], a.res[a.N + k], a.res[2 * a.N + k], a, q0, q1, q2);
+}
+
+__global__ void __launch_bounds__(CNT) k_qcrt_carry(QCrtArgs a) {
+    __shared__ u64 s_hw[CNT / 32];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const PrimeQ q0 = c_q[0], q1 = c_q[1], q2 = c_q[2];
+    const u64 tile = carry_ticket(a.ticket);
+    const u64 j0 = tile * CTILE + (u64)tid * CE;       // output limbs j0 .. j0+15
+    const u64 k0 = 2 * j0;                             // digit coefficients k0 .. k0+31
+    u64 lo[CE];
+    u32 h[CE];
+    u64 phi = 0;                                       // C_{j-1}.hi
+    const bool full = k0 + 2 * CE <= a.nvalid;
+#pragma unroll
+    for (int e2 = 0; e2 < CE; e2 += 2) {              // two limbs = four coefficients at a time
+        u32 r0[4], r1[4], r2[4];
+        if (full) {
+            const uint4 v0 = *reinterpret_cast<const uint4*>(a.res + k0 + 2 * e2);
+            const uint4 v1 = *reinterpret_cast<const uint4*>(a.res + a.N + k0 + 2 * e2);
+            const uint4 v2 = *reinterpret_cast<const uint4*>(a.res + 2 * a.N + k0 + 2 * e2);
+            r0[0] = v0.x, r0[1] = v0.y, r0[2] = v0.z, r0[3] = v0.w;
+            r1[0] = v1.x, r1[1] = v1.y, r1[2] = v1.z, r1[3] = v1.w;
+            r2[0] = v2.x, r2[1] = v2.y, r2[2] = v2.z, r2[3] = v2.w;
+        }
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+            const int e = e2 + u;
+            u128 cl, ch;
+            if (full) {
+                cl = qcrt(r0[2 * u], r1[2 * u], r2[2 * u], a, q0, q1, q2);
+                ch = qcrt(r0[2 * u + 1], r1[2 * u + 1], r2[2 * u + 1], a, q0, q1, q2);
+            } else {
+                cl = qcoef(a, k0 + 2 * e, q0, q1, q2);
+                ch = qcoef(a, k0 + 2 * e + 1, q0, q1, q2);
+            }
+            const u128 C = cl + (ch << 32);
+            u64 l = (u64)C;
+            u32 hh = 0;
+            add_to(l, hh, phi);
+            lo[e] = l;
+            h[e] = hh;
+            phi = (u64)(C >> 64);
+        }
+    }
+    // C_{j0-1}.hi from the previous thread, warp or CTA
+    u64 nb = __shfl_up_sync(0xffffffffu, phi, 1);
+    if (lane == 31) s_hw[warp] = phi;
+    __syncthreads();
+    if (lane == 0) {
+        if (warp > 0) {
+            nb = s_hw[warp - 1];
+        } else if (j0 > 0) {
+            const u128 C = qcoef(a, k0 - 2, q0, q1, q2) + (qcoef(a, k0 - 1, q0, q1, q2) << 32);
+            nb = (u64)(C >> 64);
+        } else {
+            nb = 0;
+        }
+    }
+    add_to(lo[0], h[0], nb);
+    carry_finish(lo, h, tile, j0, a.state, a.err, a.out, a.out_len);
+}
+
+// ------------------------------------------------------------------ host: tables
+static u64 h_mulmod(u64 a, u64 b, u64 m) { return (u64)(((u128)a * b) % m); }
+static u64 h_pow(u64 b, u64 e, u64 m) {
+    u64 r = 1;
+    b %= m;
+    while (e) {
+        if (e & 1) r = h_mulmod(r, b, m);
+        b = h_mulmod(b, b, m);
+        e >>= 1;
+    }
+    return r;
+}
+static const u32 kQ[3] = {Q32_P0, Q32_P1, Q32_P2};
+
+// Smallest primitive root of p (trial factorisation of p - 1).
+static u64 primitive_root(u64 p) {
+    std::vector<u64> f;
+    u64 m = p - 1;
+    for (u64 d = 2; d * d <= m; ++d)
+        if (m % d == 0) {
+            f.push_back(d);
+            while (m % d == 0) m /= d;
+        }
+    if (m > 1) f.push_back(m);
+    for (u64 g = 2;; ++g) {
+        bool ok = true;
+        for (u64 x : f)
+            if (h_pow(g, (p - 1) / x, p) == 1) {
+                ok = false;
+                break;
+            }
+        if (ok) return g;
+    }
+}
+
+struct HostTables {
+    std::vector<u32> rt;   // [2][3][RT_SIZE][2]: (w, floor(w 2^32 / q)) Shoup pairs
+    std::vector<u32> tw;   // [2][3][1 << QTWB]: Montgomery form
+};
+
+static const HostTables& host_tables() {
+    static HostTables T;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        T.rt.assign((size_t)2 * 3 * RT_SIZE * 2, 0);
+        T.tw.assign((size_t)2 * 3 * (1u << QTWB), 0);
+        for (int i = 0; i < 3; ++i) {
+            const u64 p = kQ[i];
+            const u64 w = h_pow(primitive_root(p), (p - 1) >> Q32_MAX_LOG_N, p);   // order 2^26
+            std::vector<u64> lo(1u << QTWB), hi(1u << QTWB);
+            const u64 whi = h_pow(w, 1ull << QTWB, p);
+            u64 cl = 1, ch = 1;
+            for (u32 x = 0; x < (1u << QTWB); ++x) {
+                lo[x] = cl;
+                hi[x] = ch;
+                cl = h_mulmod(cl, w, p);
+                ch = h_mulmod(ch, whi, p);
+            }
+            auto wpow = [&](u64 e) {   // w^e, e mod 2^26
+                e &= MASK_N;
+                return h_mulmod(hi[e >> QTWB], lo[e & ((1u << QTWB) - 1)], p);
+            };
+            for (u32 x = 0; x < (1u << QTWB); ++x) {
+                T.tw[((size_t)0 * 3 + i) * (1u << QTWB) + x] = (u32)((lo[x] << 32) % p);
+                T.tw[((size_t)1 * 3 + i) * (1u << QTWB) + x] = (u32)((hi[x] << 32) % p);
+            }
+            for (int r = 1; r <= 4; ++r)
+                for (int top = r - 1; top < RT_MAXLOGL; ++top) {
+                    const int R = 1 << r, spl = top - r + 1;
+                    for (int qq = 0; qq < (1 << spl); ++qq)
+                        for (int s = 0; s < r; ++s)
+                            for (int u = 0; u < (R >> (s + 1)); ++u) {
+                                // w_{2^(top-s+1)}^(qq + u 2^spl) = w^((qq + u 2^spl) 2^(26-(top-s+1)))
+                                const u64 e = ((u64)qq + ((u64)u << spl)) << (Q32_MAX_LOG_N - (top - s + 1));
+                                const size_t at = (size_t)rt_off(r, top) + (size_t)qq * R + (R - (R >> s)) + u;
+                                const u64 wf = wpow(e);
+                                const u64 wi = wpow((1ull << Q32_MAX_LOG_N) - (e & MASK_N));
+                                const size_t f0 = (((size_t)0 * 3 + i) * RT_SIZE + at) * 2;
+                                const size_t i0 = (((size_t)1 * 3 + i) * RT_SIZE + at) * 2;
+                                T.rt[f0] = (u32)wf;
+                                T.rt[f0 + 1] = (u32)((wf << 32) / p);
+                                T.rt[i0] = (u32)wi;
+                                T.rt[i0 + 1] = (u32)((wi << 32) / p);
+                            }
+                }
+        }
+    });
+    return T;
+}
+
+// ------------------------------------------------------------------ host: kernels
+typedef void (*QKernel)(QArgs);
+enum { V_FWD, V_FWD_E, V_LAST, V_LAST_E, V_FUSED, V_FUSED_E, V_SQR, V_SQR_E, V_INV, V_FUSED2, NV };
+
+template <int LOGL>
+static void fill_row(QKernel (&t)[NV][MAX_PASS_BITS + 1]) {
+    constexpr int LS = LOGL >= 5 ? LOGL : 5;                      // strided passes: >= 5 bits
+    constexpr int LM = (LOGL >= 5 && LOGL <= 8) ? LOGL : 5;       // merged pass: two tiles
+    t[V_FWD][LOGL] = LOGL >= 5 ? k_qpass<M_FWD, LS, false, false> : nullptr;
+    t[V_FWD_E][LOGL] = LOGL >= 5 ? k_qpass<M_FWD, LS, true, false> : nullptr;
+    t[V_INV][LOGL] = LOGL >= 5 ? k_qpass<M_INV, LS, false, false> : nullptr;
+    t[V_FUSED2][LOGL] = (LOGL >= 5 && LOGL <= 8) ? k_qpass<M_FUSED2, LM, false, false> : nullptr;
+    t[V_LAST][LOGL] = k_qpass<M_FWD_LAST, LOGL, false, false>;
+    t[V_LAST_E][LOGL] = k_qpass<M_FWD_LAST, LOGL, true, false>;
+    t[V_FUSED][LOGL] = k_qpass<M_FUSED, LOGL, false, false>;
+    t[V_FUSED_E][LOGL] = k_qpass<M_FUSED, LOGL, true, false>;
+    t[V_SQR][LOGL] = k_qpass<M_FUSED, LOGL, false, true>;
+    t[V_SQR_E][LOGL] = k_qpass<M_FUSED, LOGL, true, true>;
+}
+
+struct KernelTable {
+    QKernel k[NV][MAX_PASS_BITS + 1];
+    KernelTable() {
+        memset(k, 0, sizeof(k));
+        fill_row<0>(k);
+        fill_row<1>(k);
+        fill_row<2>(k);
+        fill_row<3>(k);
+        fill_row<4>(k);
+        fill_row<5>(k);
+        fill_row<6>(k);
+        fill_row<7>(k);
+        fill_row<8>(k);
+        fill_row<9>(k);
+    }
+};
+static const KernelTable& ktab() {
+    static KernelTable t;
+    return t;
+}
+
+// tile + the 16 x 32 four-step twiddle factors of strided passes; two tiles when merged
+static size_t pass_smem(int logl, int variant) {
+    const size_t tile = (size_t)TP * ((size_t)1 << logl);
+    return (variant == V_FUSED2 ? 2 * tile : tile + TC * 16) * sizeof(u32);
+}
+
+static cudaError_t ensure_tables() {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    static std::mutex mu;
+    static std::vector<int> done;
+    std::lock_guard<std::mutex> lock(mu);
+    for (int d : done)
+        if (d == dev) return cudaSuccess;
+    const HostTables& T = host_tables();
+    e = cudaMemcpyToSymbol(g_qrt, T.rt.data(), T.rt.size() * sizeof(u32));
+    if (e != cudaSuccess) return e;
+    e = cudaMemcpyToSymbol(g_qtw, T.tw.data(), T.tw.size() * sizeof(u32));
+    if (e != cudaSuccess) return e;
+    const KernelTable& K = ktab();
+    for (int v = 0; v < NV; ++v)
+        for (int l = 0; l <= MAX_PASS_BITS; ++l)
+            if (K.k[v][l]) {
+                e = cudaFuncSetAttribute((const void*)K.k[v][l], cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)pass_smem(l, v));
+                if (e != cudaSuccess) return e;
+                e = cudaFuncSetAttribute((const void*)K.k[v][l], cudaFuncAttributePreferredSharedMemoryCarveout,
+                                         (int)cudaSharedmemCarveoutMaxShared);
+                if (e != cudaSuccess) return e;
+            }
+    done.push_back(dev);
+    return cudaSuccess;
+}
+
+// ------------------------------------------------------------------ host: plans and jobs
+// Passes of a 2^n-digit transform: as even as possible, largest first; a strided pass leaves
+// at least 32 columns (later passes take >= 5 bits) and takes >= 5 bits itself.
+static Plan qplan(int n) {
+    Plan p;
+    memset(&p, 0, sizeof(p));
+    p.n = n;
+    if (n <= MAX_PASS_BITS) {
+        p.passes = 1;
+        p.bits[0] = n;
+    } else if (n <= 2 * MAX_PASS_BITS) {
+        p.passes = 2;
+        p.bits[1] = n / 2;
+        p.bits[0] = n - n / 2;
+    } else {
+        p.passes = 3;
+        p.bits[0] = (n + 2) / 3;
+        p.bits[1] = (n - p.bits[0] + 1) / 2;
+        p.bits[2] = n - p.bits[0] - p.bits[1];
+    }
+    return p;
+}
+
+static u64 ceil_pow2(u64 x) {
+    u64 r = 1;
+    while (r < x) r <<= 1;
+    return r;
+}
+static int ilog2(u64 x) {
+    int r = 0;
+    while ((1ull << r) < x) ++r;
+    return r;
+}
+static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+// Workspace: [error word, 256 B][A residues][B residues][ticket + state], as in fmn_ntt.cu.
+struct QLayout {
+    u64 N;
+    int n;
+    size_t a, b, ticket, state, total;
+    u64 ncta;
+};
+static QLayout layout(u64 la, u64 lb, int sqr) {
+    QLayout w;
+    memset(&w, 0, sizeof(w));
+    const u64 out_len = la + lb;
+    if (la == 0 || lb == 0) return w;
+    w.N = ceil_pow2(2 * out_len - 1);
+    w.n = ilog2(w.N);
+    w.ncta = (out_len + CTILE - 1) / CTILE;
+    size_t off = 256;
+    w.a = off;
+    off = align256(off + 3 * w.N * sizeof(u32));
+    w.b = off;
+    if (!sqr) off = align256(off + 3 * w.N * sizeof(u32));
+    w.ticket = off;
+    w.state = off + 16;
+    off = align256(w.state + w.ncta * sizeof(u32));
+    w.total = off;
+    return w;
+}
+
+}  // namespace q32
+
+bool q32_fits(u64 la, u64 lb) {
+    if (la == 0 || lb == 0) return false;
+    const u64 out_len = la + lb;
+    return out_len <= (1ull << (Q32_MAX_LOG_N - 1));   // 2 * out_len - 1 < 2^26
+}
+
+size_t q32_workspace_bytes(u64 la, u64 lb, int sqr) {
+    const size_t t = q32::layout(la, lb, sqr).total;
+    return t ? t : 256;
+}
+
+int q32_launches(u64 la, u64 lb, int sqr) {
+    if (la == 0 || lb == 0) return 0;
+    const q32::QLayout w = q32::layout(la, lb, sqr);
+    const Plan pl = q32::qplan(w.n);
+    const int P = pl.passes;
+    const int lastl = pl.bits[P - 1];
+    if (!sqr && P >= 2 && lastl >= 5 && lastl <= 8) return 2 * (P - 1) + 1 + (P - 1) + 1;
+    return sqr ? (P - 1) + 1 + (P - 1) + 1 : 2 * (P - 1) + 1 + 1 + (P - 1) + 1;
+}
+
+cudaError_t q32_enqueue(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s, cudaEvent_t b_ready, int crt_chunks,
+                        ChunkDone after_chunk, void* ctx) {
+    using namespace q32;
+    const u64 out_len = j.la + j.lb;
+    if (out_len == 0) return cudaSuccess;
+    if (j.la == 0 || j.lb == 0) return cudaMemsetAsync(j.out, 0, out_len * sizeof(u64), s);
+    if (!q32_fits(j.la, j.lb)) return cudaErrorInvalidValue;
+    const int sqr = j.sqr ? 1 : 0;
+    const QLayout w = layout(j.la, j.lb, sqr);
+    if (ws_bytes < w.total) return cudaErrorInvalidValue;
+    cudaError_t e = q32::ensure_tables();
+    if (e != cudaSuccess) return e;
+    char* base = (char*)ws;
+    u32* A = (u32*)(base + w.a);
+    u32* B = sqr ? A : (u32*)(base + w.b);
+    const Plan pl = qplan(w.n);
+    const int P = pl.passes;
+    const u64 N = w.N;
+    int logB[MAX_PASSES];
+    logB[0] = w.n;
+    for (int p = 1; p < P; ++p) logB[p] = logB[p - 1] - pl.bits[p - 1];
+    const int lastl = pl.bits[P - 1];
+    const u64 nblk_last = N >> lastl;
+    const u64 tiles_last = (nblk_last + TC - 1) / TC;
+    const int ncols_last = nblk_last < (u64)TC ? (int)nblk_last : TC;
+    bool waited = (b_ready == nullptr);
+
+    auto launch = [&](int variant, int logl, const QArgs& a, u64 tiles) -> cudaError_t {
+        QKernel k = ktab().k[variant][logl];
+        if (!k) return cudaErrorInvalidValue;
+        if (!waited && !sqr && a.src == j.b && j.b) {
+            cudaError_t e2 = cudaStreamWaitEvent(s, b_ready, 0);   // second operand copied meanwhile
+            if (e2 != cudaSuccess) return e2;
+            waited = true;
+        }
+        if (!waited && variant == V_FUSED2) {
+            cudaError_t e2 = cudaStreamWaitEvent(s, b_ready, 0);
+            if (e2 != cudaSuccess) return e2;
+            waited = true;
+        }
+        const double vec = 3.0 * (double)N * 4.0, bfly = 3.0 * ((double)N / 2.0) * logl;
+        const bool entry = (variant == V_FWD_E || variant == V_LAST_E || variant == V_FUSED_E || variant == V_SQR_E);
+        double bytes = entry ? (double)a.len * 8.0 + vec : 2.0 * vec, mm = bfly + (entry ? 6.0 * (double)a.len : 0.0);
+        int kind = K_FUSED;
+        if (variant == V_FWD || variant == V_FWD_E) kind = K_FWD;
+        else if (variant == V_LAST || variant == V_LAST_E) kind = K_FWD_LAST;
+        else if (variant == V_INV) kind = K_INV;
+        if (variant == V_FUSED2) {
+            bytes += vec;
+            mm = 3.0 * bfly + 3.0 * (double)N;
+        } else if (kind == K_FUSED) {
+            if (variant == V_FUSED || variant == V_FUSED_E) bytes += vec;
+            mm = 2.0 * bfly + 3.0 * (double)N + (entry ? 6.0 * (double)a.len : 0.0);
+        }
+        const ProfMark m = prof_begin(kind, bytes, mm, s);
+        k<<<(unsigned)(tiles * 3), NT, pass_smem(logl, variant), s>>>(a);
+        cudaError_t e2 = cudaGetLastError();
+        prof_end(m, s);
+        return e2;
+    };
+
+    QArgs pa;
+    memset(&pa, 0, sizeof(pa));
+    pa.N = N;
+    pa.ncols = TC;
+    auto fwd_strided = [&](const u64* src, u64 len, u32* data) -> cudaError_t {
+        for (int p = 0; p + 1 < P; ++p) {
+            pa.src = src;
+            pa.len = len;
+            pa.data = data;
+            pa.logB = logB[p];
+            cudaError_t e2 = launch(p == 0 ? V_FWD_E : V_FWD, pl.bits[p], pa, N >> (pl.bits[p] + LOG_TC));
+            if (e2 != cudaSuccess) return e2;
+        }
+        return cudaSuccess;
+    };
+    const bool merged = !sqr && P >= 2 && lastl >= 5 && lastl <= 8;
+    if (merged) {
+        if ((e = fwd_strided(j.a, j.la, A)) != cudaSuccess) return e;
+        if ((e = fwd_strided(j.b, j.lb, B)) != cudaSuccess) return e;
+        pa.src = nullptr;
+        pa.len = 0;
+        pa.data = B;
+        pa.other = A;
+        pa.logB = logB[P - 1];
+        pa.ncols = TC;
+        if ((e = launch(V_FUSED2, lastl, pa, tiles_last)) != cudaSuccess) return e;
+    } else if (!sqr) {
+        if ((e = fwd_strided(j.a, j.la, A)) != cudaSuccess) return e;
+        pa.src = j.a;
+        pa.len = j.la;
+        pa.data = A;
+        pa.other = nullptr;
+        pa.logB = logB[P - 1];
+        pa.ncols = ncols_last;
+        if ((e = launch(P == 1 ? V_LAST_E : V_LAST, lastl, pa, tiles_last)) != cudaSuccess) return e;
+        pa.ncols = TC;
+        if ((e = fwd_strided(j.b, j.lb, B)) != cudaSuccess) return e;
+        pa.src = j.b;
+        pa.len = j.lb;
+        pa.data = B;
+        pa.other = A;
+        pa.logB = logB[P - 1];
+        pa.ncols = ncols_last;
+        if ((e = launch(P == 1 ? V_FUSED_E : V_FUSED, lastl, pa, tiles_last)) != cudaSuccess) return e;
+    } else {
+        if ((e = fwd_strided(j.a, j.la, A)) != cudaSuccess) return e;
+        pa.src = j.a;
+        pa.len = j.la;
+        pa.data = A;
+        pa.other = A;
+        pa.logB = logB[P - 1];
+        pa.ncols = ncols_last;
+        if ((e = launch(P == 1 ? V_SQR_E : V_SQR, lastl, pa, tiles_last)) != cudaSuccess) return e;
+    }
+    pa.ncols = TC;
+    pa.src = nullptr;
+    pa.len = 0;
+    pa.other = nullptr;
+    for (int p = P - 2; p >= 0; --p) {
+        pa.data = A;
+        pa.logB = logB[p];
+        if ((e = launch(V_INV, pl.bits[p], pa, N >> (pl.bits[p] + LOG_TC))) != cudaSuccess) return e;
+    }
+    if (!waited && (e = cudaStreamWaitEvent(s, b_ready, 0)) != cudaSuccess) return e;
+
+    QCrtArgs ca;
+    memset(&ca, 0, sizeof(ca));
+    for (int i = 0; i < 3; ++i) {
+        const u64 p = kQ[i];
+        u64 M = 1;
+        for (int k = 0; k < 3; ++k)
+            if (k != i) M = h_mulmod(M, kQ[k], p);
+        const u64 minv = h_pow(M, p - 2, p);
+        const u64 ninv = h_pow(N % p, p - 2, p);
+        const u64 r2 = h_pow(2, 64, p);
+        ca.cst[i] = (u32)h_mulmod(h_mulmod(minv, ninv, p), r2, p);
+    }
+    ca.res = A;
+    ca.N = N;
+    ca.nvalid = 2 * out_len - 1;
+    ca.out = j.out;
+    ca.out_len = out_len;
+    ca.state = (u32*)(base + w.state);
+    ca.ticket = (u32*)(base + w.ticket);
+    ca.err = (u32*)base;
+    if ((e = cudaMemsetAsync(base + w.ticket, 0, w.total - w.ticket, s)) != cudaSuccess) return e;
+    if (crt_chunks < 1) crt_chunks = 1;
+    const u64 per = (w.ncta + crt_chunks - 1) / crt_chunks;
+    for (u64 t0 = 0; t0 < w.ncta; t0 += per) {
+        const u64 n = t0 + per <= w.ncta ? per : w.ncta - t0;
+        const double crt_bytes = 3.0 * (double)ca.nvalid * 4.0 + (double)out_len * 8.0;
+        const ProfMark m = prof_begin(K_CRT, crt_bytes * (double)n / (double)w.ncta,
+                                      3.0 * (double)ca.nvalid * (double)n / (double)w.ncta, s);
+        k_qcrt_carry<<<(unsigned)n, CNT, 0, s>>>(ca);
+        e = cudaGetLastError();
+        prof_end(m, s);
+        if (e != cudaSuccess) return e;
+        const u64 lo = t0 * CTILE, hi = (t0 + n) * CTILE < out_len ? (t0 + n) * CTILE : out_len;
+        if (after_chunk && (e = after_chunk(ctx, lo, hi)) != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+}  // namespace fmn

@@ -53,6 +53,7 @@ double time_plan(int n, const u64* a, const u64* b, u64* out, void* ws, size_t w
     j.lb = half;
     j.out = out;
     j.sqr = 0;
+    j.engine = fmn::ENGINE_64;      // plans are those of the 64-bit residue engine
     const size_t tb = fmn::twiddle_table_bytes(n);
     void* tbuf = nullptr;
     fmn::TwiddleSet ts;
@@ -148,7 +149,13 @@ int fmn_autotune(int n_lo, int n_hi, const char* save_path) {
         const std::vector<fmn::Plan> cands = fmn::candidate_plans(n);
         if (cands.size() <= 1) continue;
         const u64 half = 1ull << (n - 1);
-        const size_t wsb = fmn::job_workspace_bytes(half, half, 0);
+        fmn::Job wj;
+        wj.a = wj.b = nullptr;
+        wj.out = nullptr;
+        wj.la = wj.lb = half;
+        wj.sqr = 0;
+        wj.engine = fmn::ENGINE_64;
+        const size_t wsb = fmn::job_workspace_bytes(wj);
         u64 *a = nullptr, *b = nullptr, *out = nullptr;
         void* ws = nullptr;
         if ((e = cudaMalloc(&a, half * 8)) != cudaSuccess || (e = cudaMalloc(&b, half * 8)) != cudaSuccess ||

@@ -175,6 +175,25 @@ int fmn_server_replay(fmn_server* s, const fmn_request* reqs, const double* arri
                       double* latency_ms, double* wall_s);
 void fmn_server_destroy(fmn_server* s);
 
+/* ----------------------------------------------------------------- residue engines
+ * Two interchangeable transforms compute every product; the result is the same integer.
+ * FMN_ENGINE_64 works like the reference (src/fast_mul.c:308-460): 64-bit limbs modulo its
+ * three 62-bit primes (src/data.h:79-81), for transforms up to 2^30 points.
+ * FMN_ENGINE_32 splits each limb into two 32-bit digits and works modulo three 31-bit
+ * primes, whose modular products are single 32-bit multiplies on the GPU; it covers
+ * products of up to 2^25 limbs (len1 + len2 <= 33554432).  FMN_ENGINE_AUTO (the default)
+ * takes FMN_ENGINE_32 wherever it applies and FMN_ENGINE_64 elsewhere.  Batches and
+ * resident operands always run on FMN_ENGINE_64.  No counterpart in the reference. */
+#define FMN_ENGINE_AUTO 0
+#define FMN_ENGINE_64 1
+#define FMN_ENGINE_32 2
+/* Process-wide engine choice for single products (FMN_ENGINE_32 falls back to
+ * FMN_ENGINE_64 for products beyond its range).  Workspace sizes follow the choice. */
+int fmn_set_engine(int engine);
+int fmn_get_engine(void);
+/* The engine (FMN_ENGINE_64 or FMN_ENGINE_32) that a product of these lengths runs on. */
+int fmn_engine_for(u64 len1, u64 len2, int sqr);
+
 /* ----------------------------------------------------------------- pass plans and tuning
  * A 2^n-point transform runs as passes of <= 9 index bits each; the split is a plan (e.g.
  * 2^25: 9+8+8).  Plans come from the default split, from fmn_set_plan, or from a plan file

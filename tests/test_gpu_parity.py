@@ -12,11 +12,20 @@ from tests.helpers import digest, operands_for, residue_check
 pytestmark = pytest.mark.gpu
 
 
+@pytest.fixture(params=["e32", "e64"])
+def engine(request, fmn):
+    """Runs a test once per residue engine: the 32-bit-digit engine (what AUTO picks for
+    these sizes) and the 64-bit engine with the reference's primes."""
+    fmn.set_engine(fmn.ENGINE_32 if request.param == "e32" else fmn.ENGINE_64)
+    yield request.param
+    fmn.set_engine(fmn.ENGINE_AUTO)
+
+
 def run(fmn, c, a, b):
     return fmn.abs_sqr64(a) if c["op"] == "sqr" else fmn.abs_mul64(a, b)
 
 
-def test_golden_small_and_medium(fmn, golden):
+def test_golden_small_and_medium(fmn, golden, engine):
     """All golden cases up to 140k output limbs: sizes 1..2000 in every pairing pattern,
     uniform / all-ones / sparse operands, squares, 10k x 10k (transform length 2^15),
     unbalanced products and transform-length boundaries."""
@@ -31,7 +40,7 @@ def test_golden_small_and_medium(fmn, golden):
     assert n > 800
 
 
-def test_random_shapes_vs_oracle(fmn, oracle):
+def test_random_shapes_vs_oracle(fmn, oracle, engine):
     """Seeded random (possibly very unbalanced) shapes against the oracle restatement."""
     rng = np.random.default_rng(2024)
     for i in range(60):
@@ -45,7 +54,7 @@ def test_random_shapes_vs_oracle(fmn, oracle):
             assert np.array_equal(fmn.abs_sqr64(a), oracle.sqr(a)), (kind, la)
 
 
-def test_transform_length_boundaries(fmn, oracle):
+def test_transform_length_boundaries(fmn, oracle, engine):
     """conv_len = 2^k - 1, 2^k, 2^k + 1 for every k up to 2^20: each pass plan (1, 2 and 3
     passes) and its edges."""
     for k in range(0, 21):
@@ -60,7 +69,7 @@ def test_transform_length_boundaries(fmn, oracle):
             assert np.array_equal(fmn.abs_mul64(a, b), oracle.mul(a, b)), (k, la, lb)
 
 
-def test_carry_chains(fmn, oracle):
+def test_carry_chains(fmn, oracle, engine):
     """All-ones operands (longest carry chains) and products that are all-ones runs."""
     for n in (1, 2, 3, 1000, 4096, 65537, 300000):
         a = synth.limbs("ones", n)
@@ -76,7 +85,7 @@ def test_carry_chains(fmn, oracle):
     assert np.array_equal(fmn.abs_mul64(a, b), oracle.mul(a, b))
 
 
-def test_out_aliases_input(fmn, oracle):
+def test_out_aliases_input(fmn, oracle, engine):
     """out may alias in1 (the reference copies inputs before writing out)."""
     lib = fmn.load_library()
     a, b = synth.operands("uniform", 5000, 3000, 11)
@@ -88,7 +97,7 @@ def test_out_aliases_input(fmn, oracle):
     assert np.array_equal(buf, want)
 
 
-def test_same_block_is_square(fmn, oracle):
+def test_same_block_is_square(fmn, oracle, engine):
     a = synth.limbs("uniform", 12345, 4)
     lib = fmn.load_library()
     out = np.zeros(2 * len(a), np.uint64)
@@ -97,7 +106,7 @@ def test_same_block_is_square(fmn, oracle):
     assert np.array_equal(out, oracle.sqr(a))
 
 
-def test_pinned_host_buffers(fmn, oracle):
+def test_pinned_host_buffers(fmn, oracle, engine):
     """abs_mul64 / abs_sqr64 on pinned host memory take the overlapped path (second operand
     copied while the first is transformed, output copied back in chunks)."""
     import torch
@@ -115,7 +124,7 @@ def test_pinned_host_buffers(fmn, oracle):
         assert np.array_equal(hs, oracle.sqr(a)), la
 
 
-def test_device_api_and_caller_workspace(fmn, oracle):
+def test_device_api_and_caller_workspace(fmn, oracle, engine):
     import torch
     a, b = synth.operands("uniform", 70000, 50000, 21)
     want = oracle.mul(a, b)
@@ -147,10 +156,51 @@ def test_device_api_and_caller_workspace(fmn, oracle):
 ])
 def test_full_size_golden(fmn, oracle, golden, op, kind, l1, l2):
     """The full-size configurations against the reference's own outputs (SHA-256 of all
-    limbs) and the residue property mod three 61-bit primes."""
+    limbs) and the residue property mod three 61-bit primes, on the engine AUTO picks."""
     c = next(c for c in golden if (c["op"], c["kind"], c["len1"], c["len2"]) == (op, kind, l1, l2))
     a, b = operands_for(c)
     out = run(fmn, c, a, b)
     assert digest(out) == c["sha256"]
     assert [f"{int(v):016x}" for v in out[:4]] == c["head"]
     assert residue_check(oracle, a, b, out, sqr=(op == "sqr"))
+
+
+@pytest.mark.parametrize("op,kind,l1,l2", [
+    ("mul", "uniform", 1000000, 1000000), ("sqr", "uniform", 10000000, 10000000),
+    ("mul", "ones", 10000000, 10000000),
+])
+def test_full_size_golden_64bit_engine(fmn, oracle, golden, op, kind, l1, l2):
+    """Sizes that AUTO runs on the 32-bit engine, forced onto the 64-bit engine."""
+    c = next(c for c in golden if (c["op"], c["kind"], c["len1"], c["len2"]) == (op, kind, l1, l2))
+    a, b = operands_for(c)
+    fmn.set_engine(fmn.ENGINE_64)
+    try:
+        out = run(fmn, c, a, b)
+    finally:
+        fmn.set_engine(fmn.ENGINE_AUTO)
+    assert digest(out) == c["sha256"]
+
+
+@pytest.mark.parametrize("kind", ["uniform", "ones"])
+def test_engines_agree_at_the_32bit_limit(fmn, oracle, kind):
+    """2^24 x 2^24 limbs: the largest product the 32-bit engine takes (a 2^26-digit transform
+    whose coefficients come closest to the product of its primes).  Both engines must give
+    the same limbs, which must pass the residue check."""
+    import torch
+    n = 1 << 24
+    a, b = synth.operands(kind, n, n, 77)
+    da = torch.from_numpy(a.view(np.int64)).cuda()
+    db = torch.from_numpy(b.view(np.int64)).cuda()
+    outs = []
+    for eng in (fmn.ENGINE_32, fmn.ENGINE_64):
+        fmn.set_engine(eng)
+        try:
+            assert fmn.engine_for(n, n) == eng
+            o = torch.empty(2 * n, dtype=torch.int64, device="cuda")
+            fmn.mul_device(da, db, o)
+            fmn.sync()
+            outs.append(o)
+        finally:
+            fmn.set_engine(fmn.ENGINE_AUTO)
+    assert torch.equal(outs[0], outs[1])
+    assert residue_check(oracle, a, b, outs[0].cpu().numpy().view(np.uint64))

@@ -52,9 +52,11 @@ def test_set_plan_validates_and_restores():
 
 @pytest.mark.gpu
 def test_products_under_every_plan_shape(fmn, oracle):
-    """Alternative splits (2 and 3 passes, last pass 9 bits or fewer) give the same numbers."""
+    """Alternative splits (2 and 3 passes, last pass 9 bits or fewer) give the same numbers.
+    Plans belong to the 64-bit residue engine, which these products are pinned to."""
     import torch
     cases = {15: [[7, 8], [5, 5, 5], [9, 6]], 18: [[9, 9], [6, 6, 6], [5, 9, 4]], 21: [[9, 6, 6], [5, 8, 8], [7, 7, 7]]}
+    fmn.set_engine(fmn.ENGINE_64)
     try:
         for n, plans in cases.items():
             half = 1 << (n - 1)
@@ -81,5 +83,34 @@ def test_products_under_every_plan_shape(fmn, oracle):
             fmn.sync()
             assert torch.equal(out, ref), bits
     finally:
+        fmn.set_engine(fmn.ENGINE_AUTO)
         for n in (15, 18, 21, 24):
             fmn.set_plan(n, None)
+
+
+def test_engine_selection_rules():
+    """AUTO takes the 32-bit residue engine up to 2^25 output limbs and the 64-bit one beyond;
+    a forced engine is honoured where it applies; resident/batched paths are documented as
+    64-bit only."""
+    assert fmn.get_engine() == fmn.ENGINE_AUTO
+    assert fmn.engine_for(10_000_000, 10_000_000) == fmn.ENGINE_32
+    assert fmn.engine_for(1 << 24, 1 << 24) == fmn.ENGINE_32             # 2^26-digit transform
+    assert fmn.engine_for(1 << 24, (1 << 24) + 1) == fmn.ENGINE_64
+    assert fmn.engine_for(64_000_000, 250_000) == fmn.ENGINE_64
+    assert fmn.engine_for(1, 1, sqr=True) == fmn.ENGINE_32
+    fmn.set_engine(fmn.ENGINE_64)
+    try:
+        assert fmn.engine_for(10_000_000, 10_000_000) == fmn.ENGINE_64
+        ws64 = fmn.workspace_size(1000, 3000)
+    finally:
+        fmn.set_engine(fmn.ENGINE_AUTO)
+    fmn.set_engine(fmn.ENGINE_32)
+    try:
+        assert fmn.engine_for(64_000_000, 64_000_000) == fmn.ENGINE_64      # beyond its range
+        ws32 = fmn.workspace_size(1000, 3000)
+    finally:
+        fmn.set_engine(fmn.ENGINE_AUTO)
+    # 4000 limbs: 2^12-point transform of u64 vs 2^13 digits of u32 -- the same residue bytes
+    assert ws32 == ws64
+    with pytest.raises(fmn.FastMulError):
+        fmn.set_engine(7)
