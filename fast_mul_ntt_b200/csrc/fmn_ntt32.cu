@@ -58,7 +58,9 @@ __device__ __forceinline__ u32 qroot(u32 x, int pi, const PrimeQ& q) {
 }
 
 constexpr int TP = TC + 1;              // padded row pitch of a shared-memory tile (words)
-__device__ __forceinline__ int tix(int j, int c) { return j * TP + c; }
+// Odd columns swap the two halves of the row (c ^ 16), a permutation within the row: a warp
+// that covers 16 rows of two adjacent columns then touches two disjoint bank ranges.
+__device__ __forceinline__ int tix(int j, int c) { return j * TP + (c ^ ((c & 1) << 4)); }
 
 enum { M_FWD = 0, M_FWD_LAST = 1, M_FUSED = 2, M_INV = 3, M_FUSED2 = 4 };
 
@@ -462,8 +464,15 @@ __device__ __forceinline__ void body_fused2(u32* sm, const QArgs& a, u64 tile, i
     run_round<LOGL, RB0, LOGL - 1, true, true>(lds, stg, pi, q);
 }
 
+// Kernels whose tiles limit them to 3 CTAs per SM anyway (9-bit strided passes, the merged
+// pass) get the registers of 3 CTAs; 8-bit strided passes too (their radix-16 rounds spill at 64).
+template <int MODE, int LOGL>
+constexpr int min_ctas() {
+    return ((MODE == M_FWD || MODE == M_INV) && LOGL >= 8) || MODE == M_FUSED2 ? 3 : 4;
+}
+
 template <int MODE, int LOGL, bool ENTRY, bool SQR>
-__global__ void __launch_bounds__(NT, (MODE == M_FWD || MODE == M_INV) && LOGL >= 9 ? 3 : 4) k_qpass(QArgs a) {
+__global__ void __launch_bounds__(NT, (min_ctas<MODE, LOGL>())) k_qpass(QArgs a) {
     extern __shared__ __align__(16) u32 qsm[];
     const int pi = blockIdx.x % 3;          // the three CTAs of a tile read the same limbs together
     const u64 tile = blockIdx.x / 3;
