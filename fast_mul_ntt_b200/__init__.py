@@ -33,7 +33,8 @@ EXPORTS = ["abs_mul64", "abs_sqr64", "fmn_init", "fmn_shutdown", "fmn_last_error
            "fmn_operand_workspace_size", "fmn_mul_operand_ws", "fmn_server_create", "fmn_server_submit",
            "fmn_server_wait", "fmn_server_take", "fmn_server_get_stats", "fmn_server_replay", "fmn_server_destroy",
            "fmn_get_plan", "fmn_set_plan", "fmn_autotune", "fmn_load_plans", "fmn_load_default_plans",
-           "fmn_set_engine", "fmn_get_engine", "fmn_engine_for"]
+           "fmn_set_engine", "fmn_get_engine", "fmn_engine_for", "fmn_pieces_for",
+           "fmn_force_pieces"]
 
 ENGINE_AUTO, ENGINE_64, ENGINE_32 = 0, 1, 2
 
@@ -178,6 +179,10 @@ def load_library(path=None):
     lib.fmn_get_engine.restype = ctypes.c_int
     lib.fmn_engine_for.argtypes = [_u64, _u64, ctypes.c_int]
     lib.fmn_engine_for.restype = ctypes.c_int
+    lib.fmn_pieces_for.argtypes = [_u64, _u64, ctypes.c_int]
+    lib.fmn_pieces_for.restype = ctypes.c_int
+    lib.fmn_force_pieces.argtypes = [ctypes.c_int]
+    lib.fmn_force_pieces.restype = ctypes.c_int
     if path is None:
         _lib = lib
     return lib
@@ -473,6 +478,16 @@ def get_engine():
 def engine_for(len1, len2, sqr=False):
     """The engine (ENGINE_64 or ENGINE_32) a product of these lengths runs on."""
     return load_library().fmn_engine_for(len1, len2, 1 if sqr else 0)
+
+
+def pieces_for(len1, len2, sqr=False):
+    """Pieces a product is split into on the 32-bit engine (1: one whole transform)."""
+    return load_library().fmn_pieces_for(len1, len2, 1 if sqr else 0)
+
+
+def force_pieces(pieces):
+    """Tests and tuning: split products into this many pieces where possible (0: cost model)."""
+    _check(load_library().fmn_force_pieces(pieces))
 
 
 def autotune(n_lo=10, n_hi=27, save_path=None):

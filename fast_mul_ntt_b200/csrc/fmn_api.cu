@@ -539,6 +539,22 @@ int fmn_set_engine(int engine) {
 
 int fmn_get_engine(void) { return fmn::default_engine(); }
 
+int fmn_force_pieces(int pieces) {
+    if (pieces < 0) return set_err(FMN_ERR_ARG, "pieces must be >= 0");
+    fmn::q32_force_pieces(pieces);
+    return FMN_OK;
+}
+
+int fmn_pieces_for(u64 len1, u64 len2, int sqr) {
+    fmn::Job j;
+    j.a = j.b = nullptr;
+    j.out = nullptr;
+    j.la = len1;
+    j.lb = len2;
+    j.sqr = sqr ? 1 : 0;
+    return fmn::job_engine(j) == fmn::ENGINE_32 ? fmn::q32_pieces(len1, len2, sqr ? 1 : 0) : 1;
+}
+
 int fmn_engine_for(u64 len1, u64 len2, int sqr) {
     fmn::Job j;
     j.a = j.b = nullptr;

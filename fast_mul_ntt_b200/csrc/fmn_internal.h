@@ -47,16 +47,21 @@ struct Job {
 
 // Residue engines.  ENGINE_64 transforms 64-bit limbs modulo the reference's three 62-bit
 // primes (fmn_ntt.cu); ENGINE_32 transforms 32-bit digits modulo three 31-bit primes
-// (fmn_ntt32.cu), which is faster but limited to transforms of 2^26 digits (products of up
-// to 2^25 limbs).  ENGINE_AUTO takes ENGINE_32 wherever it applies.  Both give the same
+// (fmn_ntt32.cu), which is faster; it transforms at most 2^26 digits, so it runs products of up
+// to 2^25 limbs whole and splits longer ones whose shorter operand has at most 2^25 limbs.
+// ENGINE_AUTO takes the one with the lower modelled cost (ENGINE_32 wherever it applies,
+// except where a split would need many pieces).  Both give the same
 // integer product.  Batches and resident operands always use ENGINE_64.
 enum Engine { ENGINE_AUTO = 0, ENGINE_64 = 1, ENGINE_32 = 2 };
 void set_default_engine(int engine);
 int default_engine();
 int job_engine(const Job& j);      // the engine that runs j (never ENGINE_AUTO)
-bool q32_fits(u64 la, u64 lb);
+bool q32_fits(u64 la, u64 lb, int sqr);        // the 32-bit engine can run this product
+double q32_cost(u64 la, u64 lb, int sqr);      // its modelled cost (32-bit points x bits)
 size_t q32_workspace_bytes(u64 la, u64 lb, int sqr);
 int q32_launches(u64 la, u64 lb, int sqr);
+int q32_pieces(u64 la, u64 lb, int sqr);        // 1: whole product; > 1: split into pieces
+void q32_force_pieces(int m);                  // tests: split into m pieces where possible (0: model)
 typedef cudaError_t (*ChunkDone)(void* ctx, u64 first_limb, u64 end_limb);
 cudaError_t q32_enqueue(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s, cudaEvent_t b_ready, int crt_chunks,
                         ChunkDone after_chunk, void* ctx);

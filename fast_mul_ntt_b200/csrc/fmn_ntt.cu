@@ -997,11 +997,21 @@ static std::atomic<int> g_engine{ENGINE_AUTO};
 void set_default_engine(int engine) { g_engine.store(engine); }
 int default_engine() { return g_engine.load(); }
 
+// A (point x bit) of this engine's transform costs about 2.4 times one of the 32-bit engine
+// (measured on B200: 10M x 10M limbs, 2^25 64-bit points in 6.73 ms against 2^26 32-bit
+// digits in 5.74 ms).
+constexpr double kCost64 = 2.4;
+
 int job_engine(const Job& j) {
     if (j.spectrum) return ENGINE_64;
     const int e = j.engine ? j.engine : default_engine();
     if (e == ENGINE_64) return ENGINE_64;
-    return q32_fits(j.la, j.lb) ? ENGINE_32 : ENGINE_64;
+    const int sqr = j.sqr ? 1 : 0;
+    if (!q32_fits(j.la, j.lb, sqr)) return ENGINE_64;
+    if (e == ENGINE_32) return ENGINE_32;
+    const u64 N = ceil_pow2(j.la + j.lb - 1);
+    const double c64 = kCost64 * (sqr ? 2.0 : 3.0) * (double)N * (ilog2(N) + 1);
+    return q32_cost(j.la, j.lb, sqr) <= c64 ? ENGINE_32 : ENGINE_64;
 }
 
 static Job plain_job(u64 la, u64 lb, int sqr) {

@@ -22,6 +22,7 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <atomic>
 #include <mutex>
 #include <vector>
 
@@ -40,7 +41,9 @@ constexpr int QTWB = 13;                // two-level root tables: w^x = HI[x >> 
 constexpr u32 MASK_N = (1u << Q32_MAX_LOG_N) - 1;
 static_assert(2 * QTWB == Q32_MAX_LOG_N, "two-level table covers roots of order 2^26");
 
-__device__ __align__(16) uint2 g_qrt[2][3][RT_SIZE];   // [forward/inverse][prime]: (w, w') Shoup pairs
+// [forward/inverse][prime]: (w, w') Shoup pairs, stored stage-major: the twiddle of stage
+// entry j of the group with low offset q is at rt_off(RB, TOP) + j * 2^(TOP-RB+1) + q.
+__device__ __align__(16) uint2 g_qrt[2][3][RT_SIZE];
 __device__ __align__(16) u32 g_qtw[2][3][1 << QTWB];   // [low/high level][prime], Montgomery form
 __constant__ PrimeQ c_q[3] = {prime_q(Q32_P0), prime_q(Q32_P1), prime_q(Q32_P2)};
 
@@ -62,16 +65,24 @@ constexpr int TP = TC + 1;              // padded row pitch of a shared-memory t
 // that covers 16 rows of two adjacent columns then touches two disjoint bank ranges.
 __device__ __forceinline__ int tix(int j, int c) { return j * TP + (c ^ ((c & 1) << 4)); }
 
-enum { M_FWD = 0, M_FWD_LAST = 1, M_FUSED = 2, M_INV = 3, M_FUSED2 = 4 };
+enum { M_FWD = 0, M_FWD_LAST = 1, M_FUSED = 2, M_INV = 3, M_FUSED2 = 4, M_INV_ACC = 5 };
 
 struct QArgs {
     const u64* src;   // ENTRY: limbs of the operand being transformed
     u64 len;          // ENTRY: number of limbs (2 * len digits)
     u32* data;        // residue arrays of the operand being transformed
     u32* other;       // M_FUSED / M_FUSED2: the other operand's spectrum; the product goes here
+    u32* dst;         // M_FUSED: where the product goes when `other` must stay intact (else null)
     u64 N;            // transform length (digits)
     int logB;         // log2 block length of this pass
     int ncols;        // contiguous passes: number of blocks (columns) in a tile, <= 32
+    // M_INV_ACC (the last inverse pass of one piece of a split product): coefficient i < acc_valid
+    // of this piece goes to acc[prime * acc_stride + i], added mod q where i < acc_fresh (the
+    // overlap with the previous piece) and stored elsewhere.
+    u32* acc;
+    u64 acc_stride;
+    u64 acc_valid;
+    u64 acc_fresh;
 };
 
 // ------------------------------------------------------------------ one round
@@ -102,7 +113,7 @@ __device__ __forceinline__ void run_round(LD ld, ST st, int pi, const PrimeQ& q)
 #pragma unroll
             for (int t = 0; t < R; ++t) x[t] = ld(row0 + t * SP, c);
         }
-        const uint2* tw = tab + qlo * R;
+        const uint2* tw = tab + qlo;       // stage-major table: lanes of consecutive groups coalesce
         if (!INV) {
 #pragma unroll
             for (int s = 0; s < RB; ++s) {
@@ -114,7 +125,7 @@ __device__ __forceinline__ void run_round(LD ld, ST st, int pi, const PrimeQ& q)
                     if (LOWEST && u == 0)
                         qbfly_dif1(x[t], x[t + half], q);
                     else
-                        qbfly_dif(x[t], x[t + half], __ldg(tw + (R - (R >> s)) + u), q);
+                        qbfly_dif(x[t], x[t + half], __ldg(tw + ((R - (R >> s)) + u) * SP), q);
                 }
             }
         } else {
@@ -128,7 +139,7 @@ __device__ __forceinline__ void run_round(LD ld, ST st, int pi, const PrimeQ& q)
                     if (LOWEST && u == 0)
                         qbfly_dit1(x[t], x[t + half], q);
                     else
-                        qbfly_dit(x[t], x[t + half], __ldg(tw + (R - (R >> s)) + u), q);
+                        qbfly_dit(x[t], x[t + half], __ldg(tw + ((R - (R >> s)) + u) * SP), q);
                 }
             }
         }
@@ -260,8 +271,9 @@ __device__ __forceinline__ void body_fwd(u32* sm, const QArgs& a, u64 tile, int 
     rounds<LOGL, false, false, 0, true>(sm, ld0, stl, pi, q);
 }
 
-// Inverse strided pass: inverse four-step twiddle, then the inverse sub-transform.
-template <int LOGL>
+// Inverse strided pass: inverse four-step twiddle, then the inverse sub-transform.  ACC: the
+// coefficients go to the accumulator of a split product instead (see QArgs).
+template <int LOGL, bool ACC>
 __device__ __forceinline__ void body_inv(u32* sm, const QArgs& a, u64 tile, int pi, const PrimeQ& q) {
     constexpr int L = 1 << LOGL;
     constexpr int RB = round_bits(LOGL, rounds_count(LOGL) - 1), R = 1 << RB;
@@ -286,8 +298,18 @@ __device__ __forceinline__ void body_inv(u32* sm, const QArgs& a, u64 tile, int 
             x[t] = qmont(x[t], qmont_lazy(al, beta[tp * TC + c], q), q);
         }
     };
-    auto stl = [=](int j, int c, u32 v) { d[gbase + c + ((u32)j << logS)] = v; };
-    rounds<LOGL, true, false, 0, false, true>(sm, ld0, stl, pi, q);
+    if constexpr (ACC) {
+        u32* __restrict__ acc = a.acc + (u64)pi * a.acc_stride;
+        const u64 valid = a.acc_valid, fresh = a.acc_fresh;
+        auto stl = [=](int j, int c, u32 v) {
+            const u32 i = gbase + c + ((u32)j << logS);
+            if (i < valid) acc[i] = i < fresh ? qadd(acc[i], v, q) : v;
+        };
+        rounds<LOGL, true, false, 0, false, true>(sm, ld0, stl, pi, q);
+    } else {
+        auto stl = [=](int j, int c, u32 v) { d[gbase + c + ((u32)j << logS)] = v; };
+        rounds<LOGL, true, false, 0, false, true>(sm, ld0, stl, pi, q);
+    }
 }
 
 // Forward last pass over contiguous blocks (first operand of a product).
@@ -383,8 +405,9 @@ __device__ __forceinline__ void body_fused(u32* sm, const QArgs& a, u64 tile, in
     constexpr int NR = rounds_count(LOGL);
     const u32 gbase = (u32)tile << (LOGL + LOG_TC);
     const int ncols = a.ncols;
-    const u32* __restrict__ d = a.data + (u64)pi * a.N;
-    u32* __restrict__ o = a.other + (u64)pi * a.N;
+    const u32* d = a.data + (u64)pi * a.N;
+    const u32* o = a.other + (u64)pi * a.N;
+    u32* dd = (a.dst ? a.dst : a.other) + (u64)pi * a.N;   // may be `data` itself (in place)
     const u64* __restrict__ src = a.src;
     const u64 len = a.len;
     auto ldg = [=](int j, int c) -> u32 {
@@ -394,7 +417,7 @@ __device__ __forceinline__ void body_fused(u32* sm, const QArgs& a, u64 tile, in
         else return d[g];
     };
     auto stg = [=](int j, int c, u32 v) {
-        if (c < ncols) o[gbase + (u32)c * L + j] = v;
+        if (c < ncols) dd[gbase + (u32)c * L + j] = v;
     };
     auto lds = [sm](int j, int c) { return sm[tix(j, c)]; };
     auto sts = [sm](int j, int c, u32 v) { sm[tix(j, c)] = v; };
@@ -468,7 +491,7 @@ __device__ __forceinline__ void body_fused2(u32* sm, const QArgs& a, u64 tile, i
 // pass) get the registers of 3 CTAs; 8-bit strided passes too (their radix-16 rounds spill at 64).
 template <int MODE, int LOGL>
 constexpr int min_ctas() {
-    return ((MODE == M_FWD || MODE == M_INV) && LOGL >= 8) || MODE == M_FUSED2 ? 3 : 4;
+    return ((MODE == M_FWD || MODE == M_INV || MODE == M_INV_ACC) && LOGL >= 8) || MODE == M_FUSED2 ? 3 : 4;
 }
 
 template <int MODE, int LOGL, bool ENTRY, bool SQR>
@@ -478,7 +501,8 @@ __global__ void __launch_bounds__(NT, (min_ctas<MODE, LOGL>())) k_qpass(QArgs a)
     const u64 tile = blockIdx.x / 3;
     const PrimeQ q = c_q[pi];
     if constexpr (MODE == M_FWD) body_fwd<LOGL, ENTRY>(qsm, a, tile, pi, q);
-    else if constexpr (MODE == M_INV) body_inv<LOGL>(qsm, a, tile, pi, q);
+    else if constexpr (MODE == M_INV) body_inv<LOGL, false>(qsm, a, tile, pi, q);
+    else if constexpr (MODE == M_INV_ACC) body_inv<LOGL, true>(qsm, a, tile, pi, q);
     else if constexpr (MODE == M_FWD_LAST) body_fwd_last<LOGL, ENTRY>(qsm, a, tile, pi, q);
     else if constexpr (MODE == M_FUSED2) body_fused2<(LOGL >= 5 ? LOGL : 5)>(qsm, a, tile, pi, q);
     else body_fused<LOGL, ENTRY, SQR>(qsm, a, tile, pi, q);
@@ -652,7 +676,8 @@ static const HostTables& host_tables() {
                             for (int u = 0; u < (R >> (s + 1)); ++u) {
                                 // w_{2^(top-s+1)}^(qq + u 2^spl) = w^((qq + u 2^spl) 2^(26-(top-s+1)))
                                 const u64 e = ((u64)qq + ((u64)u << spl)) << (Q32_MAX_LOG_N - (top - s + 1));
-                                const size_t at = (size_t)rt_off(r, top) + (size_t)qq * R + (R - (R >> s)) + u;
+                                // stage-major: entry j = (R - (R >> s)) + u of group offset qq
+                                const size_t at = (size_t)rt_off(r, top) + ((size_t)(R - (R >> s)) + u << spl) + qq;
                                 const u64 wf = wpow(e);
                                 const u64 wi = wpow((1ull << Q32_MAX_LOG_N) - (e & MASK_N));
                                 const size_t f0 = (((size_t)0 * 3 + i) * RT_SIZE + at) * 2;
@@ -670,7 +695,7 @@ static const HostTables& host_tables() {
 
 // ------------------------------------------------------------------ host: kernels
 typedef void (*QKernel)(QArgs);
-enum { V_FWD, V_FWD_E, V_LAST, V_LAST_E, V_FUSED, V_FUSED_E, V_SQR, V_SQR_E, V_INV, V_FUSED2, NV };
+enum { V_FWD, V_FWD_E, V_LAST, V_LAST_E, V_FUSED, V_FUSED_E, V_SQR, V_SQR_E, V_INV, V_FUSED2, V_INV_ACC, NV };
 
 template <int LOGL>
 static void fill_row(QKernel (&t)[NV][MAX_PASS_BITS + 1]) {
@@ -679,6 +704,7 @@ static void fill_row(QKernel (&t)[NV][MAX_PASS_BITS + 1]) {
     t[V_FWD][LOGL] = LOGL >= 5 ? k_qpass<M_FWD, LS, false, false> : nullptr;
     t[V_FWD_E][LOGL] = LOGL >= 5 ? k_qpass<M_FWD, LS, true, false> : nullptr;
     t[V_INV][LOGL] = LOGL >= 5 ? k_qpass<M_INV, LS, false, false> : nullptr;
+    t[V_INV_ACC][LOGL] = LOGL >= 5 ? k_qpass<M_INV_ACC, LS, false, false> : nullptr;
     t[V_FUSED2][LOGL] = (LOGL >= 5 && LOGL <= 8) ? k_qpass<M_FUSED2, LM, false, false> : nullptr;
     t[V_LAST][LOGL] = k_qpass<M_FWD_LAST, LOGL, false, false>;
     t[V_LAST_E][LOGL] = k_qpass<M_FWD_LAST, LOGL, true, false>;
@@ -779,103 +805,140 @@ static int ilog2(u64 x) {
 }
 static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
-// Workspace: [error word, 256 B][A residues][B residues][ticket + state], as in fmn_ntt.cu.
-struct QLayout {
-    u64 N;
+// How one product runs on this engine.
+//   whole: both operands are transformed at the product's length 2^n >= 2 (la + lb) - 1 digits,
+//     their last forward passes merged with the pointwise product.
+//   split (conv_single reuse, reference src/fast_mul.c:135-212, applied to the long operand):
+//     the shorter operand S (ls limbs) is transformed once at a smaller length 2^n; the longer
+//     operand is cut into m pieces of cb limbs, each multiplied with S's resident spectrum;
+//     every piece's coefficients are accumulated at digit offset 2 k cb into one residue array
+//     over the whole product (mod q; consecutive pieces overlap in 2 ls - 1 digits), and one
+//     CRT + carry pass turns the sum into limbs.  The sum is the full product's coefficient,
+//     which the three primes represent exactly while ls <= 2^25.
+//   The plan with the smaller modelled cost wins: (1 + 2m) transforms of 2^n points x (n + 1)
+//   (butterfly levels plus one for the per-pass memory work), plus a fixed cost per piece for
+//   its launches.
+struct QJob {
+    bool ok;
+    double cost;           // modelled cost in (32-bit points x bits)
+    int m;                 // pieces (1: whole product)
+    bool swap;             // split: the short operand is the second one
+    u64 ls, ll, cb;        // split: short and long lengths, limbs per piece
     int n;
-    size_t a, b, ticket, state, total;
+    u64 N;                 // transform length (digits)
+    u64 stride;            // split: accumulator digits per prime
+    size_t a, b, acc, ticket, state, total;   // workspace offsets (split: a = S's spectrum, b = piece)
     u64 ncta;
 };
-static QLayout layout(u64 la, u64 lb, int sqr) {
-    QLayout w;
-    memset(&w, 0, sizeof(w));
+
+constexpr int kMinSplitLog = 12;           // pieces transform at least 2^12 digits (>= 2 passes)
+std::atomic<int> g_force_pieces{0};        // > 1: split every product that allows it into this many pieces
+constexpr u64 kMaxPieces = 1ull << 16;
+constexpr double kPieceCost = 3.0e7;       // launch overhead of one piece, in (points x bits)
+
+static QJob plan_job(u64 la, u64 lb, int sqr) {
+    QJob J;
+    memset(&J, 0, sizeof(J));
     const u64 out_len = la + lb;
-    if (la == 0 || lb == 0) return w;
-    w.N = ceil_pow2(2 * out_len - 1);
-    w.n = ilog2(w.N);
-    w.ncta = (out_len + CTILE - 1) / CTILE;
+    if (la == 0 || lb == 0) return J;
+    double best = 1e300;
+    if (out_len <= (1ull << (Q32_MAX_LOG_N - 1))) {             // whole: 2 out_len - 1 <= 2^26
+        J.ok = true;
+        J.m = 1;
+        J.N = ceil_pow2(2 * out_len - 1);
+        J.n = ilog2(J.N);
+        best = (sqr ? 2.0 : 3.0) * (double)J.N * (J.n + 1);
+    }
+    const u64 ls = la < lb ? la : lb, ll = la < lb ? lb : la;
+    const int force = g_force_pieces.load();
+    if (force > 1 && !sqr && ls <= (1ull << (Q32_MAX_LOG_N - 1)) && ll >= (u64)force) {
+        const u64 cb = (ll + force - 1) / force;
+        const u64 m = (ll + cb - 1) / cb;
+        int n = ilog2(2 * (ls + cb) - 1);
+        if (n < kMinSplitLog) n = kMinSplitLog;
+        if (m >= 2 && n <= Q32_MAX_LOG_N) {
+            best = -1.0;                                        // forced: wins over every other plan
+            J.ok = true;
+            J.m = (int)m;
+            J.swap = lb < la;
+            J.ls = ls;
+            J.ll = ll;
+            J.cb = cb;
+            J.n = n;
+            J.N = 1ull << n;
+        }
+    }
+    if (!sqr && best >= 0.0 && ls <= (1ull << (Q32_MAX_LOG_N - 1))) {
+        for (int n = kMinSplitLog; n <= Q32_MAX_LOG_N; ++n) {
+            const u64 half = 1ull << (n - 1);                   // piece product: ls + cb <= 2^(n-1) limbs
+            if (half <= ls) continue;
+            const u64 cbmax = half - ls;
+            u64 m = (ll + cbmax - 1) / cbmax;
+            if (m < 2 || m > kMaxPieces) continue;
+            const u64 cb = (ll + m - 1) / m;
+            m = (ll + cb - 1) / cb;                             // no empty last piece
+            if (m < 2) continue;
+            const double cost = (1.0 + 2.0 * (double)m) * (double)(1ull << n) * (n + 1) + (double)m * kPieceCost;
+            if (cost < best) {
+                best = cost;
+                J.ok = true;
+                J.m = (int)m;
+                J.swap = lb < la;
+                J.ls = ls;
+                J.ll = ll;
+                J.cb = cb;
+                J.n = n;
+                J.N = 1ull << n;
+            }
+        }
+    }
+    if (!J.ok) return J;
+    J.cost = best;
+    J.ncta = (out_len + CTILE - 1) / CTILE;
     size_t off = 256;
-    w.a = off;
-    off = align256(off + 3 * w.N * sizeof(u32));
-    w.b = off;
-    if (!sqr) off = align256(off + 3 * w.N * sizeof(u32));
-    w.ticket = off;
-    w.state = off + 16;
-    off = align256(w.state + w.ncta * sizeof(u32));
-    w.total = off;
-    return w;
+    J.a = off;
+    off = align256(off + 3 * J.N * sizeof(u32));
+    J.b = off;
+    if (!(J.m == 1 && sqr)) off = align256(off + 3 * J.N * sizeof(u32));
+    if (J.m > 1) {
+        J.stride = (2 * out_len + 63) & ~63ull;
+        J.acc = off;
+        off = align256(off + 3 * J.stride * sizeof(u32));
+    }
+    J.ticket = off;
+    J.state = off + 16;
+    off = align256(J.state + J.ncta * sizeof(u32));
+    J.total = off;
+    return J;
 }
 
-}  // namespace q32
+// Launch sequencing of one product on one stream: kernel lookup, the wait for the second
+// operand's copy before its first reader, per-launch timing records.
+struct Launcher {
+    const Job& j;
+    cudaStream_t s;
+    cudaEvent_t b_ready;
+    bool waited;
+    u64 N;
 
-bool q32_fits(u64 la, u64 lb) {
-    if (la == 0 || lb == 0) return false;
-    const u64 out_len = la + lb;
-    return out_len <= (1ull << (Q32_MAX_LOG_N - 1));   // 2 * out_len - 1 < 2^26
-}
-
-size_t q32_workspace_bytes(u64 la, u64 lb, int sqr) {
-    const size_t t = q32::layout(la, lb, sqr).total;
-    return t ? t : 256;
-}
-
-int q32_launches(u64 la, u64 lb, int sqr) {
-    if (la == 0 || lb == 0) return 0;
-    const q32::QLayout w = q32::layout(la, lb, sqr);
-    const Plan pl = q32::qplan(w.n);
-    const int P = pl.passes;
-    const int lastl = pl.bits[P - 1];
-    if (!sqr && P >= 2 && lastl >= 5 && lastl <= 8) return 2 * (P - 1) + 1 + (P - 1) + 1;
-    return sqr ? (P - 1) + 1 + (P - 1) + 1 : 2 * (P - 1) + 1 + 1 + (P - 1) + 1;
-}
-
-cudaError_t q32_enqueue(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s, cudaEvent_t b_ready, int crt_chunks,
-                        ChunkDone after_chunk, void* ctx) {
-    using namespace q32;
-    const u64 out_len = j.la + j.lb;
-    if (out_len == 0) return cudaSuccess;
-    if (j.la == 0 || j.lb == 0) return cudaMemsetAsync(j.out, 0, out_len * sizeof(u64), s);
-    if (!q32_fits(j.la, j.lb)) return cudaErrorInvalidValue;
-    const int sqr = j.sqr ? 1 : 0;
-    const QLayout w = layout(j.la, j.lb, sqr);
-    if (ws_bytes < w.total) return cudaErrorInvalidValue;
-    cudaError_t e = q32::ensure_tables();
-    if (e != cudaSuccess) return e;
-    char* base = (char*)ws;
-    u32* A = (u32*)(base + w.a);
-    u32* B = sqr ? A : (u32*)(base + w.b);
-    const Plan pl = qplan(w.n);
-    const int P = pl.passes;
-    const u64 N = w.N;
-    int logB[MAX_PASSES];
-    logB[0] = w.n;
-    for (int p = 1; p < P; ++p) logB[p] = logB[p - 1] - pl.bits[p - 1];
-    const int lastl = pl.bits[P - 1];
-    const u64 nblk_last = N >> lastl;
-    const u64 tiles_last = (nblk_last + TC - 1) / TC;
-    const int ncols_last = nblk_last < (u64)TC ? (int)nblk_last : TC;
-    bool waited = (b_ready == nullptr);
-
-    auto launch = [&](int variant, int logl, const QArgs& a, u64 tiles) -> cudaError_t {
+    cudaError_t wait_b() {
+        if (waited) return cudaSuccess;
+        waited = true;
+        return cudaStreamWaitEvent(s, b_ready, 0);
+    }
+    cudaError_t operator()(int variant, int logl, const QArgs& a, u64 tiles) {
         QKernel k = ktab().k[variant][logl];
         if (!k) return cudaErrorInvalidValue;
-        if (!waited && !sqr && a.src == j.b && j.b) {
-            cudaError_t e2 = cudaStreamWaitEvent(s, b_ready, 0);   // second operand copied meanwhile
-            if (e2 != cudaSuccess) return e2;
-            waited = true;
-        }
-        if (!waited && variant == V_FUSED2) {
-            cudaError_t e2 = cudaStreamWaitEvent(s, b_ready, 0);
-            if (e2 != cudaSuccess) return e2;
-            waited = true;
-        }
+        cudaError_t e;
+        const bool reads_b = j.b && !j.sqr && a.src && a.src >= j.b && a.src < j.b + j.lb;
+        if ((reads_b || variant == V_FUSED2) && (e = wait_b()) != cudaSuccess) return e;
         const double vec = 3.0 * (double)N * 4.0, bfly = 3.0 * ((double)N / 2.0) * logl;
         const bool entry = (variant == V_FWD_E || variant == V_LAST_E || variant == V_FUSED_E || variant == V_SQR_E);
         double bytes = entry ? (double)a.len * 8.0 + vec : 2.0 * vec, mm = bfly + (entry ? 6.0 * (double)a.len : 0.0);
         int kind = K_FUSED;
         if (variant == V_FWD || variant == V_FWD_E) kind = K_FWD;
         else if (variant == V_LAST || variant == V_LAST_E) kind = K_FWD_LAST;
-        else if (variant == V_INV) kind = K_INV;
+        else if (variant == V_INV || variant == V_INV_ACC) kind = K_INV;
         if (variant == V_FUSED2) {
             bytes += vec;
             mm = 3.0 * bfly + 3.0 * (double)N;
@@ -885,10 +948,81 @@ cudaError_t q32_enqueue(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s,
         }
         const ProfMark m = prof_begin(kind, bytes, mm, s);
         k<<<(unsigned)(tiles * 3), NT, pass_smem(logl, variant), s>>>(a);
-        cudaError_t e2 = cudaGetLastError();
+        e = cudaGetLastError();
         prof_end(m, s);
-        return e2;
-    };
+        return e;
+    }
+};
+
+// CRT constants for residues that went through a 2^n-point transform: M_i^-1 N^-1 2^64 mod q_i.
+static void crt_constants(u64 N, u32 (&cst)[3]) {
+    for (int i = 0; i < 3; ++i) {
+        const u64 p = kQ[i];
+        u64 M = 1;
+        for (int k = 0; k < 3; ++k)
+            if (k != i) M = h_mulmod(M, kQ[k], p);
+        const u64 minv = h_pow(M, p - 2, p);
+        const u64 ninv = h_pow(N % p, p - 2, p);
+        const u64 r2 = h_pow(2, 64, p);
+        cst[i] = (u32)h_mulmod(h_mulmod(minv, ninv, p), r2, p);
+    }
+}
+
+}  // namespace q32
+
+bool q32_fits(u64 la, u64 lb, int sqr) { return q32::plan_job(la, lb, sqr).ok; }
+
+void q32_force_pieces(int m) { q32::g_force_pieces.store(m > 1 ? m : 0); }
+
+double q32_cost(u64 la, u64 lb, int sqr) {
+    const q32::QJob J = q32::plan_job(la, lb, sqr);
+    return J.ok ? J.cost : 1e300;
+}
+
+size_t q32_workspace_bytes(u64 la, u64 lb, int sqr) {
+    const q32::QJob J = q32::plan_job(la, lb, sqr);
+    return J.ok ? J.total : 256;
+}
+
+int q32_launches(u64 la, u64 lb, int sqr) {
+    const q32::QJob J = q32::plan_job(la, lb, sqr);
+    if (!J.ok) return 0;
+    const Plan pl = q32::qplan(J.n);
+    const int P = pl.passes;
+    const int lastl = pl.bits[P - 1];
+    if (J.m > 1) return P + J.m * ((P - 1) + 1 + (P - 1)) + 1;
+    if (!sqr && P >= 2 && lastl >= 5 && lastl <= 8) return 2 * (P - 1) + 1 + (P - 1) + 1;
+    return sqr ? (P - 1) + 1 + (P - 1) + 1 : 2 * (P - 1) + 1 + 1 + (P - 1) + 1;
+}
+
+int q32_pieces(u64 la, u64 lb, int sqr) {
+    const q32::QJob J = q32::plan_job(la, lb, sqr);
+    return J.ok ? J.m : 0;
+}
+
+cudaError_t q32_enqueue(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s, cudaEvent_t b_ready, int crt_chunks,
+                        ChunkDone after_chunk, void* ctx) {
+    using namespace q32;
+    const u64 out_len = j.la + j.lb;
+    if (out_len == 0) return cudaSuccess;
+    if (j.la == 0 || j.lb == 0) return cudaMemsetAsync(j.out, 0, out_len * sizeof(u64), s);
+    const int sqr = j.sqr ? 1 : 0;
+    const QJob J = plan_job(j.la, j.lb, sqr);
+    if (!J.ok || ws_bytes < J.total) return cudaErrorInvalidValue;
+    cudaError_t e = q32::ensure_tables();
+    if (e != cudaSuccess) return e;
+    char* base = (char*)ws;
+    const Plan pl = qplan(J.n);
+    const int P = pl.passes;
+    const u64 N = J.N;
+    int logB[MAX_PASSES];
+    logB[0] = J.n;
+    for (int p = 1; p < P; ++p) logB[p] = logB[p - 1] - pl.bits[p - 1];
+    const int lastl = pl.bits[P - 1];
+    const u64 nblk_last = N >> lastl;
+    const u64 tiles_last = (nblk_last + TC - 1) / TC;
+    const int ncols_last = nblk_last < (u64)TC ? (int)nblk_last : TC;
+    Launcher launch{j, s, b_ready, b_ready == nullptr, N};
 
     QArgs pa;
     memset(&pa, 0, sizeof(pa));
@@ -905,84 +1039,126 @@ cudaError_t q32_enqueue(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s,
         }
         return cudaSuccess;
     };
-    const bool merged = !sqr && P >= 2 && lastl >= 5 && lastl <= 8;
-    if (merged) {
-        if ((e = fwd_strided(j.a, j.la, A)) != cudaSuccess) return e;
-        if ((e = fwd_strided(j.b, j.lb, B)) != cudaSuccess) return e;
+    auto inverse_strided = [&](u32* data, int last_p) -> cudaError_t {   // passes P-2 .. last_p
         pa.src = nullptr;
         pa.len = 0;
-        pa.data = B;
-        pa.other = A;
-        pa.logB = logB[P - 1];
-        pa.ncols = TC;
-        if ((e = launch(V_FUSED2, lastl, pa, tiles_last)) != cudaSuccess) return e;
-    } else if (!sqr) {
-        if ((e = fwd_strided(j.a, j.la, A)) != cudaSuccess) return e;
-        pa.src = j.a;
-        pa.len = j.la;
-        pa.data = A;
         pa.other = nullptr;
-        pa.logB = logB[P - 1];
-        pa.ncols = ncols_last;
-        if ((e = launch(P == 1 ? V_LAST_E : V_LAST, lastl, pa, tiles_last)) != cudaSuccess) return e;
+        pa.dst = nullptr;
         pa.ncols = TC;
-        if ((e = fwd_strided(j.b, j.lb, B)) != cudaSuccess) return e;
-        pa.src = j.b;
-        pa.len = j.lb;
-        pa.data = B;
-        pa.other = A;
-        pa.logB = logB[P - 1];
-        pa.ncols = ncols_last;
-        if ((e = launch(P == 1 ? V_FUSED_E : V_FUSED, lastl, pa, tiles_last)) != cudaSuccess) return e;
-    } else {
-        if ((e = fwd_strided(j.a, j.la, A)) != cudaSuccess) return e;
-        pa.src = j.a;
-        pa.len = j.la;
-        pa.data = A;
-        pa.other = A;
-        pa.logB = logB[P - 1];
-        pa.ncols = ncols_last;
-        if ((e = launch(P == 1 ? V_SQR_E : V_SQR, lastl, pa, tiles_last)) != cudaSuccess) return e;
-    }
-    pa.ncols = TC;
-    pa.src = nullptr;
-    pa.len = 0;
-    pa.other = nullptr;
-    for (int p = P - 2; p >= 0; --p) {
-        pa.data = A;
-        pa.logB = logB[p];
-        if ((e = launch(V_INV, pl.bits[p], pa, N >> (pl.bits[p] + LOG_TC))) != cudaSuccess) return e;
-    }
-    if (!waited && (e = cudaStreamWaitEvent(s, b_ready, 0)) != cudaSuccess) return e;
+        for (int p = P - 2; p >= last_p; --p) {
+            pa.data = data;
+            pa.logB = logB[p];
+            cudaError_t e2 = launch(V_INV, pl.bits[p], pa, N >> (pl.bits[p] + LOG_TC));
+            if (e2 != cudaSuccess) return e2;
+        }
+        return cudaSuccess;
+    };
 
     QCrtArgs ca;
     memset(&ca, 0, sizeof(ca));
-    for (int i = 0; i < 3; ++i) {
-        const u64 p = kQ[i];
-        u64 M = 1;
-        for (int k = 0; k < 3; ++k)
-            if (k != i) M = h_mulmod(M, kQ[k], p);
-        const u64 minv = h_pow(M, p - 2, p);
-        const u64 ninv = h_pow(N % p, p - 2, p);
-        const u64 r2 = h_pow(2, 64, p);
-        ca.cst[i] = (u32)h_mulmod(h_mulmod(minv, ninv, p), r2, p);
+    crt_constants(N, ca.cst);
+    if (J.m == 1) {
+        u32* A = (u32*)(base + J.a);
+        u32* B = sqr ? A : (u32*)(base + J.b);
+        const bool merged = !sqr && P >= 2 && lastl >= 5 && lastl <= 8;
+        if (merged) {
+            if ((e = fwd_strided(j.a, j.la, A)) != cudaSuccess) return e;
+            if ((e = fwd_strided(j.b, j.lb, B)) != cudaSuccess) return e;
+            pa.src = nullptr;
+            pa.len = 0;
+            pa.data = B;
+            pa.other = A;
+            pa.logB = logB[P - 1];
+            pa.ncols = TC;
+            if ((e = launch(V_FUSED2, lastl, pa, tiles_last)) != cudaSuccess) return e;
+        } else if (!sqr) {
+            if ((e = fwd_strided(j.a, j.la, A)) != cudaSuccess) return e;
+            pa.src = j.a;
+            pa.len = j.la;
+            pa.data = A;
+            pa.other = nullptr;
+            pa.logB = logB[P - 1];
+            pa.ncols = ncols_last;
+            if ((e = launch(P == 1 ? V_LAST_E : V_LAST, lastl, pa, tiles_last)) != cudaSuccess) return e;
+            pa.ncols = TC;
+            if ((e = fwd_strided(j.b, j.lb, B)) != cudaSuccess) return e;
+            pa.src = j.b;
+            pa.len = j.lb;
+            pa.data = B;
+            pa.other = A;
+            pa.logB = logB[P - 1];
+            pa.ncols = ncols_last;
+            if ((e = launch(P == 1 ? V_FUSED_E : V_FUSED, lastl, pa, tiles_last)) != cudaSuccess) return e;
+        } else {
+            if ((e = fwd_strided(j.a, j.la, A)) != cudaSuccess) return e;
+            pa.src = j.a;
+            pa.len = j.la;
+            pa.data = A;
+            pa.other = A;
+            pa.logB = logB[P - 1];
+            pa.ncols = ncols_last;
+            if ((e = launch(P == 1 ? V_SQR_E : V_SQR, lastl, pa, tiles_last)) != cudaSuccess) return e;
+        }
+        if ((e = inverse_strided(A, 0)) != cudaSuccess) return e;
+        ca.res = A;
+        ca.N = N;
+    } else {
+        // split: S's spectrum once, then every piece of the long operand against it
+        u32* R = (u32*)(base + J.a);
+        u32* C = (u32*)(base + J.b);
+        u32* ACC = (u32*)(base + J.acc);
+        const u64* S_src = J.swap ? j.b : j.a;
+        const u64* L_src = J.swap ? j.a : j.b;
+        if ((e = fwd_strided(S_src, J.ls, R)) != cudaSuccess) return e;
+        pa.src = nullptr;
+        pa.len = 0;
+        pa.data = R;
+        pa.other = nullptr;
+        pa.dst = nullptr;
+        pa.logB = logB[P - 1];
+        pa.ncols = ncols_last;
+        if ((e = launch(V_LAST, lastl, pa, tiles_last)) != cudaSuccess) return e;
+        for (int k = 0; k < J.m; ++k) {
+            const u64 first = (u64)k * J.cb;
+            const u64 len = J.ll - first < J.cb ? J.ll - first : J.cb;
+            if ((e = fwd_strided(L_src + first, len, C)) != cudaSuccess) return e;
+            pa.src = nullptr;
+            pa.len = 0;
+            pa.data = C;
+            pa.other = R;
+            pa.dst = C;
+            pa.logB = logB[P - 1];
+            pa.ncols = ncols_last;
+            if ((e = launch(V_FUSED, lastl, pa, tiles_last)) != cudaSuccess) return e;
+            if ((e = inverse_strided(C, 1)) != cudaSuccess) return e;
+            pa.data = C;
+            pa.logB = logB[0];
+            pa.acc = ACC + 2 * first;
+            pa.acc_stride = J.stride;
+            pa.acc_valid = 2 * (J.ls + len) - 1;
+            pa.acc_fresh = k == 0 ? 0 : 2 * J.ls - 1;
+            if ((e = launch(V_INV_ACC, pl.bits[0], pa, N >> (pl.bits[0] + LOG_TC))) != cudaSuccess) return e;
+            pa.acc = nullptr;
+        }
+        ca.res = ACC;
+        ca.N = J.stride;
     }
-    ca.res = A;
-    ca.N = N;
+    if ((e = launch.wait_b()) != cudaSuccess) return e;
+
     ca.nvalid = 2 * out_len - 1;
     ca.out = j.out;
     ca.out_len = out_len;
-    ca.state = (u32*)(base + w.state);
-    ca.ticket = (u32*)(base + w.ticket);
+    ca.state = (u32*)(base + J.state);
+    ca.ticket = (u32*)(base + J.ticket);
     ca.err = (u32*)base;
-    if ((e = cudaMemsetAsync(base + w.ticket, 0, w.total - w.ticket, s)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(base + J.ticket, 0, J.total - J.ticket, s)) != cudaSuccess) return e;
     if (crt_chunks < 1) crt_chunks = 1;
-    const u64 per = (w.ncta + crt_chunks - 1) / crt_chunks;
-    for (u64 t0 = 0; t0 < w.ncta; t0 += per) {
-        const u64 n = t0 + per <= w.ncta ? per : w.ncta - t0;
+    const u64 per = (J.ncta + crt_chunks - 1) / crt_chunks;
+    for (u64 t0 = 0; t0 < J.ncta; t0 += per) {
+        const u64 n = t0 + per <= J.ncta ? per : J.ncta - t0;
         const double crt_bytes = 3.0 * (double)ca.nvalid * 4.0 + (double)out_len * 8.0;
-        const ProfMark m = prof_begin(K_CRT, crt_bytes * (double)n / (double)w.ncta,
-                                      3.0 * (double)ca.nvalid * (double)n / (double)w.ncta, s);
+        const ProfMark m = prof_begin(K_CRT, crt_bytes * (double)n / (double)J.ncta,
+                                      3.0 * (double)ca.nvalid * (double)n / (double)J.ncta, s);
         k_qcrt_carry<<<(unsigned)n, CNT, 0, s>>>(ca);
         e = cudaGetLastError();
         prof_end(m, s);

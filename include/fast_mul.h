@@ -181,7 +181,8 @@ void fmn_server_destroy(fmn_server* s);
  * three 62-bit primes (src/data.h:79-81), for transforms up to 2^30 points.
  * FMN_ENGINE_32 splits each limb into two 32-bit digits and works modulo three 31-bit
  * primes, whose modular products are single 32-bit multiplies on the GPU; it covers
- * products of up to 2^25 limbs (len1 + len2 <= 33554432).  FMN_ENGINE_AUTO (the default)
+ * products whose shorter operand has at most 2^25 limbs (longer ones are split, see
+ * fmn_pieces_for).  FMN_ENGINE_AUTO (the default)
  * takes FMN_ENGINE_32 wherever it applies and FMN_ENGINE_64 elsewhere.  Batches and
  * resident operands always run on FMN_ENGINE_64.  No counterpart in the reference. */
 #define FMN_ENGINE_AUTO 0
@@ -193,6 +194,16 @@ int fmn_set_engine(int engine);
 int fmn_get_engine(void);
 /* The engine (FMN_ENGINE_64 or FMN_ENGINE_32) that a product of these lengths runs on. */
 int fmn_engine_for(u64 len1, u64 len2, int sqr);
+/* Pieces the product is computed in: 1 = one transform of the whole product; m > 1 = the
+ * shorter operand is transformed once and multiplied with m pieces of the longer one, each at
+ * a smaller transform length (the reference's conv_single reuse, src/fast_mul.c:135-212),
+ * and the pieces' coefficients are summed before one CRT + carry pass.  FMN_ENGINE_32 only;
+ * chosen by a cost model (fewer butterflies for lengths that would pad a power of two
+ * poorly, and the only way the 32-bit engine reaches unbalanced products above 2^25 limbs). */
+int fmn_pieces_for(u64 len1, u64 len2, int sqr);
+/* Testing and tuning: split every product that allows it into `pieces` pieces regardless of
+ * the cost model (0 or 1 restores the model).  Process-wide. */
+int fmn_force_pieces(int pieces);
 
 /* ----------------------------------------------------------------- pass plans and tuning
  * A 2^n-point transform runs as passes of <= 9 index bits each; the split is a plan (e.g.

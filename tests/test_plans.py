@@ -95,9 +95,24 @@ def test_engine_selection_rules():
     assert fmn.get_engine() == fmn.ENGINE_AUTO
     assert fmn.engine_for(10_000_000, 10_000_000) == fmn.ENGINE_32
     assert fmn.engine_for(1 << 24, 1 << 24) == fmn.ENGINE_32             # 2^26-digit transform
+    # one limb more: the 64-bit engine's transform (2^25 points) is cheaper than any split
     assert fmn.engine_for(1 << 24, (1 << 24) + 1) == fmn.ENGINE_64
-    assert fmn.engine_for(64_000_000, 250_000) == fmn.ENGINE_64
-    assert fmn.engine_for(1, 1, sqr=True) == fmn.ENGINE_32
+    assert fmn.engine_for(1000, 1000, sqr=True) == fmn.ENGINE_32
+    # split products: 10M x 10M in two 10M x 5M pieces at 2^25 digits; unbalanced products
+    # above 2^25 limbs reach the 32-bit engine only split
+    assert fmn.pieces_for(10_000_000, 10_000_000) == 2
+    assert fmn.engine_for(64_000_000, 250_000) == fmn.ENGINE_32
+    assert fmn.pieces_for(64_000_000, 250_000) > 1
+    assert fmn.pieces_for(1_000_000, 1_000_000) == 1
+    assert fmn.pieces_for(10_000_000, 10_000_000, sqr=True) == 1       # squares are never split
+    assert fmn.engine_for(33_000_000, 33_000_000) == fmn.ENGINE_64      # a split would need 60 pieces
+    assert fmn.engine_for(64_000_000, 64_000_000) == fmn.ENGINE_64      # beyond the coefficient range
+    fmn.force_pieces(3)
+    try:
+        assert fmn.pieces_for(1000, 5000) == 3 and fmn.pieces_for(5000, 1000) == 3
+        assert fmn.pieces_for(1000, 1000, sqr=True) == 1
+    finally:
+        fmn.force_pieces(0)
     fmn.set_engine(fmn.ENGINE_64)
     try:
         assert fmn.engine_for(10_000_000, 10_000_000) == fmn.ENGINE_64
