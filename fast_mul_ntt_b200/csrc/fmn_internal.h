@@ -108,6 +108,28 @@ cudaError_t enqueue_job(const Job& job, void* ws, size_t ws_bytes, cudaStream_t 
 cudaError_t enqueue_job_overlapped(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s, const TwiddleSet* tw,
                                    cudaEvent_t b_ready, int crt_chunks, ChunkDone after_chunk, void* ctx);
 
+// ---- 32-bit engine batches (whole products; see enqueue_batch)
+struct Q32Group {
+    int m, count;                           // products, launches per product
+    int variant[3 * MAX_PASSES + 2], logl[3 * MAX_PASSES + 2];
+    u64 tiles[3 * MAX_PASSES + 2];
+    size_t args_off[3 * MAX_PASSES + 2];    // descriptor offsets: m launch-argument records each
+    size_t crt_off, ncta_off;
+    unsigned max_ncta;
+};
+int q32_batch_log_n(const Job& j);          // transform log length, < 0 if not a 32-bit batch product
+size_t q32_batch_res_bytes(const Job& j);   // residue arrays of one product
+size_t q32_batch_state_bytes(const Job& j); // carry-scan ticket + state of one product
+size_t q32_batch_desc_bytes_per_job();      // descriptor bytes one product needs (upper bound)
+// Plan the group jobs[idx[0..m)] (same transform length and kind): scratch carved from `res`
+// and `st` at *roff / *soff (advanced), descriptors written into host staging `h` at 16-byte
+// aligned offsets from *hoff (advanced, at most hcap).
+cudaError_t q32_batch_plan(const Job* jobs, const int* idx, int m, char* res, size_t* roff, char* st, size_t* soff,
+                           unsigned* err, char* h, size_t* hoff, size_t hcap, Q32Group* g);
+// Launch a planned group whose descriptors were copied to d_desc (same offsets as in h).
+cudaError_t q32_batch_launch(const Q32Group& g, const char* d_desc, cudaStream_t s);
+cudaError_t q32_prepare();                  // tables + kernel attributes on the current device
+
 // ---- batches of products
 // Workspace bytes for a batch (device) and host staging bytes for its launch descriptors.
 size_t batch_workspace_bytes(const Job* jobs, int count);

@@ -41,7 +41,9 @@ constexpr int TC = 16;            // columns per tile
 constexpr int TWB = 15;           // two-level twiddle tables: w^x = HI[x >> 15] * LO[x & 0x7fff]
 static_assert(2 * TWB == MAX_LOG_N, "two-level table covers roots of order 2^30");
 
-__device__ __align__(16) ulonglong2 g_rt[2][3][RT_SIZE];   // [forward/inverse][prime]: (w, w') Shoup pairs
+// [forward/inverse][prime]: (w, w') Shoup pairs, stored stage-major: the twiddle of stage
+// entry j of the group with low offset q is at rt_off(RB, TOP) + j * 2^(TOP-RB+1) + q.
+__device__ __align__(16) ulonglong2 g_rt[2][3][RT_SIZE];
 __device__ __align__(16) u64 g_tw[2][3][1 << TWB];     // [low/high level][prime]
 __constant__ PrimeRT c_prime[3] = {prime_rt<0>(), prime_rt<1>(), prime_rt<2>()};
 
@@ -100,7 +102,7 @@ __device__ __forceinline__ void run_round(LD ld, ST st, int pi, const PrimeRT& q
 #pragma unroll
             for (int t = 0; t < R; ++t) x[t] = ld(row0 + t * SP, c);
         }
-        const ulonglong2* tw = tab + qlo * R;
+        const ulonglong2* tw = tab + qlo;   // stage-major table: lanes of consecutive groups coalesce
         if (!INV) {
 #pragma unroll
             for (int s = 0; s < RB; ++s) {
@@ -112,7 +114,7 @@ __device__ __forceinline__ void run_round(LD ld, ST st, int pi, const PrimeRT& q
                     if (LOWEST && u == 0)
                         bfly_dif1(x[t], x[t + half], q);
                     else
-                        bfly_dif(x[t], x[t + half], __ldg(tw + (R - (R >> s)) + u), q);
+                        bfly_dif(x[t], x[t + half], __ldg(tw + ((R - (R >> s)) + u) * SP), q);
                 }
             }
         } else {
@@ -126,7 +128,7 @@ __device__ __forceinline__ void run_round(LD ld, ST st, int pi, const PrimeRT& q
                     if (LOWEST && u == 0)
                         bfly_dit1(x[t], x[t + half], q);
                     else
-                        bfly_dit(x[t], x[t + half], __ldg(tw + (R - (R >> s)) + u), q);
+                        bfly_dit(x[t], x[t + half], __ldg(tw + ((R - (R >> s)) + u) * SP), q);
                 }
             }
         }
@@ -751,7 +753,8 @@ static const HostTables& host_tables() {
                             for (int u = 0; u < (R >> (s + 1)); ++u) {
                                 // w_{2^(top-s+1)}^(q + u 2^spl) = w^((q + u 2^spl) 2^(30-(top-s+1)))
                                 const u64 e = ((u64)q + ((u64)u << spl)) << (MAX_LOG_N - (top - s + 1));
-                                const size_t at = (size_t)rt_off(r, top) + (size_t)q * R + (R - (R >> s)) + u;
+                                // stage-major: entry j = (R - (R >> s)) + u of group offset q
+                                const size_t at = (size_t)rt_off(r, top) + ((size_t)(R - (R >> s)) + u << spl) + q;
                                 const u64 wf = wpow(e);
                                 const u64 wi = wpow((1ull << MAX_LOG_N) - (e & ((1ull << MAX_LOG_N) - 1)));
                                 const size_t f0 = (((size_t)0 * 3 + i) * RT_SIZE + at) * 2;
@@ -1496,23 +1499,44 @@ static cudaError_t set_batch_attrs() {
 // Products are grouped by (transform length, square); each group's launches run on one of
 // the streams in `streams` (round robin), forked from and joined back into `s`.
 struct BatchGroup {
-    int n, kind;          // kind: 0 multiply, 1 square, 2 resident first operand
+    int engine, n, kind;  // kind: 0 multiply, 1 square, 2 resident first operand
     std::vector<int> idx;
 };
 static int job_kind(const Job& j) { return j.spectrum ? 2 : (j.sqr ? 1 : 0); }
+
+// Engine of a batched product: the 32-bit engine for every whole product it can take (batched
+// products are small; resident operands keep 64-bit spectra), unless ENGINE_64 is selected.
+static int batch_engine(const Job& j) {
+    if (j.spectrum) return ENGINE_64;
+    const int e = j.engine ? j.engine : default_engine();
+    if (e == ENGINE_64) return ENGINE_64;
+    return q32_batch_log_n(j) >= 0 ? ENGINE_32 : ENGINE_64;
+}
+
+static void batch_sizes(const Job& j, size_t* res, size_t* st) {
+    if (batch_engine(j) == ENGINE_32) {
+        *res += q32_batch_res_bytes(j);
+        *st += q32_batch_state_bytes(j);
+        return;
+    }
+    const WsLayout w = ws_layout(j.la, j.lb, j.sqr, j.spectrum ? j.log_n : 0);
+    *res += align256(3 * w.N * sizeof(u64)) * (j.sqr ? 1 : 2);
+    *st += 16 + ((w.ncta * sizeof(u32) + 15) & ~(size_t)15);
+}
 
 static void batch_groups(const Job* jobs, int count, std::vector<BatchGroup>& groups) {
     groups.clear();
     for (int i = 0; i < count; ++i) {
         const Job& j = jobs[i];
         if (j.la == 0 || j.lb == 0) continue;
-        const int n = ws_layout(j.la, j.lb, j.sqr, j.spectrum ? j.log_n : 0).n;
+        const int eng = batch_engine(j);
+        const int n = eng == ENGINE_32 ? q32_batch_log_n(j) : ws_layout(j.la, j.lb, j.sqr, j.spectrum ? j.log_n : 0).n;
         const int sq = job_kind(j);
         BatchGroup* g = nullptr;
         for (auto& x : groups)
-            if (x.n == n && x.kind == sq) g = &x;
+            if (x.engine == eng && x.n == n && x.kind == sq) g = &x;
         if (!g) {
-            groups.push_back(BatchGroup{n, sq, {}});
+            groups.push_back(BatchGroup{eng, n, sq, {}});
             g = &groups.back();
         }
         g->idx.push_back(i);
@@ -1526,9 +1550,7 @@ size_t batch_workspace_bytes(const Job* jobs, int count) {
     for (int i = 0; i < count; ++i) {
         const Job& j = jobs[i];
         if (j.la == 0 || j.lb == 0) continue;
-        const WsLayout w = ws_layout(j.la, j.lb, j.sqr, j.spectrum ? j.log_n : 0);
-        res += align256(3 * w.N * sizeof(u64)) * (j.sqr ? 1 : 2);
-        st += 16 + ((w.ncta * sizeof(u32) + 15) & ~(size_t)15);
+        batch_sizes(j, &res, &st);
     }
     return 256 + align256(res) + align256(st) + align256(batch_stage_bytes(jobs, count));
 }
@@ -1554,9 +1576,7 @@ cudaError_t enqueue_batch(const Job* jobs, int count, void* ws, size_t ws_bytes,
     for (int i = 0; i < count; ++i) {
         const Job& j = jobs[i];
         if (j.la == 0 || j.lb == 0) continue;
-        const WsLayout w = ws_layout(j.la, j.lb, j.sqr, j.spectrum ? j.log_n : 0);
-        res += align256(3 * w.N * sizeof(u64)) * (j.sqr ? 1 : 2);
-        st += 16 + ((w.ncta * sizeof(u32) + 15) & ~(size_t)15);
+        batch_sizes(j, &res, &st);
     }
     char* res_base = base + 256;
     char* st_base = res_base + align256(res);
@@ -1581,11 +1601,18 @@ cudaError_t enqueue_batch(const Job* jobs, int count, void* ws, size_t ws_bytes,
         size_t st_bytes;
     };
     std::vector<GroupLaunch> gl(groups.size());
+    std::vector<Q32Group> qg(groups.size());
     size_t roff = 0, soff = 0;
     std::vector<JobLaunches> jl;
     for (size_t g = 0; g < groups.size(); ++g) {
         const BatchGroup& G = groups[g];
         const int m = (int)G.idx.size();
+        if (G.engine == ENGINE_32) {
+            e = q32_batch_plan(jobs, G.idx.data(), m, res_base, &roff, st_base, &soff, (u32*)base, hp, &hoff,
+                               stage_bytes, &qg[g]);
+            if (e != cudaSuccess) return e;
+            continue;
+        }
         const TwiddleSet* tws = tw_lookup ? tw_lookup(tw_ctx, G.n) : nullptr;
         jl.assign(m, JobLaunches());
         GroupLaunch& L = gl[g];
@@ -1645,6 +1672,10 @@ cudaError_t enqueue_batch(const Job* jobs, int count, void* ws, size_t ws_bytes,
     for (size_t g = 0; g < groups.size(); ++g) {
         const GroupLaunch& L = gl[g];
         cudaStream_t gs = nstreams > 0 ? streams[g % nstreams] : s;
+        if (groups[g].engine == ENGINE_32) {
+            if ((e = q32_batch_launch(qg[g], desc_base, gs)) != cudaSuccess) return e;
+            continue;
+        }
         for (int k = 0; k < L.count; ++k) {
             BatchKernel kk = BK.k[L.variant[k]][L.logl[k]];
             if (!kk) return cudaErrorInvalidValue;
@@ -1676,14 +1707,16 @@ cudaError_t prepare_batch() {
     for (int d : done)
         if (d == dev) return cudaSuccess;
     if ((e = set_batch_attrs()) != cudaSuccess) return e;
+    if ((e = q32_prepare()) != cudaSuccess) return e;
     done.push_back(dev);
     return cudaSuccess;
 }
 
 size_t batch_stage_bytes(const Job* jobs, int count) {
     size_t desc = 0;
-    for (int i = 0; i < count; ++i)
-        desc += (3 * MAX_PASSES + 2) * (sizeof(PassArgs) + 16) + sizeof(CrtArgs) + sizeof(u32) + 32;
+    const size_t per64 = (3 * MAX_PASSES + 2) * (sizeof(PassArgs) + 16) + sizeof(CrtArgs) + sizeof(u32) + 32;
+    const size_t per32 = q32_batch_desc_bytes_per_job();
+    for (int i = 0; i < count; ++i) desc += per64 > per32 ? per64 : per32;
     return desc + 4096;
 }
 

@@ -508,6 +508,24 @@ __global__ void __launch_bounds__(NT, (min_ctas<MODE, LOGL>())) k_qpass(QArgs a)
     else body_fused<LOGL, ENTRY, SQR>(qsm, a, tile, pi, q);
 }
 
+// Batched form: products with the same transform length and kind share every launch; CTA b
+// works on product b / (3 * tiles), tile (b / 3) % tiles, prime b % 3.
+template <int MODE, int LOGL, bool ENTRY, bool SQR>
+__global__ void __launch_bounds__(NT, (min_ctas<MODE, LOGL>())) k_qpass_batch(const QArgs* __restrict__ args,
+                                                                              u32 tiles) {
+    extern __shared__ __align__(16) u32 qsm[];
+    const int pi = blockIdx.x % 3;
+    const u32 rest = blockIdx.x / 3;
+    const QArgs a = args[rest / tiles];
+    const u64 tile = rest % tiles;
+    const PrimeQ q = c_q[pi];
+    if constexpr (MODE == M_FWD) body_fwd<LOGL, ENTRY>(qsm, a, tile, pi, q);
+    else if constexpr (MODE == M_INV) body_inv<LOGL, false>(qsm, a, tile, pi, q);
+    else if constexpr (MODE == M_FWD_LAST) body_fwd_last<LOGL, ENTRY>(qsm, a, tile, pi, q);
+    else if constexpr (MODE == M_FUSED2) body_fused2<(LOGL >= 5 ? LOGL : 5)>(qsm, a, tile, pi, q);
+    else body_fused<LOGL, ENTRY, SQR>(qsm, a, tile, pi, q);
+}
+
 // ------------------------------------------------------------------ CRT + carry
 // Digit coefficient k of the product, c_k < Q = q0 q1 q2 < 2^91, from its residues by
 // c_k = sum_i y_i M_i mod Q with y_i = r_i * M_i^-1 (M_i = Q / q_i; the CRT of
@@ -542,11 +560,12 @@ __device__ __forceinline__ u128 qcoef(const QCrtArgs& a, u64 k, const PrimeQ& q0
     return qcrt(a.res[k], a.res[a.N + k], a.res[2 * a.N + k], a, q0, q1, q2);
 }
 
-__global__ void __launch_bounds__(CNT) k_qcrt_carry(QCrtArgs a) {
+__device__ __forceinline__ void qcrt_carry_body(const QCrtArgs& a, u32 ncta) {
     __shared__ u64 s_hw[CNT / 32];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const PrimeQ q0 = c_q[0], q1 = c_q[1], q2 = c_q[2];
     const u64 tile = carry_ticket(a.ticket);
+    if (tile >= ncta) return;                          // batch launches cover the largest product
     const u64 j0 = tile * CTILE + (u64)tid * CE;       // output limbs j0 .. j0+15
     const u64 k0 = 2 * j0;                             // digit coefficients k0 .. k0+31
     u64 lo[CE];
@@ -600,6 +619,16 @@ __global__ void __launch_bounds__(CNT) k_qcrt_carry(QCrtArgs a) {
     }
     add_to(lo[0], h[0], nb);
     carry_finish(lo, h, tile, j0, a.state, a.err, a.out, a.out_len);
+}
+
+__global__ void __launch_bounds__(CNT) k_qcrt_carry(QCrtArgs a) { qcrt_carry_body(a, 0xffffffffu); }
+
+// CRT + carry of many products: CTAs take per-product tickets; tickets beyond a product's
+// CTA count exit at once.
+__global__ void __launch_bounds__(CNT) k_qcrt_carry_batch(const QCrtArgs* __restrict__ args, u32 ctas_per_job,
+                                                          const u32* __restrict__ ncta) {
+    const u32 job = blockIdx.x / ctas_per_job;
+    qcrt_carry_body(args[job], ncta[job]);
 }
 
 // ------------------------------------------------------------------ host: tables
@@ -735,6 +764,43 @@ static const KernelTable& ktab() {
     return t;
 }
 
+typedef void (*QBatchKernel)(const QArgs*, u32);
+template <int LOGL>
+static void fill_brow(QBatchKernel (&t)[NV][MAX_PASS_BITS + 1]) {
+    constexpr int LS = LOGL >= 5 ? LOGL : 5;
+    constexpr int LM = (LOGL >= 5 && LOGL <= 8) ? LOGL : 5;
+    t[V_FWD][LOGL] = LOGL >= 5 ? k_qpass_batch<M_FWD, LS, false, false> : nullptr;
+    t[V_FWD_E][LOGL] = LOGL >= 5 ? k_qpass_batch<M_FWD, LS, true, false> : nullptr;
+    t[V_INV][LOGL] = LOGL >= 5 ? k_qpass_batch<M_INV, LS, false, false> : nullptr;
+    t[V_FUSED2][LOGL] = (LOGL >= 5 && LOGL <= 8) ? k_qpass_batch<M_FUSED2, LM, false, false> : nullptr;
+    t[V_LAST][LOGL] = k_qpass_batch<M_FWD_LAST, LOGL, false, false>;
+    t[V_LAST_E][LOGL] = k_qpass_batch<M_FWD_LAST, LOGL, true, false>;
+    t[V_FUSED][LOGL] = k_qpass_batch<M_FUSED, LOGL, false, false>;
+    t[V_FUSED_E][LOGL] = k_qpass_batch<M_FUSED, LOGL, true, false>;
+    t[V_SQR][LOGL] = k_qpass_batch<M_FUSED, LOGL, false, true>;
+    t[V_SQR_E][LOGL] = k_qpass_batch<M_FUSED, LOGL, true, true>;
+}
+struct BatchKernelTable {
+    QBatchKernel k[NV][MAX_PASS_BITS + 1];
+    BatchKernelTable() {
+        memset(k, 0, sizeof(k));
+        fill_brow<0>(k);
+        fill_brow<1>(k);
+        fill_brow<2>(k);
+        fill_brow<3>(k);
+        fill_brow<4>(k);
+        fill_brow<5>(k);
+        fill_brow<6>(k);
+        fill_brow<7>(k);
+        fill_brow<8>(k);
+        fill_brow<9>(k);
+    }
+};
+static const BatchKernelTable& bktab() {
+    static BatchKernelTable t;
+    return t;
+}
+
 // tile + the 16 x 32 four-step twiddle factors of strided passes; two tiles when merged
 static size_t pass_smem(int logl, int variant) {
     const size_t tile = (size_t)TP * ((size_t)1 << logl);
@@ -756,13 +822,14 @@ static cudaError_t ensure_tables() {
     e = cudaMemcpyToSymbol(g_qtw, T.tw.data(), T.tw.size() * sizeof(u32));
     if (e != cudaSuccess) return e;
     const KernelTable& K = ktab();
+    const BatchKernelTable& BK = bktab();
     for (int v = 0; v < NV; ++v)
         for (int l = 0; l <= MAX_PASS_BITS; ++l)
-            if (K.k[v][l]) {
-                e = cudaFuncSetAttribute((const void*)K.k[v][l], cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)pass_smem(l, v));
+            for (const void* f : {(const void*)K.k[v][l], (const void*)BK.k[v][l]}) {
+                if (!f) continue;
+                e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pass_smem(l, v));
                 if (e != cudaSuccess) return e;
-                e = cudaFuncSetAttribute((const void*)K.k[v][l], cudaFuncAttributePreferredSharedMemoryCarveout,
+                e = cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout,
                                          (int)cudaSharedmemCarveoutMaxShared);
                 if (e != cudaSuccess) return e;
             }
@@ -968,6 +1035,109 @@ static void crt_constants(u64 N, u32 (&cst)[3]) {
     }
 }
 
+// Launch list of a whole product: a 2^n-digit transform of both operands in scratch A and B
+// (B unused for a square), the product left in A in natural order for the CRT.
+struct QRec {
+    int variant, logl;
+    QArgs a;
+    u64 tiles;
+};
+struct QWhole {
+    int count;
+    QRec rec[3 * MAX_PASSES + 2];
+};
+
+static void plan_whole(const Job& j, int n, u32* A, u32* B, QWhole* out) {
+    const int sqr = j.sqr ? 1 : 0;
+    if (sqr) B = A;
+    const Plan pl = qplan(n);
+    const int P = pl.passes;
+    const u64 N = 1ull << n;
+    int logB[MAX_PASSES];
+    logB[0] = n;
+    for (int p = 1; p < P; ++p) logB[p] = logB[p - 1] - pl.bits[p - 1];
+    const int lastl = pl.bits[P - 1];
+    const u64 nblk_last = N >> lastl;
+    const u64 tiles_last = (nblk_last + TC - 1) / TC;
+    const int ncols_last = nblk_last < (u64)TC ? (int)nblk_last : TC;
+    out->count = 0;
+    QArgs pa;
+    memset(&pa, 0, sizeof(pa));
+    pa.N = N;
+    pa.ncols = TC;
+    auto add = [&](int variant, int logl, u64 tiles) {
+        QRec& r = out->rec[out->count++];
+        r.variant = variant;
+        r.logl = logl;
+        r.a = pa;
+        r.tiles = tiles;
+    };
+    auto fwd_strided = [&](const u64* src, u64 len, u32* data) {
+        for (int p = 0; p + 1 < P; ++p) {
+            pa.src = src;
+            pa.len = len;
+            pa.data = data;
+            pa.logB = logB[p];
+            add(p == 0 ? V_FWD_E : V_FWD, pl.bits[p], N >> (pl.bits[p] + LOG_TC));
+        }
+    };
+    const bool merged = !sqr && P >= 2 && lastl >= 5 && lastl <= 8;
+    if (merged) {
+        fwd_strided(j.a, j.la, A);
+        fwd_strided(j.b, j.lb, B);
+        pa.src = nullptr;
+        pa.len = 0;
+        pa.data = B;
+        pa.other = A;
+        pa.logB = logB[P - 1];
+        pa.ncols = TC;
+        add(V_FUSED2, lastl, tiles_last);
+    } else if (!sqr) {
+        fwd_strided(j.a, j.la, A);
+        pa.src = j.a;
+        pa.len = j.la;
+        pa.data = A;
+        pa.other = nullptr;
+        pa.logB = logB[P - 1];
+        pa.ncols = ncols_last;
+        add(P == 1 ? V_LAST_E : V_LAST, lastl, tiles_last);
+        pa.ncols = TC;
+        fwd_strided(j.b, j.lb, B);
+        pa.src = j.b;
+        pa.len = j.lb;
+        pa.data = B;
+        pa.other = A;
+        pa.logB = logB[P - 1];
+        pa.ncols = ncols_last;
+        add(P == 1 ? V_FUSED_E : V_FUSED, lastl, tiles_last);
+    } else {
+        fwd_strided(j.a, j.la, A);
+        pa.src = j.a;
+        pa.len = j.la;
+        pa.data = A;
+        pa.other = A;
+        pa.logB = logB[P - 1];
+        pa.ncols = ncols_last;
+        add(P == 1 ? V_SQR_E : V_SQR, lastl, tiles_last);
+    }
+    pa.src = nullptr;
+    pa.len = 0;
+    pa.other = nullptr;
+    pa.ncols = TC;
+    for (int p = P - 2; p >= 0; --p) {
+        pa.data = A;
+        pa.logB = logB[p];
+        add(V_INV, pl.bits[p], N >> (pl.bits[p] + LOG_TC));
+    }
+}
+
+// Transform length (log2 digits) of a whole product, -1 if it has none on this engine.
+static int whole_log_n(u64 la, u64 lb) {
+    const u64 out_len = la + lb;
+    if (la == 0 || lb == 0 || out_len > (1ull << (Q32_MAX_LOG_N - 1))) return -1;
+    return ilog2(2 * out_len - 1);
+}
+
 }  // namespace q32
 
 bool q32_fits(u64 la, u64 lb, int sqr) { return q32::plan_job(la, lb, sqr).ok; }
@@ -998,6 +1168,109 @@ int q32_launches(u64 la, u64 lb, int sqr) {
 int q32_pieces(u64 la, u64 lb, int sqr) {
     const q32::QJob J = q32::plan_job(la, lb, sqr);
     return J.ok ? J.m : 0;
+}
+
+// ---- batches: whole products grouped by transform length and kind share every launch
+int q32_batch_log_n(const Job& j) { return j.spectrum ? -1 : q32::whole_log_n(j.la, j.lb); }
+
+size_t q32_batch_res_bytes(const Job& j) {
+    const int n = q32_batch_log_n(j);
+    if (n < 0) return 0;
+    return q32::align256(3 * (1ull << n) * sizeof(u32)) * (j.sqr ? 1 : 2);
+}
+
+size_t q32_batch_state_bytes(const Job& j) {
+    const u64 ncta = (j.la + j.lb + CTILE - 1) / CTILE;
+    return 16 + ((ncta * sizeof(u32) + 15) & ~(size_t)15);
+}
+
+size_t q32_batch_desc_bytes_per_job() {
+    return (3 * MAX_PASSES + 2) * (sizeof(q32::QArgs) + 16) + sizeof(q32::QCrtArgs) + sizeof(u32) + 32;
+}
+
+cudaError_t q32_prepare() { return q32::ensure_tables(); }
+
+cudaError_t q32_batch_plan(const Job* jobs, const int* idx, int m, char* res, size_t* roff, char* st, size_t* soff,
+                           u32* err, char* h, size_t* hoff, size_t hcap, Q32Group* g) {
+    using namespace q32;
+    if (m <= 0) return cudaErrorInvalidValue;
+    auto reserve = [&](size_t bytes) -> size_t {
+        const size_t o = *hoff;
+        *hoff = (*hoff + bytes + 15) & ~(size_t)15;
+        return o;
+    };
+    std::vector<QWhole> W(m);
+    std::vector<QCrtArgs> C(m);
+    std::vector<u32> nc(m);
+    u32 maxc = 0;
+    const int n = q32_batch_log_n(jobs[idx[0]]);
+    if (n < 0) return cudaErrorInvalidValue;
+    u32 cst[3];
+    crt_constants(1ull << n, cst);
+    for (int t = 0; t < m; ++t) {
+        const Job& j = jobs[idx[t]];
+        if (q32_batch_log_n(j) != n) return cudaErrorInvalidValue;
+        const u64 N = 1ull << n, out_len = j.la + j.lb;
+        u32* A = (u32*)(res + *roff);
+        *roff += align256(3 * N * sizeof(u32));
+        u32* B = A;
+        if (!j.sqr) {
+            B = (u32*)(res + *roff);
+            *roff += align256(3 * N * sizeof(u32));
+        }
+        u32* ticket = (u32*)(st + *soff);
+        *soff += q32_batch_state_bytes(j);
+        plan_whole(j, n, A, B, &W[t]);
+        QCrtArgs& ca = C[t];
+        memset(&ca, 0, sizeof(ca));
+        memcpy(ca.cst, cst, sizeof(cst));
+        ca.res = A;
+        ca.N = N;
+        ca.nvalid = 2 * out_len - 1;
+        ca.out = j.out;
+        ca.out_len = out_len;
+        ca.ticket = ticket;
+        ca.state = ticket + 4;
+        ca.err = err;
+        nc[t] = (u32)((out_len + CTILE - 1) / CTILE);
+        if (nc[t] > maxc) maxc = nc[t];
+        if (W[t].count != W[0].count) return cudaErrorInvalidValue;
+    }
+    g->m = m;
+    g->count = W[0].count;
+    g->max_ncta = maxc;
+    for (int k = 0; k < g->count; ++k) {
+        g->variant[k] = W[0].rec[k].variant;
+        g->logl[k] = W[0].rec[k].logl;
+        g->tiles[k] = W[0].rec[k].tiles;
+        g->args_off[k] = reserve((size_t)m * sizeof(QArgs));
+        if (*hoff > hcap) return cudaErrorInvalidValue;
+        QArgs* d = (QArgs*)(h + g->args_off[k]);
+        for (int t = 0; t < m; ++t) d[t] = W[t].rec[k].a;
+    }
+    g->crt_off = reserve((size_t)m * sizeof(QCrtArgs));
+    g->ncta_off = reserve((size_t)m * sizeof(u32));
+    if (*hoff > hcap) return cudaErrorInvalidValue;
+    memcpy(h + g->crt_off, C.data(), (size_t)m * sizeof(QCrtArgs));
+    memcpy(h + g->ncta_off, nc.data(), (size_t)m * sizeof(u32));
+    return cudaSuccess;
+}
+
+cudaError_t q32_batch_launch(const Q32Group& g, const char* d_desc, cudaStream_t s) {
+    using namespace q32;
+    const BatchKernelTable& BK = bktab();
+    cudaError_t e;
+    for (int k = 0; k < g.count; ++k) {
+        QBatchKernel kk = BK.k[g.variant[k]][g.logl[k]];
+        if (!kk) return cudaErrorInvalidValue;
+        const unsigned grid = (unsigned)((u64)g.m * g.tiles[k] * 3);
+        kk<<<grid, NT, pass_smem(g.logl[k], g.variant[k]), s>>>((const QArgs*)(d_desc + g.args_off[k]),
+                                                                (u32)g.tiles[k]);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
+    k_qcrt_carry_batch<<<(unsigned)(g.m * g.max_ncta), CNT, 0, s>>>((const QCrtArgs*)(d_desc + g.crt_off), g.max_ncta,
+                                                                    (const u32*)(d_desc + g.ncta_off));
+    return cudaGetLastError();
 }
 
 cudaError_t q32_enqueue(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s, cudaEvent_t b_ready, int crt_chunks,
@@ -1060,46 +1333,10 @@ cudaError_t q32_enqueue(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s,
     if (J.m == 1) {
         u32* A = (u32*)(base + J.a);
         u32* B = sqr ? A : (u32*)(base + J.b);
-        const bool merged = !sqr && P >= 2 && lastl >= 5 && lastl <= 8;
-        if (merged) {
-            if ((e = fwd_strided(j.a, j.la, A)) != cudaSuccess) return e;
-            if ((e = fwd_strided(j.b, j.lb, B)) != cudaSuccess) return e;
-            pa.src = nullptr;
-            pa.len = 0;
-            pa.data = B;
-            pa.other = A;
-            pa.logB = logB[P - 1];
-            pa.ncols = TC;
-            if ((e = launch(V_FUSED2, lastl, pa, tiles_last)) != cudaSuccess) return e;
-        } else if (!sqr) {
-            if ((e = fwd_strided(j.a, j.la, A)) != cudaSuccess) return e;
-            pa.src = j.a;
-            pa.len = j.la;
-            pa.data = A;
-            pa.other = nullptr;
-            pa.logB = logB[P - 1];
-            pa.ncols = ncols_last;
-            if ((e = launch(P == 1 ? V_LAST_E : V_LAST, lastl, pa, tiles_last)) != cudaSuccess) return e;
-            pa.ncols = TC;
-            if ((e = fwd_strided(j.b, j.lb, B)) != cudaSuccess) return e;
-            pa.src = j.b;
-            pa.len = j.lb;
-            pa.data = B;
-            pa.other = A;
-            pa.logB = logB[P - 1];
-            pa.ncols = ncols_last;
-            if ((e = launch(P == 1 ? V_FUSED_E : V_FUSED, lastl, pa, tiles_last)) != cudaSuccess) return e;
-        } else {
-            if ((e = fwd_strided(j.a, j.la, A)) != cudaSuccess) return e;
-            pa.src = j.a;
-            pa.len = j.la;
-            pa.data = A;
-            pa.other = A;
-            pa.logB = logB[P - 1];
-            pa.ncols = ncols_last;
-            if ((e = launch(P == 1 ? V_SQR_E : V_SQR, lastl, pa, tiles_last)) != cudaSuccess) return e;
-        }
-        if ((e = inverse_strided(A, 0)) != cudaSuccess) return e;
+        QWhole W;
+        plan_whole(j, J.n, A, B, &W);
+        for (int k = 0; k < W.count; ++k)
+            if ((e = launch(W.rec[k].variant, W.rec[k].logl, W.rec[k].a, W.rec[k].tiles)) != cudaSuccess) return e;
         ca.res = A;
         ca.N = N;
     } else {

@@ -22,7 +22,9 @@ __host__ __device__ constexpr int round_top(int logl, int idx) {
 // Round twiddle tables.  For a round of RB bits whose top index bit is TOP, the group with
 // low offset q (q < 2^(TOP-RB+1)) needs, for stage s (span 2^(TOP-s)) and u < 2^(RB-1-s):
 //     w_{2^(TOP-s+1)}^(q + u * 2^(TOP-RB+1))
-// stored at rt_off(RB, TOP) + q * 2^RB + (2^RB - 2^(RB-s)) + u (entry 2^RB - 1 is padding).
+// as its stage entry j = 2^RB - 2^(RB-s) + u (j < 2^RB - 1), stored stage-major at
+// rt_off(RB, TOP) + j * 2^(TOP-RB+1) + q, so lanes holding consecutive groups read
+// consecutive entries.
 __host__ __device__ constexpr int rt_base(int r) {
     return r <= 1 ? 0 : rt_base(r - 1) + (1 << (r - 1)) * ((1 << (RT_MAXLOGL - r + 2)) - 1);
 }

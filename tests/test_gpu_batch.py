@@ -30,7 +30,15 @@ def make_batch(count, lo, hi, seed, sqr_frac=0.2):
     return cases
 
 
-def test_mixed_batch_matches_oracle(fmn, oracle):
+@pytest.fixture(params=["e32", "e64"])
+def engine(request, fmn):
+    """Batches on the 32-bit engine (what AUTO picks for whole products) and on the 64-bit one."""
+    fmn.set_engine(fmn.ENGINE_AUTO if request.param == "e32" else fmn.ENGINE_64)
+    yield request.param
+    fmn.set_engine(fmn.ENGINE_AUTO)
+
+
+def test_mixed_batch_matches_oracle(fmn, oracle, engine):
     import torch
     cases = make_batch(300, 1, 40000, 3)
     cases.append((synth.limbs("uniform", 5, 1), np.zeros(0, np.uint64)))   # zero product
@@ -49,7 +57,7 @@ def test_mixed_batch_matches_oracle(fmn, oracle):
         assert np.array_equal(_host(out), want), (len(a), len(b), b is a)
 
 
-def test_batch_equals_per_call_on_the_mixed_size_stream(fmn):
+def test_batch_equals_per_call_on_the_mixed_size_stream(fmn, engine):
     """The configuration the batched form is measured on: each side log-uniform in
     [1000, 100000] limbs, 20% squares (a 512-product sample of it)."""
     import torch
