@@ -13,7 +13,7 @@ length taken as the max over ranks.
   roofline / roofline_int
           the dominant kernel, timed live with CUDA events inside the timed region, against
           the measured HBM copy bandwidth (MEASURED_PEAKS.json) and against the measured
-          peak of this library's Montgomery product (microbenchmark run here);
+          peak of the engine's butterfly arithmetic (microbenchmark run here);
   cpu_baseline
           the reference's own src/ abs_mul64 (oracle/_ref, compiled unmodified) on one host
           core, one 10M x 10M product (rank 0, N = 1 only).
@@ -40,7 +40,8 @@ SEED = 0
 KIND = "uniform"
 METRIC = "abs_mul64 products/s at 10M x 10M limbs (bit-exact)"
 UNIT = "products/s"
-WORKLOAD = "abs_mul64 10,000,000 x 10,000,000 limbs (uniform u64, seed 0), NTT length 2^25 over 3 primes"
+WORKLOAD = ("abs_mul64 10,000,000 x 10,000,000 limbs (uniform u64, seed 0); 32-bit engine: the product "
+            "split into two 10M x 5M pieces, 2^25-digit transforms over 3 primes")
 DATA = "synthetic: splitmix64 seed 0, uniform u64 limbs, top limb nonzero (no dataset involved)"
 
 
@@ -493,6 +494,11 @@ def run_ours(args, ws, rank, local):
         hbm_src = "measured" if hbm_peak else "fallback"
         hbm_peak = hbm_peak or 6650.0
         mm_peak, bf_peak = fmn.bench_modmul()
+        engine = fmn.engine_for(l1, l2)
+        pieces = fmn.pieces_for(l1, l2)
+        if engine == fmn.ENGINE_32:
+            # the 32-bit engine's pass kernels are held against its own butterfly peak
+            mm_peak = bf_peak = fmn.bench_bfly32()
         dom = max(prof.items(), key=lambda kv: kv[1]["ms"])
         name, st = dom
         per_launch_ms = st["ms"] / max(1, st["launches"])
@@ -514,11 +520,16 @@ def run_ours(args, ws, rank, local):
         result = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": per_step_ms, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": DATA,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u32" if engine == fmn.ENGINE_32 else "u64",
+            "data": DATA,
             "config": {"workload": WORKLOAD if l1 == LEN1 else f"abs_mul64 {l1} x {l2} limbs",
-                       "len1": l1, "len2": l2, "ntt_len": fmn.ntt_len(l1, l2),
+                       "len1": l1, "len2": l2,
+                       "engine": ("32-bit digits mod three 31-bit primes" if engine == fmn.ENGINE_32
+                                  else "64-bit limbs mod the reference's three 62-bit primes"),
+                       "pieces": pieces, "reference_ntt_len": fmn.ntt_len(l1, l2),
                        "parallelism": "replicas: one independent product per GPU" if ws > 1 else "single GPU",
-                       "l2_policy": "no flush: operands (160 MB) and residues (1.6 GB) per product exceed the 126 MB L2"},
+                       "l2_policy": "no flush: operands (%d MB) and scratch (%d MB) per product exceed the 126 MB L2"
+                                    % (16 * (l1 + l2) >> 20, fmn.workspace_size(l1, l2) >> 20)},
             "us_per_product": 1e3 * per_step_ms,
             "limbs_per_s": (l1 + l2) * value,
             "bit_exact": bit_exact,
@@ -527,10 +538,13 @@ def run_ours(args, ws, rank, local):
                          "peak_source": f"{hbm_src} (MEASURED_PEAKS.json hbm_gbs)" if hbm_src == "measured"
                          else "fallback 6.65 TB/s",
                          "algorithmic_bytes_per_launch": bytes_per_launch, "ms_per_launch": per_launch_ms},
-            "roofline_int": {"bound": "imad (integer multiply pipe)", "kernel": name,
-                             "achieved": achieved_mm / 1e9, "peak": mm_peak / 1e9, "unit": "Gmodmul/s",
+            "roofline_int": {"bound": "integer issue (butterfly arithmetic)", "kernel": name,
+                             "achieved": achieved_mm / 1e9, "peak": mm_peak / 1e9,
+                             "unit": "Gbutterfly/s" if engine == fmn.ENGINE_32 else "Gmodmul/s",
                              "frac": achieved_mm / mm_peak,
-                             "peak_source": "measured: independent Montgomery-product chains on this GPU",
+                             "peak_source": ("measured: independent 32-bit butterfly chains on this GPU"
+                                             if engine == fmn.ENGINE_32 else
+                                             "measured: independent Montgomery-product chains on this GPU"),
                              "butterfly_peak": bf_peak / 1e9,
                              "frac_of_butterfly_peak": achieved_mm / bf_peak,
                              "algorithmic_modmuls_per_launch": mm_per_launch,

@@ -34,7 +34,7 @@ EXPORTS = ["abs_mul64", "abs_sqr64", "fmn_init", "fmn_shutdown", "fmn_last_error
            "fmn_server_wait", "fmn_server_take", "fmn_server_get_stats", "fmn_server_replay", "fmn_server_destroy",
            "fmn_get_plan", "fmn_set_plan", "fmn_autotune", "fmn_load_plans", "fmn_load_default_plans",
            "fmn_set_engine", "fmn_get_engine", "fmn_engine_for", "fmn_pieces_for",
-           "fmn_force_pieces"]
+           "fmn_force_pieces", "fmn_bench_bfly32"]
 
 ENGINE_AUTO, ENGINE_64, ENGINE_32 = 0, 1, 2
 
@@ -123,6 +123,8 @@ def load_library(path=None):
     lib.fmn_launches_per_product.restype = ctypes.c_int
     lib.fmn_bench_modmul.argtypes = [_dp, _dp]
     lib.fmn_bench_modmul.restype = ctypes.c_int
+    lib.fmn_bench_bfly32.argtypes = [_dp]
+    lib.fmn_bench_bfly32.restype = ctypes.c_int
     lib.fmn_mul_device_noalloc.argtypes = [_vp, _u64, _vp, _u64, _vp, _vp]
     lib.fmn_mul_device_noalloc.restype = ctypes.c_int
     _jp = ctypes.POINTER(FmnJob)
@@ -315,6 +317,13 @@ def bench_modmul():
     a, b = ctypes.c_double(), ctypes.c_double()
     _check(load_library().fmn_bench_modmul(ctypes.byref(a), ctypes.byref(b)))
     return a.value, b.value
+
+
+def bench_bfly32():
+    """Butterflies/s peak of the 32-bit engine's arithmetic on the current device."""
+    a = ctypes.c_double()
+    _check(load_library().fmn_bench_bfly32(ctypes.byref(a)))
+    return a.value
 
 
 def _job_array(jobs):

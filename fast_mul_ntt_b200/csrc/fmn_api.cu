@@ -812,6 +812,17 @@ int fmn_bench_modmul(double* modmul_per_s, double* butterfly_per_s) {
     return FMN_OK;
 }
 
+int fmn_bench_bfly32(double* butterfly_per_s) {
+    DevCtx* c;
+    int rc = get_ctx(&c);
+    if (rc) return rc;
+    double a = 0;
+    cudaError_t e = fmn::q32_bench_bfly(&a);
+    if (e != cudaSuccess) return set_err(FMN_ERR_CUDA, "butterfly microbenchmark", e);
+    if (butterfly_per_s) *butterfly_per_s = a;
+    return FMN_OK;
+}
+
 u64 fmn_ntt_len(u64 len1, u64 len2) {
     const u64 conv = len1 + len2 ? len1 + len2 - 1 : 0;
     u64 n = 1;

@@ -181,6 +181,8 @@ cudaError_t fill_limbs(u64* p, u64 n, u64 seed, cudaStream_t s);
 // Throughput microbenchmark of independent Montgomery products (peak of the integer pipe
 // for this arithmetic): returns products per second.
 cudaError_t bench_modmul(double* per_second, double* butterflies_per_second);
+// Same for the 32-bit engine's butterfly (Shoup product plus reductions), per second.
+cudaError_t q32_bench_bfly(double* per_second);
 
 }  // namespace fmn
 

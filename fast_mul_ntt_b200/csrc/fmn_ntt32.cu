@@ -1273,6 +1273,57 @@ cudaError_t q32_batch_launch(const Q32Group& g, const char* d_desc, cudaStream_t
     return cudaGetLastError();
 }
 
+// ---- butterfly throughput microbenchmark (the peak the 32-bit pass kernels are held against)
+namespace q32 {
+constexpr int BB_CHAINS = 8, BB_ITERS = 4096;
+__global__ void __launch_bounds__(256) k_bench_qbfly(u32* sink, uint2 w) {
+    const PrimeQ q = c_q[0];
+    u32 x[2 * BB_CHAINS];
+#pragma unroll
+    for (int i = 0; i < 2 * BB_CHAINS; ++i) x[i] = ((blockIdx.x * 256 + threadIdx.x) * 2654435761u + i * 97u) % q.p;
+#pragma unroll 1
+    for (int it = 0; it < BB_ITERS; ++it) {
+#pragma unroll
+        for (int i = 0; i < BB_CHAINS; ++i) qbfly_dif(x[i], x[i + BB_CHAINS], w, q);
+    }
+    u32 acc = 0;
+#pragma unroll
+    for (int i = 0; i < 2 * BB_CHAINS; ++i) acc ^= x[i];
+    if (acc == 0x12345u) sink[0] = acc;
+}
+}  // namespace q32
+
+cudaError_t q32_bench_bfly(double* per_second) {
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    u32* sink = nullptr;
+    cudaError_t e = cudaMalloc(&sink, 64);
+    if (e != cudaSuccess) return e;
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    const u32 w0 = 1234567u;
+    const uint2 w = make_uint2(w0, (u32)(((u64)w0 << 32) / Q32_P0));
+    const unsigned grid = (unsigned)sms * 8;
+    float best = 1e30f;
+    for (int rep = 0; rep < 4; ++rep) {
+        cudaEventRecord(a);
+        q32::k_bench_qbfly<<<grid, 256>>>(sink, w);
+        cudaEventRecord(b);
+        cudaEventSynchronize(b);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, a, b);
+        if (rep && ms < best) best = ms;
+    }
+    e = cudaGetLastError();
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaFree(sink);
+    *per_second = (double)grid * 256.0 * q32::BB_CHAINS * q32::BB_ITERS / (best * 1e-3);
+    return e;
+}
+
 cudaError_t q32_enqueue(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s, cudaEvent_t b_ready, int crt_chunks,
                         ChunkDone after_chunk, void* ctx) {
     using namespace q32;

@@ -240,6 +240,8 @@ int fmn_launches_per_product(u64 len1, u64 len2, int sqr);
 /* Peak of this library's Montgomery product on the current device: a microbenchmark of
  * independent modmul chains and of decimation-in-frequency butterflies (per second). */
 int fmn_bench_modmul(double* modmul_per_s, double* butterfly_per_s);
+/* Peak of the 32-bit engine's butterfly (independent chains, per second). */
+int fmn_bench_bfly32(double* butterfly_per_s);
 
 /* Transform length used for a product: the next power of two >= len1 + len2 - 1
  * (int_ceil2, src/fast_mul.c:299-312). */
