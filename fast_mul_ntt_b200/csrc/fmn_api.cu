@@ -61,6 +61,7 @@ struct DevCtx {
     cudaEvent_t stage_free = nullptr;   // the last batch's descriptor copy has completed
     bool stage_pending = false;
     cudaEvent_t cb_event[4] = {nullptr};   // chunked copy-back of host products
+    cudaEvent_t ci_event[8] = {nullptr};   // piecewise copy-in of the second operand
 };
 
 std::mutex g_ctx_mu;
@@ -96,6 +97,7 @@ int get_ctx(DevCtx** out) {
             e = cudaEventCreateWithFlags(&c->wevent[k], cudaEventDisableTiming);
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->stage_free, cudaEventDisableTiming);
         for (int k = 0; k < 4 && e == cudaSuccess; ++k) e = cudaEventCreateWithFlags(&c->cb_event[k], cudaEventDisableTiming);
+        for (int k = 0; k < 8 && e == cudaSuccess; ++k) e = cudaEventCreateWithFlags(&c->ci_event[k], cudaEventDisableTiming);
         if (e != cudaSuccess) {
             delete c;
             return set_err(FMN_ERR_CUDA, "creating device context streams", e);
@@ -280,15 +282,35 @@ cudaError_t copy_back_chunk(void* p, u64 lo, u64 hi) {
     return e;
 }
 
+struct CopyIn {
+    cudaStream_t copy;
+    cudaEvent_t ev[8];
+    int used;
+    u64* dst;
+    const u64* src;
+};
+
+// Copy limbs [lo, hi) of the second operand on the copy-in stream and make s wait for them.
+cudaError_t copy_in_range(void* p, u64 lo, u64 hi, cudaStream_t s) {
+    CopyIn* ci = (CopyIn*)p;
+    cudaEvent_t ev = ci->ev[ci->used++ % 8];
+    cudaError_t e = cudaMemcpyAsync(ci->dst + lo, ci->src + lo, (hi - lo) * sizeof(u64), cudaMemcpyHostToDevice, ci->copy);
+    if (e == cudaSuccess) e = cudaEventRecord(ev, ci->copy);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(s, ev, 0);
+    return e;
+}
+
 // Host product on pinned buffers: in2 is copied on a second stream while in1's forward
-// passes run, and the output comes back in chunks as the carry scan finishes them.
+// passes run (piece by piece for a split product, each just ahead of its first reader), and
+// the output comes back in chunks on a third stream as the carry scan finishes them (for a
+// split product, the limbs each piece completes while the next piece computes).
 int host_product_pinned(DevCtx* c, const u64* in1, u64 len1, const u64* in2, u64 len2, u64* out, int sqr) {
     const u64 out_len = len1 + len2;
     const size_t o1 = 0, o2 = round256(len1 * 8), oo = o2 + (sqr ? 0 : round256(len2 * 8));
     int rc;
     if ((rc = ensure_io(c, oo + round256(out_len * 8)))) return rc;
     char* io = (char*)c->io;
-    cudaStream_t s = c->stream, cs = c->wstream[0];
+    cudaStream_t s = c->stream, cs = c->wstream[0], co = c->wstream[1];
     cudaError_t e;
     fmn::Job j;
     j.a = (const u64*)(io + o1);
@@ -300,32 +322,33 @@ int host_product_pinned(DevCtx* c, const u64* in1, u64 len1, const u64* in2, u64
     const size_t need = fmn::job_workspace_bytes(j);
     if ((rc = ensure_ws(c, need))) return rc;
     if (c->done_valid && ((e = cudaStreamWaitEvent(s, c->done, 0)) != cudaSuccess ||
-                          (e = cudaStreamWaitEvent(cs, c->done, 0)) != cudaSuccess))
+                          (e = cudaStreamWaitEvent(cs, c->done, 0)) != cudaSuccess ||
+                          (e = cudaStreamWaitEvent(co, c->done, 0)) != cudaSuccess))
         return set_err(FMN_ERR_CUDA, "cudaStreamWaitEvent", e);
     const fmn::TwiddleSet* tws = fmn::job_engine(j) != fmn::ENGINE_64 ? nullptr : get_twiddles(c, ilog2_ceil(out_len - 1), s);
     if ((e = cudaMemcpyAsync(io + o1, in1, len1 * 8, cudaMemcpyHostToDevice, s)) != cudaSuccess)
         return set_err(FMN_ERR_CUDA, "copying in1 to the device", e);
-    cudaEvent_t b_ready = nullptr;
-    if (!sqr) {
-        if ((e = cudaMemcpyAsync(io + o2, in2, len2 * 8, cudaMemcpyHostToDevice, cs)) != cudaSuccess ||
-            (e = cudaEventRecord(c->wevent[1], cs)) != cudaSuccess)
-            return set_err(FMN_ERR_CUDA, "copying in2 to the device", e);
-        b_ready = c->wevent[1];
-    }
+    CopyIn ci;
+    ci.copy = cs;
+    ci.used = 0;
+    ci.dst = (u64*)(io + o2);
+    ci.src = in2;
+    for (int k = 0; k < 8; ++k) ci.ev[k] = c->ci_event[k];
     CopyBack cb;
     cb.main = s;
-    cb.copy = cs;
+    cb.copy = co;
     cb.used = 0;
     cb.dst = out;
     cb.src = j.out;
     for (int k = 0; k < 4; ++k) cb.ev[k] = c->cb_event[k];
     const int chunks = out_len >= (1u << 20) ? 4 : 1;
-    if ((e = fmn::enqueue_job_overlapped(j, c->ws, c->ws_cap, s, tws, b_ready, chunks, copy_back_chunk, &cb)) !=
-        cudaSuccess)
+    if ((e = fmn::enqueue_job_overlapped(j, c->ws, c->ws_cap, s, tws, sqr ? nullptr : copy_in_range, &ci, chunks,
+                                         copy_back_chunk, &cb)) != cudaSuccess)
         return set_err(FMN_ERR_CUDA, "kernel launch", e);
-    // the copy stream ends after the last chunk; order the main stream (and later jobs) after it
-    if ((e = cudaEventRecord(c->wevent[2], cs)) != cudaSuccess || (e = cudaStreamWaitEvent(s, c->wevent[2], 0)) != cudaSuccess)
-        return set_err(FMN_ERR_CUDA, "joining the copy stream", e);
+    // the copy streams end after the last chunk; order the main stream (and later jobs) after them
+    if ((e = cudaEventRecord(c->wevent[2], co)) != cudaSuccess || (e = cudaStreamWaitEvent(s, c->wevent[2], 0)) != cudaSuccess ||
+        (e = cudaEventRecord(c->wevent[3], cs)) != cudaSuccess || (e = cudaStreamWaitEvent(s, c->wevent[3], 0)) != cudaSuccess)
+        return set_err(FMN_ERR_CUDA, "joining the copy streams", e);
     if ((e = cudaEventRecord(c->done, s)) != cudaSuccess) return set_err(FMN_ERR_CUDA, "cudaEventRecord", e);
     c->done_valid = true;
     return take_device_error(c->ws, c->h_err, s);
@@ -492,6 +515,8 @@ void fmn_shutdown(void) {
         if (c->stage_free) cudaEventDestroy(c->stage_free);
         for (int k = 0; k < 4; ++k)
             if (c->cb_event[k]) cudaEventDestroy(c->cb_event[k]);
+        for (int k = 0; k < 8; ++k)
+            if (c->ci_event[k]) cudaEventDestroy(c->ci_event[k]);
         if (c->done) cudaEventDestroy(c->done);
         if (c->stream) cudaStreamDestroy(c->stream);
         delete c;

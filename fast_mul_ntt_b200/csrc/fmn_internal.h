@@ -63,8 +63,11 @@ int q32_launches(u64 la, u64 lb, int sqr);
 int q32_pieces(u64 la, u64 lb, int sqr);        // 1: whole product; > 1: split into pieces
 void q32_force_pieces(int m);                  // tests: split into m pieces where possible (0: model)
 typedef cudaError_t (*ChunkDone)(void* ctx, u64 first_limb, u64 end_limb);
-cudaError_t q32_enqueue(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s, cudaEvent_t b_ready, int crt_chunks,
-                        ChunkDone after_chunk, void* ctx);
+// Called before the first launch that reads limbs [first, end) of the second operand: it must
+// make stream s wait until those limbs are in device memory (e.g. an event after their copy).
+typedef cudaError_t (*NeedLimbs)(void* ctx, u64 first_limb, u64 end_limb, cudaStream_t s);
+cudaError_t q32_enqueue(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s, NeedLimbs need_b, void* need_ctx,
+                        int crt_chunks, ChunkDone after_chunk, void* ctx);
 
 // Forward transform of `len` limbs at `src` into `spec` (3 * 2^log_n u64): the spectrum a
 // resident operand keeps for products of up to 2^log_n - len + 1 partner limbs.
@@ -101,12 +104,14 @@ cudaError_t build_twiddle_tables(int log_n, u64* buf, TwiddleSet* out, cudaStrea
 cudaError_t enqueue_job(const Job& job, void* ws, size_t ws_bytes, cudaStream_t stream,
                         const TwiddleSet* tw = nullptr);
 
-// A product with copy overlap: launches that read the second operand wait for `b_ready`
-// (its host-to-device copy on another stream), and the carry scan runs in `crt_chunks`
-// launches; after each, `after_chunk(ctx, first_limb, end_limb)` is called so the caller can
-// copy those final limbs back while the next chunk computes.
+// A product with copy overlap: before the first launch that reads a range of the second
+// operand's limbs, `need_b(need_ctx, first, end, s)` is called (the caller copies that range
+// on another stream and makes s wait for it; a split product asks piece by piece), and the
+// carry scan runs in chunks: after each, `after_chunk(ctx, first_limb, end_limb)` is called
+// so the caller can copy those final limbs back while the rest computes.  A split product
+// scans the limbs that a piece completes right after that piece.
 cudaError_t enqueue_job_overlapped(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s, const TwiddleSet* tw,
-                                   cudaEvent_t b_ready, int crt_chunks, ChunkDone after_chunk, void* ctx);
+                                   NeedLimbs need_b, void* need_ctx, int crt_chunks, ChunkDone after_chunk, void* ctx);
 
 // ---- 32-bit engine batches (whole products; see enqueue_batch)
 struct Q32Group {

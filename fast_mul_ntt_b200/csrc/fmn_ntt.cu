@@ -1356,7 +1356,7 @@ cudaError_t enqueue_job(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s,
     const u64 out_len = j.la + j.lb;
     if (out_len == 0) return cudaSuccess;
     if (j.la == 0 || j.lb == 0) return cudaMemsetAsync(j.out, 0, out_len * sizeof(u64), s);
-    if (job_engine(j) == ENGINE_32) return q32_enqueue(j, ws, ws_bytes, s, nullptr, 1, nullptr, nullptr);
+    if (job_engine(j) == ENGINE_32) return q32_enqueue(j, ws, ws_bytes, s, nullptr, nullptr, 1, nullptr, nullptr);
     const int sqr = j.sqr ? 1 : 0;
     const WsLayout w = ws_layout(j.la, j.lb, sqr, j.spectrum ? j.log_n : 0);
     if (ws_bytes < w.total || w.n > MAX_LOG_N) return cudaErrorInvalidValue;
@@ -1376,10 +1376,11 @@ cudaError_t enqueue_job(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s,
 }
 
 cudaError_t enqueue_job_overlapped(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s, const TwiddleSet* tws,
-                                   cudaEvent_t b_ready, int crt_chunks, ChunkDone after_chunk, void* ctx) {
+                                   NeedLimbs need_b, void* need_ctx, int crt_chunks, ChunkDone after_chunk, void* ctx) {
     const u64 out_len = j.la + j.lb;
     if (j.la == 0 || j.lb == 0 || out_len == 0) return cudaErrorInvalidValue;
-    if (job_engine(j) == ENGINE_32) return q32_enqueue(j, ws, ws_bytes, s, b_ready, crt_chunks, after_chunk, ctx);
+    if (job_engine(j) == ENGINE_32)
+        return q32_enqueue(j, ws, ws_bytes, s, need_b, need_ctx, crt_chunks, after_chunk, ctx);
     const int sqr = j.sqr ? 1 : 0;
     const WsLayout w = ws_layout(j.la, j.lb, sqr, j.spectrum ? j.log_n : 0);
     if (ws_bytes < w.total || w.n > MAX_LOG_N) return cudaErrorInvalidValue;
@@ -1393,8 +1394,8 @@ cudaError_t enqueue_job_overlapped(const Job& j, void* ws, size_t ws_bytes, cuda
     bool waited = false;
     for (int k = 0; k < L.count; ++k) {
         const LaunchRec& r = L.rec[k];
-        if (r.needs_b && !waited && b_ready) {          // second operand copied meanwhile
-            if ((e = cudaStreamWaitEvent(s, b_ready, 0)) != cudaSuccess) return e;
+        if (r.needs_b && !waited && need_b) {           // second operand copied meanwhile
+            if ((e = need_b(need_ctx, 0, j.lb, s)) != cudaSuccess) return e;
             waited = true;
         }
         if ((e = launch_pass(r.variant, r.logl, r.pa, r.tiles, s)) != cudaSuccess) return e;

@@ -979,26 +979,20 @@ static QJob plan_job(u64 la, u64 lb, int sqr) {
     return J;
 }
 
-// Launch sequencing of one product on one stream: kernel lookup, the wait for the second
-// operand's copy before its first reader, per-launch timing records.
+// Launch sequencing of one product on one stream: kernel lookup, the caller's hook that makes
+// the stream wait for a range of the second operand's limbs, per-launch timing records.
 struct Launcher {
     const Job& j;
     cudaStream_t s;
-    cudaEvent_t b_ready;
-    bool waited;
+    NeedLimbs need_b;
+    void* need_ctx;
     u64 N;
 
-    cudaError_t wait_b() {
-        if (waited) return cudaSuccess;
-        waited = true;
-        return cudaStreamWaitEvent(s, b_ready, 0);
-    }
+    cudaError_t need(u64 first, u64 end) { return need_b ? need_b(need_ctx, first, end, s) : cudaSuccess; }
     cudaError_t operator()(int variant, int logl, const QArgs& a, u64 tiles) {
         QKernel k = ktab().k[variant][logl];
         if (!k) return cudaErrorInvalidValue;
         cudaError_t e;
-        const bool reads_b = j.b && !j.sqr && a.src && a.src >= j.b && a.src < j.b + j.lb;
-        if ((reads_b || variant == V_FUSED2) && (e = wait_b()) != cudaSuccess) return e;
         const double vec = 3.0 * (double)N * 4.0, bfly = 3.0 * ((double)N / 2.0) * logl;
         const bool entry = (variant == V_FWD_E || variant == V_LAST_E || variant == V_FUSED_E || variant == V_SQR_E);
         double bytes = entry ? (double)a.len * 8.0 + vec : 2.0 * vec, mm = bfly + (entry ? 6.0 * (double)a.len : 0.0);
@@ -1324,8 +1318,36 @@ cudaError_t q32_bench_bfly(double* per_second) {
     return e;
 }
 
-cudaError_t q32_enqueue(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s, cudaEvent_t b_ready, int crt_chunks,
-                        ChunkDone after_chunk, void* ctx) {
+namespace q32 {
+// The CRT arguments of a product whose residues are in ca->res (stride ca->N).
+static void fill_crt(const Job& j, const QJob& J, char* base, u64 out_len, QCrtArgs* ca) {
+    ca->nvalid = 2 * out_len - 1;
+    ca->out = j.out;
+    ca->out_len = out_len;
+    ca->state = (u32*)(base + J.state);
+    ca->ticket = (u32*)(base + J.ticket);
+    ca->err = (u32*)base;
+}
+
+// CRT + carry CTAs [t0, t1) of ncta (tickets continue from earlier launches), then the
+// caller's copy-back hook for the limbs they finish.
+static cudaError_t crt_launch(const QCrtArgs& ca, u64 ncta, u64 t0, u64 t1, cudaStream_t s, ChunkDone after_chunk,
+                              void* ctx) {
+    const u64 n = t1 - t0;
+    const double crt_bytes = 3.0 * (double)ca.nvalid * 4.0 + (double)ca.out_len * 8.0;
+    const ProfMark m = prof_begin(K_CRT, crt_bytes * (double)n / (double)ncta, 3.0 * (double)ca.nvalid * (double)n / (double)ncta, s);
+    k_qcrt_carry<<<(unsigned)n, CNT, 0, s>>>(ca);
+    cudaError_t e = cudaGetLastError();
+    prof_end(m, s);
+    if (e != cudaSuccess) return e;
+    const u64 lo = t0 * CTILE, hi = t1 * CTILE < ca.out_len ? t1 * CTILE : ca.out_len;
+    if (after_chunk) return after_chunk(ctx, lo, hi);
+    return cudaSuccess;
+}
+}  // namespace q32
+
+cudaError_t q32_enqueue(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s, NeedLimbs need_b, void* need_ctx,
+                        int crt_chunks, ChunkDone after_chunk, void* ctx) {
     using namespace q32;
     const u64 out_len = j.la + j.lb;
     if (out_len == 0) return cudaSuccess;
@@ -1346,7 +1368,7 @@ cudaError_t q32_enqueue(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s,
     const u64 nblk_last = N >> lastl;
     const u64 tiles_last = (nblk_last + TC - 1) / TC;
     const int ncols_last = nblk_last < (u64)TC ? (int)nblk_last : TC;
-    Launcher launch{j, s, b_ready, b_ready == nullptr, N};
+    Launcher launch{j, s, need_b, need_ctx, N};
 
     QArgs pa;
     memset(&pa, 0, sizeof(pa));
@@ -1381,13 +1403,20 @@ cudaError_t q32_enqueue(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s,
     QCrtArgs ca;
     memset(&ca, 0, sizeof(ca));
     crt_constants(N, ca.cst);
+    u64 crt_done = 0;                 // CRT CTAs launched so far (split products with copy-back)
     if (J.m == 1) {
         u32* A = (u32*)(base + J.a);
         u32* B = sqr ? A : (u32*)(base + J.b);
         QWhole W;
         plan_whole(j, J.n, A, B, &W);
-        for (int k = 0; k < W.count; ++k)
+        bool have_b = sqr != 0;
+        for (int k = 0; k < W.count; ++k) {
+            if (!have_b && W.rec[k].a.src == j.b) {            // the second operand's first reader
+                if ((e = launch.need(0, j.lb)) != cudaSuccess) return e;
+                have_b = true;
+            }
             if ((e = launch(W.rec[k].variant, W.rec[k].logl, W.rec[k].a, W.rec[k].tiles)) != cudaSuccess) return e;
+        }
         ca.res = A;
         ca.N = N;
     } else {
@@ -1397,6 +1426,7 @@ cudaError_t q32_enqueue(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s,
         u32* ACC = (u32*)(base + J.acc);
         const u64* S_src = J.swap ? j.b : j.a;
         const u64* L_src = J.swap ? j.a : j.b;
+        if (J.swap && (e = launch.need(0, j.lb)) != cudaSuccess) return e;
         if ((e = fwd_strided(S_src, J.ls, R)) != cudaSuccess) return e;
         pa.src = nullptr;
         pa.len = 0;
@@ -1406,9 +1436,15 @@ cudaError_t q32_enqueue(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s,
         pa.logB = logB[P - 1];
         pa.ncols = ncols_last;
         if ((e = launch(V_LAST, lastl, pa, tiles_last)) != cudaSuccess) return e;
+        // limbs below (k + 1) cb are final once piece k is accumulated: with a copy-back hook
+        // their carry scan runs right away (tickets continue across launches)
+        ca.res = ACC;
+        ca.N = J.stride;
+        if (after_chunk && (e = cudaMemsetAsync(base + J.ticket, 0, J.total - J.ticket, s)) != cudaSuccess) return e;
         for (int k = 0; k < J.m; ++k) {
             const u64 first = (u64)k * J.cb;
             const u64 len = J.ll - first < J.cb ? J.ll - first : J.cb;
+            if (!J.swap && (e = launch.need(first, first + len)) != cudaSuccess) return e;
             if ((e = fwd_strided(L_src + first, len, C)) != cudaSuccess) return e;
             pa.src = nullptr;
             pa.len = 0;
@@ -1427,32 +1463,24 @@ cudaError_t q32_enqueue(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s,
             pa.acc_fresh = k == 0 ? 0 : 2 * J.ls - 1;
             if ((e = launch(V_INV_ACC, pl.bits[0], pa, N >> (pl.bits[0] + LOG_TC))) != cudaSuccess) return e;
             pa.acc = nullptr;
+            if (after_chunk && k + 1 < J.m) {
+                fill_crt(j, J, base, out_len, &ca);
+                const u64 t_end = (first + J.cb) / CTILE;
+                if (t_end > crt_done && (e = crt_launch(ca, J.ncta, crt_done, t_end, s, after_chunk, ctx)) != cudaSuccess)
+                    return e;
+                if (t_end > crt_done) crt_done = t_end;
+            }
         }
-        ca.res = ACC;
-        ca.N = J.stride;
     }
-    if ((e = launch.wait_b()) != cudaSuccess) return e;
 
-    ca.nvalid = 2 * out_len - 1;
-    ca.out = j.out;
-    ca.out_len = out_len;
-    ca.state = (u32*)(base + J.state);
-    ca.ticket = (u32*)(base + J.ticket);
-    ca.err = (u32*)base;
-    if ((e = cudaMemsetAsync(base + J.ticket, 0, J.total - J.ticket, s)) != cudaSuccess) return e;
+    fill_crt(j, J, base, out_len, &ca);
+    if (crt_done == 0 && (e = cudaMemsetAsync(base + J.ticket, 0, J.total - J.ticket, s)) != cudaSuccess) return e;
     if (crt_chunks < 1) crt_chunks = 1;
-    const u64 per = (J.ncta + crt_chunks - 1) / crt_chunks;
-    for (u64 t0 = 0; t0 < J.ncta; t0 += per) {
-        const u64 n = t0 + per <= J.ncta ? per : J.ncta - t0;
-        const double crt_bytes = 3.0 * (double)ca.nvalid * 4.0 + (double)out_len * 8.0;
-        const ProfMark m = prof_begin(K_CRT, crt_bytes * (double)n / (double)J.ncta,
-                                      3.0 * (double)ca.nvalid * (double)n / (double)J.ncta, s);
-        k_qcrt_carry<<<(unsigned)n, CNT, 0, s>>>(ca);
-        e = cudaGetLastError();
-        prof_end(m, s);
-        if (e != cudaSuccess) return e;
-        const u64 lo = t0 * CTILE, hi = (t0 + n) * CTILE < out_len ? (t0 + n) * CTILE : out_len;
-        if (after_chunk && (e = after_chunk(ctx, lo, hi)) != cudaSuccess) return e;
+    const u64 rest = J.ncta - crt_done;
+    const u64 per = (rest + crt_chunks - 1) / crt_chunks;
+    for (u64 t0 = crt_done; t0 < J.ncta; t0 += per) {
+        const u64 t1 = t0 + per <= J.ncta ? t0 + per : J.ncta;
+        if ((e = crt_launch(ca, J.ncta, t0, t1, s, after_chunk, ctx)) != cudaSuccess) return e;
     }
     return cudaSuccess;
 }
