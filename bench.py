@@ -40,8 +40,7 @@ SEED = 0
 KIND = "uniform"
 METRIC = "abs_mul64 products/s at 10M x 10M limbs (bit-exact)"
 UNIT = "products/s"
-WORKLOAD = ("abs_mul64 10,000,000 x 10,000,000 limbs (uniform u64, seed 0); 32-bit engine: the product "
-            "split into two 10M x 5M pieces, 2^25-digit transforms over 3 primes")
+WORKLOAD = "abs_mul64 10,000,000 x 10,000,000 limbs (uniform u64, seed 0)"
 DATA = "synthetic: splitmix64 seed 0, uniform u64 limbs, top limb nonzero (no dataset involved)"
 
 
@@ -526,7 +525,10 @@ def run_ours(args, ws, rank, local):
                        "len1": l1, "len2": l2,
                        "engine": ("32-bit digits mod three 31-bit primes" if engine == fmn.ENGINE_32
                                   else "64-bit limbs mod the reference's three 62-bit primes"),
-                       "pieces": pieces, "reference_ntt_len": fmn.ntt_len(l1, l2),
+                       "pieces": pieces,
+                       "plan": ("the longer operand in %d pieces, each multiplied with the other's resident "
+                                "spectrum" % pieces if pieces > 1 else "one transform of the whole product"),
+                       "reference_ntt_len": fmn.ntt_len(l1, l2),
                        "parallelism": "replicas: one independent product per GPU" if ws > 1 else "single GPU",
                        "l2_policy": "no flush: operands (%d MB) and scratch (%d MB) per product exceed the 126 MB L2"
                                     % (16 * (l1 + l2) >> 20, fmn.workspace_size(l1, l2) >> 20)},
