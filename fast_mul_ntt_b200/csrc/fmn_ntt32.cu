@@ -299,13 +299,30 @@ __device__ __forceinline__ void body_inv(u32* sm, const QArgs& a, u64 tile, int 
         }
     };
     if constexpr (ACC) {
+        // the last inverse round holds rows row0 + t * SP0 of one column: all accumulator
+        // loads of a group are issued before its adds and stores
+        constexpr int RB0 = round_bits(LOGL, 0), R0 = 1 << RB0, SP0 = 1 << (LOGL - RB0);
         u32* __restrict__ acc = a.acc + (u64)pi * a.acc_stride;
         const u64 valid = a.acc_valid, fresh = a.acc_fresh;
-        auto stl = [=](int j, int c, u32 v) {
-            const u32 i = gbase + c + ((u32)j << logS);
-            if (i < valid) acc[i] = i < fresh ? qadd(acc[i], v, q) : v;
+        constexpr int H = R0 < 8 ? R0 : 8;             // eight loads in flight at a time
+        auto stl = [=](int row0, int c, const auto& x) {
+            const u32 i0 = gbase + c + ((u32)row0 << logS);
+#pragma unroll
+            for (int h = 0; h < R0; h += H) {
+                u32 old[H];
+#pragma unroll
+                for (int t = 0; t < H; ++t) {
+                    const u32 i = i0 + ((u32)((h + t) * SP0) << logS);
+                    old[t] = i < fresh ? acc[i] : 0u;
+                }
+#pragma unroll
+                for (int t = 0; t < H; ++t) {
+                    const u32 i = i0 + ((u32)((h + t) * SP0) << logS);
+                    if (i < valid) acc[i] = i < fresh ? qadd(old[t], x[h + t], q) : x[h + t];
+                }
+            }
         };
-        rounds<LOGL, true, false, 0, false, true>(sm, ld0, stl, pi, q);
+        rounds<LOGL, true, false, 0, true, true>(sm, ld0, stl, pi, q);
     } else {
         auto stl = [=](int j, int c, u32 v) { d[gbase + c + ((u32)j << logS)] = v; };
         rounds<LOGL, true, false, 0, false, true>(sm, ld0, stl, pi, q);
@@ -621,7 +638,7 @@ __device__ __forceinline__ void qcrt_carry_body(const QCrtArgs& a, u32 ncta) {
     carry_finish(lo, h, tile, j0, a.state, a.err, a.out, a.out_len);
 }
 
-__global__ void __launch_bounds__(CNT) k_qcrt_carry(QCrtArgs a) { qcrt_carry_body(a, 0xffffffffu); }
+__global__ void __launch_bounds__(CNT, 3) k_qcrt_carry(QCrtArgs a) { qcrt_carry_body(a, 0xffffffffu); }
 
 // CRT + carry of many products: CTAs take per-product tickets; tickets beyond a product's
 // CTA count exit at once.
