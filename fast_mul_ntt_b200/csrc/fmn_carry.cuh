@@ -50,18 +50,24 @@ __device__ __forceinline__ void carry_finish(u64 (&lo)[CE], u32 (&h)[CE], u64 ti
     __shared__ u32 s_warp[CNT / 32];
     __shared__ u32 s_cin;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    // carry-transfer function of this thread's limbs
-    u32 f = 0;
-#pragma unroll
-    for (u32 cin = 0; cin < 4; ++cin) {
-        u64 c = cin;
+    // carry-transfer function of this thread's limbs.  The carry out is non-decreasing in the
+    // carry in and moves by at most one over 0..3, so it is constant when the chains from 0 and
+    // from 3 agree; the chains from 1 and 2 run only in warps where some lane needs them.
+    auto chain = [&](u64 c) {
 #pragma unroll
         for (int e = 0; e < CE; ++e) {
             const u64 t = lo[e] + c;
             c = h[e] + (t < c);
         }
-        f |= (u32)c << (2 * cin);
+        return (u32)c;
+    };
+    const u32 c0 = chain(0), c3 = chain(3);
+    u32 c1 = c0, c2 = c0;
+    if (__any_sync(0xffffffffu, c0 != c3)) {
+        c1 = chain(1);
+        c2 = chain(2);
     }
+    const u32 f = c0 | (c1 << 2) | (c2 << 4) | (c3 << 6);
     // CTA scan: Kogge-Stone in each warp, then over the warps in warp 0
     u32 inc = f;
 #pragma unroll

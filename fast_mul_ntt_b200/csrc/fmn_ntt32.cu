@@ -544,33 +544,47 @@ __global__ void __launch_bounds__(NT, (min_ctas<MODE, LOGL>())) k_qpass_batch(co
 }
 
 // ------------------------------------------------------------------ CRT + carry
-// Digit coefficient k of the product, c_k < Q = q0 q1 q2 < 2^91, from its residues by
-// c_k = sum_i y_i M_i mod Q with y_i = r_i * M_i^-1 (M_i = Q / q_i; the CRT of
-// src/core.h:77-104 for these primes).  Output limb j collects the 128-bit pair
-// C_j = c_{2j} + c_{2j+1} 2^32 < 2^124: s_j = C_j.lo + C_{j-1}.hi, then the carry scan.
+// Digit coefficient k of the product, c_k < Q = q0 q1 q2 < 2^91, from its residues y_i = c_k
+// mod q_i by Garner's mixed-radix form c_k = x0 + q0 (x1 + q1 x2) (the same number as the
+// reference's CRT sum, src/core.h:77-104, without its final reduction mod Q).  Output limb j
+// collects the 128-bit pair C_j = c_{2j} + c_{2j+1} 2^32 < 2^124: s_j = C_j.lo + C_{j-1}.hi,
+// then the carry scan.
 struct QCrtArgs {
     const u32* res;     // three natural-order residue arrays (prime i at res + i*N), in [0, q)
     u64 N;
     u64 nvalid;         // digit coefficients that may be nonzero
     u64* out;
     u64 out_len;
-    u32 cst[3];         // M_i^-1 * N^-1 * 2^64 mod q_i (undoes the two Montgomery products)
+    u32 cst[3];         // N^-1 * 2^64 mod q_i (undoes N and the two Montgomery factors)
+    u32 inv01;          // Montgomery form mod q1 of q0^-1
+    u32 q0m2;           // Montgomery form mod q2 of q0
+    u32 inv012;         // Montgomery form mod q2 of (q0 q1)^-1
     u32* state;
     u32* ticket;
     u32* err;
 };
 
 typedef unsigned __int128 u128;
-constexpr u64 QM0 = (u64)Q32_P1 * Q32_P2, QM1 = (u64)Q32_P0 * Q32_P2, QM2 = (u64)Q32_P0 * Q32_P1;
-constexpr u128 QALL = (u128)QM2 * Q32_P2;
+constexpr u64 Q01 = (u64)Q32_P0 * Q32_P1;
 
 __device__ __forceinline__ u128 qcrt(u32 r0, u32 r1, u32 r2, const QCrtArgs& a, const PrimeQ& q0, const PrimeQ& q1,
                                      const PrimeQ& q2) {
-    const u64 y0 = qmont(r0, a.cst[0], q0), y1 = qmont(r1, a.cst[1], q1), y2 = qmont(r2, a.cst[2], q2);
-    u128 s = (u128)y0 * QM0 + (u128)y1 * QM1 + (u128)y2 * QM2;   // < 3 Q
-    if (s >= QALL) s -= QALL;
-    if (s >= QALL) s -= QALL;
-    return s;
+    const u32 x0 = qmont(r0, a.cst[0], q0);                    // c mod q0
+    const u32 y1 = qmont(r1, a.cst[1], q1);                    // c mod q1
+    const u32 y2 = qmont(r2, a.cst[2], q2);                    // c mod q2
+    const u32 x0r = x0 >= q1.p ? x0 - q1.p : x0;               // q0 < 2 q1
+    const u32 x1 = qmont(qsub(y1, x0r, q1), a.inv01, q1);      // (c - x0) / q0 mod q1
+    const u32 t = qadd(qsmul(x0, 1u, q2.one, q2), qmont(x1, a.q0m2, q2), q2);
+    const u32 x2 = qmont(qsub(y2, t, q2), a.inv012, q2);       // (c - x0 - q0 x1) / (q0 q1) mod q2
+    // c = x0 + q0 x1 + q0 q1 x2 < 2^91, exactly
+    const u64 s1 = (u64)x0 + (u64)Q32_P0 * x1;
+    const u64 lo0 = (u64)x2 * (u32)Q01, mid = (u64)x2 * (u32)(Q01 >> 32);
+    u64 lo = s1 + lo0;
+    u64 hi = lo < lo0;
+    const u64 ml = mid << 32;
+    lo += ml;
+    hi += (lo < ml) + (mid >> 32);
+    return ((u128)hi << 64) | lo;
 }
 __device__ __forceinline__ u128 qcoef(const QCrtArgs& a, u64 k, const PrimeQ& q0, const PrimeQ& q1, const PrimeQ& q2) {
     if (k >= a.nvalid) return 0;
@@ -1032,18 +1046,18 @@ struct Launcher {
     }
 };
 
-// CRT constants for residues that went through a 2^n-point transform: M_i^-1 N^-1 2^64 mod q_i.
-static void crt_constants(u64 N, u32 (&cst)[3]) {
+// CRT constants for residues that went through a 2^n-point transform (see QCrtArgs).
+static void crt_constants(u64 N, QCrtArgs* ca) {
     for (int i = 0; i < 3; ++i) {
         const u64 p = kQ[i];
-        u64 M = 1;
-        for (int k = 0; k < 3; ++k)
-            if (k != i) M = h_mulmod(M, kQ[k], p);
-        const u64 minv = h_pow(M, p - 2, p);
         const u64 ninv = h_pow(N % p, p - 2, p);
-        const u64 r2 = h_pow(2, 64, p);
-        cst[i] = (u32)h_mulmod(h_mulmod(minv, ninv, p), r2, p);
+        ca->cst[i] = (u32)h_mulmod(ninv, h_pow(2, 64, p), p);
     }
+    const u64 q0 = kQ[0], q1 = kQ[1], q2 = kQ[2];
+    auto mont = [](u64 v, u64 p) { return (u32)h_mulmod(v % p, h_pow(2, 32, p), p); };
+    ca->inv01 = mont(h_pow(q0 % q1, q1 - 2, q1), q1);
+    ca->q0m2 = mont(q0, q2);
+    ca->inv012 = mont(h_pow(h_mulmod(q0, q1, q2), q2 - 2, q2), q2);
 }
 
 // Launch list of a whole product: a 2^n-digit transform of both operands in scratch A and B
@@ -1216,8 +1230,9 @@ cudaError_t q32_batch_plan(const Job* jobs, const int* idx, int m, char* res, si
     u32 maxc = 0;
     const int n = q32_batch_log_n(jobs[idx[0]]);
     if (n < 0) return cudaErrorInvalidValue;
-    u32 cst[3];
-    crt_constants(1ull << n, cst);
+    QCrtArgs proto;
+    memset(&proto, 0, sizeof(proto));
+    crt_constants(1ull << n, &proto);
     for (int t = 0; t < m; ++t) {
         const Job& j = jobs[idx[t]];
         if (q32_batch_log_n(j) != n) return cudaErrorInvalidValue;
@@ -1233,8 +1248,7 @@ cudaError_t q32_batch_plan(const Job* jobs, const int* idx, int m, char* res, si
         *soff += q32_batch_state_bytes(j);
         plan_whole(j, n, A, B, &W[t]);
         QCrtArgs& ca = C[t];
-        memset(&ca, 0, sizeof(ca));
-        memcpy(ca.cst, cst, sizeof(cst));
+        ca = proto;
         ca.res = A;
         ca.N = N;
         ca.nvalid = 2 * out_len - 1;
@@ -1419,7 +1433,7 @@ cudaError_t q32_enqueue(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s,
 
     QCrtArgs ca;
     memset(&ca, 0, sizeof(ca));
-    crt_constants(N, ca.cst);
+    crt_constants(N, &ca);
     u64 crt_done = 0;                 // CRT CTAs launched so far (split products with copy-back)
     if (J.m == 1) {
         u32* A = (u32*)(base + J.a);
