@@ -1,7 +1,10 @@
-// fmn_ntt.cu -- sm_100a kernels of the 3-prime NTT multiplication path and their launchers.
+// fmn_ntt.cu -- the 64-bit residue engine (the reference's three 62-bit primes): sm_100a
+// kernels and launchers, plus the host logic shared by both engines (engine choice, batches,
+// kernel timing).  The 32-bit engine lives in fmn_ntt32.cu.
 //
 // Path (reference src/fast_mul.c:308-396 abs_mul64, :398-460 abs_sqr64):
-//   limbs -> Montgomery residues mod p0, p1, p2 (entry fused into the first pass)
+//   limbs -> residues mod p0, p1, p2 (entry fused into the first pass; plain representatives,
+//   constant twiddles applied as Shoup products, variable products as Montgomery REDC)
 //   -> forward NTT of each operand (four-step, passes of <= 2^9 points per CTA)
 //   -> pointwise product fused between the last forward and first inverse pass
 //   -> inverse NTT -> CRT to a 192-bit coefficient -> carry propagation by a single-pass
@@ -47,7 +50,8 @@ __device__ __align__(16) ulonglong2 g_rt[2][3][RT_SIZE];
 __device__ __align__(16) u64 g_tw[2][3][1 << TWB];     // [low/high level][prime]
 __constant__ PrimeRT c_prime[3] = {prime_rt<0>(), prime_rt<1>(), prime_rt<2>()};
 
-// w_{2^30}^x for x < 2^30 (Montgomery form, < 2p), prime index pi.
+// w_{2^30}^x for x < 2^30 in Montgomery form (< 2p), prime index pi: multiplying a plain
+// residue by it with mmul gives the plain product.
 __device__ __forceinline__ u64 root30(u32 x, int pi, const PrimeRT& q) {
     return mmul(__ldg(&g_tw[1][pi][x >> TWB]), __ldg(&g_tw[0][pi][x & ((1u << TWB) - 1)]), q);
 }
