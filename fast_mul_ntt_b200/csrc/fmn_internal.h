@@ -42,7 +42,8 @@ struct Job {
     // spectrum_enqueue for a transform of 2^log_n points; la is its length.  Null otherwise.
     const u64* spectrum = nullptr;
     int log_n = 0;
-    int engine = 0;    // ENGINE_*: 0 follows the process-wide default
+    int engine = 0;    // ENGINE_*: 0 follows the process-wide default; with `spectrum`, the
+                       // engine that spectrum belongs to (log_n in that engine's points)
 };
 
 // Residue engines.  ENGINE_64 transforms 64-bit limbs modulo the reference's three 62-bit
@@ -61,6 +62,12 @@ double q32_cost(u64 la, u64 lb, int sqr);      // its modelled cost (32-bit poin
 size_t q32_workspace_bytes(u64 la, u64 lb, int sqr);
 int q32_launches(u64 la, u64 lb, int sqr);
 int q32_pieces(u64 la, u64 lb, int sqr);        // 1: whole product; > 1: split into pieces
+size_t q32_job_workspace_bytes(const Job& j);  // also for a product with a 32-bit resident spectrum
+// Transform length (log2 digits) of a 32-bit resident spectrum for products of `len` limbs with
+// partners of up to max_partner limbs; < 0 if the 32-bit engine cannot hold it.
+int q32_spectrum_log_n(u64 len, u64 max_partner);
+// Forward transform of `len` limbs into a 32-bit resident spectrum (3 * 2^log_n u32).
+cudaError_t q32_spectrum_enqueue(const u64* src, u64 len, int log_n, void* spec, cudaStream_t s);
 void q32_force_pieces(int m);                  // tests: split into m pieces where possible (0: model)
 typedef cudaError_t (*ChunkDone)(void* ctx, u64 first_limb, u64 end_limb);
 // Called before the first launch that reads limbs [first, end) of the second operand: it must
@@ -194,9 +201,10 @@ cudaError_t q32_bench_bfly(double* per_second);
 // A resident operand (include/fast_mul.h): its forward spectrum stays in device memory.
 struct fmn_operand {
     int dev;
+    int engine;          // fmn::ENGINE_64 or fmn::ENGINE_32: the layout of `spec`
     const u64* src;      // the caller's limbs (used by the plain per-call path)
     u64 len;
-    int log_n;           // transform length of its products
+    int log_n;           // transform length of its products (points of its engine)
     u64 max_partner;     // longest partner it was sized for
-    u64* spec;           // 3 * 2^log_n residues, forward-transformed
+    u64* spec;           // 3 * 2^log_n residues (u64 or u32 by engine), forward-transformed
 };

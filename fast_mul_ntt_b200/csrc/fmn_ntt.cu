@@ -1010,7 +1010,7 @@ int default_engine() { return g_engine.load(); }
 constexpr double kCost64 = 2.4;
 
 int job_engine(const Job& j) {
-    if (j.spectrum) return ENGINE_64;
+    if (j.spectrum) return j.engine == ENGINE_32 ? ENGINE_32 : ENGINE_64;
     const int e = j.engine ? j.engine : default_engine();
     if (e == ENGINE_64) return ENGINE_64;
     const int sqr = j.sqr ? 1 : 0;
@@ -1031,7 +1031,7 @@ static Job plain_job(u64 la, u64 lb, int sqr) {
 }
 
 size_t job_workspace_bytes(const Job& j) {
-    if (job_engine(j) == ENGINE_32) return q32_workspace_bytes(j.la, j.lb, j.sqr ? 1 : 0);
+    if (job_engine(j) == ENGINE_32) return q32_job_workspace_bytes(j);
     const size_t t = ws_layout(j.la, j.lb, j.sqr, j.spectrum ? j.log_n : 0).total;
     return t ? t : 256;
 }
@@ -1512,7 +1512,7 @@ static int job_kind(const Job& j) { return j.spectrum ? 2 : (j.sqr ? 1 : 0); }
 // Engine of a batched product: the 32-bit engine for every whole product it can take (batched
 // products are small; resident operands keep 64-bit spectra), unless ENGINE_64 is selected.
 static int batch_engine(const Job& j) {
-    if (j.spectrum) return ENGINE_64;
+    if (j.spectrum) return j.engine == ENGINE_32 ? ENGINE_32 : ENGINE_64;
     const int e = j.engine ? j.engine : default_engine();
     if (e == ENGINE_64) return ENGINE_64;
     return q32_batch_log_n(j) >= 0 ? ENGINE_32 : ENGINE_64;

@@ -1010,6 +1010,29 @@ static QJob plan_job(u64 la, u64 lb, int sqr) {
     return J;
 }
 
+// A product with a 32-bit resident spectrum of 2^log_n digits: [status][partner / product
+// residues][ticket + state].
+static QJob plan_resident(const Job& j) {
+    QJob J;
+    memset(&J, 0, sizeof(J));
+    const u64 out_len = j.la + j.lb;
+    if (j.la == 0 || j.lb == 0 || j.log_n < 1 || j.log_n > Q32_MAX_LOG_N || 2 * out_len - 1 > (1ull << j.log_n))
+        return J;
+    J.ok = true;
+    J.m = 1;
+    J.n = j.log_n;
+    J.N = 1ull << j.log_n;
+    J.ncta = (out_len + CTILE - 1) / CTILE;
+    size_t off = 256;
+    J.a = J.b = off;
+    off = align256(off + 3 * J.N * sizeof(u32));
+    J.ticket = off;
+    J.state = off + 16;
+    off = align256(J.state + J.ncta * sizeof(u32));
+    J.total = off;
+    return J;
+}
+
 // Launch sequencing of one product on one stream: kernel lookup, the caller's hook that makes
 // the stream wait for a range of the second operand's limbs, per-launch timing records.
 struct Launcher {
@@ -1074,7 +1097,7 @@ struct QWhole {
 
 static void plan_whole(const Job& j, int n, u32* A, u32* B, QWhole* out) {
     const int sqr = j.sqr ? 1 : 0;
-    if (sqr) B = A;
+    if (sqr || j.spectrum) B = A;
     const Plan pl = qplan(n);
     const int P = pl.passes;
     const u64 N = 1ull << n;
@@ -1106,8 +1129,21 @@ static void plan_whole(const Job& j, int n, u32* A, u32* B, QWhole* out) {
             add(p == 0 ? V_FWD_E : V_FWD, pl.bits[p], N >> (pl.bits[p] + LOG_TC));
         }
     };
-    const bool merged = !sqr && P >= 2 && lastl >= 5 && lastl <= 8;
-    if (merged) {
+    const bool merged = !sqr && !j.spectrum && P >= 2 && lastl >= 5 && lastl <= 8;
+    if (j.spectrum) {
+        // resident first operand (conv_single, src/fast_mul.c:135-212): only the partner is
+        // transformed, in A; the product goes back into A, the spectrum stays intact
+        fwd_strided(j.b, j.lb, A);
+        pa.src = j.b;
+        pa.len = j.lb;
+        pa.data = A;
+        pa.other = (u32*)j.spectrum;
+        pa.dst = A;
+        pa.logB = logB[P - 1];
+        pa.ncols = ncols_last;
+        add(P == 1 ? V_FUSED_E : V_FUSED, lastl, tiles_last);
+        pa.dst = nullptr;
+    } else if (merged) {
         fwd_strided(j.a, j.la, A);
         fwd_strided(j.b, j.lb, B);
         pa.src = nullptr;
@@ -1169,6 +1205,47 @@ bool q32_fits(u64 la, u64 lb, int sqr) { return q32::plan_job(la, lb, sqr).ok; }
 
 void q32_force_pieces(int m) { q32::g_force_pieces.store(m > 1 ? m : 0); }
 
+size_t q32_job_workspace_bytes(const Job& j) {
+    if (!j.spectrum) return q32_workspace_bytes(j.la, j.lb, j.sqr ? 1 : 0);
+    const q32::QJob J = q32::plan_resident(j);
+    return J.ok ? J.total : 256;
+}
+
+int q32_spectrum_log_n(u64 len, u64 max_partner) {
+    if (len == 0 || max_partner == 0 || len + max_partner > (1ull << (Q32_MAX_LOG_N - 1))) return -1;
+    return q32::ilog2(2 * (len + max_partner) - 1);
+}
+
+cudaError_t q32_spectrum_enqueue(const u64* src, u64 len, int log_n, void* spec, cudaStream_t s) {
+    using namespace q32;
+    cudaError_t e = q32::ensure_tables();
+    if (e != cudaSuccess) return e;
+    const Plan pl = qplan(log_n);
+    const int P = pl.passes;
+    const u64 N = 1ull << log_n;
+    Job j;
+    memset(&j, 0, sizeof(j));
+    Launcher launch{j, s, nullptr, nullptr, N};
+    QArgs pa;
+    memset(&pa, 0, sizeof(pa));
+    pa.N = N;
+    pa.ncols = TC;
+    pa.src = src;
+    pa.len = len;
+    pa.data = (u32*)spec;
+    int logB = log_n;
+    for (int p = 0; p + 1 < P; ++p) {
+        pa.logB = logB;
+        if ((e = launch(p == 0 ? V_FWD_E : V_FWD, pl.bits[p], pa, N >> (pl.bits[p] + LOG_TC))) != cudaSuccess) return e;
+        logB -= pl.bits[p];
+    }
+    const int lastl = pl.bits[P - 1];
+    const u64 nblk = N >> lastl;
+    pa.logB = logB;
+    pa.ncols = nblk < (u64)TC ? (int)nblk : TC;
+    return launch(P == 1 ? V_LAST_E : V_LAST, lastl, pa, (nblk + TC - 1) / TC);
+}
+
 double q32_cost(u64 la, u64 lb, int sqr) {
     const q32::QJob J = q32::plan_job(la, lb, sqr);
     return J.ok ? J.cost : 1e300;
@@ -1196,12 +1273,15 @@ int q32_pieces(u64 la, u64 lb, int sqr) {
 }
 
 // ---- batches: whole products grouped by transform length and kind share every launch
-int q32_batch_log_n(const Job& j) { return j.spectrum ? -1 : q32::whole_log_n(j.la, j.lb); }
+int q32_batch_log_n(const Job& j) {
+    if (j.spectrum) return j.engine == ENGINE_32 && q32::plan_resident(j).ok ? j.log_n : -1;
+    return q32::whole_log_n(j.la, j.lb);
+}
 
 size_t q32_batch_res_bytes(const Job& j) {
     const int n = q32_batch_log_n(j);
     if (n < 0) return 0;
-    return q32::align256(3 * (1ull << n) * sizeof(u32)) * (j.sqr ? 1 : 2);
+    return q32::align256(3 * (1ull << n) * sizeof(u32)) * (j.sqr || j.spectrum ? 1 : 2);
 }
 
 size_t q32_batch_state_bytes(const Job& j) {
@@ -1240,7 +1320,7 @@ cudaError_t q32_batch_plan(const Job* jobs, const int* idx, int m, char* res, si
         u32* A = (u32*)(res + *roff);
         *roff += align256(3 * N * sizeof(u32));
         u32* B = A;
-        if (!j.sqr) {
+        if (!j.sqr && !j.spectrum) {
             B = (u32*)(res + *roff);
             *roff += align256(3 * N * sizeof(u32));
         }
@@ -1384,7 +1464,7 @@ cudaError_t q32_enqueue(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s,
     if (out_len == 0) return cudaSuccess;
     if (j.la == 0 || j.lb == 0) return cudaMemsetAsync(j.out, 0, out_len * sizeof(u64), s);
     const int sqr = j.sqr ? 1 : 0;
-    const QJob J = plan_job(j.la, j.lb, sqr);
+    const QJob J = j.spectrum ? plan_resident(j) : plan_job(j.la, j.lb, sqr);
     if (!J.ok || ws_bytes < J.total) return cudaErrorInvalidValue;
     cudaError_t e = q32::ensure_tables();
     if (e != cudaSuccess) return e;

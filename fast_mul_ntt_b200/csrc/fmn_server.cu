@@ -150,6 +150,7 @@ fmn::Job to_job(const fmn_request& r, bool reuse, u64* out) {
             j.a = nullptr;
             j.spectrum = o->spec;
             j.log_n = o->log_n;
+            j.engine = o->engine;
         } else {
             j.a = o->src;
         }
@@ -173,7 +174,9 @@ size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
 // Transform length (log2) of a request's product.
 int request_log_n(const fmn_request& r, bool reuse) {
-    if (r.op == FMN_OP_MUL_OPERAND && reuse) return r.operand->log_n;
+    // in 64-bit points (a 32-bit spectrum has two digits per limb)
+    if (r.op == FMN_OP_MUL_OPERAND && reuse)
+        return r.operand->engine == fmn::ENGINE_32 ? r.operand->log_n - 1 : r.operand->log_n;
     const u64 ol = out_len_of(r);
     return ol > 1 ? ilog2c(ol - 1) : 0;
 }
@@ -219,7 +222,7 @@ bool launch_batch(fmn_server* s, Slot* sl, const std::vector<size_t>& idx) {
             jobs[k].out = (u64*)ob;
             ob += align256(out_len_of(r) * sizeof(u64));
         }
-        if (jobs[k].la && jobs[k].lb) {
+        if (jobs[k].la && jobs[k].lb && fmn::job_engine(jobs[k]) == fmn::ENGINE_64) {
             const int n = jobs[k].spectrum ? jobs[k].log_n : ilog2c(jobs[k].la + jobs[k].lb - 1);
             ensure_server_twiddles(s, n, sl->stream);
         }
@@ -383,14 +386,19 @@ int fmn_operand_create(const u64* d_in, u64 len, u64 max_partner_len, void* stre
     o->src = d_in;
     o->len = len;
     o->max_partner = max_partner_len;
-    o->log_n = ilog2c(len + max_partner_len - 1);
-    const size_t bytes = 3 * ((size_t)1 << o->log_n) * sizeof(u64);
+    // the 32-bit engine wherever it can hold the spectrum (its products cost about half)
+    const int n32 = fmn::default_engine() == fmn::ENGINE_64 ? -1 : fmn::q32_spectrum_log_n(len, max_partner_len);
+    o->engine = n32 >= 0 ? fmn::ENGINE_32 : fmn::ENGINE_64;
+    o->log_n = n32 >= 0 ? n32 : ilog2c(len + max_partner_len - 1);
+    const size_t bytes = 3 * ((size_t)1 << o->log_n) * (n32 >= 0 ? sizeof(unsigned) : sizeof(u64));
     if ((e = cudaMalloc((void**)&o->spec, bytes)) != cudaSuccess) {
         cudaGetLastError();
         delete o;
         return fmn::api_set_error(FMN_ERR_NOMEM, "resident operand spectrum", e);
     }
-    if ((e = fmn::spectrum_enqueue(d_in, len, o->log_n, o->spec, (cudaStream_t)stream, nullptr)) != cudaSuccess ||
+    e = o->engine == fmn::ENGINE_32 ? fmn::q32_spectrum_enqueue(d_in, len, o->log_n, o->spec, (cudaStream_t)stream)
+                                    : fmn::spectrum_enqueue(d_in, len, o->log_n, o->spec, (cudaStream_t)stream, nullptr);
+    if (e != cudaSuccess ||
         (e = cudaStreamSynchronize((cudaStream_t)stream)) != cudaSuccess) {
         cudaFree(o->spec);
         delete o;
@@ -422,6 +430,7 @@ int fmn_mul_operand_ws(const fmn_operand* o, const u64* d_in2, u64 len2, u64* d_
     j.sqr = 0;
     j.spectrum = o->spec;
     j.log_n = o->log_n;
+    j.engine = o->engine;
     if (len2 == 0) {
         cudaError_t e = cudaMemsetAsync(d_out, 0, (o->len + len2) * sizeof(u64), (cudaStream_t)stream);
         return e == cudaSuccess ? FMN_OK : fmn::api_set_error(FMN_ERR_CUDA, "cudaMemsetAsync", e);
@@ -443,6 +452,7 @@ size_t fmn_operand_workspace_size(const fmn_operand* o, u64 len2) {
     j.sqr = 0;
     j.spectrum = o->spec;
     j.log_n = o->log_n;
+    j.engine = o->engine;
     return fmn::job_workspace_bytes(j);
 }
 

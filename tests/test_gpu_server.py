@@ -22,7 +22,16 @@ def _host(t):
     return t.cpu().numpy().view(np.uint64)
 
 
-def test_resident_operand_products(fmn, oracle):
+@pytest.fixture(params=["e32", "e64"])
+def engine(request, fmn):
+    """Resident spectra on the 32-bit engine (AUTO) and on the 64-bit engine (ENGINE_64 set
+    while the operands are created and used)."""
+    fmn.set_engine(fmn.ENGINE_AUTO if request.param == "e32" else fmn.ENGINE_64)
+    yield request.param
+    fmn.set_engine(fmn.ENGINE_AUTO)
+
+
+def test_resident_operand_products(fmn, oracle, engine):
     import torch
     a = synth.limbs("uniform", 30000, 41)
     da = _dev(a)
@@ -34,6 +43,10 @@ def test_resident_operand_products(fmn, oracle):
             op.mul(_dev(b), out)
             fmn.sync()
             assert np.array_equal(_host(out), oracle.mul(a, b)), (kind, l2)
+            out2 = torch.zeros_like(out)                     # again: the spectrum stays intact
+            op.mul(_dev(b), out2)
+            fmn.sync()
+            assert torch.equal(out, out2)
     finally:
         op.close()
 
@@ -79,7 +92,7 @@ def _requests(fmn, oracle, count, seed, with_operand=True):
     return reqs, outs, wants, (keep, operands)
 
 
-def test_server_mix_equals_alone_and_oracle(fmn, oracle):
+def test_server_mix_equals_alone_and_oracle(fmn, oracle, engine):
     reqs, outs, wants, hold = _requests(fmn, oracle, 120, 3)
     srv = fmn.Server(batching=True, max_batch=32)
     try:
