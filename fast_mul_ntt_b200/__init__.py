@@ -34,7 +34,7 @@ EXPORTS = ["abs_mul64", "abs_sqr64", "fmn_init", "fmn_shutdown", "fmn_last_error
            "fmn_server_wait", "fmn_server_take", "fmn_server_get_stats", "fmn_server_replay", "fmn_server_destroy",
            "fmn_get_plan", "fmn_set_plan", "fmn_autotune", "fmn_load_plans", "fmn_load_default_plans",
            "fmn_set_engine", "fmn_get_engine", "fmn_engine_for", "fmn_pieces_for",
-           "fmn_force_pieces", "fmn_bench_bfly32"]
+           "fmn_force_pieces", "fmn_bench_bfly32", "fmn_get_plan_engine", "fmn_set_plan_engine"]
 
 ENGINE_AUTO, ENGINE_64, ENGINE_32 = 0, 1, 2
 
@@ -173,6 +173,10 @@ def load_library(path=None):
     lib.fmn_autotune.restype = ctypes.c_int
     lib.fmn_load_plans.argtypes = [ctypes.c_char_p]
     lib.fmn_load_plans.restype = ctypes.c_int
+    lib.fmn_get_plan_engine.argtypes = [ctypes.c_int, ctypes.c_int, _ip, ctypes.c_int]
+    lib.fmn_get_plan_engine.restype = ctypes.c_int
+    lib.fmn_set_plan_engine.argtypes = [ctypes.c_int, ctypes.c_int, _ip, ctypes.c_int]
+    lib.fmn_set_plan_engine.restype = ctypes.c_int
     lib.fmn_load_default_plans.argtypes = []
     lib.fmn_load_default_plans.restype = ctypes.c_int
     lib.fmn_set_engine.argtypes = [ctypes.c_int]
@@ -458,20 +462,20 @@ class Server:
 PLAN_DIR = os.path.join(HERE, "tune")
 
 
-def get_plan(log_n):
-    """Pass bits of the plan in effect for 2^log_n points."""
+def get_plan(log_n, engine=ENGINE_64):
+    """Pass bits of the plan in effect for 2^log_n points of an engine (64-bit by default)."""
     bits = (ctypes.c_int * 4)()
-    p = load_library().fmn_get_plan(log_n, bits, 4)
+    p = load_library().fmn_get_plan_engine(engine, log_n, bits, 4)
     if p < 0:
         raise FastMulError(-p, "bad length")
     return [bits[i] for i in range(p)]
 
 
-def set_plan(log_n, bits=None):
-    """Replace the plan of 2^log_n points (None restores the default)."""
+def set_plan(log_n, bits=None, engine=ENGINE_64):
+    """Replace the plan of 2^log_n points of an engine (None restores the default)."""
     bits = list(bits or [])
     arr = (ctypes.c_int * max(1, len(bits)))(*bits)
-    _check(load_library().fmn_set_plan(log_n, arr, len(bits)))
+    _check(load_library().fmn_set_plan_engine(engine, log_n, arr, len(bits)))
 
 
 def set_engine(engine):

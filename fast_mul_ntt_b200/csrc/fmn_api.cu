@@ -800,6 +800,7 @@ int fmn_mul_operand_device(const fmn_operand* op, const u64* d_in2, u64 len2, u6
     j.spectrum = op->spec;
     j.log_n = op->log_n;
     j.engine = op->engine;
+    j.splan = op->plan;
     return run_job_ctx(c, j, s);
 }
 

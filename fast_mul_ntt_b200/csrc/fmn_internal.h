@@ -44,6 +44,7 @@ struct Job {
     int log_n = 0;
     int engine = 0;    // ENGINE_*: 0 follows the process-wide default; with `spectrum`, the
                        // engine that spectrum belongs to (log_n in that engine's points)
+    Plan splan = Plan{};   // with `spectrum`: the pass plan it was transformed with
 };
 
 // Residue engines.  ENGINE_64 transforms 64-bit limbs modulo the reference's three 62-bit
@@ -67,8 +68,15 @@ size_t q32_job_workspace_bytes(const Job& j);  // also for a product with a 32-b
 // partners of up to max_partner limbs; < 0 if the 32-bit engine cannot hold it.
 int q32_spectrum_log_n(u64 len, u64 max_partner);
 // Forward transform of `len` limbs into a 32-bit resident spectrum (3 * 2^log_n u32).
-cudaError_t q32_spectrum_enqueue(const u64* src, u64 len, int log_n, void* spec, cudaStream_t s);
+cudaError_t q32_spectrum_enqueue(const u64* src, u64 len, int log_n, void* spec, cudaStream_t s, const Plan& plan);
 void q32_force_pieces(int m);                  // tests: split into m pieces where possible (0: model)
+// Pass plans of the 32-bit engine (2^n digits, n <= 26), tuned or set per length.
+Plan q32_make_plan(int log_n);
+Plan q32_default_plan(int log_n);
+bool q32_valid_plan(const Plan& p);
+bool q32_set_plan(const Plan& p);
+void q32_clear_plan(int log_n);
+std::vector<Plan> q32_candidate_plans(int log_n);
 typedef cudaError_t (*ChunkDone)(void* ctx, u64 first_limb, u64 end_limb);
 // Called before the first launch that reads limbs [first, end) of the second operand: it must
 // make stream s wait until those limbs are in device memory (e.g. an event after their copy).
@@ -79,7 +87,7 @@ cudaError_t q32_enqueue(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s,
 // Forward transform of `len` limbs at `src` into `spec` (3 * 2^log_n u64): the spectrum a
 // resident operand keeps for products of up to 2^log_n - len + 1 partner limbs.
 cudaError_t spectrum_enqueue(const u64* src, u64 len, int log_n, u64* spec, cudaStream_t s,
-                             const struct TwiddleSet* tw);
+                             const struct TwiddleSet* tw, const Plan& plan);
 
 // Scratch needed by one product: residue arrays + carry-scan state.
 size_t job_workspace_bytes(u64 la, u64 lb, int sqr);
@@ -202,6 +210,7 @@ cudaError_t q32_bench_bfly(double* per_second);
 struct fmn_operand {
     int dev;
     int engine;          // fmn::ENGINE_64 or fmn::ENGINE_32: the layout of `spec`
+    fmn::Plan plan;      // pass plan `spec` was transformed with (its products use the same)
     const u64* src;      // the caller's limbs (used by the plain per-call path)
     u64 len;
     int log_n;           // transform length of its products (points of its engine)

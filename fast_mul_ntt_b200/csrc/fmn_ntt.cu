@@ -1040,10 +1040,11 @@ size_t job_workspace_bytes(u64 la, u64 lb, int sqr) { return job_workspace_bytes
 
 static cudaError_t launch_pass(int variant, int logl, const PassArgs& a, u64 tiles, cudaStream_t s);
 
-cudaError_t spectrum_enqueue(const u64* src, u64 len, int log_n, u64* spec, cudaStream_t s, const TwiddleSet* tws) {
+cudaError_t spectrum_enqueue(const u64* src, u64 len, int log_n, u64* spec, cudaStream_t s, const TwiddleSet* tws,
+                             const Plan& pl) {
     cudaError_t e = ensure_tables();
     if (e != cudaSuccess) return e;
-    const Plan pl = make_plan(log_n);
+    if (!valid_plan(pl) || pl.n != log_n) return cudaErrorInvalidValue;
     if (tws && (tws->log_n != log_n || !same_plan(tws->plan, pl))) tws = nullptr;
     const int P = pl.passes;
     const u64 N = 1ull << log_n;
@@ -1226,7 +1227,7 @@ static void plan_job(const Job& j, const JobScratch& sc, const TwiddleSet* tws, 
     const WsLayout w = ws_layout(j.la, j.lb, sqr, j.spectrum ? j.log_n : 0);
     u64* A = sc.A;
     u64* B = sqr ? A : sc.B;
-    const Plan pl = make_plan(w.n);
+    const Plan pl = j.spectrum && j.splan.passes ? j.splan : make_plan(w.n);   // a spectrum keeps its plan
     const int P = pl.passes;
     const u64 N = w.N;
     if (tws && (tws->log_n != w.n || !same_plan(tws->plan, pl))) tws = nullptr;

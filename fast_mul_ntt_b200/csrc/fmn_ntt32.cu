@@ -869,9 +869,9 @@ static cudaError_t ensure_tables() {
 }
 
 // ------------------------------------------------------------------ host: plans and jobs
-// Passes of a 2^n-digit transform: as even as possible, largest first; a strided pass leaves
-// at least 32 columns (later passes take >= 5 bits) and takes >= 5 bits itself.
-static Plan qplan(int n) {
+// Default passes of a 2^n-digit transform: as even as possible, largest first; a strided pass
+// leaves at least 32 columns (later passes take >= 5 bits) and takes >= 5 bits itself.
+static Plan qplan_default(int n) {
     Plan p;
     memset(&p, 0, sizeof(p));
     p.n = n;
@@ -889,6 +889,36 @@ static Plan qplan(int n) {
         p.bits[2] = n - p.bits[0] - p.bits[1];
     }
     return p;
+}
+
+static bool qplan_valid(const Plan& p) {
+    if (p.n < 0 || p.n > Q32_MAX_LOG_N || p.passes < 1 || p.passes > MAX_PASSES) return false;
+    int sum = 0;
+    for (int i = 0; i < p.passes; ++i) {
+        if (p.bits[i] < 1 || p.bits[i] > MAX_PASS_BITS) return false;
+        sum += p.bits[i];
+    }
+    if (sum != p.n) return false;
+    if (p.passes == 1) return true;
+    int rest = p.n;
+    for (int i = 0; i + 1 < p.passes; ++i) {
+        rest -= p.bits[i];
+        if (p.bits[i] < 5 || rest < LOG_TC) return false;   // >= 32 columns per strided tile
+    }
+    return true;
+}
+
+// Plans in effect (tuned or set), per transform length; default otherwise.
+static std::mutex g_qplan_mu;
+static Plan g_qplan_tab[Q32_MAX_LOG_N + 1];
+static bool g_qplan_set[Q32_MAX_LOG_N + 1] = {false};
+
+static Plan qplan(int n) {
+    if (n >= 0 && n <= Q32_MAX_LOG_N) {
+        std::lock_guard<std::mutex> lk(g_qplan_mu);
+        if (g_qplan_set[n]) return g_qplan_tab[n];
+    }
+    return qplan_default(n);
 }
 
 static u64 ceil_pow2(u64 x) {
@@ -1098,7 +1128,7 @@ struct QWhole {
 static void plan_whole(const Job& j, int n, u32* A, u32* B, QWhole* out) {
     const int sqr = j.sqr ? 1 : 0;
     if (sqr || j.spectrum) B = A;
-    const Plan pl = qplan(n);
+    const Plan pl = j.spectrum && j.splan.passes ? j.splan : qplan(n);   // a spectrum keeps its plan
     const int P = pl.passes;
     const u64 N = 1ull << n;
     int logB[MAX_PASSES];
@@ -1205,6 +1235,56 @@ bool q32_fits(u64 la, u64 lb, int sqr) { return q32::plan_job(la, lb, sqr).ok; }
 
 void q32_force_pieces(int m) { q32::g_force_pieces.store(m > 1 ? m : 0); }
 
+Plan q32_make_plan(int log_n) { return q32::qplan(log_n); }
+Plan q32_default_plan(int log_n) { return q32::qplan_default(log_n); }
+bool q32_valid_plan(const Plan& p) { return q32::qplan_valid(p); }
+
+bool q32_set_plan(const Plan& p) {
+    if (!q32::qplan_valid(p)) return false;
+    std::lock_guard<std::mutex> lk(q32::g_qplan_mu);
+    q32::g_qplan_tab[p.n] = p;
+    q32::g_qplan_set[p.n] = true;
+    return true;
+}
+
+void q32_clear_plan(int log_n) {
+    if (log_n < 0 || log_n > Q32_MAX_LOG_N) return;
+    std::lock_guard<std::mutex> lk(q32::g_qplan_mu);
+    q32::g_qplan_set[log_n] = false;
+}
+
+std::vector<Plan> q32_candidate_plans(int n) {
+    std::vector<Plan> out;
+    if (n < 1 || n > Q32_MAX_LOG_N) return out;
+    if (n <= MAX_PASS_BITS) {
+        out.push_back(q32::qplan_default(n));
+        return out;
+    }
+    const int p0 = (n + MAX_PASS_BITS - 1) / MAX_PASS_BITS;
+    for (int P = p0; P <= p0 + 1 && P <= 3; ++P) {
+        int b[MAX_PASSES] = {0};
+        auto rec = [&](auto&& self, int i, int left) -> void {
+            if (i == P - 1) {
+                if (left < 1 || left > MAX_PASS_BITS) return;
+                b[i] = left;
+                Plan p;
+                memset(&p, 0, sizeof(p));
+                p.n = n;
+                p.passes = P;
+                for (int k = 0; k < P; ++k) p.bits[k] = b[k];
+                if (q32::qplan_valid(p)) out.push_back(p);
+                return;
+            }
+            for (int m = 5; m <= MAX_PASS_BITS; ++m) {
+                b[i] = m;
+                self(self, i + 1, left - m);
+            }
+        };
+        rec(rec, 0, n);
+    }
+    return out;
+}
+
 size_t q32_job_workspace_bytes(const Job& j) {
     if (!j.spectrum) return q32_workspace_bytes(j.la, j.lb, j.sqr ? 1 : 0);
     const q32::QJob J = q32::plan_resident(j);
@@ -1216,11 +1296,11 @@ int q32_spectrum_log_n(u64 len, u64 max_partner) {
     return q32::ilog2(2 * (len + max_partner) - 1);
 }
 
-cudaError_t q32_spectrum_enqueue(const u64* src, u64 len, int log_n, void* spec, cudaStream_t s) {
+cudaError_t q32_spectrum_enqueue(const u64* src, u64 len, int log_n, void* spec, cudaStream_t s, const Plan& pl) {
     using namespace q32;
     cudaError_t e = q32::ensure_tables();
     if (e != cudaSuccess) return e;
-    const Plan pl = qplan(log_n);
+    if (!qplan_valid(pl) || pl.n != log_n) return cudaErrorInvalidValue;
     const int P = pl.passes;
     const u64 N = 1ull << log_n;
     Job j;
@@ -1469,7 +1549,7 @@ cudaError_t q32_enqueue(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s,
     cudaError_t e = q32::ensure_tables();
     if (e != cudaSuccess) return e;
     char* base = (char*)ws;
-    const Plan pl = qplan(J.n);
+    const Plan pl = j.spectrum && j.splan.passes ? j.splan : qplan(J.n);
     const int P = pl.passes;
     const u64 N = J.N;
     int logB[MAX_PASSES];

@@ -151,6 +151,7 @@ fmn::Job to_job(const fmn_request& r, bool reuse, u64* out) {
             j.spectrum = o->spec;
             j.log_n = o->log_n;
             j.engine = o->engine;
+            j.splan = o->plan;
         } else {
             j.a = o->src;
         }
@@ -390,14 +391,16 @@ int fmn_operand_create(const u64* d_in, u64 len, u64 max_partner_len, void* stre
     const int n32 = fmn::default_engine() == fmn::ENGINE_64 ? -1 : fmn::q32_spectrum_log_n(len, max_partner_len);
     o->engine = n32 >= 0 ? fmn::ENGINE_32 : fmn::ENGINE_64;
     o->log_n = n32 >= 0 ? n32 : ilog2c(len + max_partner_len - 1);
+    o->plan = n32 >= 0 ? fmn::q32_make_plan(o->log_n) : fmn::make_plan(o->log_n);
     const size_t bytes = 3 * ((size_t)1 << o->log_n) * (n32 >= 0 ? sizeof(unsigned) : sizeof(u64));
     if ((e = cudaMalloc((void**)&o->spec, bytes)) != cudaSuccess) {
         cudaGetLastError();
         delete o;
         return fmn::api_set_error(FMN_ERR_NOMEM, "resident operand spectrum", e);
     }
-    e = o->engine == fmn::ENGINE_32 ? fmn::q32_spectrum_enqueue(d_in, len, o->log_n, o->spec, (cudaStream_t)stream)
-                                    : fmn::spectrum_enqueue(d_in, len, o->log_n, o->spec, (cudaStream_t)stream, nullptr);
+    e = o->engine == fmn::ENGINE_32
+            ? fmn::q32_spectrum_enqueue(d_in, len, o->log_n, o->spec, (cudaStream_t)stream, o->plan)
+            : fmn::spectrum_enqueue(d_in, len, o->log_n, o->spec, (cudaStream_t)stream, nullptr, o->plan);
     if (e != cudaSuccess ||
         (e = cudaStreamSynchronize((cudaStream_t)stream)) != cudaSuccess) {
         cudaFree(o->spec);
@@ -431,6 +434,7 @@ int fmn_mul_operand_ws(const fmn_operand* o, const u64* d_in2, u64 len2, u64* d_
     j.spectrum = o->spec;
     j.log_n = o->log_n;
     j.engine = o->engine;
+    j.splan = o->plan;
     if (len2 == 0) {
         cudaError_t e = cudaMemsetAsync(d_out, 0, (o->len + len2) * sizeof(u64), (cudaStream_t)stream);
         return e == cudaSuccess ? FMN_OK : fmn::api_set_error(FMN_ERR_CUDA, "cudaMemsetAsync", e);
@@ -453,6 +457,7 @@ size_t fmn_operand_workspace_size(const fmn_operand* o, u64 len2) {
     j.spectrum = o->spec;
     j.log_n = o->log_n;
     j.engine = o->engine;
+    j.splan = o->plan;
     return fmn::job_workspace_bytes(j);
 }
 

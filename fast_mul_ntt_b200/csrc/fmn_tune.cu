@@ -2,9 +2,11 @@
 //
 // A transform of 2^n points can be split into passes in several ways (e.g. 2^25 as 9+8+8,
 // 8+9+8, 8+8+9, 9+9+7, ...).  fmn_autotune times every valid plan of each length on the
-// current GPU with a real product and keeps the fastest; the choices are written to a plan
-// file whose header names the GPU and the CUDA driver, and which the library loads at start
-// from <library directory>/../tune/plans-<gpu name>.txt (or FMN_PLAN_FILE) when both match.
+// current GPU with a real product and keeps the fastest, for both residue engines (64-bit
+// points up to 2^27, 32-bit digits up to 2^26); the choices are written to a plan file whose
+// header names the GPU and the CUDA driver ("n passes bits..." lines for the 64-bit engine,
+// "e32 n passes bits..." for the 32-bit one), and which the library loads at start from
+// <library directory>/../tune/plans-<gpu name>.txt (or FMN_PLAN_FILE) when both match.
 #include <cuda_runtime.h>
 #include <dlfcn.h>
 #include <stdio.h>
@@ -42,10 +44,12 @@ std::string sanitize(const std::string& s) {
     return r;
 }
 
-// Time `reps` products of two 2^(n-1)-limb operands under the plan in effect.
-double time_plan(int n, const u64* a, const u64* b, u64* out, void* ws, size_t ws_bytes, cudaStream_t s, int reps,
-                 cudaEvent_t e0, cudaEvent_t e1, cudaError_t* err) {
-    const u64 half = 1ull << (n - 1);
+// Time `reps` products whose transform has 2^n points under the plan in effect: two
+// 2^(n-1)-limb operands on the 64-bit engine, two 2^(n-2)-limb operands (2^n digits) on the
+// 32-bit engine.
+double time_plan(int engine, int n, const u64* a, const u64* b, u64* out, void* ws, size_t ws_bytes, cudaStream_t s,
+                 int reps, cudaEvent_t e0, cudaEvent_t e1, cudaError_t* err) {
+    const u64 half = 1ull << (engine == fmn::ENGINE_32 ? n - 2 : n - 1);
     fmn::Job j;
     j.a = a;
     j.la = half;
@@ -53,8 +57,8 @@ double time_plan(int n, const u64* a, const u64* b, u64* out, void* ws, size_t w
     j.lb = half;
     j.out = out;
     j.sqr = 0;
-    j.engine = fmn::ENGINE_64;      // plans are those of the 64-bit residue engine
-    const size_t tb = fmn::twiddle_table_bytes(n);
+    j.engine = engine;
+    const size_t tb = engine == fmn::ENGINE_32 ? 0 : fmn::twiddle_table_bytes(n);
     void* tbuf = nullptr;
     fmn::TwiddleSet ts;
     const fmn::TwiddleSet* tws = nullptr;
@@ -75,6 +79,30 @@ double time_plan(int n, const u64* a, const u64* b, u64* out, void* ws, size_t w
 }  // namespace
 
 extern "C" {
+
+int fmn_get_plan_engine(int engine, int log_n, int* bits, int max_passes) {
+    if (engine != FMN_ENGINE_32) return fmn_get_plan(log_n, bits, max_passes);
+    if (log_n < 0 || log_n > 26 || !bits) return -FMN_ERR_ARG;
+    const fmn::Plan p = fmn::q32_make_plan(log_n);
+    for (int i = 0; i < p.passes && i < max_passes; ++i) bits[i] = p.bits[i];
+    return p.passes;
+}
+
+int fmn_set_plan_engine(int engine, int log_n, const int* bits, int passes) {
+    if (engine != FMN_ENGINE_32) return fmn_set_plan(log_n, bits, passes);
+    if (passes == 0) {
+        fmn::q32_clear_plan(log_n);
+        return FMN_OK;
+    }
+    fmn::Plan p;
+    memset(&p, 0, sizeof(p));
+    if (!bits || passes < 0 || passes > fmn::MAX_PASSES) return fmn::api_set_error(FMN_ERR_ARG, "bad plan", cudaSuccess);
+    p.n = log_n;
+    p.passes = passes;
+    for (int i = 0; i < passes; ++i) p.bits[i] = bits[i];
+    if (!fmn::q32_set_plan(p)) return fmn::api_set_error(FMN_ERR_ARG, "invalid pass plan", cudaSuccess);
+    return FMN_OK;
+}
 
 int fmn_get_plan(int log_n, int* bits, int max_passes) {
     if (log_n < 0 || log_n > fmn::MAX_LOG_N || !bits) return -FMN_ERR_ARG;
@@ -106,7 +134,7 @@ int fmn_load_plans(const char* path) {
     char line[512];
     std::string fgpu;
     int fdriver = -1;
-    std::vector<fmn::Plan> plans;
+    std::vector<fmn::Plan> plans, plans32;
     while (fgets(line, sizeof(line), f)) {
         if (line[0] == '#' || line[0] == '\n') continue;
         if (!strncmp(line, "gpu ", 4)) {
@@ -120,6 +148,13 @@ int fmn_load_plans(const char* path) {
         }
         fmn::Plan p;
         memset(&p, 0, sizeof(p));
+        if (!strncmp(line, "e32 ", 4)) {
+            if (sscanf(line + 4, "%d %d %d %d %d %d", &p.n, &p.passes, &p.bits[0], &p.bits[1], &p.bits[2], &p.bits[3]) >=
+                    3 &&
+                fmn::q32_valid_plan(p))
+                plans32.push_back(p);
+            continue;
+        }
         if (sscanf(line, "%d %d %d %d %d %d", &p.n, &p.passes, &p.bits[0], &p.bits[1], &p.bits[2], &p.bits[3]) >= 3 &&
             fmn::valid_plan(p))
             plans.push_back(p);
@@ -128,6 +163,7 @@ int fmn_load_plans(const char* path) {
     if (fgpu != gpu || fdriver != driver)
         return fmn::api_set_error(FMN_ERR_ARG, "plan file was tuned on another GPU or driver", cudaSuccess);
     for (const auto& p : plans) fmn::set_plan(p);
+    for (const auto& p : plans32) fmn::q32_set_plan(p);
     return FMN_OK;
 }
 
@@ -145,52 +181,57 @@ int fmn_autotune(int n_lo, int n_hi, const char* save_path) {
     cudaEventCreate(&e1);
     std::vector<std::string> lines;
     int rc = FMN_OK;
-    for (int n = n_lo; n <= n_hi && rc == FMN_OK; ++n) {
-        const std::vector<fmn::Plan> cands = fmn::candidate_plans(n);
-        if (cands.size() <= 1) continue;
-        const u64 half = 1ull << (n - 1);
-        fmn::Job wj;
-        wj.a = wj.b = nullptr;
-        wj.out = nullptr;
-        wj.la = wj.lb = half;
-        wj.sqr = 0;
-        wj.engine = fmn::ENGINE_64;
-        const size_t wsb = fmn::job_workspace_bytes(wj);
-        u64 *a = nullptr, *b = nullptr, *out = nullptr;
-        void* ws = nullptr;
-        if ((e = cudaMalloc(&a, half * 8)) != cudaSuccess || (e = cudaMalloc(&b, half * 8)) != cudaSuccess ||
-            (e = cudaMalloc(&out, 2 * half * 8)) != cudaSuccess || (e = cudaMalloc(&ws, wsb)) != cudaSuccess) {
-            rc = fmn::api_set_error(FMN_ERR_NOMEM, "tuning buffers", e);
-        }
-        if (rc == FMN_OK) {
-            cudaMemsetAsync(ws, 0, 256, s);
-            fmn::fill_limbs(a, half, 1, s);
-            fmn::fill_limbs(b, half, 2, s);
-            const int reps = n >= 24 ? 3 : n >= 20 ? 10 : 40;
-            double best = 1e30;
-            fmn::Plan bp = fmn::default_plan(n);
-            for (const auto& cand : cands) {
-                fmn::set_plan(cand);
-                const double ms = time_plan(n, a, b, out, ws, wsb, s, reps, e0, e1, &e);
-                if (e != cudaSuccess) {
-                    rc = fmn::api_set_error(FMN_ERR_CUDA, "timing a plan", e);
-                    break;
-                }
-                if (ms < best) {
-                    best = ms;
-                    bp = cand;
-                }
+    for (const int engine : {fmn::ENGINE_64, fmn::ENGINE_32}) {
+        const bool e32 = engine == fmn::ENGINE_32;
+        for (int n = n_lo; n <= (e32 ? (n_hi < 26 ? n_hi : 26) : n_hi) && rc == FMN_OK; ++n) {
+            const std::vector<fmn::Plan> cands = e32 ? fmn::q32_candidate_plans(n) : fmn::candidate_plans(n);
+            if (cands.size() <= 1) continue;
+            const u64 half = 1ull << (e32 ? n - 2 : n - 1);
+            fmn::Job wj;
+            wj.a = wj.b = nullptr;
+            wj.out = nullptr;
+            wj.la = wj.lb = half;
+            wj.sqr = 0;
+            wj.engine = engine;
+            const size_t wsb = fmn::job_workspace_bytes(wj);
+            u64 *a = nullptr, *b = nullptr, *out = nullptr;
+            void* ws = nullptr;
+            if ((e = cudaMalloc(&a, half * 8)) != cudaSuccess || (e = cudaMalloc(&b, half * 8)) != cudaSuccess ||
+                (e = cudaMalloc(&out, 2 * half * 8)) != cudaSuccess || (e = cudaMalloc(&ws, wsb)) != cudaSuccess) {
+                rc = fmn::api_set_error(FMN_ERR_NOMEM, "tuning buffers", e);
             }
-            fmn::set_plan(bp);
-            char buf[128];
-            snprintf(buf, sizeof(buf), "%d %d %d %d %d %d   # %.1f us\n", bp.n, bp.passes, bp.bits[0], bp.bits[1],
-                     bp.bits[2], bp.bits[3], best * 1e3);
-            lines.push_back(buf);
+            if (rc == FMN_OK) {
+                cudaMemsetAsync(ws, 0, 256, s);
+                fmn::fill_limbs(a, half, 1, s);
+                fmn::fill_limbs(b, half, 2, s);
+                const int reps = n >= 24 ? 3 : n >= 20 ? 10 : 40;
+                double best = 1e30;
+                fmn::Plan bp = e32 ? fmn::q32_default_plan(n) : fmn::default_plan(n);
+                for (const auto& cand : cands) {
+                    if (e32) fmn::q32_set_plan(cand);
+                    else fmn::set_plan(cand);
+                    const double ms = time_plan(engine, n, a, b, out, ws, wsb, s, reps, e0, e1, &e);
+                    if (e != cudaSuccess) {
+                        rc = fmn::api_set_error(FMN_ERR_CUDA, "timing a plan", e);
+                        break;
+                    }
+                    if (ms < best) {
+                        best = ms;
+                        bp = cand;
+                    }
+                }
+                if (e32) fmn::q32_set_plan(bp);
+                else fmn::set_plan(bp);
+                char buf[160];
+                snprintf(buf, sizeof(buf), "%s%d %d %d %d %d %d   # %.1f us\n", e32 ? "e32 " : "", bp.n, bp.passes,
+                         bp.bits[0], bp.bits[1], bp.bits[2], bp.bits[3], best * 1e3);
+                lines.push_back(buf);
+            }
+            cudaFree(a);
+            cudaFree(b);
+            cudaFree(out);
+            cudaFree(ws);
         }
-        cudaFree(a);
-        cudaFree(b);
-        cudaFree(out);
-        cudaFree(ws);
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
@@ -198,7 +239,8 @@ int fmn_autotune(int n_lo, int n_hi, const char* save_path) {
     if (rc == FMN_OK && save_path) {
         FILE* f = fopen(save_path, "w");
         if (!f) return fmn::api_set_error(FMN_ERR_ARG, "cannot write plan file", cudaSuccess);
-        fprintf(f, "# fast_mul_ntt_b200 pass plans: n passes bits... (fastest product of two 2^(n-1)-limb operands)\n");
+        fprintf(f, "# fast_mul_ntt_b200 pass plans: n passes bits... (64-bit engine: fastest product of two 2^(n-1)-limb\n"
+                   "# operands); e32 n passes bits... (32-bit engine, 2^n digits: two 2^(n-2)-limb operands)\n");
         fprintf(f, "gpu %s\ndriver %d\n", gpu.c_str(), driver);
         for (const auto& l : lines) fputs(l.c_str(), f);
         fclose(f);

@@ -219,6 +219,11 @@ int fmn_set_plan(int log_n, const int* bits, int passes);
 /* Time every valid plan for 2^n_lo .. 2^n_hi points and keep the fastest; save to
  * save_path (if not NULL) as a plan file. */
 int fmn_autotune(int n_lo, int n_hi, const char* save_path);
+/* The same per engine: FMN_ENGINE_64 as above, FMN_ENGINE_32 for its 2^log_n-digit transforms
+ * (log_n <= 26; a strided pass leaves at least 32 columns).  A resident operand keeps the
+ * plan it was transformed with. */
+int fmn_get_plan_engine(int engine, int log_n, int* bits, int max_passes);
+int fmn_set_plan_engine(int engine, int log_n, const int* bits, int passes);
 int fmn_load_plans(const char* path);
 int fmn_load_default_plans(void);
 

@@ -33,6 +33,38 @@ def test_committed_plan_file_is_valid():
         assert all(b >= 5 for b in bits[:-1])
         seen.add(n)
     assert seen == set(range(10, 28))
+    # 32-bit engine lines: strided passes leave >= 32 columns (>= 5 bits after them)
+    seen32 = set()
+    for l in open(path):
+        if not l.startswith("e32 "):
+            continue
+        f = l[4:].split("#")[0].split()
+        n, p, bits = int(f[0]), int(f[1]), [int(x) for x in f[2:2 + int(f[1])]]
+        assert sum(bits) == n <= 26 and len(bits) == p and all(1 <= b <= 9 for b in bits)
+        assert all(b >= 5 and sum(bits[i + 1:]) >= 5 for i, b in enumerate(bits[:-1]))
+        seen32.add(n)
+    assert seen32 == set(range(11, 27))
+
+
+def test_engine32_plans_validate_and_restore():
+    e32 = fmn.ENGINE_32
+    for n in (14, 25, 26):
+        fmn.set_plan(n, None, engine=e32)
+    assert fmn.get_plan(25, engine=e32) == [9, 8, 8]
+    assert fmn.get_plan(26, engine=e32) == [9, 9, 8]
+    with pytest.raises(fmn.FastMulError):
+        fmn.set_plan(14, [5, 5, 4], engine=e32)       # a strided tile would have 16 columns
+    fmn.set_plan(14, [5, 5, 4])                        # fine for the 64-bit engine (16-column tiles)
+    fmn.set_plan(14, None)
+    with pytest.raises(fmn.FastMulError):
+        fmn.set_plan(27, [9, 9, 9], engine=e32)       # beyond the 32-bit engine's 2^26 digits
+    fmn.set_plan(25, [7, 9, 9], engine=e32)
+    try:
+        assert fmn.get_plan(25, engine=e32) == [7, 9, 9]
+        assert fmn.get_plan(25) == [9, 8, 8] or fmn.get_plan(25) != [7, 9, 9]   # 64-bit plans untouched
+    finally:
+        fmn.set_plan(25, None, engine=e32)
+    assert fmn.get_plan(25, engine=e32) == [9, 8, 8]
 
 
 def test_set_plan_validates_and_restores():
@@ -129,3 +161,48 @@ def test_engine_selection_rules():
     assert ws32 == ws64
     with pytest.raises(fmn.FastMulError):
         fmn.set_engine(7)
+
+
+@pytest.mark.gpu
+def test_products_under_engine32_plans(fmn, oracle):
+    """32-bit engine: whole products (2^n digits, operands of 2^(n-2) limbs) and a split product
+    under alternative plans give the reference's numbers; a resident operand created under one
+    plan stays correct after the plan of its length changes."""
+    import torch
+    e32 = fmn.ENGINE_32
+    cases = {15: [[8, 7], [5, 5, 5], [6, 9]], 18: [[9, 9], [6, 6, 6], [7, 5, 6]], 21: [[9, 6, 6], [5, 8, 8], [7, 7, 7]]}
+    fmn.set_engine(e32)
+    try:
+        for n, plans in cases.items():
+            q = 1 << (n - 2)
+            a, b = synth.operands("uniform", q, q - 3, n)
+            want, want_sq = oracle.mul(a, b), oracle.sqr(a)
+            for bits in plans:
+                fmn.set_plan(n, bits, engine=e32)
+                assert np.array_equal(fmn.abs_mul64(a, b), want), (n, bits)
+                assert np.array_equal(fmn.abs_sqr64(a), want_sq), (n, bits)
+        fmn.force_pieces(3)
+        a, b = synth.operands("ones", 20000, 70000, 8)
+        for bits in ([9, 6, 6], [7, 7, 7]):
+            fmn.set_plan(21, bits, engine=e32)
+            assert fmn.pieces_for(len(a), len(b)) == 3
+            assert np.array_equal(fmn.abs_mul64(a, b), oracle.mul(a, b)), bits
+        fmn.force_pieces(0)
+        fmn.set_plan(18, [9, 9], engine=e32)
+        a = synth.limbs("uniform", 30000, 3)
+        op = fmn.Operand(torch.from_numpy(a.view(np.int64)).cuda(), max_partner_len=30000)
+        try:
+            b = synth.limbs("uniform", 25000, 4)
+            fmn.set_plan(17, [6, 6, 5], engine=e32)
+            fmn.set_plan(18, [6, 6, 6], engine=e32)
+            out = torch.empty(len(a) + len(b), dtype=torch.int64, device="cuda")
+            op.mul(torch.from_numpy(b.view(np.int64)).cuda(), out)
+            fmn.sync()
+            assert np.array_equal(out.cpu().numpy().view(np.uint64), oracle.mul(a, b))
+        finally:
+            op.close()
+    finally:
+        fmn.force_pieces(0)
+        fmn.set_engine(fmn.ENGINE_AUTO)
+        for n in (15, 17, 18, 21):
+            fmn.set_plan(n, None, engine=e32)
