@@ -531,7 +531,7 @@ size_t twiddle_table_bytes(int log_n) {
 
 cudaError_t build_twiddle_tables(int log_n, u64* buf, TwiddleSet* out, cudaStream_t s) {
     const Plan pl = make_plan(log_n);
-    memset(out, 0, sizeof(*out));
+    *out = TwiddleSet();
     out->log_n = log_n;
     out->plan = pl;
     int logB = log_n;
@@ -937,6 +937,7 @@ std::vector<Plan> candidate_plans(int n) {
         // enumerate compositions with each part in [1, 9]
         std::vector<int> stack;
         auto rec = [&](auto&& self, int i, int left) -> void {
+            if (i >= MAX_PASSES) return;
             if (i == P - 1) {
                 if (left < 1 || left > MAX_PASS_BITS) return;
                 b[i] = left;
@@ -1022,8 +1023,7 @@ int job_engine(const Job& j) {
 }
 
 static Job plain_job(u64 la, u64 lb, int sqr) {
-    Job j;
-    memset(&j, 0, sizeof(j));
+    Job j{};
     j.la = la;
     j.lb = lb;
     j.sqr = sqr;

@@ -1264,6 +1264,7 @@ std::vector<Plan> q32_candidate_plans(int n) {
     for (int P = p0; P <= p0 + 1 && P <= 3; ++P) {
         int b[MAX_PASSES] = {0};
         auto rec = [&](auto&& self, int i, int left) -> void {
+            if (i >= MAX_PASSES) return;
             if (i == P - 1) {
                 if (left < 1 || left > MAX_PASS_BITS) return;
                 b[i] = left;
@@ -1303,8 +1304,7 @@ cudaError_t q32_spectrum_enqueue(const u64* src, u64 len, int log_n, void* spec,
     if (!qplan_valid(pl) || pl.n != log_n) return cudaErrorInvalidValue;
     const int P = pl.passes;
     const u64 N = 1ull << log_n;
-    Job j;
-    memset(&j, 0, sizeof(j));
+    const Job j{};
     Launcher launch{j, s, nullptr, nullptr, N};
     QArgs pa;
     memset(&pa, 0, sizeof(pa));
