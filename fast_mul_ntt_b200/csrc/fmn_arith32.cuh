@@ -63,12 +63,14 @@ __device__ __forceinline__ u32 qsmul(u32 x, u32 w, u32 wp, const PrimeQ& q) {
     const u32 r = x * w - hq * q.p;     // in [0, 2p)
     return umin32(r, r - q.p);
 }
-// Montgomery product a * b * 2^-32 mod p for a, b < p: result in [0, p).
+// Montgomery product a * b * 2^-32 mod p for a * b < p 2^32: result in [0, p).  hi - mh lies
+// in (-p, p); as a u32 it is either the result (< p) or the result - p wrapped above 2^32 - p,
+// and min(r, r + p) picks the reduced one in both cases.
 __device__ __forceinline__ u32 qmont(u32 a, u32 b, const PrimeQ& q) {
     const u64 t = (u64)a * b;
     const u32 m = (u32)t * q.pinv;                // t - m p = 0 mod 2^32
     const u32 r = (u32)(t >> 32) - __umulhi(m, q.p);
-    return (u32)(t >> 32) < __umulhi(m, q.p) ? r + q.p : r;
+    return umin32(r, r + q.p);
 }
 
 // Decimation-in-frequency butterfly with Shoup twiddle (w, w'): (u + v, (u - v) w).

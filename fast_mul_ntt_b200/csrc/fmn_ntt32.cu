@@ -13,10 +13,14 @@
 // Data layout: per operand three residue arrays of N u32 (prime-major).  A strided pass
 // views a block of B = 2^logB digits as a [2^m][B / 2^m] row-major matrix; a CTA takes 32
 // adjacent columns (a 128-byte stretch of each row) and transforms every column in shared
-// memory.  The tile stores element (row j, column c) at j * 33 + c: one padding word per row
-// keeps row-wise and column-wise access free of bank conflicts, and the offsets of a group's
-// elements are compile-time steps from one base (no per-element address arithmetic).
-// Indices within one prime's residue array are 32-bit (N <= 2^26).
+// memory.  Its tile is dense (row pitch 32 words) and arrives by asynchronous 16-byte copies
+// while the CTA computes its four-step twiddle factors, so no thread waits on a global load
+// inside the rounds.  Contiguous passes (32 blocks of 2^m digits, one per tile column) store
+// element (row j, column c) at j * 33 + c: the padding word keeps both the row-wise and the
+// column-wise rounds free of bank conflicts.  Their results leave through the tile, row by
+// row, as 128-byte stores, and the fused pass copies the other operand's tile in while its
+// forward rounds run.  The offsets of a group's elements are compile-time steps from one
+// base.  Indices within one prime's residue array are 32-bit (N <= 2^26).
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <stdio.h>
@@ -64,6 +68,30 @@ constexpr int TP = TC + 1;              // padded row pitch of a shared-memory t
 // Odd columns swap the two halves of the row (c ^ 16), a permutation within the row: a warp
 // that covers 16 rows of two adjacent columns then touches two disjoint bank ranges.
 __device__ __forceinline__ int tix(int j, int c) { return j * TP + (c ^ ((c & 1) << 4)); }
+// Dense tiles (row pitch 32 words, rows 16-byte aligned) for strided passes, whose rounds all
+// run with the 32 lanes of a warp on the 32 columns of one row: conflict-free without
+// padding, and each row is a 128-byte copy target.
+__device__ __forceinline__ int dix(int j, int c) { return j * TC + c; }
+
+// 16-byte asynchronous copy global -> shared (no registers held while it is in flight).
+__device__ __forceinline__ void cp_async16(u32* sdst, const u32* gsrc) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_commit_wait() {
+    asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;\n" ::: "memory");
+}
+// Rows 0 .. L-1 of a strided tile (32 words each, row r at g + r * 2^logS) into a dense tile.
+template <int L>
+__device__ __forceinline__ void stage_tile(u32* sm, const u32* __restrict__ g, int logS) {
+#pragma unroll 4
+    for (int e = threadIdx.x; e < L * (TC / 4); e += NT) {
+        const int r = e / (TC / 4), k = e % (TC / 4);
+        cp_async16(sm + r * TC + 4 * k, g + ((u32)r << logS) + 4 * k);
+    }
+}
 
 enum { M_FWD = 0, M_FWD_LAST = 1, M_FUSED = 2, M_INV = 3, M_FUSED2 = 4, M_INV_ACC = 5 };
 
@@ -152,18 +180,7 @@ __device__ __forceinline__ void run_round(LD ld, ST st, int pi, const PrimeQ& q)
     }
 }
 
-// R consecutive u32 (aligned to 4R bytes) with vector stores / loads.
-template <int R>
-__device__ __forceinline__ void st_vec(u32* p, const u32 (&x)[R]) {
-    if constexpr (R == 1) {
-        p[0] = x[0];
-    } else if constexpr (R == 2) {
-        *reinterpret_cast<uint2*>(p) = make_uint2(x[0], x[1]);
-    } else {
-#pragma unroll
-        for (int t = 0; t < R; t += 4) *reinterpret_cast<uint4*>(p + t) = make_uint4(x[t], x[t + 1], x[t + 2], x[t + 3]);
-    }
-}
+// R consecutive u32 (aligned to 4R bytes) with vector loads.
 template <int R>
 __device__ __forceinline__ void ld_vec(const u32* p, u32 (&x)[R]) {
     if constexpr (R == 1) {
@@ -187,26 +204,28 @@ __device__ __forceinline__ void ld_vec(const u32* p, u32 (&x)[R]) {
 // Rounds IDX.. of a sub-transform (forward: round 0 holds the top bits; inverse round k
 // undoes forward round NR-1-k).  The first round reads with `ld0`, the last writes with
 // `stl`, the rest go through shared memory.
-template <int LOGL, bool INV, bool CONTIG, int IDX, bool GST = false, bool GLD = false, class LD0, class STL>
+template <int LOGL, bool INV, bool CONTIG, int IDX, bool GST = false, bool GLD = false, bool DENSE = false, class LD0,
+          class STL>
 __device__ __forceinline__ void rounds(u32* sm, LD0 ld0, STL stl, int pi, const PrimeQ& q) {
     constexpr int NR = rounds_count(LOGL);
     constexpr int FR = INV ? NR - 1 - IDX : IDX;
     constexpr int RB = round_bits(LOGL, FR), TOP = round_top(LOGL, FR);
     constexpr bool QF = CONTIG && (TOP == LOGL - 1);
-    auto lds = [sm](int j, int c) { return sm[tix(j, c)]; };
-    auto sts = [sm](int j, int c, u32 v) { sm[tix(j, c)] = v; };
+    static_assert(!(DENSE && CONTIG), "dense tiles serve strided passes only");
+    auto lds = [sm](int j, int c) { return sm[DENSE ? dix(j, c) : tix(j, c)]; };
+    auto sts = [sm](int j, int c, u32 v) { sm[DENSE ? dix(j, c) : tix(j, c)] = v; };
     if constexpr (NR == 1) {
         run_round<LOGL, RB, TOP, INV, QF, GST, GLD>(ld0, stl, pi, q);
     } else if constexpr (IDX == 0) {
         run_round<LOGL, RB, TOP, INV, QF, false, GLD>(ld0, sts, pi, q);
         __syncthreads();
-        rounds<LOGL, INV, CONTIG, 1, GST>(sm, ld0, stl, pi, q);
+        rounds<LOGL, INV, CONTIG, 1, GST, false, DENSE>(sm, ld0, stl, pi, q);
     } else if constexpr (IDX == NR - 1) {
         run_round<LOGL, RB, TOP, INV, QF, GST>(lds, stl, pi, q);
     } else {
         run_round<LOGL, RB, TOP, INV, QF>(lds, sts, pi, q);
         __syncthreads();
-        rounds<LOGL, INV, CONTIG, IDX + 1, GST>(sm, ld0, stl, pi, q);
+        rounds<LOGL, INV, CONTIG, IDX + 1, GST, false, DENSE>(sm, ld0, stl, pi, q);
     }
 }
 
@@ -252,23 +271,33 @@ __device__ __forceinline__ void body_fwd(u32* sm, const QArgs& a, u64 tile, int 
     const u64* __restrict__ src = a.src;
     const u64 len = a.len;
     const int shift = Q32_MAX_LOG_N - a.logB;
-    u32* beta = sm + TP * L;
+    // Residue tiles are copied in asynchronously while the twiddle factors are computed; the
+    // entry pass reads the caller's limbs directly (8-byte alignment only, zero past the end).
+    constexpr bool STAGED = !ENTRY;
+    u32* beta = sm + (STAGED ? TC : TP) * L;
+    if constexpr (STAGED) stage_tile<L>(sm, d + gbase, logS);
     fill_beta<LOGL, false>(beta, col0, shift, pi, q);     // read after the first round's barrier
+    if constexpr (STAGED) {
+        cp_async_commit_wait();
+        __syncthreads();
+    }
     auto ld0 = [=](int j, int c) -> u32 {
+        if constexpr (STAGED) return sm[dix(j, c)];
         const u32 g = gbase + c + ((u32)j << logS);
         if constexpr (ENTRY) return entry_val(src, len, g, q);
         else return d[g];
     };
     auto stl = [=](int row0, int c, const auto& x) {
         const u32 al = group_alpha<LOGL, false>(col0 + c, row0, shift, pi, q);
-        const u32 o = gbase + c + ((u32)row0 << logS);
+        u32* __restrict__ po = d + (gbase + c + ((u32)row0 << logS));
+        const u32 S = 1u << logS;                 // row stride: t * S is a multiply-add address
 #pragma unroll
         for (int t = 0; t < R; ++t) {
             const int tp = RB ? (int)(__brev((u32)t) >> (32 - RB)) : 0;
-            d[o + ((u32)t << logS)] = qmont(x[t], qmont_lazy(al, beta[tp * TC + c], q), q);
+            po[(u32)t * S] = qmont(x[t], qmont_lazy(al, beta[tp * TC + c], q), q);
         }
     };
-    rounds<LOGL, false, false, 0, true>(sm, ld0, stl, pi, q);
+    rounds<LOGL, false, false, 0, true, false, STAGED>(sm, ld0, stl, pi, q);
 }
 
 // Inverse strided pass: inverse four-step twiddle, then the inverse sub-transform.  ACC: the
@@ -284,13 +313,14 @@ __device__ __forceinline__ void body_inv(u32* sm, const QArgs& a, u64 tile, int 
     const u32 gbase = (blk << a.logB) + col0;
     u32* __restrict__ d = a.data + (u64)pi * a.N;
     const int shift = Q32_MAX_LOG_N - a.logB;
-    u32* beta = sm + TP * L;
+    u32* beta = sm + TC * L;
+    stage_tile<L>(sm, d + gbase, logS);                   // in flight during fill_beta
     fill_beta<LOGL, true>(beta, col0, shift, pi, q);
+    cp_async_commit_wait();
     __syncthreads();
     auto ld0 = [=](int row0, int c, auto& x) {
-        const u32 o = gbase + c + ((u32)row0 << logS);
 #pragma unroll
-        for (int t = 0; t < R; ++t) x[t] = d[o + ((u32)t << logS)];
+        for (int t = 0; t < R; ++t) x[t] = sm[dix(row0 + t, c)];
         const u32 al = group_alpha<LOGL, true>(col0 + c, row0, shift, pi, q);
 #pragma unroll
         for (int t = 0; t < R; ++t) {
@@ -322,10 +352,10 @@ __device__ __forceinline__ void body_inv(u32* sm, const QArgs& a, u64 tile, int 
                 }
             }
         };
-        rounds<LOGL, true, false, 0, true, true>(sm, ld0, stl, pi, q);
+        rounds<LOGL, true, false, 0, true, true, true>(sm, ld0, stl, pi, q);
     } else {
         auto stl = [=](int j, int c, u32 v) { d[gbase + c + ((u32)j << logS)] = v; };
-        rounds<LOGL, true, false, 0, false, true>(sm, ld0, stl, pi, q);
+        rounds<LOGL, true, false, 0, false, true, true>(sm, ld0, stl, pi, q);
     }
 }
 
@@ -347,16 +377,24 @@ __device__ __forceinline__ void body_fwd_last(u32* sm, const QArgs& a, u64 tile,
     if constexpr (LOGL == 0) {
         if (threadIdx.x < (unsigned)ncols) d[gbase + threadIdx.x] = ld0(0, threadIdx.x);
     } else {
-        auto stl = [=](int row0, int c, const auto& x) {
-            if (c < ncols) st_vec(d + gbase + (u32)c * L + row0, x);
-        };
-        rounds<LOGL, false, true, 0, true>(sm, ld0, stl, pi, q);
+        // the last round (a thread per column) writes the tile; the blocks then leave row by
+        // row with the lanes of a warp on consecutive words (128-byte stores)
+        auto sts = [sm](int j, int c, u32 v) { sm[tix(j, c)] = v; };
+        rounds<LOGL, false, true, 0, false>(sm, ld0, sts, pi, q);
+        __syncthreads();
+#pragma unroll 4
+        for (int e = threadIdx.x; e < TC * L; e += NT) {
+            const int c = e >> LOGL, j = e & (L - 1);
+            if (c < ncols) d[gbase + (u32)c * L + j] = sm[tix(j, c)];
+        }
     }
 }
 
 // The lowest forward round, the pointwise product and the lowest inverse round of one
 // contiguous tile, all in registers.
-template <int LOGL, bool SQR, bool OTH_SMEM = false, class LD, class ST>
+// OTH: where the other operand's transformed tile is read: 0 global memory, 1 a second tile in
+// the tix layout, 2 a column-major staging buffer (column c at oth + c * (L + 4)).
+template <int LOGL, bool SQR, int OTH = 0, class LD, class ST>
 __device__ __forceinline__ void fused_lowest(LD ld, ST st, const u32* __restrict__ oth, u32 gbase, int ncols, int pi,
                                              const PrimeQ& q) {
     constexpr int L = 1 << LOGL;
@@ -388,9 +426,14 @@ __device__ __forceinline__ void fused_lowest(LD ld, ST st, const u32* __restrict
             if constexpr (SQR) {
 #pragma unroll
                 for (int t = 0; t < R; ++t) x[t] = qmont(x[t], x[t], q);
-            } else if constexpr (OTH_SMEM) {
+            } else if constexpr (OTH == 1) {
 #pragma unroll
                 for (int t = 0; t < R; ++t) x[t] = qmont(x[t], oth[tix(row0 + t, c)], q);
+            } else if constexpr (OTH == 2) {
+                u32 y[R];
+                ld_vec(oth + c * (L + 4) + row0, y);      // 8 lanes per phase on disjoint banks
+#pragma unroll
+                for (int t = 0; t < R; ++t) x[t] = qmont(x[t], y[t], q);
             } else {
                 u32 y[R];
                 ld_vec(oth + gbase + (u32)c * L + row0, y);
@@ -448,15 +491,27 @@ __device__ __forceinline__ void body_fused(u32* sm, const QArgs& a, u64 tile, in
     } else if constexpr (NR == 1) {
         fused_lowest<LOGL, SQR>(ldg, stg, o, gbase, ncols, pi, q);
     } else {
+        // the other operand's tile, column by column, is copied in while the forward rounds run
+        constexpr bool OS = !SQR && LOGL <= 8;           // 9-bit tiles: no room for a second one
+        u32* oth_s = sm + TP * L;
+        if constexpr (OS) {
+#pragma unroll 4
+            for (int e = threadIdx.x; e < TC * (L / 4); e += NT) {
+                const int c = e / (L / 4), k = e % (L / 4);
+                if (c < ncols) cp_async16(oth_s + c * (L + 4) + 4 * k, o + gbase + (u32)c * L + 4 * k);
+            }
+            cp_async_commit();
+        }
         constexpr int RB0 = round_bits(LOGL, 0);
         run_round<LOGL, RB0, LOGL - 1, false, true>(ldg, sts, pi, q);
-        __syncthreads();
         if constexpr (NR == 3) {
+            __syncthreads();
             constexpr int RB1 = round_bits(LOGL, 1), T1 = round_top(LOGL, 1);
             run_round<LOGL, RB1, T1, false, false>(lds, sts, pi, q);
-            __syncthreads();
         }
-        fused_lowest<LOGL, SQR>(lds, sts, o, gbase, ncols, pi, q);
+        if constexpr (OS) cp_async_wait_all();
+        __syncthreads();
+        fused_lowest<LOGL, SQR, OS ? 2 : 0>(lds, sts, OS ? oth_s : o, gbase, ncols, pi, q);
         __syncthreads();
         if constexpr (NR == 3) {
             constexpr int RB1 = round_bits(LOGL, 1), T1 = round_top(LOGL, 1);
@@ -494,7 +549,7 @@ __device__ __forceinline__ void body_fused2(u32* sm, const QArgs& a, u64 tile, i
         run_round<LOGL, RB1, T1, false, false>(lds, sts, pi, q);
         __syncthreads();
     }
-    fused_lowest<LOGL, false, true>(lds, sts, smA, gbase, TC, pi, q);
+    fused_lowest<LOGL, false, 1>(lds, sts, smA, gbase, TC, pi, q);
     __syncthreads();
     if constexpr (NR == 3) {
         constexpr int RB1 = round_bits(LOGL, 1), T1 = round_top(LOGL, 1);
@@ -508,7 +563,10 @@ __device__ __forceinline__ void body_fused2(u32* sm, const QArgs& a, u64 tile, i
 // pass) get the registers of 3 CTAs; 8-bit strided passes too (their radix-16 rounds spill at 64).
 template <int MODE, int LOGL>
 constexpr int min_ctas() {
-    return ((MODE == M_FWD || MODE == M_INV || MODE == M_INV_ACC) && LOGL >= 8) || MODE == M_FUSED2 ? 3 : 4;
+    return ((MODE == M_FWD || MODE == M_INV || MODE == M_INV_ACC) && LOGL >= 8) || MODE == M_FUSED2 ||
+                   (MODE == M_FUSED && LOGL == 8)
+               ? 3
+               : 4;
 }
 
 template <int MODE, int LOGL, bool ENTRY, bool SQR>
@@ -834,8 +892,11 @@ static const BatchKernelTable& bktab() {
 
 // tile + the 16 x 32 four-step twiddle factors of strided passes; two tiles when merged
 static size_t pass_smem(int logl, int variant) {
-    const size_t tile = (size_t)TP * ((size_t)1 << logl);
-    return (variant == V_FUSED2 ? 2 * tile : tile + TC * 16) * sizeof(u32);
+    const size_t L = (size_t)1 << logl, tile = (size_t)TP * L;
+    size_t w = variant == V_FUSED2 ? 2 * tile : tile + TC * 16;
+    // staging buffer of the other operand's tile (body_fused, multi-round tiles of <= 8 bits)
+    if ((variant == V_FUSED || variant == V_FUSED_E) && logl >= 5 && logl <= 8) w += TC * (L + 4);
+    return w * sizeof(u32);
 }
 
 static cudaError_t ensure_tables() {

@@ -44,7 +44,7 @@ def qmont(a, b, p):
     m = ((t & M32) * pow(p, -1, 1 << 32)) & M32
     hi, mh = t >> 32, (m * p) >> 32
     r = (hi - mh) & M32
-    return (r + p) & M32 if hi < mh else r
+    return min(r, (r + p) & M32)
 
 
 def qsmul(x, w, p):
@@ -80,6 +80,8 @@ def test_shoup_and_montgomery_identities():
             assert qsmul(x, w, p) == x * w % p
             a, b = rng.randrange(p), rng.randrange(p)
             assert qmont(a, b, p) == a * b * pow(2, -32, p) % p
+            b2 = rng.randrange(1, 2 * p)          # a lazy Montgomery result as second factor
+            assert qmont(a, b2, p) == a * b2 * pow(2, -32, p) % p
         for x in (0, 1, p - 1, p, 2 * p - 1, M32):
             assert qsmul(x, p - 1, p) == x * (p - 1) % p
 
