@@ -4,12 +4,18 @@
 // Each device gets a context with a cached scratch workspace, a stream and an event that
 // orders uses of the workspace across streams.  Host-pointer calls copy the operands to the
 // device, run the product and copy the result back (out may alias the inputs, as in the
-// reference, because the inputs are consumed before the output is written).
+// reference, because the inputs are consumed before the output is written).  They run on
+// host lanes: a few per device (FMN_HOST_LANES, default 4), each with its own workspace,
+// operand buffers and streams.  A call holds the device lock only while it enqueues its
+// copies and kernels, so the calls of several host threads overlap on the GPU (one product's
+// copies over PCIe beside another's kernels), as the reference's calls on several host
+// threads run side by side on the CPU cores.
 #include <cuda_runtime.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
 
+#include <condition_variable>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -32,6 +38,22 @@ int set_err(int code, const char* what, cudaError_t e = cudaSuccess) {
 
 constexpr int MAX_DEV = 64;
 
+// Resources of one in-flight host-pointer product (see the file comment).
+struct HostLane {
+    cudaStream_t s = nullptr, cs = nullptr, co = nullptr;   // kernels, copy-in, copy-back
+    cudaEvent_t done = nullptr;                              // the lane's last product
+    bool done_valid = false;
+    cudaEvent_t join[2] = {nullptr, nullptr};
+    cudaEvent_t cb_event[4] = {nullptr};   // chunked copy-back
+    cudaEvent_t ci_event[8] = {nullptr};   // piecewise copy-in of the second operand
+    void* ws = nullptr;
+    size_t ws_cap = 0;
+    u64* io = nullptr;                     // device copies of the operands and the product
+    size_t io_cap = 0;
+    unsigned* h_err = nullptr;             // pinned word for reading the device error flag
+    bool busy = false;
+};
+
 struct DevCtx {
     std::mutex mu;
     int dev = -1;
@@ -40,8 +62,6 @@ struct DevCtx {
     bool done_valid = false;
     void* ws = nullptr;
     size_t ws_cap = 0;
-    u64* io = nullptr;                // device staging for host-pointer calls
-    size_t io_cap = 0;
     unsigned* h_err = nullptr;        // pinned word for reading the device error flag
     // precomputed four-step twiddles, one set per transform length, least recently used evicted
     struct Tw {
@@ -60,8 +80,10 @@ struct DevCtx {
     size_t stage_cap = 0;
     cudaEvent_t stage_free = nullptr;   // the last batch's descriptor copy has completed
     bool stage_pending = false;
-    cudaEvent_t cb_event[4] = {nullptr};   // chunked copy-back of host products
-    cudaEvent_t ci_event[8] = {nullptr};   // piecewise copy-in of the second operand
+    // host lanes: created on demand up to host_lanes(), handed out under lane_mu
+    std::vector<HostLane*> lanes;
+    std::mutex lane_mu;
+    std::condition_variable lane_cv;
 };
 
 std::mutex g_ctx_mu;
@@ -96,8 +118,6 @@ int get_ctx(DevCtx** out) {
         for (int k = 0; k <= DevCtx::NSTREAM && e == cudaSuccess; ++k)
             e = cudaEventCreateWithFlags(&c->wevent[k], cudaEventDisableTiming);
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->stage_free, cudaEventDisableTiming);
-        for (int k = 0; k < 4 && e == cudaSuccess; ++k) e = cudaEventCreateWithFlags(&c->cb_event[k], cudaEventDisableTiming);
-        for (int k = 0; k < 8 && e == cudaSuccess; ++k) e = cudaEventCreateWithFlags(&c->ci_event[k], cudaEventDisableTiming);
         if (e != cudaSuccess) {
             delete c;
             return set_err(FMN_ERR_CUDA, "creating device context streams", e);
@@ -109,42 +129,99 @@ int get_ctx(DevCtx** out) {
     return FMN_OK;
 }
 
-// Grow the cached workspace of `c` (caller holds c->mu).  The error word at offset 0 is
-// zeroed on allocation.
-int ensure_ws(DevCtx* c, size_t bytes) {
-    if (c->ws_cap >= bytes) return FMN_OK;
+// Grow a cached device buffer to `bytes` (its owner's lock held).  A workspace's error word
+// at offset 0 is zeroed on allocation.
+int ensure_buf(void** buf, size_t* cap, size_t bytes, bool workspace) {
+    if (*cap >= bytes) return FMN_OK;
     cudaError_t e;
-    if (c->ws) {
+    if (*buf) {
         if ((e = cudaDeviceSynchronize()) != cudaSuccess) return set_err(FMN_ERR_CUDA, "sync before regrow", e);
-        cudaFree(c->ws);
-        c->ws = nullptr;
-        c->ws_cap = 0;
+        cudaFree(*buf);
+        *buf = nullptr;
+        *cap = 0;
     }
-    if ((e = cudaMalloc(&c->ws, bytes)) != cudaSuccess) {
+    if ((e = cudaMalloc(buf, bytes)) != cudaSuccess) {
         cudaGetLastError();
-        return set_err(FMN_ERR_NOMEM, "cudaMalloc of the product workspace", e);
+        return set_err(FMN_ERR_NOMEM, workspace ? "cudaMalloc of the product workspace" : "cudaMalloc of the operand buffers", e);
     }
-    if ((e = cudaMemset(c->ws, 0, 256)) != cudaSuccess) return set_err(FMN_ERR_CUDA, "cudaMemset", e);
-    c->ws_cap = bytes;
+    if (workspace && (e = cudaMemset(*buf, 0, 256)) != cudaSuccess) return set_err(FMN_ERR_CUDA, "cudaMemset", e);
+    *cap = bytes;
     return FMN_OK;
 }
 
-int ensure_io(DevCtx* c, size_t bytes) {
-    if (c->io_cap >= bytes) return FMN_OK;
-    cudaError_t e;
-    if (c->io) {
-        if ((e = cudaDeviceSynchronize()) != cudaSuccess) return set_err(FMN_ERR_CUDA, "sync before regrow", e);
-        cudaFree(c->io);
-        c->io = nullptr;
-        c->io_cap = 0;
+// The cached workspace of `c` (caller holds c->mu).
+int ensure_ws(DevCtx* c, size_t bytes) { return ensure_buf(&c->ws, &c->ws_cap, bytes, true); }
+
+// Number of host lanes per device: FMN_HOST_LANES (1 .. 8), default 4.
+int host_lanes() {
+    static const int n = [] {
+        const char* v = getenv("FMN_HOST_LANES");
+        const int k = v ? atoi(v) : 4;
+        return k < 1 ? 1 : (k > 8 ? 8 : k);
+    }();
+    return n;
+}
+
+void destroy_lane(HostLane* L) {
+    if (L->ws) cudaFree(L->ws);
+    if (L->io) cudaFree(L->io);
+    if (L->h_err) cudaFreeHost(L->h_err);
+    for (cudaStream_t st : {L->s, L->cs, L->co})
+        if (st) cudaStreamDestroy(st);
+    for (cudaEvent_t ev : {L->done, L->join[0], L->join[1]})
+        if (ev) cudaEventDestroy(ev);
+    for (cudaEvent_t ev : L->cb_event)
+        if (ev) cudaEventDestroy(ev);
+    for (cudaEvent_t ev : L->ci_event)
+        if (ev) cudaEventDestroy(ev);
+    delete L;
+}
+
+// A free host lane of `c`, created if fewer than host_lanes() exist; waits for one otherwise.
+int acquire_lane(DevCtx* c, HostLane** out) {
+    std::unique_lock<std::mutex> lk(c->lane_mu);
+    for (;;) {
+        for (HostLane* L : c->lanes)
+            if (!L->busy) {
+                L->busy = true;
+                *out = L;
+                return FMN_OK;
+            }
+        if ((int)c->lanes.size() < host_lanes()) break;
+        c->lane_cv.wait(lk);
     }
-    if ((e = cudaMalloc((void**)&c->io, bytes)) != cudaSuccess) {
-        cudaGetLastError();
-        return set_err(FMN_ERR_NOMEM, "cudaMalloc of the operand buffers", e);
+    HostLane* L = new HostLane();
+    cudaError_t e = cudaSuccess;
+    for (cudaStream_t* st : {&L->s, &L->cs, &L->co})
+        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(st, cudaStreamNonBlocking);
+    for (cudaEvent_t* ev : {&L->done, &L->join[0], &L->join[1]})
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming);
+    for (cudaEvent_t& ev : L->cb_event)
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+    for (cudaEvent_t& ev : L->ci_event)
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaMallocHost((void**)&L->h_err, sizeof(unsigned));
+    if (e != cudaSuccess) {
+        destroy_lane(L);
+        return set_err(FMN_ERR_CUDA, "creating a host lane", e);
     }
-    c->io_cap = bytes;
+    L->busy = true;
+    c->lanes.push_back(L);
+    *out = L;
     return FMN_OK;
 }
+
+struct LaneGuard {
+    DevCtx* c;
+    HostLane* L;
+    ~LaneGuard() {
+        {
+            std::lock_guard<std::mutex> lk(c->lane_mu);
+            L->busy = false;
+        }
+        c->lane_cv.notify_one();
+    }
+};
 
 // Coefficients are < min(len1, len2) * 2^128 and must stay below p0 p1 p2 (about 2^184.7);
 // transforms are limited to 2^30 points by the twiddle tables.
@@ -202,7 +279,8 @@ const fmn::TwiddleSet* get_twiddles(DevCtx* c, int log_n, cudaStream_t s) {
     t.buf = buf;
     t.bytes = bytes;
     t.last_use = ++c->tick;
-    if (fmn::build_twiddle_tables(log_n, (u64*)buf, &t.set, s) != cudaSuccess) {
+    // built on s; finished here, since later jobs on other streams read the cached tables
+    if (fmn::build_twiddle_tables(log_n, (u64*)buf, &t.set, s) != cudaSuccess || cudaStreamSynchronize(s) != cudaSuccess) {
         cudaGetLastError();
         cudaFree(buf);
         return nullptr;
@@ -303,55 +381,60 @@ cudaError_t copy_in_range(void* p, u64 lo, u64 hi, cudaStream_t s) {
 // Host product on pinned buffers: in2 is copied on a second stream while in1's forward
 // passes run (piece by piece for a split product, each just ahead of its first reader), and
 // the output comes back in chunks on a third stream as the carry scan finishes them (for a
-// split product, the limbs each piece completes while the next piece computes).
-int host_product_pinned(DevCtx* c, const u64* in1, u64 len1, const u64* in2, u64 len2, u64* out, int sqr) {
+// split product, the limbs each piece completes while the next piece computes).  Everything
+// is enqueued under the device lock; the wait for the result is not.
+int host_product_pinned(DevCtx* c, HostLane* L, const u64* in1, u64 len1, const u64* in2, u64 len2, u64* out,
+                        int sqr) {
     const u64 out_len = len1 + len2;
     const size_t o1 = 0, o2 = round256(len1 * 8), oo = o2 + (sqr ? 0 : round256(len2 * 8));
     int rc;
-    if ((rc = ensure_io(c, oo + round256(out_len * 8)))) return rc;
-    char* io = (char*)c->io;
-    cudaStream_t s = c->stream, cs = c->wstream[0], co = c->wstream[1];
-    cudaError_t e;
-    fmn::Job j;
-    j.a = (const u64*)(io + o1);
-    j.la = len1;
-    j.b = sqr ? j.a : (const u64*)(io + o2);
-    j.lb = len2;
-    j.out = (u64*)(io + oo);
-    j.sqr = sqr;
-    const size_t need = fmn::job_workspace_bytes(j);
-    if ((rc = ensure_ws(c, need))) return rc;
-    if (c->done_valid && ((e = cudaStreamWaitEvent(s, c->done, 0)) != cudaSuccess ||
-                          (e = cudaStreamWaitEvent(cs, c->done, 0)) != cudaSuccess ||
-                          (e = cudaStreamWaitEvent(co, c->done, 0)) != cudaSuccess))
-        return set_err(FMN_ERR_CUDA, "cudaStreamWaitEvent", e);
-    const fmn::TwiddleSet* tws = fmn::job_engine(j) != fmn::ENGINE_64 ? nullptr : get_twiddles(c, ilog2_ceil(out_len - 1), s);
-    if ((e = cudaMemcpyAsync(io + o1, in1, len1 * 8, cudaMemcpyHostToDevice, s)) != cudaSuccess)
-        return set_err(FMN_ERR_CUDA, "copying in1 to the device", e);
-    CopyIn ci;
-    ci.copy = cs;
-    ci.used = 0;
-    ci.dst = (u64*)(io + o2);
-    ci.src = in2;
-    for (int k = 0; k < 8; ++k) ci.ev[k] = c->ci_event[k];
-    CopyBack cb;
-    cb.main = s;
-    cb.copy = co;
-    cb.used = 0;
-    cb.dst = out;
-    cb.src = j.out;
-    for (int k = 0; k < 4; ++k) cb.ev[k] = c->cb_event[k];
-    const int chunks = out_len >= (1u << 20) ? 4 : 1;
-    if ((e = fmn::enqueue_job_overlapped(j, c->ws, c->ws_cap, s, tws, sqr ? nullptr : copy_in_range, &ci, chunks,
-                                         copy_back_chunk, &cb)) != cudaSuccess)
-        return set_err(FMN_ERR_CUDA, "kernel launch", e);
-    // the copy streams end after the last chunk; order the main stream (and later jobs) after them
-    if ((e = cudaEventRecord(c->wevent[2], co)) != cudaSuccess || (e = cudaStreamWaitEvent(s, c->wevent[2], 0)) != cudaSuccess ||
-        (e = cudaEventRecord(c->wevent[3], cs)) != cudaSuccess || (e = cudaStreamWaitEvent(s, c->wevent[3], 0)) != cudaSuccess)
-        return set_err(FMN_ERR_CUDA, "joining the copy streams", e);
-    if ((e = cudaEventRecord(c->done, s)) != cudaSuccess) return set_err(FMN_ERR_CUDA, "cudaEventRecord", e);
-    c->done_valid = true;
-    return take_device_error(c->ws, c->h_err, s);
+    {
+        std::lock_guard<std::mutex> lk(c->mu);
+        if ((rc = ensure_buf((void**)&L->io, &L->io_cap, oo + round256(out_len * 8), false))) return rc;
+        char* io = (char*)L->io;
+        cudaStream_t s = L->s, cs = L->cs, co = L->co;
+        cudaError_t e;
+        fmn::Job j;
+        j.a = (const u64*)(io + o1);
+        j.la = len1;
+        j.b = sqr ? j.a : (const u64*)(io + o2);
+        j.lb = len2;
+        j.out = (u64*)(io + oo);
+        j.sqr = sqr;
+        if ((rc = ensure_buf(&L->ws, &L->ws_cap, fmn::job_workspace_bytes(j), true))) return rc;
+        if (L->done_valid && ((e = cudaStreamWaitEvent(s, L->done, 0)) != cudaSuccess ||
+                              (e = cudaStreamWaitEvent(cs, L->done, 0)) != cudaSuccess ||
+                              (e = cudaStreamWaitEvent(co, L->done, 0)) != cudaSuccess))
+            return set_err(FMN_ERR_CUDA, "cudaStreamWaitEvent", e);
+        const fmn::TwiddleSet* tws =
+            fmn::job_engine(j) != fmn::ENGINE_64 ? nullptr : get_twiddles(c, ilog2_ceil(out_len - 1), s);
+        if ((e = cudaMemcpyAsync(io + o1, in1, len1 * 8, cudaMemcpyHostToDevice, s)) != cudaSuccess)
+            return set_err(FMN_ERR_CUDA, "copying in1 to the device", e);
+        CopyIn ci;
+        ci.copy = cs;
+        ci.used = 0;
+        ci.dst = (u64*)(io + o2);
+        ci.src = in2;
+        for (int k = 0; k < 8; ++k) ci.ev[k] = L->ci_event[k];
+        CopyBack cb;
+        cb.main = s;
+        cb.copy = co;
+        cb.used = 0;
+        cb.dst = out;
+        cb.src = j.out;
+        for (int k = 0; k < 4; ++k) cb.ev[k] = L->cb_event[k];
+        const int chunks = out_len >= (1u << 20) ? 4 : 1;
+        if ((e = fmn::enqueue_job_overlapped(j, L->ws, L->ws_cap, s, tws, sqr ? nullptr : copy_in_range, &ci, chunks,
+                                             copy_back_chunk, &cb)) != cudaSuccess)
+            return set_err(FMN_ERR_CUDA, "kernel launch", e);
+        // the copy streams end after the last chunk; order the main stream (and later jobs) after them
+        if ((e = cudaEventRecord(L->join[0], co)) != cudaSuccess || (e = cudaStreamWaitEvent(s, L->join[0], 0)) != cudaSuccess ||
+            (e = cudaEventRecord(L->join[1], cs)) != cudaSuccess || (e = cudaStreamWaitEvent(s, L->join[1], 0)) != cudaSuccess)
+            return set_err(FMN_ERR_CUDA, "joining the copy streams", e);
+        if ((e = cudaEventRecord(L->done, s)) != cudaSuccess) return set_err(FMN_ERR_CUDA, "cudaEventRecord", e);
+        L->done_valid = true;
+    }
+    return take_device_error(L->ws, L->h_err, L->s);
 }
 
 int host_product(const u64* in1, u64 len1, const u64* in2, u64 len2, u64* out, int sqr) {
@@ -366,32 +449,51 @@ int host_product(const u64* in1, u64 len1, const u64* in2, u64 len2, u64* out, i
     if (rc) return rc;
     DevCtx* c;
     if ((rc = get_ctx(&c))) return rc;
-    std::lock_guard<std::mutex> lk(c->mu);
+    HostLane* L;
+    if ((rc = acquire_lane(c, &L))) return rc;
+    LaneGuard guard{c, L};
     // pinned buffers that do not overlap each other: overlapped copies
     if (is_pinned(in1) && (sqr || is_pinned(in2)) && is_pinned(out) &&
         ((const char*)out + (len1 + len2) * 8 <= (const char*)in1 || (const char*)out >= (const char*)(in1 + len1)) &&
         (sqr || (const char*)out + (len1 + len2) * 8 <= (const char*)in2 || (const char*)out >= (const char*)(in2 + len2)))
-        return host_product_pinned(c, in1, len1, in2, len2, out, sqr);
-    // device layout: [in1][in2][out], each 256-byte aligned
+        return host_product_pinned(c, L, in1, len1, in2, len2, out, sqr);
+    // pageable buffers: copies through the driver's staging (they may block the calling
+    // thread, so they are issued outside the device lock); device layout [in1][in2][out]
     const size_t o1 = 0, o2 = round256(len1 * 8), oo = o2 + (sqr ? 0 : round256(len2 * 8));
-    if ((rc = ensure_io(c, oo + round256(out_len * 8)))) return rc;
-    char* io = (char*)c->io;
-    cudaError_t e;
-    if ((e = cudaMemcpyAsync(io + o1, in1, len1 * 8, cudaMemcpyHostToDevice, c->stream)) != cudaSuccess)
-        return set_err(FMN_ERR_CUDA, "copying in1 to the device", e);
-    if (!sqr && (e = cudaMemcpyAsync(io + o2, in2, len2 * 8, cudaMemcpyHostToDevice, c->stream)) != cudaSuccess)
-        return set_err(FMN_ERR_CUDA, "copying in2 to the device", e);
     fmn::Job j;
+    cudaError_t e;
+    {
+        std::lock_guard<std::mutex> lk(c->mu);
+        if ((rc = ensure_buf((void**)&L->io, &L->io_cap, oo + round256(out_len * 8), false))) return rc;
+    }
+    char* io = (char*)L->io;
     j.a = (const u64*)(io + o1);
     j.la = len1;
     j.b = sqr ? j.a : (const u64*)(io + o2);
     j.lb = len2;
     j.out = (u64*)(io + oo);
     j.sqr = sqr;
-    if ((rc = run_job_ctx(c, j, c->stream))) return rc;
-    if ((e = cudaMemcpyAsync(out, io + oo, out_len * 8, cudaMemcpyDeviceToHost, c->stream)) != cudaSuccess)
+    if (L->done_valid && (e = cudaStreamWaitEvent(L->s, L->done, 0)) != cudaSuccess)
+        return set_err(FMN_ERR_CUDA, "cudaStreamWaitEvent", e);
+    if ((e = cudaMemcpyAsync(io + o1, in1, len1 * 8, cudaMemcpyHostToDevice, L->s)) != cudaSuccess)
+        return set_err(FMN_ERR_CUDA, "copying in1 to the device", e);
+    if (!sqr && (e = cudaMemcpyAsync(io + o2, in2, len2 * 8, cudaMemcpyHostToDevice, L->s)) != cudaSuccess)
+        return set_err(FMN_ERR_CUDA, "copying in2 to the device", e);
+    {
+        std::lock_guard<std::mutex> lk(c->mu);
+        if ((rc = ensure_buf(&L->ws, &L->ws_cap, fmn::job_workspace_bytes(j), true))) return rc;
+        const fmn::TwiddleSet* tws =
+            fmn::job_engine(j) != fmn::ENGINE_64 ? nullptr : get_twiddles(c, ilog2_ceil(out_len - 1), L->s);
+        if ((e = fmn::enqueue_job(j, L->ws, L->ws_cap, L->s, tws)) != cudaSuccess) {
+            std::string m = std::string("kernel launch (") + fmn::launch_diag() + ")";
+            return set_err(FMN_ERR_CUDA, m.c_str(), e);
+        }
+        if ((e = cudaEventRecord(L->done, L->s)) != cudaSuccess) return set_err(FMN_ERR_CUDA, "cudaEventRecord", e);
+        L->done_valid = true;
+    }
+    if ((e = cudaMemcpyAsync(out, io + oo, out_len * 8, cudaMemcpyDeviceToHost, L->s)) != cudaSuccess)
         return set_err(FMN_ERR_CUDA, "copying the product to the host", e);
-    return take_device_error(c->ws, c->h_err, c->stream);
+    return take_device_error(L->ws, L->h_err, L->s);
 }
 
 int device_product(const u64* d1, u64 len1, const u64* d2, u64 len2, u64* dout, int sqr, void* stream) {
@@ -504,7 +606,8 @@ void fmn_shutdown(void) {
         cudaSetDevice(d);
         cudaDeviceSynchronize();
         if (c->ws) cudaFree(c->ws);
-        if (c->io) cudaFree(c->io);
+        for (HostLane* L : c->lanes) destroy_lane(L);
+        c->lanes.clear();
         if (c->h_err) cudaFreeHost(c->h_err);
         for (auto& t : c->tw) cudaFree(t.buf);
         if (c->stage) cudaFreeHost(c->stage);
@@ -513,10 +616,6 @@ void fmn_shutdown(void) {
         for (int k = 0; k <= DevCtx::NSTREAM; ++k)
             if (c->wevent[k]) cudaEventDestroy(c->wevent[k]);
         if (c->stage_free) cudaEventDestroy(c->stage_free);
-        for (int k = 0; k < 4; ++k)
-            if (c->cb_event[k]) cudaEventDestroy(c->cb_event[k]);
-        for (int k = 0; k < 8; ++k)
-            if (c->ci_event[k]) cudaEventDestroy(c->ci_event[k]);
         if (c->done) cudaEventDestroy(c->done);
         if (c->stream) cudaStreamDestroy(c->stream);
         delete c;

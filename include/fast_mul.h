@@ -53,7 +53,12 @@ void fmn_shutdown(void);
 /* Text of the last error seen by the calling thread ("" if none). */
 const char* fmn_last_error(void);
 
-/* Status-returning forms of abs_mul64 / abs_sqr64 (host pointers, synchronous). */
+/* Status-returning forms of abs_mul64 / abs_sqr64 (host pointers, synchronous).
+ * Host-pointer calls (these and abs_mul64 / abs_sqr64) may come from several threads at
+ * once: each runs on one of a few host lanes per device (FMN_HOST_LANES, 1..8, default 4;
+ * further callers wait for a free lane), with its own device workspace, operand buffers and
+ * streams, so one call's host<->device copies overlap another's kernels.  Each lane keeps
+ * device memory for the largest product it has run until fmn_shutdown(). */
 int fmn_mul(const u64* in1, u64 len1, const u64* in2, u64 len2, u64* out);
 int fmn_sqr(const u64* in1, u64 len1, u64* out);
 
