@@ -45,10 +45,8 @@ __device__ __forceinline__ u32 carry_ticket(u32* ticket) {
 // Completes the scan for limbs j0 .. j0+CE-1 of this thread (CTA `tile`, sums lo/h with the
 // contributions from lower limbs already added) and stores the final limbs.  `state` holds one
 // word per CTA (zeroed before the first launch); a look-back that waits too long sets *err.
-// With `sbuf` (shared memory, CNT rows of 2 CE + 4 words, this thread's row free to overwrite)
-// the limbs leave through it as coalesced 16-byte stores instead of per-thread runs.
 __device__ __forceinline__ void carry_finish(u64 (&lo)[CE], u32 (&h)[CE], u64 tile, u64 j0, u32* state, u32* err,
-                                             u64* out, u64 out_len, u32* sbuf = nullptr) {
+                                             u64* out, u64 out_len) {
     __shared__ u32 s_warp[CNT / 32];
     __shared__ u32 s_cin;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -150,27 +148,7 @@ __device__ __forceinline__ void carry_finish(u64 (&lo)[CE], u32 (&h)[CE], u64 ti
         c = h[e] + (t < c);
         outv[e] = t;
     }
-    if (sbuf) {
-        constexpr int PW = 2 * CE + 4;
-        u64* row = reinterpret_cast<u64*>(sbuf + tid * PW);
-#pragma unroll
-        for (int e = 0; e < CE; e += 2) *reinterpret_cast<ulonglong2*>(row + e) = make_ulonglong2(outv[e], outv[e + 1]);
-        __syncthreads();
-        const u64 jt = tile * CTILE;
-        const bool al16 = (reinterpret_cast<uintptr_t>(out) & 15) == 0;
-#pragma unroll 4
-        for (int r = tid; r < CTILE / 2; r += CNT) {   // limbs jt + 2r, jt + 2r + 1
-            const ulonglong2 v =
-                *reinterpret_cast<const ulonglong2*>(sbuf + (r / (CE / 2)) * PW + 4 * (r % (CE / 2)));
-            const u64 j = jt + 2 * (u64)r;
-            if (j + 1 < out_len && al16) {
-                *reinterpret_cast<ulonglong2*>(out + j) = v;
-            } else {
-                if (j < out_len) out[j] = v.x;
-                if (j + 1 < out_len) out[j + 1] = v.y;
-            }
-        }
-    } else if (j0 + CE <= out_len && ((reinterpret_cast<uintptr_t>(out) & 15) == 0)) {
+    if (j0 + CE <= out_len && ((reinterpret_cast<uintptr_t>(out) & 15) == 0)) {
 #pragma unroll
         for (int e = 0; e < CE; e += 2)
             *reinterpret_cast<ulonglong2*>(out + j0 + e) = make_ulonglong2(outv[e], outv[e + 1]);

@@ -649,55 +649,22 @@ __device__ __forceinline__ u128 qcoef(const QCrtArgs& a, u64 k, const PrimeQ& q0
     return qcrt(a.res[k], a.res[a.N + k], a.res[2 * a.N + k], a, q0, q1, q2);
 }
 
-// Staged form: the CTA's 3 x 2 CTILE residues arrive by coalesced 16-byte asynchronous copies
-// (zero past nvalid) into per-thread rows of CRT_PW words, padded so that the 16-byte reads
-// of 8 lanes fall on disjoint banks.
-constexpr int CRT_PW = 2 * CE + 4;
-constexpr size_t CRT_SMEM = 3 * CNT * CRT_PW * sizeof(u32);
-
-template <bool STAGE>
 __device__ __forceinline__ void qcrt_carry_body(const QCrtArgs& a, u32 ncta) {
     __shared__ u64 s_hw[CNT / 32];
-    extern __shared__ __align__(16) u32 crt_sm[];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const PrimeQ q0 = c_q[0], q1 = c_q[1], q2 = c_q[2];
     const u64 tile = carry_ticket(a.ticket);
     if (tile >= ncta) return;                          // batch launches cover the largest product
     const u64 j0 = tile * CTILE + (u64)tid * CE;       // output limbs j0 .. j0+15
     const u64 k0 = 2 * j0;                             // digit coefficients k0 .. k0+31
-    const bool staged = STAGE && (a.N & 3) == 0 && (reinterpret_cast<uintptr_t>(a.res) & 15) == 0;
-    if (staged) {
-        constexpr int CPT = 2 * CTILE / 4;             // 16-byte chunks per prime
-        const u64 kt = 2 * tile * CTILE;
-#pragma unroll 4
-        for (int qi = tid; qi < 3 * CPT; qi += CNT) {
-            const int p = qi / CPT, r = qi % CPT;
-            const u64 k = kt + 4 * (u64)r;
-            const unsigned bytes = k >= a.nvalid ? 0u : (a.nvalid - k >= 4 ? 16u : (unsigned)(a.nvalid - k) * 4u);
-            const u32* src = bytes ? a.res + (u64)p * a.N + k : a.res;
-            u32* dst = crt_sm + (p * CNT + r / (2 * CE / 4)) * CRT_PW + 4 * (r % (2 * CE / 4));
-            const unsigned sa = (unsigned)__cvta_generic_to_shared(dst);
-            asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sa), "l"(src), "r"(bytes) : "memory");
-        }
-        cp_async_commit_wait();
-        __syncthreads();
-    }
     u64 lo[CE];
     u32 h[CE];
     u64 phi = 0;                                       // C_{j-1}.hi
-    const bool full = !staged && k0 + 2 * CE <= a.nvalid;
+    const bool full = k0 + 2 * CE <= a.nvalid;
 #pragma unroll
     for (int e2 = 0; e2 < CE; e2 += 2) {              // two limbs = four coefficients at a time
         u32 r0[4], r1[4], r2[4];
-        if (staged) {
-            const u32* row = crt_sm + tid * CRT_PW + 2 * e2;
-            const uint4 v0 = *reinterpret_cast<const uint4*>(row);
-            const uint4 v1 = *reinterpret_cast<const uint4*>(row + CNT * CRT_PW);
-            const uint4 v2 = *reinterpret_cast<const uint4*>(row + 2 * CNT * CRT_PW);
-            r0[0] = v0.x, r0[1] = v0.y, r0[2] = v0.z, r0[3] = v0.w;
-            r1[0] = v1.x, r1[1] = v1.y, r1[2] = v1.z, r1[3] = v1.w;
-            r2[0] = v2.x, r2[1] = v2.y, r2[2] = v2.z, r2[3] = v2.w;
-        } else if (full) {
+        if (full) {
             const uint4 v0 = *reinterpret_cast<const uint4*>(a.res + k0 + 2 * e2);
             const uint4 v1 = *reinterpret_cast<const uint4*>(a.res + a.N + k0 + 2 * e2);
             const uint4 v2 = *reinterpret_cast<const uint4*>(a.res + 2 * a.N + k0 + 2 * e2);
@@ -709,7 +676,7 @@ __device__ __forceinline__ void qcrt_carry_body(const QCrtArgs& a, u32 ncta) {
         for (int u = 0; u < 2; ++u) {
             const int e = e2 + u;
             u128 cl, ch;
-            if (staged || full) {
+            if (full) {
                 cl = qcrt(r0[2 * u], r1[2 * u], r2[2 * u], a, q0, q1, q2);
                 ch = qcrt(r0[2 * u + 1], r1[2 * u + 1], r2[2 * u + 1], a, q0, q1, q2);
             } else {
@@ -740,21 +707,17 @@ __device__ __forceinline__ void qcrt_carry_body(const QCrtArgs& a, u32 ncta) {
         }
     }
     add_to(lo[0], h[0], nb);
-#ifdef FMN_CRT_NO_STORE_STAGE
     carry_finish(lo, h, tile, j0, a.state, a.err, a.out, a.out_len);
-#else
-    carry_finish(lo, h, tile, j0, a.state, a.err, a.out, a.out_len, staged ? crt_sm : nullptr);
-#endif
 }
 
-__global__ void __launch_bounds__(CNT, 2) k_qcrt_carry(QCrtArgs a) { qcrt_carry_body<true>(a, 0xffffffffu); }
+__global__ void __launch_bounds__(CNT, 3) k_qcrt_carry(QCrtArgs a) { qcrt_carry_body(a, 0xffffffffu); }
 
 // CRT + carry of many products: CTAs take per-product tickets; tickets beyond a product's
 // CTA count exit at once.
 __global__ void __launch_bounds__(CNT) k_qcrt_carry_batch(const QCrtArgs* __restrict__ args, u32 ctas_per_job,
                                                           const u32* __restrict__ ncta) {
     const u32 job = blockIdx.x / ctas_per_job;
-    qcrt_carry_body<false>(args[job], ncta[job]);
+    qcrt_carry_body(args[job], ncta[job]);
 }
 
 // ------------------------------------------------------------------ host: tables
@@ -962,8 +925,6 @@ static cudaError_t ensure_tables() {
                                          (int)cudaSharedmemCarveoutMaxShared);
                 if (e != cudaSuccess) return e;
             }
-    e = cudaFuncSetAttribute((const void*)k_qcrt_carry, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CRT_SMEM);
-    if (e != cudaSuccess) return e;
     done.push_back(dev);
     return cudaSuccess;
 }
@@ -1627,7 +1588,7 @@ static cudaError_t crt_launch(const QCrtArgs& ca, u64 ncta, u64 t0, u64 t1, cuda
     const u64 n = t1 - t0;
     const double crt_bytes = 3.0 * (double)ca.nvalid * 4.0 + (double)ca.out_len * 8.0;
     const ProfMark m = prof_begin(K_CRT, crt_bytes * (double)n / (double)ncta, 3.0 * (double)ca.nvalid * (double)n / (double)ncta, s);
-    k_qcrt_carry<<<(unsigned)n, CNT, CRT_SMEM, s>>>(ca);
+    k_qcrt_carry<<<(unsigned)n, CNT, 0, s>>>(ca);
     cudaError_t e = cudaGetLastError();
     prof_end(m, s);
     if (e != cudaSuccess) return e;
