@@ -1186,10 +1186,16 @@ struct QWhole {
     QRec rec[3 * MAX_PASSES + 2];
 };
 
-static void plan_whole(const Job& j, int n, u32* A, u32* B, QWhole* out) {
+// `batched`: the product is one of a batch whose launches are shared.  The tuned plans are the
+// fastest for one product on the GPU at a time; in a batch, where many products' tiles fill
+// the GPU together, the default (even) plans are faster (4096 products of 1k-100k limbs:
+// 137k against 104k products/s on B200).
+static void plan_whole(const Job& j, int n, u32* A, u32* B, QWhole* out, bool batched = false) {
     const int sqr = j.sqr ? 1 : 0;
     if (sqr || j.spectrum) B = A;
-    const Plan pl = j.spectrum && j.splan.passes ? j.splan : qplan(n);   // a spectrum keeps its plan
+    const Plan pl = j.spectrum && j.splan.passes ? j.splan                 // a spectrum keeps its plan
+                    : batched                    ? qplan_default(n)
+                                                 : qplan(n);
     const int P = pl.passes;
     const u64 N = 1ull << n;
     int logB[MAX_PASSES];
@@ -1467,7 +1473,7 @@ cudaError_t q32_batch_plan(const Job* jobs, const int* idx, int m, char* res, si
         }
         u32* ticket = (u32*)(st + *soff);
         *soff += q32_batch_state_bytes(j);
-        plan_whole(j, n, A, B, &W[t]);
+        plan_whole(j, n, A, B, &W[t], true);
         QCrtArgs& ca = C[t];
         ca = proto;
         ca.res = A;
