@@ -54,6 +54,9 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the reference CPU timing")
     ap.add_argument("--len", type=int, default=None, help="override operand length (profiling runs)")
+    ap.add_argument("--len2", type=int, default=None, help="second operand's length (default: --len)")
+    ap.add_argument("--engine", default="auto", choices=["auto", "32", "64"],
+                    help="residue engine (default: the library's cost model)")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-stream comparison")
     ap.add_argument("--batch-only", action="store_true", help="only the batched-stream comparison")
     ap.add_argument("--batch-count", type=int, default=4096)
@@ -416,6 +419,8 @@ def run_ours(args, ws, rank, local):
         torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     fmn.init(local)
+    if args.engine != "auto":
+        fmn.set_engine(fmn.ENGINE_32 if args.engine == "32" else fmn.ENGINE_64)
     if args.batch_only:
         print(json.dumps(batch_compare(fmn, torch, dev, args.batch_count)), flush=True)
         return
@@ -423,7 +428,7 @@ def run_ours(args, ws, rank, local):
         print(json.dumps(serve_compare(fmn, torch, dev, args.serve_requests, args.serve_rate)), flush=True)
         return
     l1 = args.len or LEN1
-    l2 = args.len or LEN2
+    l2 = args.len2 or args.len or LEN2
     a, b = synth.operands(KIND, l1, l2, SEED)
     da = torch.from_numpy(a.view(np.int64)).to(dev)
     db = torch.from_numpy(b.view(np.int64)).to(dev)
@@ -554,7 +559,7 @@ def run_ours(args, ws, rank, local):
             "warmup": args.warmup, "ms_per_step": per_step_ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u32" if engine == fmn.ENGINE_32 else "u64",
             "data": DATA,
-            "config": {"workload": WORKLOAD if l1 == LEN1 else f"abs_mul64 {l1} x {l2} limbs",
+            "config": {"workload": WORKLOAD if (l1, l2) == (LEN1, LEN2) else f"abs_mul64 {l1} x {l2} limbs",
                        "len1": l1, "len2": l2,
                        "engine": ("32-bit digits mod three 31-bit primes" if engine == fmn.ENGINE_32
                                   else "64-bit limbs mod the reference's three 62-bit primes"),
@@ -600,14 +605,14 @@ def run_ours(args, ws, rank, local):
     if dist:
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
-    if rank == 0 and not args.no_batch and l1 == LEN1:
+    if rank == 0 and not args.no_batch and (l1, l2) == (LEN1, LEN2):
         del da, db, dout
         torch.cuda.empty_cache()
         result["batch"] = batch_compare(fmn, torch, dev, args.batch_count)
-    if rank == 0 and not args.no_serve and l1 == LEN1:
+    if rank == 0 and not args.no_serve and (l1, l2) == (LEN1, LEN2):
         torch.cuda.empty_cache()
         result["serve"] = serve_compare(fmn, torch, dev, args.serve_requests, args.serve_rate)
-    if rank == 0 and ws == 1 and not args.no_cpu_baseline and l1 == LEN1:
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline and (l1, l2) == (LEN1, LEN2):
         cb, cout = cpu_baseline(a, b)
         cb["bit_exact_vs_gpu"] = bool(np.array_equal(cout, got))
         result["cpu_baseline"] = cb

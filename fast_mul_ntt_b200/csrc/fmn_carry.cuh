@@ -42,10 +42,12 @@ __device__ __forceinline__ u32 carry_ticket(u32* ticket) {
     return s_tile;
 }
 
-// Completes the scan for limbs j0 .. j0+CE-1 of this thread (CTA `tile`, sums lo/h with the
-// contributions from lower limbs already added) and stores the final limbs.  `state` holds one
-// word per CTA (zeroed before the first launch); a look-back that waits too long sets *err.
-__device__ __forceinline__ void carry_finish(u64 (&lo)[CE], u32 (&h)[CE], u64 tile, u64 j0, u32* state, u32* err,
+// Completes the scan for limbs j0 .. j0+NE-1 of this thread (CTA `tile` of CNT * NE limbs,
+// sums lo/h with the contributions from lower limbs already added) and stores the final limbs.
+// `state` holds one word per CTA (zeroed before the first launch); a look-back that waits too
+// long sets *err.
+template <int NE>
+__device__ __forceinline__ void carry_finish(u64 (&lo)[NE], u32 (&h)[NE], u64 tile, u64 j0, u32* state, u32* err,
                                              u64* out, u64 out_len) {
     __shared__ u32 s_warp[CNT / 32];
     __shared__ u32 s_cin;
@@ -55,7 +57,7 @@ __device__ __forceinline__ void carry_finish(u64 (&lo)[CE], u32 (&h)[CE], u64 ti
     // from 3 agree; the chains from 1 and 2 run only in warps where some lane needs them.
     auto chain = [&](u64 c) {
 #pragma unroll
-        for (int e = 0; e < CE; ++e) {
+        for (int e = 0; e < NE; ++e) {
             const u64 t = lo[e] + c;
             c = h[e] + (t < c);
         }
@@ -141,20 +143,20 @@ __device__ __forceinline__ void carry_finish(u64 (&lo)[CE], u32 (&h)[CE], u64 ti
     }
     __syncthreads();
     u64 c = fn_apply(exc, fn_apply(s_warp[warp], s_cin));
-    u64 outv[CE];
+    u64 outv[NE];
 #pragma unroll
-    for (int e = 0; e < CE; ++e) {
+    for (int e = 0; e < NE; ++e) {
         const u64 t = lo[e] + c;
         c = h[e] + (t < c);
         outv[e] = t;
     }
-    if (j0 + CE <= out_len && ((reinterpret_cast<uintptr_t>(out) & 15) == 0)) {
+    if (j0 + NE <= out_len && ((reinterpret_cast<uintptr_t>(out) & 15) == 0)) {
 #pragma unroll
-        for (int e = 0; e < CE; e += 2)
+        for (int e = 0; e < NE; e += 2)
             *reinterpret_cast<ulonglong2*>(out + j0 + e) = make_ulonglong2(outv[e], outv[e + 1]);
     } else {
 #pragma unroll
-        for (int e = 0; e < CE; ++e)
+        for (int e = 0; e < NE; ++e)
             if (j0 + e < out_len) out[j0 + e] = outv[e];
     }
 }

@@ -65,9 +65,24 @@ __device__ __forceinline__ u32 qroot(u32 x, int pi, const PrimeQ& q) {
 }
 
 constexpr int TP = TC + 1;              // padded row pitch of a shared-memory tile (words)
-// Odd columns swap the two halves of the row (c ^ 16), a permutation within the row: a warp
-// that covers 16 rows of two adjacent columns then touches two disjoint bank ranges.
-__device__ __forceinline__ int tix(int j, int c) { return j * TP + (c ^ ((c & 1) << 4)); }
+// Element (row j, column c) of a 2^LOGL-row tile sits at j * 33 + c', c' a permutation of the
+// columns within the row.  Rounds with a thread per column (lanes on the 32 columns of a row)
+// are conflict-free for any permutation.  The first round of a contiguous pass puts the lanes
+// of a warp on G consecutive rows of 32 / G adjacent columns (G = 2^LOGL over its radix), so
+// those columns must start G banks apart: c' rotates c right by log2(32 / G) bits (for LOGL
+// 5..8; 2-way conflicts on every access of that round with a fixed swizzle).  Other sizes
+// keep c ^ 16 (c & 1), which also suits the row-wise copy-out of tiles of < 32 rows.
+template <int LOGL>
+__device__ __forceinline__ int tix(int j, int c) {
+    if constexpr (LOGL >= 5 && LOGL <= 8) {
+        constexpr int G = (1 << LOGL) >> round_bits(LOGL, 0);
+        constexpr int w = G >= 32 ? 0 : (G == 16 ? 1 : G == 8 ? 2 : G == 4 ? 3 : G == 2 ? 4 : 5);
+        static_assert(G >= 2 && G <= 16, "first-round groups per column");
+        return j * TP + (((c >> w) | (c << (5 - w))) & (TC - 1));
+    } else {
+        return j * TP + (c ^ ((c & 1) << 4));
+    }
+}
 // Dense tiles (row pitch 32 words, rows 16-byte aligned) for strided passes, whose rounds all
 // run with the 32 lanes of a warp on the 32 columns of one row: conflict-free without
 // padding, and each row is a 128-byte copy target.
@@ -212,8 +227,8 @@ __device__ __forceinline__ void rounds(u32* sm, LD0 ld0, STL stl, int pi, const 
     constexpr int RB = round_bits(LOGL, FR), TOP = round_top(LOGL, FR);
     constexpr bool QF = CONTIG && (TOP == LOGL - 1);
     static_assert(!(DENSE && CONTIG), "dense tiles serve strided passes only");
-    auto lds = [sm](int j, int c) { return sm[DENSE ? dix(j, c) : tix(j, c)]; };
-    auto sts = [sm](int j, int c, u32 v) { sm[DENSE ? dix(j, c) : tix(j, c)] = v; };
+    auto lds = [sm](int j, int c) { return sm[DENSE ? dix(j, c) : tix<LOGL>(j, c)]; };
+    auto sts = [sm](int j, int c, u32 v) { sm[DENSE ? dix(j, c) : tix<LOGL>(j, c)] = v; };
     if constexpr (NR == 1) {
         run_round<LOGL, RB, TOP, INV, QF, GST, GLD>(ld0, stl, pi, q);
     } else if constexpr (IDX == 0) {
@@ -379,13 +394,13 @@ __device__ __forceinline__ void body_fwd_last(u32* sm, const QArgs& a, u64 tile,
     } else {
         // the last round (a thread per column) writes the tile; the blocks then leave row by
         // row with the lanes of a warp on consecutive words (128-byte stores)
-        auto sts = [sm](int j, int c, u32 v) { sm[tix(j, c)] = v; };
+        auto sts = [sm](int j, int c, u32 v) { sm[tix<LOGL>(j, c)] = v; };
         rounds<LOGL, false, true, 0, false>(sm, ld0, sts, pi, q);
         __syncthreads();
 #pragma unroll 4
         for (int e = threadIdx.x; e < TC * L; e += NT) {
             const int c = e >> LOGL, j = e & (L - 1);
-            if (c < ncols) d[gbase + (u32)c * L + j] = sm[tix(j, c)];
+            if (c < ncols) d[gbase + (u32)c * L + j] = sm[tix<LOGL>(j, c)];
         }
     }
 }
@@ -428,7 +443,7 @@ __device__ __forceinline__ void fused_lowest(LD ld, ST st, const u32* __restrict
                 for (int t = 0; t < R; ++t) x[t] = qmont(x[t], x[t], q);
             } else if constexpr (OTH == 1) {
 #pragma unroll
-                for (int t = 0; t < R; ++t) x[t] = qmont(x[t], oth[tix(row0 + t, c)], q);
+                for (int t = 0; t < R; ++t) x[t] = qmont(x[t], oth[tix<LOGL>(row0 + t, c)], q);
             } else if constexpr (OTH == 2) {
                 u32 y[R];
                 ld_vec(oth + c * (L + 4) + row0, y);      // 8 lanes per phase on disjoint banks
@@ -479,8 +494,8 @@ __device__ __forceinline__ void body_fused(u32* sm, const QArgs& a, u64 tile, in
     auto stg = [=](int j, int c, u32 v) {
         if (c < ncols) dd[gbase + (u32)c * L + j] = v;
     };
-    auto lds = [sm](int j, int c) { return sm[tix(j, c)]; };
-    auto sts = [sm](int j, int c, u32 v) { sm[tix(j, c)] = v; };
+    auto lds = [sm](int j, int c) { return sm[tix<LOGL>(j, c)]; };
+    auto sts = [sm](int j, int c, u32 v) { sm[tix<LOGL>(j, c)] = v; };
     if constexpr (LOGL == 0) {
         if (threadIdx.x < (unsigned)ncols) {
             const int c = threadIdx.x;
@@ -535,12 +550,12 @@ __device__ __forceinline__ void body_fused2(u32* sm, const QArgs& a, u64 tile, i
     u32* __restrict__ o = a.other + (u64)pi * a.N;
     u32* smA = sm + TP * L;
     auto ldA = [=](int j, int c) -> u32 { return o[gbase + (u32)c * L + j]; };
-    auto stA = [smA](int j, int c, u32 v) { smA[tix(j, c)] = v; };
+    auto stA = [smA](int j, int c, u32 v) { smA[tix<LOGL>(j, c)] = v; };
     rounds<LOGL, false, true, 0>(smA, ldA, stA, pi, q);
     auto ldg = [=](int j, int c) -> u32 { return d[gbase + (u32)c * L + j]; };
     auto stg = [=](int j, int c, u32 v) { o[gbase + (u32)c * L + j] = v; };
-    auto lds = [sm](int j, int c) { return sm[tix(j, c)]; };
-    auto sts = [sm](int j, int c, u32 v) { sm[tix(j, c)] = v; };
+    auto lds = [sm](int j, int c) { return sm[tix<LOGL>(j, c)]; };
+    auto sts = [sm](int j, int c, u32 v) { sm[tix<LOGL>(j, c)] = v; };
     constexpr int RB0 = round_bits(LOGL, 0);
     run_round<LOGL, RB0, LOGL - 1, false, true>(ldg, sts, pi, q);
     __syncthreads();                                   // also publishes smA
@@ -624,6 +639,11 @@ struct QCrtArgs {
 
 typedef unsigned __int128 u128;
 constexpr u64 Q01 = (u64)Q32_P0 * Q32_P1;
+#ifndef FMN_QCE
+#define FMN_QCE 16
+#endif
+constexpr int QCE = FMN_QCE;            // output limbs per thread of the CRT + carry kernel
+constexpr u64 QCTILE = (u64)CNT * QCE;  // output limbs per CTA
 
 __device__ __forceinline__ u128 qcrt(u32 r0, u32 r1, u32 r2, const QCrtArgs& a, const PrimeQ& q0, const PrimeQ& q1,
                                      const PrimeQ& q2) {
@@ -655,14 +675,14 @@ __device__ __forceinline__ void qcrt_carry_body(const QCrtArgs& a, u32 ncta) {
     const PrimeQ q0 = c_q[0], q1 = c_q[1], q2 = c_q[2];
     const u64 tile = carry_ticket(a.ticket);
     if (tile >= ncta) return;                          // batch launches cover the largest product
-    const u64 j0 = tile * CTILE + (u64)tid * CE;       // output limbs j0 .. j0+15
+    const u64 j0 = tile * QCTILE + (u64)tid * QCE;     // output limbs j0 .. j0+QCE-1
     const u64 k0 = 2 * j0;                             // digit coefficients k0 .. k0+31
-    u64 lo[CE];
-    u32 h[CE];
+    u64 lo[QCE];
+    u32 h[QCE];
     u64 phi = 0;                                       // C_{j-1}.hi
-    const bool full = k0 + 2 * CE <= a.nvalid;
+    const bool full = k0 + 2 * QCE <= a.nvalid;
 #pragma unroll
-    for (int e2 = 0; e2 < CE; e2 += 2) {              // two limbs = four coefficients at a time
+    for (int e2 = 0; e2 < QCE; e2 += 2) {             // two limbs = four coefficients at a time
         u32 r0[4], r1[4], r2[4];
         if (full) {
             const uint4 v0 = *reinterpret_cast<const uint4*>(a.res + k0 + 2 * e2);
@@ -710,7 +730,7 @@ __device__ __forceinline__ void qcrt_carry_body(const QCrtArgs& a, u32 ncta) {
     carry_finish(lo, h, tile, j0, a.state, a.err, a.out, a.out_len);
 }
 
-__global__ void __launch_bounds__(CNT, 3) k_qcrt_carry(QCrtArgs a) { qcrt_carry_body(a, 0xffffffffu); }
+__global__ void __launch_bounds__(CNT, QCE <= 8 ? 4 : 3) k_qcrt_carry(QCrtArgs a) { qcrt_carry_body(a, 0xffffffffu); }
 
 // CRT + carry of many products: CTAs take per-product tickets; tickets beyond a product's
 // CTA count exit at once.
@@ -1083,7 +1103,7 @@ static QJob plan_job(u64 la, u64 lb, int sqr) {
     }
     if (!J.ok) return J;
     J.cost = best;
-    J.ncta = (out_len + CTILE - 1) / CTILE;
+    J.ncta = (out_len + QCTILE - 1) / QCTILE;
     size_t off = 256;
     J.a = off;
     off = align256(off + 3 * J.N * sizeof(u32));
@@ -1113,7 +1133,7 @@ static QJob plan_resident(const Job& j) {
     J.m = 1;
     J.n = j.log_n;
     J.N = 1ull << j.log_n;
-    J.ncta = (out_len + CTILE - 1) / CTILE;
+    J.ncta = (out_len + QCTILE - 1) / QCTILE;
     size_t off = 256;
     J.a = J.b = off;
     off = align256(off + 3 * J.N * sizeof(u32));
@@ -1432,7 +1452,7 @@ size_t q32_batch_res_bytes(const Job& j) {
 }
 
 size_t q32_batch_state_bytes(const Job& j) {
-    const u64 ncta = (j.la + j.lb + CTILE - 1) / CTILE;
+    const u64 ncta = (j.la + j.lb + q32::QCTILE - 1) / q32::QCTILE;
     return 16 + ((ncta * sizeof(u32) + 15) & ~(size_t)15);
 }
 
@@ -1484,7 +1504,7 @@ cudaError_t q32_batch_plan(const Job* jobs, const int* idx, int m, char* res, si
         ca.ticket = ticket;
         ca.state = ticket + 4;
         ca.err = err;
-        nc[t] = (u32)((out_len + CTILE - 1) / CTILE);
+        nc[t] = (u32)((out_len + QCTILE - 1) / QCTILE);
         if (nc[t] > maxc) maxc = nc[t];
         if (W[t].count != W[0].count) return cudaErrorInvalidValue;
     }
@@ -1598,7 +1618,7 @@ static cudaError_t crt_launch(const QCrtArgs& ca, u64 ncta, u64 t0, u64 t1, cuda
     cudaError_t e = cudaGetLastError();
     prof_end(m, s);
     if (e != cudaSuccess) return e;
-    const u64 lo = t0 * CTILE, hi = t1 * CTILE < ca.out_len ? t1 * CTILE : ca.out_len;
+    const u64 lo = t0 * QCTILE, hi = t1 * QCTILE < ca.out_len ? t1 * QCTILE : ca.out_len;
     if (after_chunk) return after_chunk(ctx, lo, hi);
     return cudaSuccess;
 }
@@ -1723,7 +1743,7 @@ cudaError_t q32_enqueue(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s,
             pa.acc = nullptr;
             if (after_chunk && k + 1 < J.m) {
                 fill_crt(j, J, base, out_len, &ca);
-                const u64 t_end = (first + J.cb) / CTILE;
+                const u64 t_end = (first + J.cb) / QCTILE;
                 if (t_end > crt_done && (e = crt_launch(ca, J.ncta, crt_done, t_end, s, after_chunk, ctx)) != cudaSuccess)
                     return e;
                 if (t_end > crt_done) crt_done = t_end;
