@@ -350,20 +350,22 @@ __device__ __forceinline__ void body_inv(u32* sm, const QArgs& a, u64 tile, int 
         u32* __restrict__ acc = a.acc + (u64)pi * a.acc_stride;
         const u64 valid = a.acc_valid, fresh = a.acc_fresh;
         constexpr int H = R0 < 8 ? R0 : 8;             // eight loads in flight at a time
+        const u32 S0 = (u32)SP0 << logS;               // row stride of the group's outputs
         auto stl = [=](int row0, int c, const auto& x) {
             const u32 i0 = gbase + c + ((u32)row0 << logS);
+            u32* __restrict__ pa = acc + i0;
 #pragma unroll
             for (int h = 0; h < R0; h += H) {
                 u32 old[H];
 #pragma unroll
                 for (int t = 0; t < H; ++t) {
-                    const u32 i = i0 + ((u32)((h + t) * SP0) << logS);
-                    old[t] = i < fresh ? acc[i] : 0u;
+                    const u32 off = (u32)(h + t) * S0;
+                    old[t] = i0 + off < fresh ? pa[off] : 0u;
                 }
 #pragma unroll
                 for (int t = 0; t < H; ++t) {
-                    const u32 i = i0 + ((u32)((h + t) * SP0) << logS);
-                    if (i < valid) acc[i] = i < fresh ? qadd(old[t], x[h + t], q) : x[h + t];
+                    const u32 off = (u32)(h + t) * S0;
+                    if (i0 + off < valid) pa[off] = i0 + off < fresh ? qadd(old[t], x[h + t], q) : x[h + t];
                 }
             }
         };
@@ -639,10 +641,10 @@ struct QCrtArgs {
 
 typedef unsigned __int128 u128;
 constexpr u64 Q01 = (u64)Q32_P0 * Q32_P1;
-#ifndef FMN_QCE
-#define FMN_QCE 16
-#endif
-constexpr int QCE = FMN_QCE;            // output limbs per thread of the CRT + carry kernel
+// Output limbs per thread of the CRT + carry kernel: 8 (half the 64-bit engine's 16) keeps a
+// thread's sums in 57 registers, so 4 CTAs share an SM where 16 allowed 3 (0.28 -> 0.23 ms at
+// 10M x 10M; the kernel waits on its look-back and loads, and more CTAs cover the waits).
+constexpr int QCE = 8;
 constexpr u64 QCTILE = (u64)CNT * QCE;  // output limbs per CTA
 
 __device__ __forceinline__ u128 qcrt(u32 r0, u32 r1, u32 r2, const QCrtArgs& a, const PrimeQ& q0, const PrimeQ& q1,
