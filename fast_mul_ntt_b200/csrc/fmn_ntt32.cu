@@ -126,6 +126,10 @@ struct QArgs {
     u64 acc_stride;
     u64 acc_valid;
     u64 acc_fresh;
+    // strided passes: the four-step twiddles of this pass as Shoup pairs, [prime][k][i] with
+    // 2^logB entries per prime (frequency k of the column transform, column i), or null to
+    // compute them from the root tables
+    const uint2* tw;
 };
 
 // ------------------------------------------------------------------ one round
@@ -272,6 +276,14 @@ __device__ __forceinline__ u32 group_alpha(u32 i, int row0, int shift, int pi, c
     return qroot(x, pi, q);
 }
 
+// Table twiddles of a group of the lowest round (rows row0 .. row0 + 2^RB - 1 of column c):
+// element t has frequency k = bitrev(row0 + t) over LOGL bits, entry k * 2^logS + col.
+template <int LOGL, int RB>
+__device__ __forceinline__ const uint2* tw_group(const uint2* tw, u32 col, int row0, int logS) {
+    const u32 kq = LOGL > RB ? __brev((u32)(row0 >> RB)) >> (32 - (LOGL - RB)) : 0u;
+    return tw + ((kq << logS) + col);
+}
+
 // Forward strided pass (pass p < P-1 of a multi-pass transform).
 template <int LOGL, bool ENTRY>
 __device__ __forceinline__ void body_fwd(u32* sm, const QArgs& a, u64 tile, int pi, const PrimeQ& q) {
@@ -290,8 +302,9 @@ __device__ __forceinline__ void body_fwd(u32* sm, const QArgs& a, u64 tile, int 
     // entry pass reads the caller's limbs directly (8-byte alignment only, zero past the end).
     constexpr bool STAGED = !ENTRY;
     u32* beta = sm + (STAGED ? TC : TP) * L;
+    const uint2* __restrict__ tw = a.tw ? a.tw + ((u64)pi << a.logB) : nullptr;
     if constexpr (STAGED) stage_tile<L>(sm, d + gbase, logS);
-    fill_beta<LOGL, false>(beta, col0, shift, pi, q);     // read after the first round's barrier
+    if (!tw) fill_beta<LOGL, false>(beta, col0, shift, pi, q);   // read after the first round's barrier
     if constexpr (STAGED) {
         cp_async_commit_wait();
         __syncthreads();
@@ -303,13 +316,24 @@ __device__ __forceinline__ void body_fwd(u32* sm, const QArgs& a, u64 tile, int 
         else return d[g];
     };
     auto stl = [=](int row0, int c, const auto& x) {
-        const u32 al = group_alpha<LOGL, false>(col0 + c, row0, shift, pi, q);
         u32* __restrict__ po = d + (gbase + c + ((u32)row0 << logS));
         const u32 S = 1u << logS;                 // row stride: t * S is a multiply-add address
+        if (tw) {
+            const uint2* __restrict__ tg = tw_group<LOGL, RB>(tw, col0 + c, row0, logS);
+            const u32 ST = S << (LOGL - RB);      // table stride between the group's frequencies
 #pragma unroll
-        for (int t = 0; t < R; ++t) {
-            const int tp = RB ? (int)(__brev((u32)t) >> (32 - RB)) : 0;
-            po[(u32)t * S] = qmont(x[t], qmont_lazy(al, beta[tp * TC + c], q), q);
+            for (int t = 0; t < R; ++t) {
+                const u32 tp = RB ? __brev((u32)t) >> (32 - RB) : 0u;
+                const uint2 w = __ldg(tg + tp * ST);
+                po[(u32)t * S] = qsmul(x[t], w.x, w.y, q);
+            }
+        } else {
+            const u32 al = group_alpha<LOGL, false>(col0 + c, row0, shift, pi, q);
+#pragma unroll
+            for (int t = 0; t < R; ++t) {
+                const int tp = RB ? (int)(__brev((u32)t) >> (32 - RB)) : 0;
+                po[(u32)t * S] = qmont(x[t], qmont_lazy(al, beta[tp * TC + c], q), q);
+            }
         }
     };
     rounds<LOGL, false, false, 0, true, false, STAGED>(sm, ld0, stl, pi, q);
@@ -329,18 +353,30 @@ __device__ __forceinline__ void body_inv(u32* sm, const QArgs& a, u64 tile, int 
     u32* __restrict__ d = a.data + (u64)pi * a.N;
     const int shift = Q32_MAX_LOG_N - a.logB;
     u32* beta = sm + TC * L;
+    const uint2* __restrict__ tw = a.tw ? a.tw + ((u64)pi << a.logB) : nullptr;
     stage_tile<L>(sm, d + gbase, logS);                   // in flight during fill_beta
-    fill_beta<LOGL, true>(beta, col0, shift, pi, q);
+    if (!tw) fill_beta<LOGL, true>(beta, col0, shift, pi, q);
     cp_async_commit_wait();
     __syncthreads();
     auto ld0 = [=](int row0, int c, auto& x) {
 #pragma unroll
         for (int t = 0; t < R; ++t) x[t] = sm[dix(row0 + t, c)];
-        const u32 al = group_alpha<LOGL, true>(col0 + c, row0, shift, pi, q);
+        if (tw) {
+            const uint2* __restrict__ tg = tw_group<LOGL, RB>(tw, col0 + c, row0, logS);
+            const u32 ST = (1u << logS) << (LOGL - RB);
 #pragma unroll
-        for (int t = 0; t < R; ++t) {
-            const int tp = RB ? (int)(__brev((u32)t) >> (32 - RB)) : 0;
-            x[t] = qmont(x[t], qmont_lazy(al, beta[tp * TC + c], q), q);
+            for (int t = 0; t < R; ++t) {
+                const u32 tp = RB ? __brev((u32)t) >> (32 - RB) : 0u;
+                const uint2 w = __ldg(tg + tp * ST);
+                x[t] = qsmul(x[t], w.x, w.y, q);
+            }
+        } else {
+            const u32 al = group_alpha<LOGL, true>(col0 + c, row0, shift, pi, q);
+#pragma unroll
+            for (int t = 0; t < R; ++t) {
+                const int tp = RB ? (int)(__brev((u32)t) >> (32 - RB)) : 0;
+                x[t] = qmont(x[t], qmont_lazy(al, beta[tp * TC + c], q), q);
+            }
         }
     };
     if constexpr (ACC) {
@@ -371,8 +407,15 @@ __device__ __forceinline__ void body_inv(u32* sm, const QArgs& a, u64 tile, int 
         };
         rounds<LOGL, true, false, 0, true, true, true>(sm, ld0, stl, pi, q);
     } else {
-        auto stl = [=](int j, int c, u32 v) { d[gbase + c + ((u32)j << logS)] = v; };
-        rounds<LOGL, true, false, 0, false, true, true>(sm, ld0, stl, pi, q);
+        // rows row0 + t * SP0 of one column (the last inverse round), by pointer and stride
+        constexpr int RB0 = round_bits(LOGL, 0), R0 = 1 << RB0, SP0 = 1 << (LOGL - RB0);
+        const u32 S0 = (u32)SP0 << logS;
+        auto stl = [=](int row0, int c, const auto& x) {
+            u32* __restrict__ po = d + (gbase + c + ((u32)row0 << logS));
+#pragma unroll
+            for (int t = 0; t < R0; ++t) po[(u32)t * S0] = x[t];
+        };
+        rounds<LOGL, true, false, 0, true, true, true>(sm, ld0, stl, pi, q);
     }
 }
 
@@ -1208,11 +1251,83 @@ struct QWhole {
     QRec rec[3 * MAX_PASSES + 2];
 };
 
+// ---- four-step twiddle tables of strided passes: w_B^(+-i k) as Shoup pairs for every column
+// i and frequency k of a pass over blocks of B = 2^logB <= 2^TW_MAX_LOGB digits (B entries per
+// prime and direction, 8 MB at most), so such a pass multiplies each digit by one table entry
+// read from L2 instead of forming the twiddle from two Montgomery products.
+constexpr int TW_MAX_LOGB = 20;
+
+__global__ void __launch_bounds__(256) k_qtw_build(uint2* T, int logB, int logS, int inv) {
+    const int pi = blockIdx.y;
+    const PrimeQ q = c_q[pi];
+    const u32 B = 1u << logB;
+    for (u32 e = blockIdx.x * blockDim.x + threadIdx.x; e < B; e += gridDim.x * blockDim.x) {
+        const u32 k = e >> logS, i = e & ((1u << logS) - 1);
+        u32 x = (i * k) << (Q32_MAX_LOG_N - logB);              // i k < B: w_B^(i k) = w_2^26^x
+        if (inv) x = (0u - x) & MASK_N;
+        const u32 w = qmont(qroot(x, pi, q), 1u, q);             // out of Montgomery form
+        T[(u64)pi * B + e] = make_uint2(w, (u32)(((u64)w << 32) / q.p));
+    }
+}
+
+struct TwPass {
+    const uint2* fwd = nullptr;
+    const uint2* inv = nullptr;
+};
+struct TwEntry {
+    int dev, logB, logl;
+    uint2* buf;
+};
+static std::mutex g_tw_mu;
+static std::vector<TwEntry> g_tw;
+
+// The tables of a strided pass of 2^logl rows over 2^logB-digit blocks on the current device:
+// built on s and finished the first time (not while s is being captured into a graph, nor
+// beyond TW_MAX_LOGB); empty when unavailable, and the pass then computes its twiddles.
+static TwPass tw_tables(int logB, int logl, cudaStream_t s) {
+    TwPass r;
+    if (logB > TW_MAX_LOGB) return r;
+    int dev = 0;
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaStreamIsCapturing(s, &cap) != cudaSuccess) {
+        cudaGetLastError();
+        return r;
+    }
+    const size_t per = (size_t)3 << logB;
+    std::lock_guard<std::mutex> lk(g_tw_mu);
+    for (const TwEntry& t : g_tw)
+        if (t.dev == dev && t.logB == logB && t.logl == logl) {
+            r.fwd = t.buf;
+            r.inv = t.buf + per;
+            return r;
+        }
+    if (cap != cudaStreamCaptureStatusNone) return r;
+    uint2* buf = nullptr;
+    if (cudaMalloc(&buf, 2 * per * sizeof(uint2)) != cudaSuccess) {
+        cudaGetLastError();
+        return r;
+    }
+    const unsigned bx = (unsigned)(((1ull << logB) + 255) / 256 < 1024 ? ((1ull << logB) + 255) / 256 : 1024);
+    k_qtw_build<<<dim3(bx, 3), 256, 0, s>>>(buf, logB, logB - logl, 0);
+    k_qtw_build<<<dim3(bx, 3), 256, 0, s>>>(buf + per, logB, logB - logl, 1);
+    if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(s) != cudaSuccess) {
+        cudaGetLastError();
+        cudaFree(buf);
+        return r;
+    }
+    g_tw.push_back(TwEntry{dev, logB, logl, buf});
+    r.fwd = buf;
+    r.inv = buf + per;
+    return r;
+}
+
 // `batched`: the product is one of a batch whose launches are shared.  The tuned plans are the
 // fastest for one product on the GPU at a time; in a batch, where many products' tiles fill
 // the GPU together, the default (even) plans are faster (4096 products of 1k-100k limbs:
 // 137k against 104k products/s on B200).
-static void plan_whole(const Job& j, int n, u32* A, u32* B, QWhole* out, bool batched = false) {
+// `tws`: per pass, its twiddle tables (null: computed in the kernels).
+static void plan_whole(const Job& j, int n, u32* A, u32* B, QWhole* out, bool batched = false,
+                       const TwPass* tws = nullptr) {
     const int sqr = j.sqr ? 1 : 0;
     if (sqr || j.spectrum) B = A;
     const Plan pl = j.spectrum && j.splan.passes ? j.splan                 // a spectrum keeps its plan
@@ -1245,8 +1360,10 @@ static void plan_whole(const Job& j, int n, u32* A, u32* B, QWhole* out, bool ba
             pa.len = len;
             pa.data = data;
             pa.logB = logB[p];
+            pa.tw = tws ? tws[p].fwd : nullptr;
             add(p == 0 ? V_FWD_E : V_FWD, pl.bits[p], N >> (pl.bits[p] + LOG_TC));
         }
+        pa.tw = nullptr;
     };
     const bool merged = !sqr && !j.spectrum && P >= 2 && lastl >= 5 && lastl <= 8;
     if (j.spectrum) {
@@ -1307,6 +1424,7 @@ static void plan_whole(const Job& j, int n, u32* A, u32* B, QWhole* out, bool ba
     for (int p = P - 2; p >= 0; --p) {
         pa.data = A;
         pa.logB = logB[p];
+        pa.tw = tws ? tws[p].inv : nullptr;
         add(V_INV, pl.bits[p], N >> (pl.bits[p] + LOG_TC));
     }
 }
@@ -1649,6 +1767,8 @@ cudaError_t q32_enqueue(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s,
     const u64 tiles_last = (nblk_last + TC - 1) / TC;
     const int ncols_last = nblk_last < (u64)TC ? (int)nblk_last : TC;
     Launcher launch{j, s, need_b, need_ctx, N};
+    TwPass tws[MAX_PASSES];
+    for (int p = 0; p + 1 < P; ++p) tws[p] = tw_tables(logB[p], pl.bits[p], s);
 
     QArgs pa;
     memset(&pa, 0, sizeof(pa));
@@ -1660,7 +1780,9 @@ cudaError_t q32_enqueue(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s,
             pa.len = len;
             pa.data = data;
             pa.logB = logB[p];
+            pa.tw = tws[p].fwd;
             cudaError_t e2 = launch(p == 0 ? V_FWD_E : V_FWD, pl.bits[p], pa, N >> (pl.bits[p] + LOG_TC));
+            pa.tw = nullptr;
             if (e2 != cudaSuccess) return e2;
         }
         return cudaSuccess;
@@ -1674,7 +1796,9 @@ cudaError_t q32_enqueue(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s,
         for (int p = P - 2; p >= last_p; --p) {
             pa.data = data;
             pa.logB = logB[p];
+            pa.tw = tws[p].inv;
             cudaError_t e2 = launch(V_INV, pl.bits[p], pa, N >> (pl.bits[p] + LOG_TC));
+            pa.tw = nullptr;
             if (e2 != cudaSuccess) return e2;
         }
         return cudaSuccess;
@@ -1688,7 +1812,7 @@ cudaError_t q32_enqueue(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s,
         u32* A = (u32*)(base + J.a);
         u32* B = sqr ? A : (u32*)(base + J.b);
         QWhole W;
-        plan_whole(j, J.n, A, B, &W);
+        plan_whole(j, J.n, A, B, &W, false, tws);
         bool have_b = sqr != 0;
         for (int k = 0; k < W.count; ++k) {
             if (!have_b && W.rec[k].a.src == j.b) {            // the second operand's first reader
@@ -1741,7 +1865,10 @@ cudaError_t q32_enqueue(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s,
             pa.acc_stride = J.stride;
             pa.acc_valid = 2 * (J.ls + len) - 1;
             pa.acc_fresh = k == 0 ? 0 : 2 * J.ls - 1;
-            if ((e = launch(V_INV_ACC, pl.bits[0], pa, N >> (pl.bits[0] + LOG_TC))) != cudaSuccess) return e;
+            pa.tw = tws[0].inv;
+            e = launch(V_INV_ACC, pl.bits[0], pa, N >> (pl.bits[0] + LOG_TC));
+            pa.tw = nullptr;
+            if (e != cudaSuccess) return e;
             pa.acc = nullptr;
             if (after_chunk && k + 1 < J.m) {
                 fill_crt(j, J, base, out_len, &ca);
