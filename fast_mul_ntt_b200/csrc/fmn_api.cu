@@ -124,6 +124,7 @@ int get_ctx(DevCtx** out) {
         }
         g_ctx[dev] = c;
         fmn_load_default_plans();              // tuned plans for this GPU, if a plan file matches
+        fmn::q32_prepare_tables();             // best effort: a pass without a table computes its twiddles
     }
     *out = g_ctx[dev];
     return FMN_OK;
@@ -608,6 +609,7 @@ void fmn_shutdown(void) {
         if (c->ws) cudaFree(c->ws);
         for (HostLane* L : c->lanes) destroy_lane(L);
         c->lanes.clear();
+        fmn::q32_release_tables(d);
         if (c->h_err) cudaFreeHost(c->h_err);
         for (auto& t : c->tw) cudaFree(t.buf);
         if (c->stage) cudaFreeHost(c->stage);

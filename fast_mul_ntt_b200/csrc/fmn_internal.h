@@ -67,6 +67,12 @@ size_t q32_job_workspace_bytes(const Job& j);  // also for a product with a 32-b
 // Transform length (log2 digits) of a 32-bit resident spectrum for products of `len` limbs with
 // partners of up to max_partner limbs; < 0 if the 32-bit engine cannot hold it.
 int q32_spectrum_log_n(u64 len, u64 max_partner);
+// Builds, on the current device, the four-step twiddle tables that the 32-bit engine's
+// current pass plans use (about 110 MB with the B200 plans), so that no product meets a
+// first-use build (an allocation and a stream synchronisation) while others run.
+cudaError_t q32_prepare_tables();
+// Frees those tables on device `dev` (its context is being shut down).
+void q32_release_tables(int dev);
 // Forward transform of `len` limbs into a 32-bit resident spectrum (3 * 2^log_n u32).
 cudaError_t q32_spectrum_enqueue(const u64* src, u64 len, int log_n, void* spec, cudaStream_t s, const Plan& plan);
 void q32_force_pieces(int m);                  // tests: split into m pieces where possible (0: model)

@@ -1440,6 +1440,34 @@ static int whole_log_n(u64 la, u64 lb) {
 
 bool q32_fits(u64 la, u64 lb, int sqr) { return q32::plan_job(la, lb, sqr).ok; }
 
+void q32_release_tables(int dev) {
+    using namespace q32;
+    std::lock_guard<std::mutex> lk(g_tw_mu);
+    for (size_t k = 0; k < g_tw.size();) {
+        if (g_tw[k].dev == dev) {
+            cudaFree(g_tw[k].buf);
+            g_tw.erase(g_tw.begin() + k);
+        } else {
+            ++k;
+        }
+    }
+}
+
+cudaError_t q32_prepare_tables() {
+    using namespace q32;
+    cudaError_t e = q32::ensure_tables();
+    if (e != cudaSuccess) return e;
+    for (int n = 1; n <= Q32_MAX_LOG_N; ++n) {
+        const Plan pl = qplan(n);
+        int logB = n;
+        for (int p = 0; p + 1 < pl.passes; ++p) {
+            tw_tables(logB, pl.bits[p], 0);          // legacy stream: finished before returning
+            logB -= pl.bits[p];
+        }
+    }
+    return cudaGetLastError();
+}
+
 void q32_force_pieces(int m) { q32::g_force_pieces.store(m > 1 ? m : 0); }
 
 Plan q32_make_plan(int log_n) { return q32::qplan(log_n); }
