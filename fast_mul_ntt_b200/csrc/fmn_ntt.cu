@@ -57,6 +57,28 @@ __device__ __forceinline__ u64 root30(u32 x, int pi, const PrimeRT& q) {
 }
 
 __device__ __forceinline__ int sw(int j, int c) { return (j << 4) | (c ^ (j & 15)); }
+// Dense tiles of strided passes: every round runs with the lanes on the 16 columns of a row
+// (each 64-bit half-warp phase reads one 128-byte row), so no swizzle is needed and each row
+// is a 128-byte copy target.
+__device__ __forceinline__ int dix(int j, int c) { return (j << 4) | c; }
+
+// 16-byte asynchronous copy global -> shared.
+__device__ __forceinline__ void cp_async16(u64* sdst, const u64* gsrc) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit_wait() {
+    asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;\n" ::: "memory");
+}
+// Rows 0 .. L-1 of a strided tile (16 u64 each, row r at g + r * 2^logS) into a dense tile.
+template <int L>
+__device__ __forceinline__ void stage_tile(u64* sm, const u64* __restrict__ g, int logS) {
+#pragma unroll 4
+    for (int e = threadIdx.x; e < L * 8; e += NT) {
+        const int r = e >> 3, k = e & 7;
+        cp_async16(sm + r * 16 + 2 * k, g + ((u64)r << logS) + 2 * k);
+    }
+}
 
 // ------------------------------------------------------------------ kernel arguments
 enum { M_FWD = 0, M_FWD_LAST = 1, M_FUSED = 2, M_INV = 3, M_FUSED2 = 4 };
@@ -173,26 +195,28 @@ __device__ __forceinline__ void ld_vec(const u64* p, u64 (&x)[R]) {
 // Rounds IDX.. of a sub-transform.  Forward order: round 0 holds the top bits.  Inverse
 // order: inverse round k undoes forward round NR-1-k.  The first round reads with `ld0`, the
 // last writes with `stl`, the rest go through shared memory.
-template <int LOGL, bool INV, bool CONTIG, int IDX, bool GST = false, bool GLD = false, class LD0, class STL>
+template <int LOGL, bool INV, bool CONTIG, int IDX, bool GST = false, bool GLD = false, bool DENSE = false, class LD0,
+          class STL>
 __device__ __forceinline__ void rounds(u64* sm, LD0 ld0, STL stl, int pi, const PrimeRT& q) {
     constexpr int NR = rounds_count(LOGL);
     constexpr int FR = INV ? NR - 1 - IDX : IDX;
     constexpr int RB = round_bits(LOGL, FR), TOP = round_top(LOGL, FR);
     constexpr bool QF = CONTIG && (TOP == LOGL - 1);
-    auto lds = [sm](int j, int c) { return sm[sw(j, c)]; };
-    auto sts = [sm](int j, int c, u64 v) { sm[sw(j, c)] = v; };
+    static_assert(!(DENSE && CONTIG), "dense tiles serve strided passes only");
+    auto lds = [sm](int j, int c) { return sm[DENSE ? dix(j, c) : sw(j, c)]; };
+    auto sts = [sm](int j, int c, u64 v) { sm[DENSE ? dix(j, c) : sw(j, c)] = v; };
     if constexpr (NR == 1) {
         run_round<LOGL, RB, TOP, INV, QF, GST, GLD>(ld0, stl, pi, q);
     } else if constexpr (IDX == 0) {
         run_round<LOGL, RB, TOP, INV, QF, false, GLD>(ld0, sts, pi, q);
         __syncthreads();
-        rounds<LOGL, INV, CONTIG, 1, GST>(sm, ld0, stl, pi, q);
+        rounds<LOGL, INV, CONTIG, 1, GST, false, DENSE>(sm, ld0, stl, pi, q);
     } else if constexpr (IDX == NR - 1) {
         run_round<LOGL, RB, TOP, INV, QF, GST>(lds, stl, pi, q);
     } else {
         run_round<LOGL, RB, TOP, INV, QF>(lds, sts, pi, q);
         __syncthreads();
-        rounds<LOGL, INV, CONTIG, IDX + 1, GST>(sm, ld0, stl, pi, q);
+        rounds<LOGL, INV, CONTIG, IDX + 1, GST, false, DENSE>(sm, ld0, stl, pi, q);
     }
 }
 
@@ -243,8 +267,17 @@ __device__ __forceinline__ void body_fwd(u64* sm, const PassArgs& a, u64 tile, i
     const int shift = MAX_LOG_N - a.logB;
     u64* beta = sm + TC * L;
     const u64* __restrict__ tw = a.tw ? a.tw + ((u64)pi << a.logB) + col0 : nullptr;
+    // residue tiles arrive by asynchronous copies while the twiddle factors are prepared; the
+    // entry pass reads the caller's limbs directly
+    constexpr bool STAGED = !ENTRY;
+    if constexpr (STAGED) stage_tile<L>(sm, d + gbase, logS);
     if (!tw) fill_beta<LOGL, false>(beta, col0, shift, pi, q);     // read after the first round's barrier
+    if constexpr (STAGED) {
+        cp_async_commit_wait();
+        __syncthreads();
+    }
     auto ld0 = [=](int j, int c) -> u64 {
+        if constexpr (STAGED) return sm[dix(j, c)];
         const u64 g = gbase + c + ((u64)j << logS);
         if constexpr (ENTRY) return entry_val(src, len, g, q);
         else return d[g];
@@ -266,7 +299,7 @@ __device__ __forceinline__ void body_fwd(u64* sm, const PassArgs& a, u64 tile, i
             }
         }
     };
-    rounds<LOGL, false, false, 0, true>(sm, ld0, stl, pi, q);
+    rounds<LOGL, false, false, 0, true, false, STAGED>(sm, ld0, stl, pi, q);
 }
 
 // Inverse strided pass: inverse four-step twiddle, then the inverse sub-transform.
@@ -283,13 +316,13 @@ __device__ __forceinline__ void body_inv(u64* sm, const PassArgs& a, u64 tile, i
     const int shift = MAX_LOG_N - a.logB;
     u64* beta = sm + TC * L;
     const u64* __restrict__ tw = a.tw ? a.tw + ((u64)pi << a.logB) + col0 : nullptr;
-    if (!tw) {
-        fill_beta<LOGL, true>(beta, col0, shift, pi, q);
-        __syncthreads();
-    }
+    stage_tile<L>(sm, d + gbase, logS);                   // in flight while the twiddles are prepared
+    if (!tw) fill_beta<LOGL, true>(beta, col0, shift, pi, q);
+    cp_async_commit_wait();
+    __syncthreads();
     auto ld0 = [=](int row0, int c, auto& x) {
 #pragma unroll
-        for (int t = 0; t < R; ++t) x[t] = d[gbase + c + ((u64)(row0 + t) << logS)];
+        for (int t = 0; t < R; ++t) x[t] = sm[dix(row0 + t, c)];
         if (tw) {
 #pragma unroll
             for (int t = 0; t < R; ++t) x[t] = mmul(x[t], __ldg(tw + c + ((u64)(row0 + t) << logS)), q);
@@ -304,7 +337,7 @@ __device__ __forceinline__ void body_inv(u64* sm, const PassArgs& a, u64 tile, i
         }
     };
     auto stl = [=](int j, int c, u64 v) { d[gbase + c + ((u64)j << logS)] = v; };
-    rounds<LOGL, true, false, 0, false, true>(sm, ld0, stl, pi, q);
+    rounds<LOGL, true, false, 0, false, true, true>(sm, ld0, stl, pi, q);
 }
 
 // Forward last pass over contiguous blocks (operand A of a product).
@@ -488,8 +521,15 @@ __device__ __forceinline__ void body_fused2(u64* sm, const PassArgs& a, u64 tile
 }
 
 // ------------------------------------------------------------------ pass kernels
+// 9-bit strided passes hold a 64 KB tile, so at most 3 CTAs share an SM anyway: they get the
+// registers of 3 (at 4 their radix-8 rounds spill).  8-bit ones keep 4 (measured faster).
+template <int MODE, int LOGL>
+constexpr int pass_min_ctas() {
+    return (MODE == M_FWD || MODE == M_INV) && LOGL >= 9 ? 3 : 4;
+}
+
 template <int MODE, int LOGL, bool ENTRY, bool SQR>
-__global__ void __launch_bounds__(NT, 4) k_pass(PassArgs a) {
+__global__ void __launch_bounds__(NT, (pass_min_ctas<MODE, LOGL>())) k_pass(PassArgs a) {
     extern __shared__ __align__(16) u64 sm[];
     const int pi = blockIdx.x % 3;          // prime varies fastest: the three CTAs of a tile
     const u64 tile = blockIdx.x / 3;        // read the same limbs at the same time (L2 reuse)
@@ -1423,7 +1463,8 @@ cudaError_t enqueue_job_overlapped(const Job& j, void* ws, size_t ws_bytes, cuda
 // Batched kernels: products with the same transform length and kind share every launch.
 // CTA b works on product b / (3 * tiles), tile (b / 3) % tiles, prime b % 3.
 template <int MODE, int LOGL, bool ENTRY, bool SQR>
-__global__ void __launch_bounds__(NT, 4) k_pass_batch(const PassArgs* __restrict__ args, u32 tiles) {
+__global__ void __launch_bounds__(NT, (pass_min_ctas<MODE, LOGL>())) k_pass_batch(const PassArgs* __restrict__ args,
+                                                                                  u32 tiles) {
     extern __shared__ __align__(16) u64 sm[];
     const int pi = blockIdx.x % 3;
     const u32 rest = blockIdx.x / 3;
