@@ -167,16 +167,6 @@ __device__ __forceinline__ void run_round(LD ld, ST st, int pi, const PrimeRT& q
     }
 }
 
-// Store R consecutive u64 (16-byte aligned when R >= 2) with 16-byte vector stores.
-template <int R>
-__device__ __forceinline__ void st_vec(u64* p, const u64 (&x)[R]) {
-    if constexpr (R == 1) {
-        p[0] = x[0];
-    } else {
-#pragma unroll
-        for (int t = 0; t < R; t += 2) *reinterpret_cast<ulonglong2*>(p + t) = make_ulonglong2(x[t], x[t + 1]);
-    }
-}
 // Load R consecutive u64 with 16-byte vector loads.
 template <int R>
 __device__ __forceinline__ void ld_vec(const u64* p, u64 (&x)[R]) {
@@ -358,11 +348,16 @@ __device__ __forceinline__ void body_fwd_last(u64* sm, const PassArgs& a, u64 ti
     if constexpr (LOGL == 0) {
         if (threadIdx.x < (unsigned)ncols) d[gbase + threadIdx.x] = ld0(0, threadIdx.x);
     } else {
-        // the lowest round holds consecutive rows of one block: 16-byte vector stores
-        auto stl = [=](int row0, int c, const auto& x) {
-            if (c < ncols) st_vec(d + gbase + (u64)c * L + row0, x);
-        };
-        rounds<LOGL, false, true, 0, true>(sm, ld0, stl, pi, q);
+        // the last round (a thread per column) writes the tile; the blocks then leave row by
+        // row with the lanes of a warp on consecutive words (256-byte stores)
+        auto sts = [sm](int j, int c, u64 v) { sm[sw(j, c)] = v; };
+        rounds<LOGL, false, true, 0, false>(sm, ld0, sts, pi, q);
+        __syncthreads();
+#pragma unroll 4
+        for (int e = threadIdx.x; e < TC * L; e += NT) {
+            const int c = e >> LOGL, j = e & (L - 1);
+            if (c < ncols) d[gbase + (u64)c * L + j] = sm[sw(j, c)];
+        }
     }
 }
 
@@ -668,22 +663,28 @@ __device__ __forceinline__ void crt_coef(const CrtArgs& a, u64 j, u64& w0, u64& 
     crt_of(a.res[j], a.res[a.N + j], a.res[2 * a.N + j], a.cst, w0, w1, w2, q0, q1, q2);
 }
 
+// Output limbs per thread of the CRT + carry kernel: 8 keeps a thread's sums and 192-bit CRT
+// words within the registers of 4 CTAs per SM (16 needed 90 registers: 2 CTAs; 64M x 64M
+// 28.4 -> 27.9 ms).
+constexpr int WCE = 8;
+constexpr u64 WCTILE = (u64)CNT * WCE;
+
 __device__ __forceinline__ void crt_carry_body(const CrtArgs& a, u32 ncta) {
     __shared__ u64 s_hw[CNT / 32][3];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const PrimeRT q0 = c_prime[0], q1 = c_prime[1], q2 = c_prime[2];
     const u64 tile = carry_ticket(a.ticket);
     if (tile >= ncta) return;                   // batch launches cover the largest product
-    const u64 j0 = tile * CTILE + (u64)tid * CE;
+    const u64 j0 = tile * WCTILE + (u64)tid * WCE;
 
     // coefficients j0 .. j0+15, folded into limb sums s_j = c_j[0] + c_{j-1}[1] + c_{j-2}[2]
     // (the two contributions from the previous thread's coefficients are added below)
-    u64 lo[CE];
-    u32 h[CE];
+    u64 lo[WCE];
+    u32 h[WCE];
     u64 pw1 = 0, pw2 = 0, ppw2 = 0;          // c_{j-1}[1], c_{j-1}[2], c_{j-2}[2]
-    const bool full = j0 + CE <= a.nvalid;
+    const bool full = j0 + WCE <= a.nvalid;
 #pragma unroll
-    for (int e2 = 0; e2 < CE; e2 += 2) {
+    for (int e2 = 0; e2 < WCE; e2 += 2) {
         u64 r0[2], r1[2], r2[2];
         if (full) {
             const ulonglong2 v0 = *reinterpret_cast<const ulonglong2*>(a.res + j0 + e2);
@@ -739,7 +740,7 @@ __device__ __forceinline__ void crt_carry_body(const CrtArgs& a, u32 ncta) {
     carry_finish(lo, h, tile, j0, a.state, a.err, a.out, a.out_len);
 }
 
-__global__ void __launch_bounds__(CNT) k_crt_carry(CrtArgs a) { crt_carry_body(a, 0xffffffffu); }
+__global__ void __launch_bounds__(CNT, 4) k_crt_carry(CrtArgs a) { crt_carry_body(a, 0xffffffffu); }
 
 // ------------------------------------------------------------------ host: tables
 static u64 h_mulmod(u64 a, u64 b, u64 m) { return (u64)(((unsigned __int128)a * b) % m); }
@@ -1028,7 +1029,7 @@ static WsLayout ws_layout(u64 la, u64 lb, int sqr, int force_n = 0) {
     w.N = ceil_pow2(out_len - 1);
     if (force_n > 0 && (1ull << force_n) > w.N) w.N = 1ull << force_n;
     w.n = ilog2(w.N);
-    w.ncta = (out_len + CTILE - 1) / CTILE;
+    w.ncta = (out_len + WCTILE - 1) / WCTILE;
     size_t off = 256;
     w.a = off;
     off = align256(off + 3 * w.N * sizeof(u64));
@@ -1453,7 +1454,7 @@ cudaError_t enqueue_job_overlapped(const Job& j, void* ws, size_t ws_bytes, cuda
     for (u64 t0 = 0; t0 < L.ncta; t0 += per) {
         const u64 n = t0 + per <= L.ncta ? per : L.ncta - t0;
         if ((e = launch_crt(L.crt, n, s)) != cudaSuccess) return e;
-        const u64 lo = t0 * CTILE, hi = (t0 + n) * CTILE < out_len ? (t0 + n) * CTILE : out_len;
+        const u64 lo = t0 * WCTILE, hi = (t0 + n) * WCTILE < out_len ? (t0 + n) * WCTILE : out_len;
         if (after_chunk && (e = after_chunk(ctx, lo, hi)) != cudaSuccess) return e;
     }
     return cudaSuccess;
