@@ -1,9 +1,10 @@
 """Several host threads calling abs_mul64 / abs_sqr64 at once.
 
 The reference's functions are plain reentrant C; a caller may run products from several
-threads.  Here every call shares one device context per GPU (twiddle tables, workspace,
-streams), which the library serialises; each thread's products must still equal the
-oracle's bit for bit, whatever the engine and the split plan of the shapes involved."""
+threads.  Here each call runs on one of the device's host lanes (its own workspace, buffers
+and streams; 4 by default), so more threads than lanes also exercises a caller waiting for a
+free lane.  Every thread's products must still equal the oracle's bit for bit, whatever the
+engine and the split plan of the shapes involved."""
 import threading
 
 import numpy as np
@@ -15,17 +16,18 @@ pytestmark = pytest.mark.gpu
 
 # balanced, unbalanced (split on the 32-bit engine), tiny, and squares
 SHAPES = [(20000, 20000), (3000, 90001), (90001, 3000), (1, 7), (40000, None), (777, None)]
+THREADS = 6
 
 
 def test_concurrent_host_calls(fmn, oracle):
     cases = []
-    for t in range(4):
+    for t in range(THREADS):
         for i, (la, lb) in enumerate(SHAPES):
             a, b = synth.operands("uniform", la, lb or 1, 100 * t + i)
             want = oracle.sqr(a) if lb is None else oracle.mul(a, b)
             cases.append((t, la, lb, a, b, want))
     errors = []
-    barrier = threading.Barrier(4)
+    barrier = threading.Barrier(THREADS)
 
     def worker(t):
         try:
@@ -40,7 +42,7 @@ def test_concurrent_host_calls(fmn, oracle):
         except Exception as e:                  # reported by the main thread
             errors.append((t, repr(e)))
 
-    threads = [threading.Thread(target=worker, args=(t,)) for t in range(4)]
+    threads = [threading.Thread(target=worker, args=(t,)) for t in range(THREADS)]
     for th in threads:
         th.start()
     for th in threads:
