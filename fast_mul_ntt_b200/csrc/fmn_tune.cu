@@ -101,6 +101,7 @@ int fmn_set_plan_engine(int engine, int log_n, const int* bits, int passes) {
     p.passes = passes;
     for (int i = 0; i < passes; ++i) p.bits[i] = bits[i];
     if (!fmn::q32_set_plan(p)) return fmn::api_set_error(FMN_ERR_ARG, "invalid pass plan", cudaSuccess);
+    fmn::q32_prepare_tables();      // the new plan's twiddle tables, before a product needs them
     return FMN_OK;
 }
 
@@ -164,6 +165,7 @@ int fmn_load_plans(const char* path) {
         return fmn::api_set_error(FMN_ERR_ARG, "plan file was tuned on another GPU or driver", cudaSuccess);
     for (const auto& p : plans) fmn::set_plan(p);
     for (const auto& p : plans32) fmn::q32_set_plan(p);
+    if (!plans32.empty()) fmn::q32_prepare_tables();
     return FMN_OK;
 }
 
@@ -236,6 +238,13 @@ int fmn_autotune(int n_lo, int n_hi, const char* save_path) {
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     cudaStreamDestroy(s);
+    // the candidates' twiddle tables give way to those of the chosen plans
+    int dev = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess) {
+        cudaDeviceSynchronize();
+        fmn::q32_release_tables(dev);
+        fmn::q32_prepare_tables();
+    }
     if (rc == FMN_OK && save_path) {
         FILE* f = fopen(save_path, "w");
         if (!f) return fmn::api_set_error(FMN_ERR_ARG, "cannot write plan file", cudaSuccess);

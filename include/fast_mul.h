@@ -226,7 +226,8 @@ int fmn_set_plan(int log_n, const int* bits, int passes);
 int fmn_autotune(int n_lo, int n_hi, const char* save_path);
 /* The same per engine: FMN_ENGINE_64 as above, FMN_ENGINE_32 for its 2^log_n-digit transforms
  * (log_n <= 26; a strided pass leaves at least 32 columns).  A resident operand keeps the
- * plan it was transformed with. */
+ * plan it was transformed with.  Setting or loading 32-bit plans builds their four-step
+ * twiddle tables on the current device right away (so no product waits for them). */
 int fmn_get_plan_engine(int engine, int log_n, int* bits, int max_passes);
 int fmn_set_plan_engine(int engine, int log_n, const int* bits, int passes);
 int fmn_load_plans(const char* path);

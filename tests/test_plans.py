@@ -206,3 +206,26 @@ def test_products_under_engine32_plans(fmn, oracle):
         fmn.set_engine(fmn.ENGINE_AUTO)
         for n in (15, 17, 18, 21):
             fmn.set_plan(n, None, engine=e32)
+
+
+@pytest.mark.gpu
+def test_autotune_small_range(fmn, oracle, tmp_path):
+    """The autotuner over 2^10..2^12 points writes a plan file for both engines, keeps valid
+    plans in effect, and leaves the 32-bit engine's twiddle tables rebuilt for them: products
+    of those lengths (and a longer one, whose tables were freed and rebuilt) stay exact."""
+    path = str(tmp_path / "plans.txt")
+    lib = fmn.load_library()
+    try:
+        fmn.autotune(10, 12, path)
+        lines = [l.split("#")[0].split() for l in open(path) if l.strip() and not l.startswith("#")]
+        ns64 = {int(l[0]) for l in lines if l[0].isdigit()}
+        ns32 = {int(l[1]) for l in lines if l[0] == "e32"}
+        assert ns64 == {10, 11, 12} and ns32 == {11, 12}     # 2^10 digits: a single 32-bit plan
+        for la, lb in [(200, 300), (1000, 1000), (60000, 90000)]:
+            a, b = synth.operands("uniform", la, lb, la)
+            assert np.array_equal(fmn.abs_mul64(a, b), oracle.mul(a, b)), (la, lb)
+    finally:
+        for n in (10, 11, 12):
+            fmn.set_plan(n, None)
+            fmn.set_plan(n, None, engine=fmn.ENGINE_32)
+        lib.fmn_load_default_plans()
