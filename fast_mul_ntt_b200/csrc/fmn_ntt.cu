@@ -20,9 +20,11 @@
 // blocks (16 blocks per tile).  Spectra are left in the permuted order that the matching
 // inverse passes consume; only final limbs are observable.
 //
-// Shared-memory tile: element (row j, column c) lives at (j << 4) | (c ^ (j & 15)); the XOR
-// swizzle keeps both the row-wise (16 columns of a row) and the column-wise (consecutive rows
-// of one column) access patterns free of bank conflicts.
+// Shared-memory tile of contiguous passes: element (row j, column c) lives at
+// (j << 4) | (c ^ (j & 15)); the XOR swizzle keeps both the row-wise (16 columns of a row) and
+// the column-wise (consecutive rows of one column) access patterns free of bank conflicts.
+// Strided passes, whose rounds only ever read whole rows, use a dense tile (row pitch 16) that
+// arrives by asynchronous 16-byte copies while the CTA prepares its twiddle factors.
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <stdio.h>
