@@ -138,3 +138,40 @@ def test_digit_pairs_make_limbs():
         A = sum(x << (64 * i) for i, x in enumerate(a))
         B = sum(x << (64 * i) for i, x in enumerate(b))
         assert sum(x << (64 * i) for i, x in enumerate(limbs)) == A * B
+
+
+def _round_bits(l, i):
+    if l <= 4:
+        return l
+    if l <= 8:
+        return (l + 1) // 2 if i == 0 else l // 2
+    return (l + 2) // 3 if i == 0 else (l + 1) // 3 if i == 1 else l // 3
+
+
+def _bitrev(x, bits):
+    return int(format(x, f"0{bits}b")[::-1], 2) if bits else 0
+
+
+def test_twiddle_table_index_matches_computed_twiddle():
+    """A strided pass's four-step twiddle for row j (frequency bitrev(j)) and column i is formed
+    on the fly as alpha(group) * beta(column, t') (group_alpha / fill_beta in fmn_ntt32.cu) or
+    read from the table entry k * 2^logS + i (tw_group, k_qtw_build).  Both must name the same
+    power w_B^(i k) for every element of every group of the lowest round."""
+    rng = random.Random(4)
+    for LOGL, logB in ((5, 12), (7, 15), (8, 17), (9, 17), (9, 20)):
+        NR = 1 if LOGL <= 4 else 2 if LOGL <= 8 else 3
+        RB = _round_bits(LOGL, NR - 1)
+        logS = logB - LOGL
+        shift = MAX_LOG_N - logB
+        for _ in range(200):
+            row0 = rng.randrange(1 << (LOGL - RB)) << RB
+            i = rng.randrange(1 << logS)
+            kq = _bitrev(row0 >> RB, LOGL - RB)
+            for t in range(1 << RB):
+                tp = _bitrev(t, RB)
+                x_computed = ((i * kq) << shift) + ((i * (tp << (LOGL - RB))) << shift)
+                k = kq + (tp << (LOGL - RB))
+                assert k == _bitrev(row0 + t, LOGL)
+                entry = (kq << logS) + i + tp * ((1 << logS) << (LOGL - RB))
+                assert entry == k * (1 << logS) + i and entry < (1 << logB)
+                assert x_computed % (1 << MAX_LOG_N) == ((i * k) << shift) % (1 << MAX_LOG_N)
