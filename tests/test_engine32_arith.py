@@ -4,8 +4,8 @@ The engine (fast_mul_ntt_b200/csrc/fmn_arith32.cuh, fmn_ntt32.cu) splits each 64
 into two 32-bit digits and transforms them modulo three primes below 2^31.  These tests pin
 the facts its exactness rests on: the primes and their 2-adic order, the coefficient bound
 against the primes' product, the Shoup and Montgomery reductions it uses (with the ranges
-the kernels rely on), and the CRT by Garner's mixed-radix form with the same constants the
-kernel receives."""
+the kernels rely on), the CRT by Garner's mixed-radix form with the same constants the
+kernel receives, and the indexing of the precomputed four-step twiddle tables."""
 import random
 
 P0, P1, P2 = 2013265921, 1811939329, 469762049
