@@ -102,3 +102,16 @@ def test_fixed_swizzle_had_first_round_conflicts():
     for l in range(5, 9):
         worst = max(wavefronts([old(l, j, c) for j, c in pat]) for pat in round_accesses(l, 0, True))
         assert worst == 2
+
+
+def test_dense_strided_tiles_are_conflict_free():
+    """Strided passes of both engines use dense tiles: 32 u32 columns per row (32-bit engine,
+    a warp on one row's 32 columns) and 16 u64 columns per row (64-bit engine, a warp on two
+    rows; a 64-bit access is served in two half-warp phases, each one 128-byte row).  Every
+    phase then touches each of the 32 banks once."""
+    for j0 in range(0, 64, 1):
+        assert wavefronts([j0 * 32 + c for c in range(32)]) == 1          # u32, one row
+    for j0 in range(0, 64, 2):
+        for half in (0, 1):                                               # u64, word pairs
+            words = [((j0 + half) * 16 + c) * 2 + h for c in range(16) for h in (0, 1)]
+            assert wavefronts(words) == 1
