@@ -18,7 +18,16 @@ length taken as the max over ranks.
           peak of the engine's butterfly arithmetic (microbenchmark run here);
   cpu_baseline
           the reference's own src/ abs_mul64 (oracle/_ref, compiled unmodified) on one host
-          core, one 10M x 10M product (rank 0, N = 1 only).
+          core, one 10M x 10M product (rank 0, N = 1 only);
+  extra   the other configurations of the product (10k x 10k, 1M x 1M uniform / all-ones /
+          square, 10M all-ones and square, 64M x 250K and 64M x 64M uniform and sparse, and
+          10M x 10M on the 64-bit engine with the reference's primes), each timed on the
+          device with an L2 flush between products, checked against the reference's output
+          digest, with its dominant kernel's rooflines;
+  batch   the 4,096-product mixed-size stream: per-call vs batched vs CUDA-graph replay;
+  serve   the open-loop Poisson stream (100,000 requests, 256 .. 4M limbs) through the
+          continuous-batching server and through the plain per-call path, at an offered rate
+          both keep up with (latency) and one above the per-call path's capacity (throughput).
 
 --impl reference times that reference CPU implementation with all host cores (independent
 products in parallel threads) on the same workload and prints the same JSON line.
@@ -62,8 +71,11 @@ def parse():
     ap.add_argument("--batch-count", type=int, default=4096)
     ap.add_argument("--no-serve", action="store_true", help="skip the served-stream comparison")
     ap.add_argument("--serve-only", action="store_true", help="only the served-stream comparison")
-    ap.add_argument("--serve-requests", type=int, default=5000)
-    ap.add_argument("--serve-rate", type=float, default=1500.0, help="offered requests per second")
+    ap.add_argument("--serve-requests", type=int, default=100_000)
+    ap.add_argument("--serve-rates", default="1000,4000",
+                    help="offered requests per second: one below the per-call path's capacity, one above")
+    ap.add_argument("--no-extra", action="store_true", help="skip the other configurations")
+    ap.add_argument("--extra-only", action="store_true", help="only the other configurations")
     ap.add_argument("--e2e-callers", type=int, default=4,
                     help="host threads calling abs_mul64 at once in the end-to-end measurement")
     return ap.parse_args()
@@ -308,13 +320,50 @@ def batch_compare(fmn, torch, dev, count, repeats=3):
 
 
 # ----------------------------------------------------------------------------- served stream
-def serve_compare(fmn, torch, dev, n_requests, rate, seed=0, templates=256, residents=8):
-    """Open-loop Poisson stream at `rate` requests/s: 70% multiplies, 30% squares, operand
-    lengths log-uniform in [256, 4,000,000] limbs, 25% of the multiplies by a resident
-    (already transformed) operand; HBM admission budget 120 GB.  The same stream through the
-    continuous-batching server and through the plain per-call path (one product at a time
-    on one stream, no reuse).  Every output is compared on the device with its expected
-    product, computed beforehand by the per-call path."""
+class UtilSampler:
+    """NVML GPU utilisation (percent of time a kernel was running) sampled in a thread."""
+
+    def __init__(self, index, period=0.05):
+        self.ok, self.samples, self.period = False, [], period
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.nv, self.h, self.ok = pynvml, pynvml.nvmlDeviceGetHandleByIndex(index), True
+        except Exception:
+            self.ok = False
+        self._stop = threading.Event()
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                self.samples.append(self.nv.nvmlDeviceGetUtilizationRates(self.h).gpu)
+            except Exception:
+                pass
+            time.sleep(self.period)
+
+    def __enter__(self):
+        if self.ok:
+            self.t = threading.Thread(target=self._run, daemon=True)
+            self.t.start()
+        return self
+
+    def __exit__(self, *a):
+        if self.ok:
+            self._stop.set()
+            self.t.join()
+
+    def mean(self):
+        return float(np.mean(self.samples)) if self.samples else None
+
+
+def serve_compare(fmn, torch, dev, n_requests, rates, seed=0, templates=256, residents=8):
+    """Open-loop Poisson stream: 70% multiplies, 30% squares, operand lengths log-uniform in
+    [256, 4,000,000] limbs, 25% of the multiplies by a resident (already transformed) operand;
+    HBM admission budget 120 GB.  The same stream through the continuous-batching server and
+    through the plain per-call path (one product at a time on one stream, no reuse), at each
+    offered rate.  Every output is compared on the device with its expected product, computed
+    beforehand by the per-call path.  The device time of every request template alone gives the
+    stream's GPU work, so the capacity of each path can be read against it."""
     rng = np.random.default_rng(seed)
     lo, hi = 256, 4_000_000
 
@@ -328,7 +377,7 @@ def serve_compare(fmn, torch, dev, n_requests, rate, seed=0, templates=256, resi
         da = torch.from_numpy(a.view(np.int64)).to(dev)
         hold.append(da)
         res_ops.append(fmn.Operand(da, max_partner_len=hi))
-    tmpl = []
+    tmpl, runs = [], []
     stream = torch.cuda.Stream(device=dev)
     for t in range(templates):
         r = fmn.FmnRequest()
@@ -338,7 +387,7 @@ def serve_compare(fmn, torch, dev, n_requests, rate, seed=0, templates=256, resi
             da = torch.from_numpy(synth_limbs("uniform", l1, 600_000 + t).view(np.int64)).to(dev)
             hold.append(da)
             want = torch.empty(2 * l1, dtype=torch.int64, device=dev)
-            fmn.sqr_device(da, want, stream=stream)
+            run = (lambda da=da, want=want: fmn.sqr_device(da, want, stream=stream))
             r.op, r.in1, r.len1 = fmn.FMN_OP_SQR, da.data_ptr(), l1
         elif u < 0.30 + 0.70 * 0.25:                   # multiply by a resident operand
             op = res_ops[t % residents]
@@ -346,7 +395,7 @@ def serve_compare(fmn, torch, dev, n_requests, rate, seed=0, templates=256, resi
             db = torch.from_numpy(synth_limbs("uniform", l2, 700_000 + t).view(np.int64)).to(dev)
             hold.append(db)
             want = torch.empty(op.len + l2, dtype=torch.int64, device=dev)
-            fmn.mul_device(op.limbs, db, want, stream=stream)
+            run = (lambda op=op, db=db, want=want: fmn.mul_device(op.limbs, db, want, stream=stream))
             r.op, r.operand, r.in2, r.len2 = fmn.FMN_OP_MUL_OPERAND, op.handle.value, db.data_ptr(), l2
         else:                                          # multiply
             l1, l2 = loglen(), loglen()
@@ -354,12 +403,26 @@ def serve_compare(fmn, torch, dev, n_requests, rate, seed=0, templates=256, resi
             db = torch.from_numpy(synth_limbs("uniform", l2, 900_000 + t).view(np.int64)).to(dev)
             hold += [da, db]
             want = torch.empty(l1 + l2, dtype=torch.int64, device=dev)
-            fmn.mul_device(da, db, want, stream=stream)
+            run = (lambda da=da, db=db, want=want: fmn.mul_device(da, db, want, stream=stream))
             r.op, r.in1, r.len1, r.in2, r.len2 = fmn.FMN_OP_MUL, da.data_ptr(), l1, db.data_ptr(), l2
+        run()
         hold.append(want)
         r.check = want.data_ptr()
         r.out = None
         tmpl.append(r)
+        runs.append(run)
+    fmn.sync(stream)
+    # device time of each template alone (the per-call path's kernels, back to back)
+    alone_ms = []
+    for run in runs:
+        run()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(3):
+            run()
+        e1.record(stream)
+        e1.synchronize()
+        alone_ms.append(e0.elapsed_time(e1) / 3)
     fmn.sync(stream)
     pick = rng.integers(0, templates, n_requests)
     reqs = []
@@ -368,28 +431,48 @@ def serve_compare(fmn, torch, dev, n_requests, rate, seed=0, templates=256, resi
         ctypes.pointer(r)[0] = tmpl[t]
         r.tag = i
         reqs.append(r)
-    arrivals = list(np.cumsum(rng.exponential(1.0 / rate, n_requests)))
+    gaps = rng.exponential(1.0, n_requests)
     ops = [tmpl[t].op for t in pick]
-    out = {"workload": f"{n_requests} requests, open-loop Poisson at {rate:g}/s; 70% multiply / 30% square, "
-                       f"25% of the multiplies by one of {residents} resident operands; lengths log-uniform in "
-                       f"[{lo}, {hi}] limbs ({templates} request templates, seed {seed}); HBM budget 120 GB",
+    gpu_work_s = float(sum(alone_ms[t] for t in pick)) * 1e-3
+    out = {"workload": f"{n_requests} requests, open-loop Poisson; 70% multiply / 30% square, 25% of the "
+                       f"multiplies by one of {residents} resident operands; lengths log-uniform in [{lo}, {hi}] "
+                       f"limbs ({templates} request templates, seed {seed}); HBM budget 120 GB",
+           "requests": n_requests,
            "mix": {"mul": ops.count(fmn.FMN_OP_MUL), "sqr": ops.count(fmn.FMN_OP_SQR),
-                   "mul_resident": ops.count(fmn.FMN_OP_MUL_OPERAND)}}
-    for name, batching in (("served", True), ("per_call", False)):
-        srv = fmn.Server(device=dev.index or 0, hbm_budget=120 << 30, max_batch=256, batching=batching)
-        try:
-            lat, wall = srv.replay(reqs, arrivals)
-            st = srv.stats()
-        finally:
-            srv.close()
-        lat = np.sort(np.array(lat))
-        out[name] = {"products_per_s": st["completed"] / wall, "wall_s": wall,
-                     "p50_ms": float(lat[len(lat) // 2]), "p99_ms": float(lat[min(len(lat) - 1, int(0.99 * len(lat)))]),
-                     "mean_ms": float(lat.mean()), "batches": st["batches"], "peak_scratch_gb": st["peak_bytes"] / 2**30,
-                     "mismatches": st["mismatches"], "rejected": st["rejected"], "device_errors": st["device_errors"],
-                     "bit_exact": st["mismatches"] == 0 and st["device_errors"] == 0 and st["rejected"] == 0}
-    out["throughput_ratio_served_vs_per_call"] = out["served"]["products_per_s"] / out["per_call"]["products_per_s"]
-    out["p99_ratio_per_call_vs_served"] = out["per_call"]["p99_ms"] / out["served"]["p99_ms"]
+                   "mul_resident": ops.count(fmn.FMN_OP_MUL_OPERAND)},
+           "gpu_work_alone_s": gpu_work_s,
+           "per_call_device_bound_products_per_s": n_requests / gpu_work_s,
+           "rates": {}}
+    for rate in rates:
+        arrivals = list(np.cumsum(gaps / rate))
+        res = {"offered_per_s": rate}
+        for name, batching in (("served", True), ("per_call", False)):
+            srv = fmn.Server(device=dev.index or 0, hbm_budget=120 << 30, max_batch=256, batching=batching)
+            util = UtilSampler(dev.index or 0)
+            try:
+                with util:
+                    lat, wall = srv.replay(reqs, arrivals)
+                st = srv.stats()
+            finally:
+                srv.close()
+            lat = np.sort(np.array(lat))
+            res[name] = {"products_per_s": st["completed"] / wall, "wall_s": wall,
+                         "p50_ms": float(lat[len(lat) // 2]),
+                         "p99_ms": float(lat[min(len(lat) - 1, int(0.99 * len(lat)))]),
+                         "mean_ms": float(lat.mean()), "batches": st["batches"],
+                         "peak_scratch_gb": st["peak_bytes"] / 2**30,
+                         "gpu_busy_pct": util.mean(),
+                         "gpu_work_over_wall": gpu_work_s / wall,
+                         "mismatches": st["mismatches"], "rejected": st["rejected"],
+                         "device_errors": st["device_errors"],
+                         "bit_exact": st["mismatches"] == 0 and st["device_errors"] == 0 and st["rejected"] == 0}
+        res["throughput_ratio_served_vs_per_call"] = res["served"]["products_per_s"] / res["per_call"]["products_per_s"]
+        res["p99_ratio_per_call_vs_served"] = res["per_call"]["p99_ms"] / res["served"]["p99_ms"]
+        out["rates"][f"{rate:g}"] = res
+    top = out["rates"][f"{max(rates):g}"]
+    out["capacity_ratio_served_vs_per_call"] = top["throughput_ratio_served_vs_per_call"]
+    out["meets_5x"] = top["throughput_ratio_served_vs_per_call"] >= 5.0
+    out["mismatches"] = sum(v[p]["mismatches"] for v in out["rates"].values() for p in ("served", "per_call"))
     for op in res_ops:
         op.close()
     del hold
@@ -400,6 +483,181 @@ def serve_compare(fmn, torch, dev, n_requests, rate, seed=0, templates=256, resi
 def synth_limbs(kind, n, seed):
     from fast_mul_ntt_b200 import synth
     return synth.limbs(kind, n, seed)
+
+
+# ----------------------------------------------------------------------------- rooflines
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except Exception:
+        peaks = {}
+    hbm = peaks.get("hbm_gbs")
+    return (hbm, "measured (MEASURED_PEAKS.json hbm_gbs)") if hbm else (6650.0, "fallback 6.65 TB/s")
+
+
+def traffic_for(key, kernel):
+    """DRAM bytes per launch of `kernel` from an ncu capture of exactly this configuration
+    (profiles/traffic.json, keyed by engine:op:kind:len1xlen2), or None when there is none."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            cap = json.load(f)["captures"].get(key)
+    except Exception:
+        return None, None
+    if not cap or kernel not in cap["bytes_per_launch"]:
+        return None, None
+    return cap["bytes_per_launch"][kernel], cap["source"]
+
+
+def rooflines(fmn, prof, steps, engine, peaks, traffic_key):
+    """The dominant kernel kind of `prof` (per-kind CUDA-event totals over `steps` products)
+    against the HBM copy bandwidth and against the engine's measured butterfly peak."""
+    hbm_peak, hbm_src = load_peaks()
+    bf_peak = peaks["bfly32"] if engine == fmn.ENGINE_32 else peaks["bfly64"]
+    name, st = max(prof.items(), key=lambda kv: kv[1]["ms"])
+    per_launch_ms = st["ms"] / max(1, st["launches"])
+    bytes_per_launch = st["bytes"] / max(1, st["launches"])
+    mm_per_launch = st["modmuls"] / max(1, st["launches"])
+    achieved_gbs = bytes_per_launch / (per_launch_ms * 1e-3) / 1e9
+    achieved_mm = mm_per_launch / (per_launch_ms * 1e-3)
+    traffic, tsrc = traffic_for(traffic_key, name)
+    total_ms = sum(v["ms"] for v in prof.values()) or 1.0
+    all_mm = sum(v["modmuls"] for v in prof.values()) / steps
+    hbm = {"bound": "hbm", "kernel": name, "achieved": achieved_gbs, "peak": hbm_peak, "unit": "GB/s",
+           "frac": achieved_gbs / hbm_peak, "traffic": traffic,
+           "traffic_source": tsrc or "no ncu capture of this configuration",
+           "peak_source": hbm_src, "algorithmic_bytes_per_launch": bytes_per_launch, "ms_per_launch": per_launch_ms}
+    integer = {"bound": "integer issue (butterfly arithmetic)", "kernel": name,
+               "achieved": achieved_mm / 1e9, "peak": bf_peak / 1e9,
+               "unit": "Gbutterfly/s", "frac": achieved_mm / bf_peak,
+               "peak_source": ("measured: independent 32-bit butterfly chains on this GPU" if engine == fmn.ENGINE_32
+                               else "measured: independent 64-bit Montgomery butterfly chains on this GPU"),
+               "algorithmic_butterflies_per_launch": mm_per_launch,
+               "whole_product_frac": (all_mm / (total_ms / steps * 1e-3)) / bf_peak}
+    kernels = {k: {"ms_per_step": v["ms"] / steps, "launches_per_step": v["launches"] / steps,
+                   "share": v["ms"] / total_ms} for k, v in prof.items()}
+    return hbm, integer, kernels
+
+
+def engine_label(fmn, engine):
+    return ("32-bit digits mod three 31-bit primes" if engine == fmn.ENGINE_32
+            else "64-bit limbs mod the reference's three 62-bit primes")
+
+
+# ----------------------------------------------------------------------------- other configurations
+EXTRA = [  # (name, op, kind, len1, len2, engine, steps)
+    ("mul_uniform_10k", "mul", "uniform", 10_000, 10_000, "auto", 50),
+    ("mul_uniform_1M", "mul", "uniform", 1_000_000, 1_000_000, "auto", 20),
+    ("mul_ones_1M", "mul", "ones", 1_000_000, 1_000_000, "auto", 20),
+    ("sqr_uniform_1M", "sqr", "uniform", 1_000_000, 1_000_000, "auto", 20),
+    ("mul_ones_10M", "mul", "ones", 10_000_000, 10_000_000, "auto", 10),
+    ("sqr_uniform_10M", "sqr", "uniform", 10_000_000, 10_000_000, "auto", 10),
+    ("mul_uniform_10M_engine64", "mul", "uniform", 10_000_000, 10_000_000, "64", 10),
+    ("mul_uniform_64Mx250K", "mul", "uniform", 64_000_000, 250_000, "auto", 5),
+    ("mul_sparse_64Mx250K", "mul", "sparse", 64_000_000, 250_000, "auto", 5),
+    ("mul_uniform_64Mx64M", "mul", "uniform", 64_000_000, 64_000_000, "auto", 3),
+    ("mul_sparse_64Mx64M", "mul", "sparse", 64_000_000, 64_000_000, "auto", 3),
+]
+L2_FLUSH_BYTES = 256 << 20        # twice the 126 MB L2
+
+
+def time_config(fmn, torch, dev, op, kind, l1, l2, steps, warmup, peaks):
+    """One configuration on the device: a correctness run against the reference's digest,
+    then `steps` products each timed by CUDA events on its stream with an L2 flush (a 256 MB
+    write) before it, then the same number of products with per-launch events for the kernel
+    split and rooflines."""
+    from fast_mul_ntt_b200 import synth
+    a, b = synth.operands(kind, l1, l2, SEED)
+    da = torch.from_numpy(a.view(np.int64)).to(dev)
+    db = da if op == "sqr" else torch.from_numpy(b.view(np.int64)).to(dev)
+    dout = torch.empty(l1 + l2, dtype=torch.int64, device=dev)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.int32, device=dev)
+    stream = torch.cuda.Stream(device=dev)
+
+    def step():
+        if op == "sqr":
+            fmn.sqr_device(da, dout, stream=stream)
+        else:
+            fmn.mul_device(da, db, dout, stream=stream)
+
+    step()
+    fmn.sync(stream)
+    want = golden_digest(op, kind, l1, l2)
+    got_digest = digest(dout.cpu().numpy().view(np.uint64))
+    for _ in range(warmup):
+        step()
+    stream.synchronize()
+    total = 0.0
+    with torch.cuda.stream(stream):
+        for _ in range(steps):
+            flush.fill_(1)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            step()
+            e1.record(stream)
+            e1.synchronize()
+            total += e0.elapsed_time(e1)
+    fmn.sync(stream)
+    fmn.profile_enable(True)
+    fmn.profile_take()
+    for _ in range(steps):
+        step()
+    fmn.profile_enable(False)
+    prof = fmn.profile_take()
+    fmn.sync(stream)
+    engine = fmn.engine_for(l1, l2, op == "sqr")
+    key = f"{'e32' if engine == fmn.ENGINE_32 else 'e64'}:{op}:{kind}:{l1}x{l2}"
+    hbm, integer, kernels = rooflines(fmn, prof, steps, engine, peaks, key)
+    us = 1e3 * total / steps
+    res = {"op": op, "kind": kind, "len1": l1, "len2": l2, "engine": engine_label(fmn, engine),
+           "pieces": fmn.pieces_for(l1, l2, op == "sqr"), "steps": steps, "warmup": warmup,
+           "us_per_product": us, "products_per_s": 1e6 / us, "limbs_per_s": (l1 + l2) * 1e6 / us,
+           "bit_exact": (got_digest == want) if want else None,
+           "l2_policy": "256 MB L2 flush before every timed product",
+           "roofline": hbm, "roofline_int": integer, "kernels": kernels}
+    del da, db, dout, flush
+    torch.cuda.empty_cache()
+    return res
+
+
+def extra_configs(fmn, torch, dev, peaks):
+    out = {}
+    for name, op, kind, l1, l2, eng, steps in EXTRA:
+        fmn.set_engine({"auto": fmn.ENGINE_AUTO, "64": fmn.ENGINE_64, "32": fmn.ENGINE_32}[eng])
+        try:
+            out[name] = time_config(fmn, torch, dev, op, kind, l1, l2, steps, 3, peaks)
+        finally:
+            fmn.set_engine(fmn.ENGINE_AUTO)
+    return out
+
+
+# ----------------------------------------------------------------------------- end to end
+def e2e_rate(lib, pa, l1, pb, l2, outs, steps, barrier, dev):
+    """Products/s of len(outs) host threads each calling abs_mul64 `steps` times at once (host
+    wall clock, max over ranks); one warm-up call per thread first."""
+    callers = len(outs)
+    go = threading.Barrier(callers + 1)
+
+    def caller(i, n):
+        if n > 1:
+            go.wait()
+        for _ in range(n):
+            lib.abs_mul64(pa, l1, pb, l2, outs[i])
+
+    warm = [threading.Thread(target=caller, args=(i, 1)) for i in range(callers)]
+    for t in warm:
+        t.start()
+    for t in warm:
+        t.join()
+    ths = [threading.Thread(target=caller, args=(i, steps)) for i in range(callers)]
+    for t in ths:
+        t.start()
+    barrier()
+    go.wait()
+    t0 = time.perf_counter()
+    for t in ths:
+        t.join()
+    return max_over_ranks(time.perf_counter() - t0, dev)
 
 
 # ----------------------------------------------------------------------------- ours
@@ -421,11 +679,16 @@ def run_ours(args, ws, rank, local):
     fmn.init(local)
     if args.engine != "auto":
         fmn.set_engine(fmn.ENGINE_32 if args.engine == "32" else fmn.ENGINE_64)
+    rates = [float(r) for r in args.serve_rates.split(",") if r]
     if args.batch_only:
         print(json.dumps(batch_compare(fmn, torch, dev, args.batch_count)), flush=True)
         return
     if args.serve_only:
-        print(json.dumps(serve_compare(fmn, torch, dev, args.serve_requests, args.serve_rate)), flush=True)
+        print(json.dumps(serve_compare(fmn, torch, dev, args.serve_requests, rates)), flush=True)
+        return
+    peaks = {"bfly32": fmn.bench_bfly32(), "bfly64": fmn.bench_modmul()[1]}
+    if args.extra_only:
+        print(json.dumps(extra_configs(fmn, torch, dev, peaks)), flush=True)
         return
     l1 = args.len or LEN1
     l2 = args.len2 or args.len or LEN2
@@ -473,97 +736,51 @@ def run_ours(args, ws, rank, local):
     ms = max_over_ranks(ev0.elapsed_time(ev1), dev)
     value = job_throughput(ws, args.steps, ms * 1e-3)
 
-    # e2e through the reference-facing C ABI with pinned host buffers
+    # e2e through the reference-facing C ABI: pinned host buffers (one caller, then several
+    # at once, as the reference arm runs its products on parallel host threads; the library's
+    # host lanes overlap one call's PCIe copies with another's kernels), and pageable
+    # malloc-style buffers as the reference's own callers pass them.  Inputs are shared; each
+    # caller has its own output.
     lib = fmn.load_library()
-    ha = torch.from_numpy(a.view(np.int64)).pin_memory().numpy().view(np.uint64)
-    hb = torch.from_numpy(b.view(np.int64)).pin_memory().numpy().view(np.uint64)
-    hout = torch.empty(l1 + l2, dtype=torch.int64).pin_memory().numpy().view(np.uint64)
     P = ctypes.POINTER(ctypes.c_uint64)
-    pa, pb, po = ha.ctypes.data_as(P), hb.ctypes.data_as(P), hout.ctypes.data_as(P)
     e2e_steps = max(3, min(args.steps, 10))
-    lib.abs_mul64(pa, l1, pb, l2, po)                  # warm-up (buffers, tables)
-    barrier()
-    t0 = time.perf_counter()
-    for _ in range(e2e_steps):
-        lib.abs_mul64(pa, l1, pb, l2, po)
-    e2e1_s = max_over_ranks(time.perf_counter() - t0, dev)
-    barrier()
-    e2e_exact = bool(np.array_equal(hout, got))
-    # several host threads calling abs_mul64 at once, as the reference arm runs its products on
-    # parallel host threads: the library's host lanes overlap one call's PCIe copies with
-    # another's kernels.  Each caller has its own pinned output; the inputs are shared.
     callers = args.e2e_callers
-    houts = [torch.empty(l1 + l2, dtype=torch.int64).pin_memory().numpy().view(np.uint64) for _ in range(callers)]
+
+    def pinned(x):
+        return torch.from_numpy(x.view(np.int64)).pin_memory().numpy().view(np.uint64)
+
+    ha, hb = pinned(a), pinned(b)
+    houts = [pinned(np.zeros(l1 + l2, np.uint64)) for _ in range(callers)]
+    pa, pb = ha.ctypes.data_as(P), hb.ctypes.data_as(P)
     pos = [h.ctypes.data_as(P) for h in houts]
-    go = threading.Barrier(callers + 1)
-
-    def caller(i):
-        go.wait()
-        for _ in range(e2e_steps):
-            lib.abs_mul64(pa, l1, pb, l2, pos[i])
-
-    warm = [threading.Thread(target=lambda i=i: lib.abs_mul64(pa, l1, pb, l2, pos[i])) for i in range(callers)]
-    for t in warm:
-        t.start()
-    for t in warm:
-        t.join()
-    ths = [threading.Thread(target=caller, args=(i,)) for i in range(callers)]
-    for t in ths:
-        t.start()
-    barrier()
-    go.wait()
-    t0 = time.perf_counter()
-    for t in ths:
-        t.join()
-    e2e_s = max_over_ranks(time.perf_counter() - t0, dev)
-    barrier()
+    e2e1_s = e2e_rate(lib, pa, l1, pb, l2, pos[:1], e2e_steps, barrier, dev)
+    e2e_exact = bool(np.array_equal(houts[0], got))
+    e2e_s = e2e_rate(lib, pa, l1, pb, l2, pos, e2e_steps, barrier, dev)
     e2e_exact = e2e_exact and all(bool(np.array_equal(h, got)) for h in houts)
+    del ha, hb, houts
+    pouts = [np.zeros(l1 + l2, np.uint64) for _ in range(callers)]
+    ppos = [h.ctypes.data_as(P) for h in pouts]
+    pg_pa, pg_pb = a.ctypes.data_as(P), b.ctypes.data_as(P)
+    pg1_s = e2e_rate(lib, pg_pa, l1, pg_pb, l2, ppos[:1], e2e_steps, barrier, dev)
+    pg_s = e2e_rate(lib, pg_pa, l1, pg_pb, l2, ppos, e2e_steps, barrier, dev)
+    pg_exact = all(bool(np.array_equal(h, got)) for h in pouts)
+    del pouts
 
     result = None
     if rank == 0:
-        peaks = {}
-        try:
-            with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
-                peaks = json.load(f)
-        except Exception:
-            pass
-        hbm_peak = peaks.get("hbm_gbs")
-        hbm_src = "measured" if hbm_peak else "fallback"
-        hbm_peak = hbm_peak or 6650.0
-        mm_peak, bf_peak = fmn.bench_modmul()
         engine = fmn.engine_for(l1, l2)
         pieces = fmn.pieces_for(l1, l2)
-        if engine == fmn.ENGINE_32:
-            # the 32-bit engine's pass kernels are held against its own butterfly peak
-            mm_peak = bf_peak = fmn.bench_bfly32()
-        dom = max(prof.items(), key=lambda kv: kv[1]["ms"])
-        name, st = dom
-        per_launch_ms = st["ms"] / max(1, st["launches"])
-        bytes_per_launch = st["bytes"] / max(1, st["launches"])
-        mm_per_launch = st["modmuls"] / max(1, st["launches"])
-        achieved_gbs = bytes_per_launch / (per_launch_ms * 1e-3) / 1e9
-        achieved_mm = mm_per_launch / (per_launch_ms * 1e-3)
-        traffic = None
-        tpath = os.path.join(ROOT, "profiles", "traffic.json")
-        if os.path.exists(tpath):
-            try:
-                with open(tpath) as f:
-                    traffic = json.load(f).get(name)
-            except Exception:
-                traffic = None
-        total_prof = sum(v["ms"] for v in prof.values()) or 1.0
-        all_mm = sum(v["modmuls"] for v in prof.values()) / args.steps
+        key = f"{'e32' if engine == fmn.ENGINE_32 else 'e64'}:mul:{KIND}:{l1}x{l2}"
+        hbm, integer, kernels = rooflines(fmn, prof, args.steps, engine, peaks, key)
         per_step_ms = ms / args.steps
+        io = 8 * (l1 + l2)
         result = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": per_step_ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u32" if engine == fmn.ENGINE_32 else "u64",
             "data": DATA,
             "config": {"workload": WORKLOAD if (l1, l2) == (LEN1, LEN2) else f"abs_mul64 {l1} x {l2} limbs",
-                       "len1": l1, "len2": l2,
-                       "engine": ("32-bit digits mod three 31-bit primes" if engine == fmn.ENGINE_32
-                                  else "64-bit limbs mod the reference's three 62-bit primes"),
-                       "pieces": pieces,
+                       "len1": l1, "len2": l2, "engine": engine_label(fmn, engine), "pieces": pieces,
                        "plan": ("the longer operand in %d pieces, each multiplied with the other's resident "
                                 "spectrum" % pieces if pieces > 1 else "one transform of the whole product"),
                        "reference_ntt_len": fmn.ntt_len(l1, l2),
@@ -573,46 +790,42 @@ def run_ours(args, ws, rank, local):
             "us_per_product": 1e3 * per_step_ms,
             "limbs_per_s": (l1 + l2) * value,
             "bit_exact": bit_exact,
-            "roofline": {"bound": "hbm", "kernel": name, "achieved": achieved_gbs, "peak": hbm_peak,
-                         "unit": "GB/s", "frac": achieved_gbs / hbm_peak, "traffic": traffic,
-                         "peak_source": f"{hbm_src} (MEASURED_PEAKS.json hbm_gbs)" if hbm_src == "measured"
-                         else "fallback 6.65 TB/s",
-                         "algorithmic_bytes_per_launch": bytes_per_launch, "ms_per_launch": per_launch_ms},
-            "roofline_int": {"bound": "integer issue (butterfly arithmetic)", "kernel": name,
-                             "achieved": achieved_mm / 1e9, "peak": mm_peak / 1e9,
-                             "unit": "Gbutterfly/s" if engine == fmn.ENGINE_32 else "Gmodmul/s",
-                             "frac": achieved_mm / mm_peak,
-                             "peak_source": ("measured: independent 32-bit butterfly chains on this GPU"
-                                             if engine == fmn.ENGINE_32 else
-                                             "measured: independent Montgomery-product chains on this GPU"),
-                             "butterfly_peak": bf_peak / 1e9,
-                             "frac_of_butterfly_peak": achieved_mm / bf_peak,
-                             "algorithmic_modmuls_per_launch": mm_per_launch,
-                             "whole_product_frac": (all_mm / (per_step_ms * 1e-3)) / mm_peak},
-            "kernels": {k: {"ms_per_step": v["ms"] / args.steps, "launches_per_step": v["launches"] / args.steps,
-                            "share": v["ms"] / total_prof} for k, v in prof.items()},
+            "roofline": hbm,
+            "roofline_int": integer,
+            "kernels": kernels,
             "gpu_launches": fmn.launches_per_product(l1, l2) * args.steps,
             "clocks": sampler.summary(),
             "e2e": {"value": ws * callers * e2e_steps / e2e_s, "unit": UNIT,
-                    "h2d_bytes_per_step": 8 * (l1 + l2) * callers, "d2h_bytes_per_step": 8 * (l1 + l2) * callers,
+                    "h2d_bytes_per_step": io * callers, "d2h_bytes_per_step": io * callers,
                     "steps": e2e_steps, "bit_exact": e2e_exact, "callers": callers,
                     "path": ("abs_mul64 (C ABI) on pinned host buffers from %d host threads at once, one "
                              "synchronous call each per step (host wall clock)" % callers),
                     "single_caller": {"value": ws * e2e_steps / e2e1_s, "unit": UNIT,
-                                      "h2d_bytes_per_step": 8 * (l1 + l2), "d2h_bytes_per_step": 8 * (l1 + l2),
-                                      "path": "abs_mul64 (C ABI) on pinned host buffers, one thread, synchronous"}},
+                                      "h2d_bytes_per_step": io, "d2h_bytes_per_step": io,
+                                      "path": "abs_mul64 (C ABI) on pinned host buffers, one thread, synchronous"},
+                    "pageable": {"value": ws * callers * e2e_steps / pg_s, "unit": UNIT,
+                                 "h2d_bytes_per_step": io * callers, "d2h_bytes_per_step": io * callers,
+                                 "bit_exact": pg_exact, "callers": callers,
+                                 "single_caller": ws * e2e_steps / pg1_s,
+                                 "path": ("abs_mul64 (C ABI) on pageable (malloc-style numpy) host buffers, as the "
+                                          "reference's callers pass them; %d threads at once, and one alone"
+                                          % callers)}},
         }
     if dist:
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
-    if rank == 0 and not args.no_batch and (l1, l2) == (LEN1, LEN2):
+    full = rank == 0 and (l1, l2) == (LEN1, LEN2) and ws == 1
+    if full:
         del da, db, dout
         torch.cuda.empty_cache()
+    if full and not args.no_extra:
+        result["extra"] = extra_configs(fmn, torch, dev, peaks)
+    if full and not args.no_batch:
         result["batch"] = batch_compare(fmn, torch, dev, args.batch_count)
-    if rank == 0 and not args.no_serve and (l1, l2) == (LEN1, LEN2):
+    if full and not args.no_serve:
         torch.cuda.empty_cache()
-        result["serve"] = serve_compare(fmn, torch, dev, args.serve_requests, args.serve_rate)
-    if rank == 0 and ws == 1 and not args.no_cpu_baseline and (l1, l2) == (LEN1, LEN2):
+        result["serve"] = serve_compare(fmn, torch, dev, args.serve_requests, rates)
+    if full and not args.no_cpu_baseline:
         cb, cout = cpu_baseline(a, b)
         cb["bit_exact_vs_gpu"] = bool(np.array_equal(cout, got))
         result["cpu_baseline"] = cb

@@ -34,7 +34,8 @@ EXPORTS = ["abs_mul64", "abs_sqr64", "fmn_init", "fmn_shutdown", "fmn_last_error
            "fmn_server_wait", "fmn_server_take", "fmn_server_get_stats", "fmn_server_replay", "fmn_server_destroy",
            "fmn_get_plan", "fmn_set_plan", "fmn_autotune", "fmn_load_plans", "fmn_load_default_plans",
            "fmn_set_engine", "fmn_get_engine", "fmn_engine_for", "fmn_pieces_for",
-           "fmn_force_pieces", "fmn_bench_bfly32", "fmn_get_plan_engine", "fmn_set_plan_engine"]
+           "fmn_force_pieces", "fmn_bench_bfly32", "fmn_get_plan_engine", "fmn_set_plan_engine",
+           "fmn_test_fail_allocs", "fmn_test_carry_timeout", "fmn_server_cancel", "fmn_server_pause"]
 
 ENGINE_AUTO, ENGINE_64, ENGINE_32 = 0, 1, 2
 
@@ -52,7 +53,7 @@ class FmnServerStats(ctypes.Structure):
     """fmn_server_stats of include/fast_mul.h."""
     _fields_ = [("submitted", ctypes.c_uint64), ("completed", ctypes.c_uint64), ("rejected", ctypes.c_uint64),
                 ("failed", ctypes.c_uint64), ("batches", ctypes.c_uint64), ("mismatches", ctypes.c_uint64),
-                ("device_errors", ctypes.c_uint64), ("peak_bytes", ctypes.c_size_t)]
+                ("device_errors", ctypes.c_uint64), ("peak_bytes", ctypes.c_size_t), ("cancelled", ctypes.c_uint64)]
 
 
 class FmnJob(ctypes.Structure):
@@ -125,6 +126,10 @@ def load_library(path=None):
     lib.fmn_bench_modmul.restype = ctypes.c_int
     lib.fmn_bench_bfly32.argtypes = [_dp]
     lib.fmn_bench_bfly32.restype = ctypes.c_int
+    lib.fmn_test_fail_allocs.argtypes = [ctypes.c_int]
+    lib.fmn_test_fail_allocs.restype = ctypes.c_int
+    lib.fmn_test_carry_timeout.argtypes = [_u64]
+    lib.fmn_test_carry_timeout.restype = ctypes.c_int
     lib.fmn_mul_device_noalloc.argtypes = [_vp, _u64, _vp, _u64, _vp, _vp]
     lib.fmn_mul_device_noalloc.restype = ctypes.c_int
     _jp = ctypes.POINTER(FmnJob)
@@ -164,6 +169,10 @@ def load_library(path=None):
     lib.fmn_server_replay.restype = ctypes.c_int
     lib.fmn_server_destroy.argtypes = [_vp]
     lib.fmn_server_destroy.restype = None
+    lib.fmn_server_cancel.argtypes = [_vp, _u64]
+    lib.fmn_server_cancel.restype = ctypes.c_int
+    lib.fmn_server_pause.argtypes = [_vp, ctypes.c_int]
+    lib.fmn_server_pause.restype = ctypes.c_int
     _ip = ctypes.POINTER(ctypes.c_int)
     lib.fmn_get_plan.argtypes = [ctypes.c_int, _ip, ctypes.c_int]
     lib.fmn_get_plan.restype = ctypes.c_int
@@ -423,6 +432,14 @@ class Server:
 
     def wait(self):
         _check(load_library().fmn_server_wait(self.handle))
+
+    def cancel(self, tag):
+        """Withdraw the requests with this tag that still wait for admission; False if none did."""
+        return load_library().fmn_server_cancel(self.handle, tag) == FMN_OK
+
+    def pause(self, paused=True):
+        """Hold (or resume) admission; running batches finish."""
+        _check(load_library().fmn_server_pause(self.handle, 1 if paused else 0))
 
     def take(self, max_n=1 << 16):
         tags = (ctypes.c_uint64 * max_n)()

@@ -15,6 +15,7 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <atomic>
 #include <condition_variable>
 #include <mutex>
 #include <string>
@@ -132,9 +133,23 @@ int get_ctx(DevCtx** out) {
 
 // Grow a cached device buffer to `bytes` (its owner's lock held).  A workspace's error word
 // at offset 0 is zeroed on allocation.
+// Failure-handling tests (fmn_test_fail_allocs): this many of the next device allocations of
+// workspaces and operand buffers fail as if cudaMalloc had found no memory.
+std::atomic<int> g_fail_allocs{0};
+
+bool forced_alloc_failure() {
+    int n = g_fail_allocs.load();
+    while (n > 0)
+        if (g_fail_allocs.compare_exchange_weak(n, n - 1)) return true;
+    return false;
+}
+
 int ensure_buf(void** buf, size_t* cap, size_t bytes, bool workspace) {
     if (*cap >= bytes) return FMN_OK;
     cudaError_t e;
+    if (forced_alloc_failure())
+        return set_err(FMN_ERR_NOMEM, workspace ? "cudaMalloc of the product workspace" : "cudaMalloc of the operand buffers",
+                       cudaErrorMemoryAllocation);
     if (*buf) {
         if ((e = cudaDeviceSynchronize()) != cudaSuccess) return set_err(FMN_ERR_CUDA, "sync before regrow", e);
         cudaFree(*buf);
@@ -664,6 +679,22 @@ int fmn_set_engine(int engine) {
 }
 
 int fmn_get_engine(void) { return fmn::default_engine(); }
+
+int fmn_test_fail_allocs(int count) {
+    if (count < 0) return set_err(FMN_ERR_ARG, "count must be >= 0");
+    g_fail_allocs.store(count);
+    return FMN_OK;
+}
+
+int fmn_test_carry_timeout(u64 out_limbs) {
+    DevCtx* c;
+    int rc = get_ctx(&c);
+    if (rc) return rc;
+    unsigned status = 0;
+    const cudaError_t e = fmn::q32_test_carry_timeout(out_limbs, &status);
+    if (e != cudaSuccess) return set_err(e == cudaErrorInvalidValue ? FMN_ERR_ARG : FMN_ERR_CUDA, "carry timeout test", e);
+    return status ? set_err(FMN_ERR_DEVICE, "carry scan: bounded wait expired") : FMN_OK;
+}
 
 int fmn_force_pieces(int pieces) {
     if (pieces < 0) return set_err(FMN_ERR_ARG, "pieces must be >= 0");

@@ -44,9 +44,9 @@ __device__ __forceinline__ u32 carry_ticket(u32* ticket) {
 
 // Completes the scan for limbs j0 .. j0+NE-1 of this thread (CTA `tile` of CNT * NE limbs,
 // sums lo/h with the contributions from lower limbs already added) and stores the final limbs.
-// `state` holds one word per CTA (zeroed before the first launch); a look-back that waits too
-// long sets *err.
-template <int NE>
+// `state` holds one word per CTA (zeroed before the first launch); a look-back that polls a
+// predecessor's word more than LIMIT times gives up, takes its carry as 0 and sets *err.
+template <int NE, long LIMIT = SPIN_LIMIT>
 __device__ __forceinline__ void carry_finish(u64 (&lo)[NE], u32 (&h)[NE], u64 tile, u64 j0, u32* state, u32* err,
                                              u64* out, u64 out_len) {
     __shared__ u32 s_warp[CNT / 32];
@@ -109,7 +109,7 @@ __device__ __forceinline__ void carry_finish(u64 (&lo)[NE], u32 (&h)[NE], u64 ti
                     long spins = 0;
                     v = st[p];
                     while (v == 0) {
-                        if (++spins > SPIN_LIMIT) {
+                        if (++spins > LIMIT) {
                             failed = true;
                             v = ST_PRE;
                             break;

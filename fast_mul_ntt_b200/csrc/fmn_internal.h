@@ -52,8 +52,9 @@ struct Job {
 // (fmn_ntt32.cu), which is faster; it transforms at most 2^26 digits, so it runs products of up
 // to 2^25 limbs whole and splits longer ones whose shorter operand has at most 2^25 limbs.
 // ENGINE_AUTO takes the one with the lower modelled cost (ENGINE_32 wherever it applies,
-// except where a split would need many pieces).  Both give the same
-// integer product.  Batches and resident operands always use ENGINE_64.
+// except where a split would need many pieces).  Both give the same integer product.
+// Batched products take ENGINE_32 when their whole transform fits it (batch_engine), resident
+// operands when their spectrum fits it (fmn_operand_create); ENGINE_64 otherwise.
 enum Engine { ENGINE_AUTO = 0, ENGINE_64 = 1, ENGINE_32 = 2 };
 void set_default_engine(int engine);
 int default_engine();
@@ -76,6 +77,8 @@ void q32_release_tables(int dev);
 // Forward transform of `len` limbs into a 32-bit resident spectrum (3 * 2^log_n u32).
 cudaError_t q32_spectrum_enqueue(const u64* src, u64 len, int log_n, void* spec, cudaStream_t s, const Plan& plan);
 void q32_force_pieces(int m);                  // tests: split into m pieces where possible (0: model)
+// Tests: the CRT + carry kernel with one look-back tile withheld (see fmn_ntt32.cu).
+cudaError_t q32_test_carry_timeout(u64 out_len, unsigned* status);
 // Pass plans of the 32-bit engine (2^n digits, n <= 26), tuned or set per length.
 Plan q32_make_plan(int log_n);
 Plan q32_default_plan(int log_n);

@@ -18,7 +18,13 @@
 // first call before any stream capture.  All calls share the one array and each call leaves
 // its contents behind: the carry-scan state and the status word are cleared at the start of
 // every call, and two calls whose work overlaps on the GPU (different streams or threads)
-// race on the array and corrupt each other's results.
+// race on the array and corrupt each other's results.  Every call is synchronous: it returns
+// after its work on `stream` has finished, with the kernels' status read back.
+//
+// The products run on the 64-bit residue engine with the pass plans in effect in the process
+// (the default split of each transform length unless another entry point has loaded the
+// tuned plan file: loading plans may build 32-bit twiddle tables, i.e. allocate, so this
+// entry point never loads them itself).  Its four-step twiddles are computed in the kernels.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -30,6 +36,16 @@ namespace {
 
 constexpr u64 kNoallocMaxNtt = 1ull << 16;          // largest transform the array can hold
 static __device__ __align__(256) unsigned char g_noalloc_scratch[(3u << 20) + 4096];
+
+// The 64-bit engine's workspace of the largest accepted product (len1 + len2 = 65537 limbs,
+// N = 2^16 points): [status 256 B][A: 3 N u64][B: 3 N u64][ticket 16 B][one look-back word
+// per CRT + carry CTA of 2048 limbs], rounded up to 256 bytes (fmn_ntt.cu, ws_layout).
+constexpr size_t round256c(size_t x) { return (x + 255) & ~(size_t)255; }
+constexpr size_t kNoallocMaxLayout =
+    round256c(round256c(round256c(256 + 3 * kNoallocMaxNtt * 8) + 3 * kNoallocMaxNtt * 8) + 16 +
+              4 * ((kNoallocMaxNtt + 1 + 2047) / 2048));
+static_assert(kNoallocMaxLayout == 3146240, "64-bit workspace of a 2^16-point product");
+static_assert(sizeof(g_noalloc_scratch) >= kNoallocMaxLayout, "the array holds the largest accepted product");
 
 std::mutex g_noalloc_mu;
 void* g_noalloc_addr[64] = {nullptr};               // device address of the array, per device
@@ -62,11 +78,15 @@ extern "C" int fmn_mul_device_noalloc(const u64* d_in1, u64 len1, const u64* d_i
     j.out = d_out;
     j.sqr = sq;
     j.engine = fmn::ENGINE_64;      // the scratch array is sized for this engine's layout
-    const size_t need = fmn::job_workspace_bytes(j);
-    if (out_len - 1 > kNoallocMaxNtt || need > sizeof(g_noalloc_scratch))
+    if (out_len - 1 > kNoallocMaxNtt)
         return fmn::api_set_error(FMN_ERR_TOO_LARGE,
                                   "fmn_mul_device_noalloc: product needs a transform above 65536 points "
                                   "(len1 + len2 must be <= 65537); use fmn_mul_device or fmn_mul_device_ws",
+                                  cudaSuccess);
+    const size_t need = fmn::job_workspace_bytes(j);
+    if (need > sizeof(g_noalloc_scratch))            // only if the engine's layout grew
+        return fmn::api_set_error(FMN_ERR_TOO_LARGE,
+                                  "fmn_mul_device_noalloc: the product's workspace exceeds the fixed scratch array",
                                   cudaSuccess);
     int dev = 0;
     if ((e = cudaGetDevice(&dev)) != cudaSuccess) return fmn::api_set_error(FMN_ERR_CUDA, "cudaGetDevice", e);

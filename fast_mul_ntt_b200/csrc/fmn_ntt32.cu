@@ -715,6 +715,7 @@ __device__ __forceinline__ u128 qcoef(const QCrtArgs& a, u64 k, const PrimeQ& q0
     return qcrt(a.res[k], a.res[a.N + k], a.res[2 * a.N + k], a, q0, q1, q2);
 }
 
+template <long LIMIT = SPIN_LIMIT>
 __device__ __forceinline__ void qcrt_carry_body(const QCrtArgs& a, u32 ncta) {
     __shared__ u64 s_hw[CNT / 32];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -773,10 +774,16 @@ __device__ __forceinline__ void qcrt_carry_body(const QCrtArgs& a, u32 ncta) {
         }
     }
     add_to(lo[0], h[0], nb);
-    carry_finish(lo, h, tile, j0, a.state, a.err, a.out, a.out_len);
+    carry_finish<QCE, LIMIT>(lo, h, tile, j0, a.state, a.err, a.out, a.out_len);
 }
 
 __global__ void __launch_bounds__(CNT, QCE <= 8 ? 4 : 3) k_qcrt_carry(QCrtArgs a) { qcrt_carry_body(a, 0xffffffffu); }
+
+// The same kernel with a look-back limit of 2^12 polls (milliseconds instead of seconds), for
+// the test that withholds a tile and checks that the wait expires into the status word.
+__global__ void __launch_bounds__(CNT, 4) k_qcrt_carry_short_wait(QCrtArgs a) {
+    qcrt_carry_body<(1l << 12)>(a, 0xffffffffu);
+}
 
 // CRT + carry of many products: CTAs take per-product tickets; tickets beyond a product's
 // CTA count exit at once.
@@ -1772,6 +1779,46 @@ static cudaError_t crt_launch(const QCrtArgs& ca, u64 ncta, u64 t0, u64 t1, cuda
     return cudaSuccess;
 }
 }  // namespace q32
+
+// Failure detection without a fault: the CRT + carry kernel over a zero product of `out_len`
+// limbs (at least two CTA tiles) whose ticket counter starts at 1, so the CTA that would take
+// tile 0 never exists and tile 0 never publishes its carry.  Every later tile's look-back
+// reaches tile 0, polls it up to its (short) limit, gives up and sets the status word; the
+// highest ticket is past the last tile and exits.  No wait is unbounded.  Returns the kernel
+// launch / synchronisation error; *status receives the status word (1 = a wait expired).
+cudaError_t q32_test_carry_timeout(u64 out_len, unsigned* status) {
+    using namespace q32;
+    *status = 0;
+    const u64 ncta = (out_len + QCTILE - 1) / QCTILE;
+    if (ncta < 2 || ncta > 4096) return cudaErrorInvalidValue;
+    const u64 N = 2 * ncta * QCTILE;                 // residue words per prime
+    const size_t res_b = 3 * N * sizeof(u32), out_b = out_len * sizeof(u64);
+    const size_t state_off = align256(res_b + out_b), total = state_off + 256 + (ncta + 1) * sizeof(u32);
+    char* buf = nullptr;
+    cudaError_t e = cudaMalloc((void**)&buf, total);
+    if (e != cudaSuccess) return e;
+    const u32 one = 1;
+    u32* err = (u32*)(buf + state_off);
+    u32* ticket = err + 32;
+    if ((e = cudaMemset(buf, 0, total)) == cudaSuccess && (e = cudaMemcpy(ticket, &one, sizeof(one), cudaMemcpyHostToDevice)) == cudaSuccess) {
+        QCrtArgs ca;
+        memset(&ca, 0, sizeof(ca));
+        crt_constants(N, &ca);
+        ca.res = (const u32*)buf;
+        ca.N = N;
+        ca.nvalid = 2 * out_len - 1;
+        ca.out = (u64*)(buf + align256(res_b));
+        ca.out_len = out_len;
+        ca.ticket = ticket;
+        ca.state = ticket + 1;
+        ca.err = err;
+        k_qcrt_carry_short_wait<<<(unsigned)ncta, CNT>>>(ca);
+        if ((e = cudaGetLastError()) == cudaSuccess && (e = cudaDeviceSynchronize()) == cudaSuccess)
+            e = cudaMemcpy(status, err, sizeof(u32), cudaMemcpyDeviceToHost);
+    }
+    cudaFree(buf);
+    return e;
+}
 
 cudaError_t q32_enqueue(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s, NeedLimbs need_b, void* need_ctx,
                         int crt_chunks, ChunkDone after_chunk, void* ctx) {

@@ -63,6 +63,7 @@ struct Req {
     clk::time_point arrival;
     clk::time_point done;
     size_t bytes;        // scratch charged against the budget
+    bool cancelled;      // withdrawn before admission: never computed, output untouched
 };
 
 struct Slot {
@@ -104,8 +105,9 @@ struct fmn_server {
     std::vector<size_t> completed_order;  // indices in completion order
     size_t taken = 0;                     // completions handed out by fmn_server_take
     size_t in_use = 0, peak = 0;
-    u64 batches = 0, rejected = 0, failures = 0;
+    u64 batches = 0, rejected = 0, failures = 0, cancelled = 0;
     bool stop = false;
+    bool paused = false;                  // admission held (fmn_server_pause)
     std::thread thr;
     std::string error;
 };
@@ -322,7 +324,7 @@ void dispatcher(fmn_server* s) {
                 }
             progress = true;
         };
-        if (s->batching) {
+        if (s->batching && !s->paused) {
             reject_if_too_big(s->big);
             if (!s->big.empty() && !s->slots[0]->busy) {
                 const size_t i = s->big.front();
@@ -332,7 +334,7 @@ void dispatcher(fmn_server* s) {
                 }
             }
         }
-        while (true) {
+        while (!s->paused) {
             reject_if_too_big(s->pending);
             if (s->pending.empty()) break;
             Slot* free_slot = nullptr;
@@ -528,6 +530,7 @@ static int submit_at(fmn_server* s, const fmn_request* r, clk::time_point arriva
         q.arrival = arrival;
         q.done = clk::time_point();
         q.bytes = 0;
+        q.cancelled = false;
         s->log.push_back(q);
         const size_t i = s->log.size() - 1;
         if (s->batching && request_log_n(*r, true) >= kAloneLogN) s->big.push_back(i);
@@ -540,9 +543,48 @@ static int submit_at(fmn_server* s, const fmn_request* r, clk::time_point arriva
 int fmn_server_wait(fmn_server* s) {
     if (!s) return fmn::api_set_error(FMN_ERR_ARG, "null pointer", cudaSuccess);
     std::unique_lock<std::mutex> lk(s->mu);
-    s->cv.wait(lk, [&] { return s->completed_order.size() == s->log.size(); });
+    // a paused server admits nothing: waiting for its queued requests would never end
+    auto held = [&] { return s->paused && (!s->pending.empty() || !s->big.empty()); };
+    s->cv.wait(lk, [&] { return s->completed_order.size() == s->log.size() || held(); });
+    if (s->completed_order.size() != s->log.size())
+        return fmn::api_set_error(FMN_ERR_ARG, "server paused with requests waiting for admission", cudaSuccess);
     return s->failures ? fmn::api_set_error(FMN_ERR_CUDA, s->error.empty() ? "launch failed" : s->error.c_str(), cudaSuccess)
                        : FMN_OK;
+}
+
+int fmn_server_pause(fmn_server* s, int paused) {
+    if (!s) return fmn::api_set_error(FMN_ERR_ARG, "null pointer", cudaSuccess);
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->paused = paused != 0;
+    }
+    s->cv.notify_all();
+    return FMN_OK;
+}
+
+int fmn_server_cancel(fmn_server* s, u64 tag) {
+    if (!s) return fmn::api_set_error(FMN_ERR_ARG, "null pointer", cudaSuccess);
+    int n = 0;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        const clk::time_point now = clk::now();
+        for (std::deque<size_t>* q : {&s->pending, &s->big})
+            for (auto it = q->begin(); it != q->end();) {
+                Req& r = s->log[*it];
+                if (r.r.tag != tag) {
+                    ++it;
+                    continue;
+                }
+                r.cancelled = true;
+                r.done = now;
+                s->completed_order.push_back(*it);
+                ++s->cancelled;
+                ++n;
+                it = q->erase(it);
+            }
+    }
+    s->cv.notify_all();
+    return n ? FMN_OK : fmn::api_set_error(FMN_ERR_ARG, "no request with this tag is waiting for admission", cudaSuccess);
 }
 
 int fmn_server_take(fmn_server* s, u64* tags, double* latency_ms, int max, int* n) {
@@ -569,6 +611,7 @@ int fmn_server_get_stats(fmn_server* s, fmn_server_stats* st) {
     st->failed = s->failures;
     st->batches = s->batches;
     st->peak_bytes = s->peak;
+    st->cancelled = s->cancelled;
     if (cudaMemcpy(s->h_mismatch, s->d_mismatch, 2 * sizeof(unsigned), cudaMemcpyDeviceToHost) == cudaSuccess) {
         st->mismatches = s->h_mismatch[0];
         st->device_errors = s->h_mismatch[1];

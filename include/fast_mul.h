@@ -89,8 +89,10 @@ int fmn_ws_status(const void* d_ws, u64 len1, u64 len2, int sqr, void* stream);
  * limbs (transforms up to 2^16 points) and rejects larger ones with FMN_ERR_TOO_LARGE.
  * The first call on each device looks up the array's device address and uploads the
  * twiddle tables; make it before any stream capture.  Calls share the array: they are
- * serialised with respect to `stream` (the call waits for it), and calls whose work
- * overlaps on the GPU from other streams or threads race on it.
+ * serialised with respect to `stream` (each call is synchronous: it returns once its work on
+ * `stream` has finished), and calls whose work overlaps on the GPU from other streams or
+ * threads race on it.  It runs on FMN_ENGINE_64 with the pass plans in effect in the process
+ * (it never loads the plan file itself, since that may allocate).
  * No counterpart in the reference (which allocates its scratch per call). */
 int fmn_mul_device_noalloc(const u64* d_in1, u64 len1, const u64* d_in2, u64 len2, u64* d_out, void* stream);
 
@@ -164,12 +166,21 @@ typedef struct {
     u64 mismatches;              /* requests whose product differed from `check` */
     u64 device_errors;           /* batches whose carry scan reported a bounded-wait expiry */
     size_t peak_bytes;           /* highest scratch in use */
+    u64 cancelled;               /* requests withdrawn by fmn_server_cancel (also in completed) */
 } fmn_server_stats;
 typedef struct fmn_server fmn_server;
 int fmn_server_create(int device, size_t hbm_budget_bytes, int max_batch, int batching, fmn_server** out);
 int fmn_server_submit(fmn_server* s, const fmn_request* req);
 /* Wait until every submitted request has completed. */
 int fmn_server_wait(fmn_server* s);
+/* Withdraw every request with this tag that is still waiting for admission: it is never
+ * computed (its output is not written) and completes at once, counted in `cancelled`.
+ * FMN_ERR_ARG if no such request is waiting (already admitted, finished or unknown); a
+ * request already on the GPU runs to completion. */
+int fmn_server_cancel(fmn_server* s, u64 tag);
+/* Hold (paused = 1) or resume (0) admission: running batches finish, new and queued requests
+ * wait.  fmn_server_wait returns FMN_ERR_ARG instead of blocking while paused requests wait. */
+int fmn_server_pause(fmn_server* s, int paused);
 /* Completed requests since the last call, in completion order: tags and latency
  * (completion - submission, milliseconds). */
 int fmn_server_take(fmn_server* s, u64* tags, double* latency_ms, int max, int* n);
@@ -188,8 +199,13 @@ void fmn_server_destroy(fmn_server* s);
  * primes, whose modular products are single 32-bit multiplies on the GPU; it covers
  * products whose shorter operand has at most 2^25 limbs (longer ones are split, see
  * fmn_pieces_for).  FMN_ENGINE_AUTO (the default)
- * takes FMN_ENGINE_32 wherever it applies and FMN_ENGINE_64 elsewhere.  Batches and
- * resident operands always run on FMN_ENGINE_64.  No counterpart in the reference. */
+ * takes FMN_ENGINE_32 wherever its modelled cost is lower and FMN_ENGINE_64 elsewhere.
+ * Batches (and the batching server) run each product on FMN_ENGINE_32 when its whole
+ * transform fits that engine (2 (len1 + len2) - 1 <= 2^26 digits) and on FMN_ENGINE_64
+ * otherwise; a resident operand holds a FMN_ENGINE_32 spectrum when
+ * 2 (len + max_partner_len) - 1 <= 2^26 digits and a FMN_ENGINE_64 one otherwise.  Under
+ * fmn_set_engine(FMN_ENGINE_64) everything runs on FMN_ENGINE_64.  No counterpart in the
+ * reference. */
 #define FMN_ENGINE_AUTO 0
 #define FMN_ENGINE_64 1
 #define FMN_ENGINE_32 2
@@ -253,6 +269,20 @@ int fmn_launches_per_product(u64 len1, u64 len2, int sqr);
 int fmn_bench_modmul(double* modmul_per_s, double* butterfly_per_s);
 /* Peak of the 32-bit engine's butterfly (independent chains, per second). */
 int fmn_bench_bfly32(double* butterfly_per_s);
+
+/* ----------------------------------------------------------------- failure-handling tests
+ * Hooks that make the library's error paths run without faulting the GPU (no counterpart in
+ * the reference).
+ * fmn_test_fail_allocs: the next `count` device allocations of product workspaces and operand
+ * buffers fail as if cudaMalloc had found no memory, so fmn_mul returns FMN_ERR_NOMEM and
+ * abs_mul64 prints the error and calls abort(), as the reference does when its allocation
+ * fails (src/fast_mul.c:320-323).  0 turns it off.
+ * fmn_test_carry_timeout: runs the CRT + carry kernel over a zero product of out_limbs limbs
+ * (2 to 4096 tiles of 2048 limbs) with tile 0 withheld, so every later tile's bounded
+ * look-back wait expires after a few milliseconds and sets the status word; returns
+ * FMN_ERR_DEVICE, the status a product whose wait expired reports.  The device stays usable. */
+int fmn_test_fail_allocs(int count);
+int fmn_test_carry_timeout(u64 out_limbs);
 
 /* Transform length used for a product: the next power of two >= len1 + len2 - 1
  * (int_ceil2, src/fast_mul.c:299-312). */
