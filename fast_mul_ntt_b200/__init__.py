@@ -35,7 +35,8 @@ EXPORTS = ["abs_mul64", "abs_sqr64", "fmn_init", "fmn_shutdown", "fmn_last_error
            "fmn_get_plan", "fmn_set_plan", "fmn_autotune", "fmn_load_plans", "fmn_load_default_plans",
            "fmn_set_engine", "fmn_get_engine", "fmn_engine_for", "fmn_pieces_for",
            "fmn_force_pieces", "fmn_bench_bfly32", "fmn_get_plan_engine", "fmn_set_plan_engine",
-           "fmn_test_fail_allocs", "fmn_test_carry_timeout", "fmn_server_cancel", "fmn_server_pause"]
+           "fmn_test_fail_allocs", "fmn_test_carry_timeout", "fmn_server_cancel", "fmn_server_pause",
+           "fmn_wrap_for", "fmn_force_wrap"]
 
 ENGINE_AUTO, ENGINE_64, ENGINE_32 = 0, 1, 2
 
@@ -126,6 +127,10 @@ def load_library(path=None):
     lib.fmn_bench_modmul.restype = ctypes.c_int
     lib.fmn_bench_bfly32.argtypes = [_dp]
     lib.fmn_bench_bfly32.restype = ctypes.c_int
+    lib.fmn_wrap_for.argtypes = [_u64, _u64, ctypes.c_int]
+    lib.fmn_wrap_for.restype = _u64
+    lib.fmn_force_wrap.argtypes = [ctypes.c_int]
+    lib.fmn_force_wrap.restype = ctypes.c_int
     lib.fmn_test_fail_allocs.argtypes = [ctypes.c_int]
     lib.fmn_test_fail_allocs.restype = ctypes.c_int
     lib.fmn_test_carry_timeout.argtypes = [_u64]
@@ -518,6 +523,16 @@ def pieces_for(len1, len2, sqr=False):
 def force_pieces(pieces):
     """Tests and tuning: split products into this many pieces where possible (0: cost model)."""
     _check(load_library().fmn_force_pieces(pieces))
+
+
+def wrap_for(len1, len2, sqr=False):
+    """Coefficients that wrap around the transform length of a wrapped product (0: not wrapped)."""
+    return int(load_library().fmn_wrap_for(len1, len2, 1 if sqr else 0))
+
+
+def force_wrap(on=True):
+    """Tests: wrap every product that allows it (False: cost model)."""
+    _check(load_library().fmn_force_wrap(1 if on else 0))
 
 
 def autotune(n_lo=10, n_hi=27, save_path=None):

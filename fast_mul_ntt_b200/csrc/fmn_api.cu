@@ -712,6 +712,21 @@ int fmn_pieces_for(u64 len1, u64 len2, int sqr) {
     return fmn::job_engine(j) == fmn::ENGINE_32 ? fmn::q32_pieces(len1, len2, sqr ? 1 : 0) : 1;
 }
 
+int fmn_force_wrap(int on) {
+    fmn::q32_force_wrap(on);
+    return FMN_OK;
+}
+
+u64 fmn_wrap_for(u64 len1, u64 len2, int sqr) {
+    fmn::Job j;
+    j.a = j.b = nullptr;
+    j.out = nullptr;
+    j.la = len1;
+    j.lb = len2;
+    j.sqr = sqr ? 1 : 0;
+    return fmn::job_engine(j) == fmn::ENGINE_32 ? fmn::q32_wrapped(len1, len2, sqr ? 1 : 0) : 0;
+}
+
 int fmn_engine_for(u64 len1, u64 len2, int sqr) {
     fmn::Job j;
     j.a = j.b = nullptr;

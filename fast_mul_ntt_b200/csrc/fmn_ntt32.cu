@@ -668,6 +668,12 @@ __global__ void __launch_bounds__(NT, (min_ctas<MODE, LOGL>())) k_qpass_batch(co
 // reference's CRT sum, src/core.h:77-104, without its final reduction mod Q).  Output limb j
 // collects the 128-bit pair C_j = c_{2j} + c_{2j+1} 2^32 < 2^124: s_j = C_j.lo + C_{j-1}.hi,
 // then the carry scan.
+//
+// Wrapped products (wrap = K > 0): `res` holds a cyclic convolution of length N, whose entry
+// k < K is c_k + c_{k+N} (the coefficients from N on wrap around), and `low` holds the product
+// of the operands' lowest digits, whose coefficients below K are exactly c_0 .. c_{K-1}.  So
+// c_k = low_k for k < K, res_k for K <= k < N, and res_{k-N} - low_{k-N} (mod each prime) for
+// N <= k < N + K.  Each array carries its own scale constants (its transform length differs).
 struct QCrtArgs {
     const u32* res;     // three natural-order residue arrays (prime i at res + i*N), in [0, q)
     u64 N;
@@ -681,6 +687,10 @@ struct QCrtArgs {
     u32* state;
     u32* ticket;
     u32* err;
+    const u32* low;     // wrapped products: the low product's residues (prime i at low + i*low_N)
+    u64 low_N;
+    u64 wrap;           // K: coefficients that wrapped (0: none)
+    u32 low_cst[3];     // the low product's scale constants (low_N^-1 * 2^64 mod q_i)
 };
 
 typedef unsigned __int128 u128;
@@ -691,11 +701,9 @@ constexpr u64 Q01 = (u64)Q32_P0 * Q32_P1;
 constexpr int QCE = 8;
 constexpr u64 QCTILE = (u64)CNT * QCE;  // output limbs per CTA
 
-__device__ __forceinline__ u128 qcrt(u32 r0, u32 r1, u32 r2, const QCrtArgs& a, const PrimeQ& q0, const PrimeQ& q1,
-                                     const PrimeQ& q2) {
-    const u32 x0 = qmont(r0, a.cst[0], q0);                    // c mod q0
-    const u32 y1 = qmont(r1, a.cst[1], q1);                    // c mod q1
-    const u32 y2 = qmont(r2, a.cst[2], q2);                    // c mod q2
+// c from x0 = c mod q0, y1 = c mod q1, y2 = c mod q2 (all reduced).
+__device__ __forceinline__ u128 qgarner(u32 x0, u32 y1, u32 y2, const QCrtArgs& a, const PrimeQ& q1,
+                                        const PrimeQ& q2) {
     const u32 x0r = x0 >= q1.p ? x0 - q1.p : x0;               // q0 < 2 q1
     const u32 x1 = qmont(qsub(y1, x0r, q1), a.inv01, q1);      // (c - x0) / q0 mod q1
     const u32 t = qadd(qsmul(x0, 1u, q2.one, q2), qmont(x1, a.q0m2, q2), q2);
@@ -710,12 +718,31 @@ __device__ __forceinline__ u128 qcrt(u32 r0, u32 r1, u32 r2, const QCrtArgs& a, 
     hi += (lo < ml) + (mid >> 32);
     return ((u128)hi << 64) | lo;
 }
+// Residue vectors of 4 consecutive coefficients from one array of one prime.
+__device__ __forceinline__ void ld4(const u32* p, u32 (&r)[4]) {
+    const uint4 v = *reinterpret_cast<const uint4*>(p);
+    r[0] = v.x, r[1] = v.y, r[2] = v.z, r[3] = v.w;
+}
+// Where coefficient k comes from (see QCrtArgs): 0 res_k, 1 low_k, 2 res_{k-N} - low_{k-N}.
+__device__ __forceinline__ int qsource(const QCrtArgs& a, u64 k) {
+    return k < a.wrap ? 1 : (k >= a.N && a.wrap ? 2 : 0);
+}
+// c_k mod q_i (reduced) of one prime, by source.
+__device__ __forceinline__ u32 qscaled(const QCrtArgs& a, int src, u64 k, int i, const PrimeQ& q) {
+    if (src == 0) return qmont(a.res[i * a.N + k], a.cst[i], q);
+    if (src == 1) return qmont(a.low[i * a.low_N + k], a.low_cst[i], q);
+    const u64 kk = k - a.N;
+    return qsub(qmont(a.res[i * a.N + kk], a.cst[i], q), qmont(a.low[i * a.low_N + kk], a.low_cst[i], q), q);
+}
+template <bool WRAP>
 __device__ __forceinline__ u128 qcoef(const QCrtArgs& a, u64 k, const PrimeQ& q0, const PrimeQ& q1, const PrimeQ& q2) {
     if (k >= a.nvalid) return 0;
-    return qcrt(a.res[k], a.res[a.N + k], a.res[2 * a.N + k], a, q0, q1, q2);
+    const int src = WRAP ? qsource(a, k) : 0;
+    return qgarner(qscaled(a, src, k, 0, q0), qscaled(a, src, k, 1, q1), qscaled(a, src, k, 2, q2), a, q1, q2);
 }
 
-template <long LIMIT = SPIN_LIMIT>
+// WRAP: the product is wrapped (see QCrtArgs); its kernel holds more registers per thread.
+template <bool WRAP, long LIMIT = SPIN_LIMIT>
 __device__ __forceinline__ void qcrt_carry_body(const QCrtArgs& a, u32 ncta) {
     __shared__ u64 s_hw[CNT / 32];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -727,28 +754,60 @@ __device__ __forceinline__ void qcrt_carry_body(const QCrtArgs& a, u32 ncta) {
     u64 lo[QCE];
     u32 h[QCE];
     u64 phi = 0;                                       // C_{j-1}.hi
-    const bool full = k0 + 2 * QCE <= a.nvalid;
+    // the thread's 2 QCE coefficients come from one source (k0 and N are multiples of 16),
+    // read as vectors, unless they straddle the end or the wrap boundary K
+    const int src = WRAP ? qsource(a, k0) : 0;
+    const bool full = k0 + 2 * QCE <= a.nvalid && (src != 1 || k0 + 2 * QCE <= a.wrap);
+    const u64 kb = src == 2 ? k0 - a.N : k0;
 #pragma unroll
     for (int e2 = 0; e2 < QCE; e2 += 2) {             // two limbs = four coefficients at a time
-        u32 r0[4], r1[4], r2[4];
+        u32 y0[4], y1[4], y2[4];                       // c_k mod q_i
         if (full) {
-            const uint4 v0 = *reinterpret_cast<const uint4*>(a.res + k0 + 2 * e2);
-            const uint4 v1 = *reinterpret_cast<const uint4*>(a.res + a.N + k0 + 2 * e2);
-            const uint4 v2 = *reinterpret_cast<const uint4*>(a.res + 2 * a.N + k0 + 2 * e2);
-            r0[0] = v0.x, r0[1] = v0.y, r0[2] = v0.z, r0[3] = v0.w;
-            r1[0] = v1.x, r1[1] = v1.y, r1[2] = v1.z, r1[3] = v1.w;
-            r2[0] = v2.x, r2[1] = v2.y, r2[2] = v2.z, r2[3] = v2.w;
+            const u64 k = kb + 2 * e2;
+            if (src == 1) {
+                ld4(a.low + k, y0);
+                ld4(a.low + a.low_N + k, y1);
+                ld4(a.low + 2 * a.low_N + k, y2);
+#pragma unroll
+                for (int t = 0; t < 4; ++t) {
+                    y0[t] = qmont(y0[t], a.low_cst[0], q0);
+                    y1[t] = qmont(y1[t], a.low_cst[1], q1);
+                    y2[t] = qmont(y2[t], a.low_cst[2], q2);
+                }
+            } else {
+                ld4(a.res + k, y0);
+                ld4(a.res + a.N + k, y1);
+                ld4(a.res + 2 * a.N + k, y2);
+#pragma unroll
+                for (int t = 0; t < 4; ++t) {
+                    y0[t] = qmont(y0[t], a.cst[0], q0);
+                    y1[t] = qmont(y1[t], a.cst[1], q1);
+                    y2[t] = qmont(y2[t], a.cst[2], q2);
+                }
+                if (src == 2) {
+                    u32 l0[4], l1[4], l2[4];
+                    ld4(a.low + k, l0);
+                    ld4(a.low + a.low_N + k, l1);
+                    ld4(a.low + 2 * a.low_N + k, l2);
+#pragma unroll
+                    for (int t = 0; t < 4; ++t) {
+                        y0[t] = qsub(y0[t], qmont(l0[t], a.low_cst[0], q0), q0);
+                        y1[t] = qsub(y1[t], qmont(l1[t], a.low_cst[1], q1), q1);
+                        y2[t] = qsub(y2[t], qmont(l2[t], a.low_cst[2], q2), q2);
+                    }
+                }
+            }
         }
 #pragma unroll
         for (int u = 0; u < 2; ++u) {
             const int e = e2 + u;
             u128 cl, ch;
             if (full) {
-                cl = qcrt(r0[2 * u], r1[2 * u], r2[2 * u], a, q0, q1, q2);
-                ch = qcrt(r0[2 * u + 1], r1[2 * u + 1], r2[2 * u + 1], a, q0, q1, q2);
+                cl = qgarner(y0[2 * u], y1[2 * u], y2[2 * u], a, q1, q2);
+                ch = qgarner(y0[2 * u + 1], y1[2 * u + 1], y2[2 * u + 1], a, q1, q2);
             } else {
-                cl = qcoef(a, k0 + 2 * e, q0, q1, q2);
-                ch = qcoef(a, k0 + 2 * e + 1, q0, q1, q2);
+                cl = qcoef<WRAP>(a, k0 + 2 * e, q0, q1, q2);
+                ch = qcoef<WRAP>(a, k0 + 2 * e + 1, q0, q1, q2);
             }
             const u128 C = cl + (ch << 32);
             u64 l = (u64)C;
@@ -767,7 +826,7 @@ __device__ __forceinline__ void qcrt_carry_body(const QCrtArgs& a, u32 ncta) {
         if (warp > 0) {
             nb = s_hw[warp - 1];
         } else if (j0 > 0) {
-            const u128 C = qcoef(a, k0 - 2, q0, q1, q2) + (qcoef(a, k0 - 1, q0, q1, q2) << 32);
+            const u128 C = qcoef<WRAP>(a, k0 - 2, q0, q1, q2) + (qcoef<WRAP>(a, k0 - 1, q0, q1, q2) << 32);
             nb = (u64)(C >> 64);
         } else {
             nb = 0;
@@ -777,12 +836,17 @@ __device__ __forceinline__ void qcrt_carry_body(const QCrtArgs& a, u32 ncta) {
     carry_finish<QCE, LIMIT>(lo, h, tile, j0, a.state, a.err, a.out, a.out_len);
 }
 
-__global__ void __launch_bounds__(CNT, QCE <= 8 ? 4 : 3) k_qcrt_carry(QCrtArgs a) { qcrt_carry_body(a, 0xffffffffu); }
+__global__ void __launch_bounds__(CNT, QCE <= 8 ? 4 : 3) k_qcrt_carry(QCrtArgs a) {
+    qcrt_carry_body<false>(a, 0xffffffffu);
+}
+// Wrapped products: two residue sources and a second set of scale constants take more
+// registers than 4 CTAs per SM allow without spills.
+__global__ void __launch_bounds__(CNT, 3) k_qcrt_carry_wrap(QCrtArgs a) { qcrt_carry_body<true>(a, 0xffffffffu); }
 
-// The same kernel with a look-back limit of 2^12 polls (milliseconds instead of seconds), for
+// The plain kernel with a look-back limit of 2^12 polls (milliseconds instead of seconds), for
 // the test that withholds a tile and checks that the wait expires into the status word.
 __global__ void __launch_bounds__(CNT, 4) k_qcrt_carry_short_wait(QCrtArgs a) {
-    qcrt_carry_body<(1l << 12)>(a, 0xffffffffu);
+    qcrt_carry_body<false, (1l << 12)>(a, 0xffffffffu);
 }
 
 // CRT + carry of many products: CTAs take per-product tickets; tickets beyond a product's
@@ -790,7 +854,7 @@ __global__ void __launch_bounds__(CNT, 4) k_qcrt_carry_short_wait(QCrtArgs a) {
 __global__ void __launch_bounds__(CNT) k_qcrt_carry_batch(const QCrtArgs* __restrict__ args, u32 ctas_per_job,
                                                           const u32* __restrict__ ncta) {
     const u32 job = blockIdx.x / ctas_per_job;
-    qcrt_carry_body(args[job], ncta[job]);
+    qcrt_carry_body<false>(args[job], ncta[job]);
 }
 
 // ------------------------------------------------------------------ host: tables
@@ -1091,12 +1155,48 @@ struct QJob {
     u64 stride;            // split: accumulator digits per prime
     size_t a, b, acc, ticket, state, total;   // workspace offsets (split: a = S's spectrum, b = piece)
     u64 ncta;
+    // wrapped (m == 1, wrap > 0): the product's 2 (la + lb) - 1 digit coefficients exceed N, so
+    // the transform of length N gives a cyclic convolution whose entries k < wrap hold
+    // c_k + c_{k+N}; the product of the lowest lpa / lpb limbs (whole, at 2^nl digits, residue
+    // arrays at la_off / lb_off) gives c_0 .. c_{wrap-1}, and the CRT separates the two.
+    u64 wrap;
+    u64 lpa, lpb;
+    int nl;
+    u64 NL;
+    size_t la_off, lb_off;
 };
 
 constexpr int kMinSplitLog = 12;           // pieces transform at least 2^12 digits (>= 2 passes)
 std::atomic<int> g_force_pieces{0};        // > 1: split every product that allows it into this many pieces
 constexpr u64 kMaxPieces = 1ull << 16;
 constexpr double kPieceCost = 3.0e7;       // launch overhead of one piece, in (points x bits)
+std::atomic<int> g_force_wrap{0};          // tests: wrap every product that allows it
+
+// The wrapped plan of a product of la x lb limbs (see QJob), if the product allows one: both
+// operands fit the 2^n-digit cyclic length (2^n < 2 (la + lb) - 1) and the low product is a
+// whole product on this engine.  Returns its modelled cost, or a negative value.
+static double plan_wrap(u64 la, u64 lb, int sqr, QJob* W) {
+    const u64 dc = 2 * (la + lb) - 1;                          // digit coefficients of the product
+    const int n = ilog2(dc) - 1;                                // 2^n < dc <= 2^(n+1)
+    if (n < 1 || n > Q32_MAX_LOG_N) return -1.0;
+    const u64 N = 1ull << n;
+    if (2 * la > N || 2 * lb > N) return -1.0;                 // an operand would wrap itself
+    const u64 K = dc - N;
+    const u64 half = (K + 1) / 2;                               // limbs holding digits 0 .. K-1
+    const u64 lpa = la < half ? la : half, lpb = sqr ? lpa : (lb < half ? lb : half);
+    const u64 dcl = 2 * (lpa + lpb) - 1;
+    const int nl = ilog2(dcl);
+    if (nl > Q32_MAX_LOG_N) return -1.0;
+    W->wrap = K;
+    W->lpa = lpa;
+    W->lpb = lpb;
+    W->nl = nl;
+    W->NL = 1ull << nl;
+    W->n = n;
+    W->N = N;
+    const double t = sqr ? 2.0 : 3.0;
+    return t * (double)N * (n + 1) + t * (double)W->NL * (nl + 1) + kPieceCost;
+}
 
 static QJob plan_job(u64 la, u64 lb, int sqr) {
     QJob J;
@@ -1154,6 +1254,17 @@ static QJob plan_job(u64 la, u64 lb, int sqr) {
             }
         }
     }
+    if (best >= 0.0) {
+        QJob W;
+        memset(&W, 0, sizeof(W));
+        const double cw = plan_wrap(la, lb, sqr, &W);
+        if (cw >= 0.0 && (cw < best || g_force_wrap.load())) {
+            best = cw;
+            J = W;
+            J.ok = true;
+            J.m = 1;
+        }
+    }
     if (!J.ok) return J;
     J.cost = best;
     J.ncta = (out_len + QCTILE - 1) / QCTILE;
@@ -1162,6 +1273,12 @@ static QJob plan_job(u64 la, u64 lb, int sqr) {
     off = align256(off + 3 * J.N * sizeof(u32));
     J.b = off;
     if (!(J.m == 1 && sqr)) off = align256(off + 3 * J.N * sizeof(u32));
+    if (J.wrap) {
+        J.la_off = off;
+        off = align256(off + 3 * J.NL * sizeof(u32));
+        J.lb_off = off;
+        if (!sqr) off = align256(off + 3 * J.NL * sizeof(u32));
+    }
     if (J.m > 1) {
         J.stride = (2 * out_len + 63) & ~63ull;
         J.acc = off;
@@ -1582,12 +1699,26 @@ size_t q32_workspace_bytes(u64 la, u64 lb, int sqr) {
 int q32_launches(u64 la, u64 lb, int sqr) {
     const q32::QJob J = q32::plan_job(la, lb, sqr);
     if (!J.ok) return 0;
-    const Plan pl = q32::qplan(J.n);
-    const int P = pl.passes;
-    const int lastl = pl.bits[P - 1];
-    if (J.m > 1) return P + J.m * ((P - 1) + 1 + (P - 1)) + 1;
-    if (!sqr && P >= 2 && lastl >= 5 && lastl <= 8) return 2 * (P - 1) + 1 + (P - 1) + 1;
-    return sqr ? (P - 1) + 1 + (P - 1) + 1 : 2 * (P - 1) + 1 + 1 + (P - 1) + 1;
+    // transform launches of a whole product at 2^n digits (plan_whole), without the CRT
+    auto whole = [sqr](int n) {
+        const Plan pl = q32::qplan(n);
+        const int P = pl.passes;
+        const int lastl = pl.bits[P - 1];
+        if (!sqr && P >= 2 && lastl >= 5 && lastl <= 8) return 2 * (P - 1) + 1 + (P - 1);
+        return sqr ? (P - 1) + 1 + (P - 1) : 2 * (P - 1) + 1 + 1 + (P - 1);
+    };
+    if (J.m > 1) {
+        const int P = q32::qplan(J.n).passes;
+        return P + J.m * ((P - 1) + 1 + (P - 1)) + 1;
+    }
+    return whole(J.n) + (J.wrap ? whole(J.nl) : 0) + 1;
+}
+
+void q32_force_wrap(int on) { q32::g_force_wrap.store(on ? 1 : 0); }
+
+u64 q32_wrapped(u64 la, u64 lb, int sqr) {
+    const q32::QJob J = q32::plan_job(la, lb, sqr);
+    return J.ok ? J.wrap : 0;
 }
 
 int q32_pieces(u64 la, u64 lb, int sqr) {
@@ -1770,7 +1901,8 @@ static cudaError_t crt_launch(const QCrtArgs& ca, u64 ncta, u64 t0, u64 t1, cuda
     const u64 n = t1 - t0;
     const double crt_bytes = 3.0 * (double)ca.nvalid * 4.0 + (double)ca.out_len * 8.0;
     const ProfMark m = prof_begin(K_CRT, crt_bytes * (double)n / (double)ncta, 3.0 * (double)ca.nvalid * (double)n / (double)ncta, s);
-    k_qcrt_carry<<<(unsigned)n, CNT, 0, s>>>(ca);
+    if (ca.wrap) k_qcrt_carry_wrap<<<(unsigned)n, CNT, 0, s>>>(ca);
+    else k_qcrt_carry<<<(unsigned)n, CNT, 0, s>>>(ca);
     cudaError_t e = cudaGetLastError();
     prof_end(m, s);
     if (e != cudaSuccess) return e;
@@ -1887,12 +2019,42 @@ cudaError_t q32_enqueue(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s,
     if (J.m == 1) {
         u32* A = (u32*)(base + J.a);
         u32* B = sqr ? A : (u32*)(base + J.b);
+        u64 b_ready = sqr ? j.lb : 0;                          // limbs of the second operand requested so far
+        if (J.wrap) {
+            // the product of the lowest digits first (it reads the second operand's first lpb
+            // limbs): its coefficients below `wrap` are the product's c_0 .. c_{wrap-1}
+            Job jl = j;
+            jl.la = J.lpa;
+            jl.lb = J.lpb;
+            u32* LA = (u32*)(base + J.la_off);
+            u32* LB = sqr ? LA : (u32*)(base + J.lb_off);
+            const Plan pll = qplan(J.nl);
+            TwPass twl[MAX_PASSES];
+            for (int p = 0, lg = J.nl; p + 1 < pll.passes; lg -= pll.bits[p], ++p) twl[p] = tw_tables(lg, pll.bits[p], s);
+            QWhole WL;
+            plan_whole(jl, J.nl, LA, LB, &WL, false, twl);
+            for (int k = 0; k < WL.count; ++k) {
+                if (b_ready == 0 && WL.rec[k].a.src == j.b) {
+                    if ((e = launch.need(0, J.lpb)) != cudaSuccess) return e;
+                    b_ready = J.lpb;
+                }
+                if ((e = launch(WL.rec[k].variant, WL.rec[k].logl, WL.rec[k].a, WL.rec[k].tiles)) != cudaSuccess)
+                    return e;
+            }
+            QCrtArgs cl;
+            memset(&cl, 0, sizeof(cl));
+            crt_constants(J.NL, &cl);
+            ca.low = LA;
+            ca.low_N = J.NL;
+            ca.wrap = J.wrap;
+            for (int i = 0; i < 3; ++i) ca.low_cst[i] = cl.cst[i];
+        }
         QWhole W;
         plan_whole(j, J.n, A, B, &W, false, tws);
         bool have_b = sqr != 0;
         for (int k = 0; k < W.count; ++k) {
             if (!have_b && W.rec[k].a.src == j.b) {            // the second operand's first reader
-                if ((e = launch.need(0, j.lb)) != cudaSuccess) return e;
+                if (b_ready < j.lb && (e = launch.need(b_ready, j.lb)) != cudaSuccess) return e;
                 have_b = true;
             }
             if ((e = launch(W.rec[k].variant, W.rec[k].logl, W.rec[k].a, W.rec[k].tiles)) != cudaSuccess) return e;

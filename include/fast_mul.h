@@ -225,6 +225,17 @@ int fmn_pieces_for(u64 len1, u64 len2, int sqr);
 /* Testing and tuning: split every product that allows it into `pieces` pieces regardless of
  * the cost model (0 or 1 restores the model).  Process-wide. */
 int fmn_force_pieces(int pieces);
+/* Wrapped products (FMN_ENGINE_32): a product whose 2 (len1 + len2) - 1 digit coefficients
+ * exceed a power of two 2^n by K, while both operands fit 2^n digits, can run as one cyclic
+ * transform of 2^n digits (its first K coefficients then hold c_k + c_{k+2^n}) plus the
+ * product of the operands' lowest ceil(K / 2) limbs, which gives c_0 .. c_{K-1}; the CRT
+ * separates the two.  This replaces a transform of twice the length by one of the same length
+ * and a small one: the padding a product just above a power of two would pay.  Chosen by the
+ * cost model beside whole and split products.  fmn_wrap_for returns K for a product that runs
+ * wrapped (0 otherwise); fmn_force_wrap(1) wraps every product that allows it (tests),
+ * fmn_force_wrap(0) restores the model.  No counterpart in the reference. */
+u64 fmn_wrap_for(u64 len1, u64 len2, int sqr);
+int fmn_force_wrap(int on);
 
 /* ----------------------------------------------------------------- pass plans and tuning
  * A 2^n-point transform runs as passes of <= 9 index bits each; the split is a plan (e.g.

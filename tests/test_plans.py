@@ -121,18 +121,23 @@ def test_products_under_every_plan_shape(fmn, oracle):
 
 
 def test_engine_selection_rules():
-    """AUTO takes the 32-bit residue engine up to 2^25 output limbs and the 64-bit one beyond;
-    a forced engine is honoured where it applies; resident/batched paths are documented as
-    64-bit only."""
+    """AUTO takes the 32-bit residue engine wherever its plan (whole, split or wrapped) costs
+    less than the 64-bit engine's transform, and the 64-bit one beyond; a forced engine is
+    honoured where it applies."""
     assert fmn.get_engine() == fmn.ENGINE_AUTO
     assert fmn.engine_for(10_000_000, 10_000_000) == fmn.ENGINE_32
     assert fmn.engine_for(1 << 24, 1 << 24) == fmn.ENGINE_32             # 2^26-digit transform
-    # one limb more: the 64-bit engine's transform (2^25 points) is cheaper than any split
-    assert fmn.engine_for(1 << 24, (1 << 24) + 1) == fmn.ENGINE_64
+    # one limb more: one wrapped coefficient, a 2^26-digit cyclic transform and a tiny low
+    # product, cheaper than the 64-bit engine's 2^25-point transform or any split
+    assert fmn.engine_for(1 << 24, (1 << 24) + 1) == fmn.ENGINE_32
+    assert fmn.wrap_for(1 << 24, (1 << 24) + 1) == 1
     assert fmn.engine_for(1000, 1000, sqr=True) == fmn.ENGINE_32
-    # split products: 10M x 10M in two 10M x 5M pieces at 2^25 digits; unbalanced products
-    # above 2^25 limbs reach the 32-bit engine only split
-    assert fmn.pieces_for(10_000_000, 10_000_000) == 2
+    # 10M x 10M: 40M - 1 digit coefficients, a 2^25-digit cyclic transform whose first
+    # 6,445,567 coefficients wrap, plus the 3.2M x 3.2M-limb product of the low limbs
+    assert fmn.pieces_for(10_000_000, 10_000_000) == 1
+    assert fmn.wrap_for(10_000_000, 10_000_000) == 2 * 20_000_000 - 1 - (1 << 25)
+    assert fmn.wrap_for(1_000_000, 1_000_000) == 0                        # whole at 2^22 is cheaper
+    # split products: unbalanced products above 2^25 limbs reach the 32-bit engine only split
     assert fmn.engine_for(64_000_000, 250_000) == fmn.ENGINE_32
     assert fmn.pieces_for(64_000_000, 250_000) > 1
     assert fmn.pieces_for(1_000_000, 1_000_000) == 1
