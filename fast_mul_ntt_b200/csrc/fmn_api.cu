@@ -454,6 +454,7 @@ int host_product_pinned(DevCtx* c, HostLane* L, const u64* in1, u64 len1, const 
 }
 
 int host_product(const u64* in1, u64 len1, const u64* in2, u64 len2, u64* out, int sqr) {
+    fmn::NvtxRange nvtx("fmn host product");
     const u64 out_len = len1 + len2;
     if (out_len == 0) return FMN_OK;
     if (!in1 || !out || (!sqr && !in2)) return set_err(FMN_ERR_ARG, "null pointer");
@@ -513,6 +514,7 @@ int host_product(const u64* in1, u64 len1, const u64* in2, u64 len2, u64* out, i
 }
 
 int device_product(const u64* d1, u64 len1, const u64* d2, u64 len2, u64* dout, int sqr, void* stream) {
+    fmn::NvtxRange nvtx("fmn device product");
     const u64 out_len = len1 + len2;
     if (out_len == 0) return FMN_OK;
     if (!d1 || !dout || (!sqr && !d2)) return set_err(FMN_ERR_ARG, "null pointer");
@@ -780,6 +782,7 @@ int fmn_ws_status(const void* d_ws, u64 len1, u64 len2, int sqr, void* stream) {
 }
 
 int fmn_mul_batch_device(const fmn_job* jobs, int count, void* stream) {
+    fmn::NvtxRange nvtx("fmn batch");
     std::vector<fmn::Job> v;
     int rc = to_jobs(jobs, count, v);
     if (rc || count == 0) return rc;
@@ -914,6 +917,7 @@ int fmn_batch_graph_create(const fmn_job* jobs, int count, fmn_batch_graph** out
 }
 
 int fmn_batch_graph_launch(fmn_batch_graph* g, void* stream) {
+    fmn::NvtxRange nvtx("fmn batch graph launch");
     if (!g) return set_err(FMN_ERR_ARG, "null graph");
     cudaError_t e = cudaGraphLaunch(g->exec, (cudaStream_t)stream);
     if (e != cudaSuccess) return set_err(FMN_ERR_CUDA, "cudaGraphLaunch", e);

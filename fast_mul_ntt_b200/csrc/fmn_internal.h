@@ -5,11 +5,22 @@
 #include <stddef.h>
 #include <stdint.h>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include <vector>
 
 typedef unsigned long long u64;
 
 namespace fmn {
+
+// A named range on the host timeline of profilers (NVTX; header-only, a no-op unless a tool
+// such as Nsight Systems is attached): one per product, batch or server launch.
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 constexpr int MAX_PASS_BITS = 9;     // largest sub-transform one CTA pass performs (2^9 points)
 constexpr int MAX_LOG_N = 30;        // largest transform length supported (twiddle tables)

@@ -13,9 +13,9 @@
 // Data layout: per operand three residue arrays of N u32 (prime-major).  A strided pass
 // views a block of B = 2^logB digits as a [2^m][B / 2^m] row-major matrix; a CTA takes 32
 // adjacent columns (a 128-byte stretch of each row) and transforms every column in shared
-// memory.  Its tile is dense (row pitch 32 words) and arrives by asynchronous 16-byte copies
-// while the CTA computes its four-step twiddle factors, so no thread waits on a global load
-// inside the rounds.  Contiguous passes (32 blocks of 2^m digits, one per tile column) store
+// memory.  Its tile is dense (row pitch 32 words) and arrives by bulk copies (one 128-byte
+// cp.async.bulk per row, completing on an mbarrier; fmn_tma.cuh) while the CTA computes its
+// four-step twiddle factors, so no thread waits on a global load inside the rounds.  Contiguous passes (32 blocks of 2^m digits, one per tile column) store
 // element (row j, column c) at j * 33 + c: the padding word keeps both the row-wise and the
 // column-wise rounds free of bank conflicts.  Their results leave through the tile, row by
 // row, as 128-byte stores, and the fused pass copies the other operand's tile in while its
@@ -34,6 +34,7 @@
 #include "fmn_carry.cuh"
 #include "fmn_internal.h"
 #include "fmn_rounds.cuh"
+#include "fmn_tma.cuh"
 
 namespace fmn {
 namespace q32 {
@@ -88,24 +89,28 @@ __device__ __forceinline__ int tix(int j, int c) {
 // padding, and each row is a 128-byte copy target.
 __device__ __forceinline__ int dix(int j, int c) { return j * TC + c; }
 
-// 16-byte asynchronous copy global -> shared (no registers held while it is in flight).
-__device__ __forceinline__ void cp_async16(u32* sdst, const u32* gsrc) {
-    const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gsrc) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_commit_wait() {
-    asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;\n" ::: "memory");
-}
-// Rows 0 .. L-1 of a strided tile (32 words each, row r at g + r * 2^logS) into a dense tile.
+// Rows 0 .. L-1 of a strided tile (32 words each, row r at g + r * 2^logS) into a dense tile:
+// one 128-byte bulk copy per row, issued by the lanes of warp 0, completing on `bar`.  Every
+// thread calls it (it initialises the barrier and synchronises the CTA once).
 template <int L>
-__device__ __forceinline__ void stage_tile(u32* sm, const u32* __restrict__ g, int logS) {
-#pragma unroll 4
-    for (int e = threadIdx.x; e < L * (TC / 4); e += NT) {
-        const int r = e / (TC / 4), k = e % (TC / 4);
-        cp_async16(sm + r * TC + 4 * k, g + ((u32)r << logS) + 4 * k);
+__device__ __forceinline__ void stage_tile(u32* sm, const u32* __restrict__ g, int logS, uint64_t* bar) {
+    if (threadIdx.x == 0) {
+        mbar_init(bar, 1);
+        mbar_fence_init();
     }
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        if (threadIdx.x == 0) mbar_arrive_expect_tx(bar, L * TC * (unsigned)sizeof(u32));
+        __syncwarp();
+#pragma unroll 4
+        for (int r = threadIdx.x; r < L; r += 32)
+            bulk_copy_g2s(sm + r * TC, g + ((u32)r << logS), TC * (unsigned)sizeof(u32), bar);
+    }
+}
+// Waits for a staged tile; false (in every thread) if the copy did not complete, which the
+// status word records.  Also the CTA barrier after the tile's arrival.
+__device__ __forceinline__ bool tile_arrived(uint64_t* bar, u32* err) {
+    return __syncthreads_and(mbar_wait_bounded(bar, err)) != 0;
 }
 
 enum { M_FWD = 0, M_FWD_LAST = 1, M_FUSED = 2, M_INV = 3, M_FUSED2 = 4, M_INV_ACC = 5 };
@@ -130,6 +135,7 @@ struct QArgs {
     // 2^logB entries per prime (frequency k of the column transform, column i), or null to
     // compute them from the root tables
     const uint2* tw;
+    u32* err;         // the product's status word (a tile copy that never completed is recorded here)
 };
 
 // ------------------------------------------------------------------ one round
@@ -298,16 +304,16 @@ __device__ __forceinline__ void body_fwd(u32* sm, const QArgs& a, u64 tile, int 
     const u64* __restrict__ src = a.src;
     const u64 len = a.len;
     const int shift = Q32_MAX_LOG_N - a.logB;
-    // Residue tiles are copied in asynchronously while the twiddle factors are computed; the
+    // Residue tiles arrive by bulk copies while the twiddle factors are computed; the
     // entry pass reads the caller's limbs directly (8-byte alignment only, zero past the end).
     constexpr bool STAGED = !ENTRY;
     u32* beta = sm + (STAGED ? TC : TP) * L;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(beta + TC * 16);
     const uint2* __restrict__ tw = a.tw ? a.tw + ((u64)pi << a.logB) : nullptr;
-    if constexpr (STAGED) stage_tile<L>(sm, d + gbase, logS);
+    if constexpr (STAGED) stage_tile<L>(sm, d + gbase, logS, bar);
     if (!tw) fill_beta<LOGL, false>(beta, col0, shift, pi, q);   // read after the first round's barrier
     if constexpr (STAGED) {
-        cp_async_commit_wait();
-        __syncthreads();
+        if (!tile_arrived(bar, a.err)) return;
     }
     auto ld0 = [=](int j, int c) -> u32 {
         if constexpr (STAGED) return sm[dix(j, c)];
@@ -353,11 +359,11 @@ __device__ __forceinline__ void body_inv(u32* sm, const QArgs& a, u64 tile, int 
     u32* __restrict__ d = a.data + (u64)pi * a.N;
     const int shift = Q32_MAX_LOG_N - a.logB;
     u32* beta = sm + TC * L;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(beta + TC * 16);
     const uint2* __restrict__ tw = a.tw ? a.tw + ((u64)pi << a.logB) : nullptr;
-    stage_tile<L>(sm, d + gbase, logS);                   // in flight during fill_beta
+    stage_tile<L>(sm, d + gbase, logS, bar);              // in flight during fill_beta
     if (!tw) fill_beta<LOGL, true>(beta, col0, shift, pi, q);
-    cp_async_commit_wait();
-    __syncthreads();
+    if (!tile_arrived(bar, a.err)) return;
     auto ld0 = [=](int row0, int c, auto& x) {
 #pragma unroll
         for (int t = 0; t < R; ++t) x[t] = sm[dix(row0 + t, c)];
@@ -552,15 +558,23 @@ __device__ __forceinline__ void body_fused(u32* sm, const QArgs& a, u64 tile, in
         fused_lowest<LOGL, SQR>(ldg, stg, o, gbase, ncols, pi, q);
     } else {
         // the other operand's tile, column by column, is copied in while the forward rounds run
+        // (one bulk copy of L words per column, issued by the lanes of warp 0)
         constexpr bool OS = !SQR && LOGL <= 8;           // 9-bit tiles: no room for a second one
         u32* oth_s = sm + TP * L;
+        uint64_t* bar = reinterpret_cast<uint64_t*>(oth_s + TC * (L + 4));
         if constexpr (OS) {
-#pragma unroll 4
-            for (int e = threadIdx.x; e < TC * (L / 4); e += NT) {
-                const int c = e / (L / 4), k = e % (L / 4);
-                if (c < ncols) cp_async16(oth_s + c * (L + 4) + 4 * k, o + gbase + (u32)c * L + 4 * k);
+            if (threadIdx.x == 0) {
+                mbar_init(bar, 1);
+                mbar_fence_init();
             }
-            cp_async_commit();
+            __syncthreads();
+            if (threadIdx.x < 32) {
+                if (threadIdx.x == 0) mbar_arrive_expect_tx(bar, (unsigned)ncols * L * (unsigned)sizeof(u32));
+                __syncwarp();
+                if ((int)threadIdx.x < ncols)
+                    bulk_copy_g2s(oth_s + threadIdx.x * (L + 4), o + gbase + threadIdx.x * L, L * (unsigned)sizeof(u32),
+                                  bar);
+            }
         }
         constexpr int RB0 = round_bits(LOGL, 0);
         run_round<LOGL, RB0, LOGL - 1, false, true>(ldg, sts, pi, q);
@@ -569,8 +583,11 @@ __device__ __forceinline__ void body_fused(u32* sm, const QArgs& a, u64 tile, in
             constexpr int RB1 = round_bits(LOGL, 1), T1 = round_top(LOGL, 1);
             run_round<LOGL, RB1, T1, false, false>(lds, sts, pi, q);
         }
-        if constexpr (OS) cp_async_wait_all();
-        __syncthreads();
+        if constexpr (OS) {
+            if (!tile_arrived(bar, a.err)) return;
+        } else {
+            __syncthreads();
+        }
         fused_lowest<LOGL, SQR, OS ? 2 : 0>(lds, sts, OS ? oth_s : o, gbase, ncols, pi, q);
         __syncthreads();
         if constexpr (NR == 3) {
@@ -1030,7 +1047,7 @@ static const BatchKernelTable& bktab() {
 // tile + the 16 x 32 four-step twiddle factors of strided passes; two tiles when merged
 static size_t pass_smem(int logl, int variant) {
     const size_t L = (size_t)1 << logl, tile = (size_t)TP * L;
-    size_t w = variant == V_FUSED2 ? 2 * tile : tile + TC * 16;
+    size_t w = variant == V_FUSED2 ? 2 * tile : tile + TC * 16 + 4;   // + the staging barrier (8 B)
     // staging buffer of the other operand's tile (body_fused, multi-round tiles of <= 8 bits)
     if ((variant == V_FUSED || variant == V_FUSED_E) && logl >= 5 && logl <= 8) w += TC * (L + 4);
     return w * sizeof(u32);
@@ -1451,7 +1468,7 @@ static TwPass tw_tables(int logB, int logl, cudaStream_t s) {
 // the GPU together, the default (even) plans are faster (4096 products of 1k-100k limbs:
 // 137k against 104k products/s on B200).
 // `tws`: per pass, its twiddle tables (null: computed in the kernels).
-static void plan_whole(const Job& j, int n, u32* A, u32* B, QWhole* out, bool batched = false,
+static void plan_whole(const Job& j, int n, u32* A, u32* B, QWhole* out, u32* err, bool batched = false,
                        const TwPass* tws = nullptr) {
     const int sqr = j.sqr ? 1 : 0;
     if (sqr || j.spectrum) B = A;
@@ -1472,6 +1489,7 @@ static void plan_whole(const Job& j, int n, u32* A, u32* B, QWhole* out, bool ba
     memset(&pa, 0, sizeof(pa));
     pa.N = N;
     pa.ncols = TC;
+    pa.err = err;
     auto add = [&](int variant, int logl, u64 tiles) {
         QRec& r = out->rec[out->count++];
         r.variant = variant;
@@ -1780,7 +1798,7 @@ cudaError_t q32_batch_plan(const Job* jobs, const int* idx, int m, char* res, si
         }
         u32* ticket = (u32*)(st + *soff);
         *soff += q32_batch_state_bytes(j);
-        plan_whole(j, n, A, B, &W[t], true);
+        plan_whole(j, n, A, B, &W[t], err, true);
         QCrtArgs& ca = C[t];
         ca = proto;
         ca.res = A;
@@ -1982,6 +2000,7 @@ cudaError_t q32_enqueue(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s,
     memset(&pa, 0, sizeof(pa));
     pa.N = N;
     pa.ncols = TC;
+    pa.err = (u32*)base;
     auto fwd_strided = [&](const u64* src, u64 len, u32* data) -> cudaError_t {
         for (int p = 0; p + 1 < P; ++p) {
             pa.src = src;
@@ -2032,7 +2051,7 @@ cudaError_t q32_enqueue(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s,
             TwPass twl[MAX_PASSES];
             for (int p = 0, lg = J.nl; p + 1 < pll.passes; lg -= pll.bits[p], ++p) twl[p] = tw_tables(lg, pll.bits[p], s);
             QWhole WL;
-            plan_whole(jl, J.nl, LA, LB, &WL, false, twl);
+            plan_whole(jl, J.nl, LA, LB, &WL, (u32*)base, false, twl);
             for (int k = 0; k < WL.count; ++k) {
                 if (b_ready == 0 && WL.rec[k].a.src == j.b) {
                     if ((e = launch.need(0, J.lpb)) != cudaSuccess) return e;
@@ -2050,7 +2069,7 @@ cudaError_t q32_enqueue(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s,
             for (int i = 0; i < 3; ++i) ca.low_cst[i] = cl.cst[i];
         }
         QWhole W;
-        plan_whole(j, J.n, A, B, &W, false, tws);
+        plan_whole(j, J.n, A, B, &W, (u32*)base, false, tws);
         bool have_b = sqr != 0;
         for (int k = 0; k < W.count; ++k) {
             if (!have_b && W.rec[k].a.src == j.b) {            // the second operand's first reader

@@ -200,6 +200,7 @@ size_t request_bytes(const fmn_request& r, bool reuse) {
 
 // Launch one batch of admitted requests on slot `sl` (dispatcher thread, lock held).
 bool launch_batch(fmn_server* s, Slot* sl, const std::vector<size_t>& idx) {
+    fmn::NvtxRange nvtx("fmn server batch launch");
     const bool reuse = s->batching != 0;
     std::vector<fmn::Job> jobs(idx.size());
     size_t out_bytes = 0;
@@ -377,6 +378,7 @@ void dispatcher(fmn_server* s) {
 extern "C" {
 
 int fmn_operand_create(const u64* d_in, u64 len, u64 max_partner_len, void* stream, fmn_operand** out) {
+    fmn::NvtxRange nvtx("fmn operand create");
     if (!out || !d_in || len == 0 || max_partner_len == 0) return fmn::api_set_error(FMN_ERR_ARG, "bad operand", cudaSuccess);
     *out = nullptr;
     if (len + max_partner_len - 1 > (1ull << fmn::MAX_LOG_N) || (len < max_partner_len ? len : max_partner_len) >= (1ull << 56))
