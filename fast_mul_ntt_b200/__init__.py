@@ -54,7 +54,8 @@ class FmnServerStats(ctypes.Structure):
     """fmn_server_stats of include/fast_mul.h."""
     _fields_ = [("submitted", ctypes.c_uint64), ("completed", ctypes.c_uint64), ("rejected", ctypes.c_uint64),
                 ("failed", ctypes.c_uint64), ("batches", ctypes.c_uint64), ("mismatches", ctypes.c_uint64),
-                ("device_errors", ctypes.c_uint64), ("peak_bytes", ctypes.c_size_t), ("cancelled", ctypes.c_uint64)]
+                ("device_errors", ctypes.c_uint64), ("peak_bytes", ctypes.c_size_t), ("cancelled", ctypes.c_uint64),
+                ("launch_ms", ctypes.c_double), ("alloc_ms", ctypes.c_double)]
 
 
 class FmnJob(ctypes.Structure):
@@ -456,7 +457,7 @@ class Server:
     def stats(self):
         st = FmnServerStats()
         _check(load_library().fmn_server_get_stats(self.handle, ctypes.byref(st)))
-        return {k: int(getattr(st, k)) for k, _ in FmnServerStats._fields_}
+        return {k: (float if t is ctypes.c_double else int)(getattr(st, k)) for k, t in FmnServerStats._fields_}
 
     def replay(self, requests, arrivals):
         """Open-loop replay of a request array at the given arrival times (seconds); returns

@@ -106,6 +106,7 @@ struct fmn_server {
     size_t taken = 0;                     // completions handed out by fmn_server_take
     size_t in_use = 0, peak = 0;
     u64 batches = 0, rejected = 0, failures = 0, cancelled = 0;
+    double launch_ms = 0.0, alloc_ms = 0.0;   // dispatcher host time (launch_batch, pool allocations)
     bool stop = false;
     bool paused = false;                  // admission held (fmn_server_pause)
     std::thread thr;
@@ -199,8 +200,17 @@ size_t request_bytes(const fmn_request& r, bool reuse) {
 }
 
 // Launch one batch of admitted requests on slot `sl` (dispatcher thread, lock held).
+bool launch_batch_timed(fmn_server* s, Slot* sl, const std::vector<size_t>& idx);
+
 bool launch_batch(fmn_server* s, Slot* sl, const std::vector<size_t>& idx) {
     fmn::NvtxRange nvtx("fmn server batch launch");
+    const clk::time_point t0 = clk::now();
+    const bool ok = launch_batch_timed(s, sl, idx);
+    s->launch_ms += std::chrono::duration<double, std::milli>(clk::now() - t0).count();
+    return ok;
+}
+
+bool launch_batch_timed(fmn_server* s, Slot* sl, const std::vector<size_t>& idx) {
     const bool reuse = s->batching != 0;
     std::vector<fmn::Job> jobs(idx.size());
     size_t out_bytes = 0;
@@ -215,7 +225,10 @@ bool launch_batch(fmn_server* s, Slot* sl, const std::vector<size_t>& idx) {
     ws_bytes = align256(ws_bytes);
     const size_t total = ws_bytes + out_bytes;
     void* mem = nullptr;
-    if (cudaMallocFromPoolAsync(&mem, total, s->pool, sl->stream) != cudaSuccess) {
+    const clk::time_point ta = clk::now();
+    const cudaError_t ea = cudaMallocFromPoolAsync(&mem, total, s->pool, sl->stream);
+    s->alloc_ms += std::chrono::duration<double, std::milli>(clk::now() - ta).count();
+    if (ea != cudaSuccess) {
         cudaGetLastError();
         return false;
     }
@@ -614,6 +627,8 @@ int fmn_server_get_stats(fmn_server* s, fmn_server_stats* st) {
     st->batches = s->batches;
     st->peak_bytes = s->peak;
     st->cancelled = s->cancelled;
+    st->launch_ms = s->launch_ms;
+    st->alloc_ms = s->alloc_ms;
     if (cudaMemcpy(s->h_mismatch, s->d_mismatch, 2 * sizeof(unsigned), cudaMemcpyDeviceToHost) == cudaSuccess) {
         st->mismatches = s->h_mismatch[0];
         st->device_errors = s->h_mismatch[1];

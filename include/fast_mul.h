@@ -167,6 +167,8 @@ typedef struct {
     u64 device_errors;           /* batches whose carry scan reported a bounded-wait expiry */
     size_t peak_bytes;           /* highest scratch in use */
     u64 cancelled;               /* requests withdrawn by fmn_server_cancel (also in completed) */
+    double launch_ms;            /* host time the dispatcher spent launching batches */
+    double alloc_ms;             /* of which: taking scratch from the server's memory pool */
 } fmn_server_stats;
 typedef struct fmn_server fmn_server;
 int fmn_server_create(int device, size_t hbm_budget_bytes, int max_batch, int batching, fmn_server** out);
