@@ -66,23 +66,19 @@ struct Req {
     bool cancelled;      // withdrawn before admission: never computed, output untouched
 };
 
+// A slot runs one batch at a time on its stream; an event recorded after the batch's last
+// kernel tells the dispatcher (which polls it) that the batch has finished.  Polling an event
+// leaves the stream free, where a host callback would hold it until the callback has run.
 struct Slot {
     cudaStream_t stream = nullptr;
+    cudaEvent_t done = nullptr;
     void* stage = nullptr;
     size_t stage_cap = 0;
     bool busy = false;
-    std::atomic<bool> finished{false};
-    clk::time_point done_at;
     std::vector<size_t> reqs;   // indices into the request log
     void* mem = nullptr;
     size_t bytes = 0;
 };
-
-void CUDART_CB slot_done(void* p) {
-    Slot* s = (Slot*)p;
-    s->done_at = clk::now();
-    s->finished.store(true, std::memory_order_release);
-}
 
 }  // namespace
 
@@ -93,6 +89,7 @@ struct fmn_server {
     int batching;
     int nslots;
     std::vector<Slot*> slots;
+    std::deque<Slot*> fifo;               // plain mode: busy slots in launch (= completion) order
     cudaMemPool_t pool = nullptr;
     unsigned* d_mismatch = nullptr;       // [0] output mismatches, [1] device status errors
     unsigned* h_mismatch = nullptr;
@@ -188,6 +185,7 @@ int request_log_n(const fmn_request& r, bool reuse) {
 // Products this large run alone with the single-product kernels (they fill the GPU by
 // themselves); smaller ones are batched, up to kBatchPoints transform points per batch.
 constexpr int kAloneLogN = 20;
+constexpr int kBigSlots = 2;               // batching mode: slots for large products
 constexpr u64 kBatchPoints = 1ull << 22;
 
 // Scratch a request is charged: its product workspace (as one batch of one, an upper
@@ -199,42 +197,68 @@ size_t request_bytes(const fmn_request& r, bool reuse) {
     return b;
 }
 
-// Launch one batch of admitted requests on slot `sl` (dispatcher thread, lock held).
-bool launch_batch_timed(fmn_server* s, Slot* sl, const std::vector<size_t>& idx);
+bool launch_unlocked(fmn_server* s, Slot* sl, const std::vector<fmn_request>& rq, std::vector<fmn::Job>& jobs,
+                     size_t ws_bytes, size_t total, double* alloc_ms, std::string* err);
 
-bool launch_batch(fmn_server* s, Slot* sl, const std::vector<size_t>& idx) {
+// Launch one batch of admitted requests on slot `sl` (dispatcher thread).  Called with the
+// lock held; the requests are copied and the slot and its scratch budget taken under the lock,
+// and the lock is released while the CUDA calls run (submissions and queries go on meanwhile;
+// only the dispatcher launches, retires or touches slots and twiddle tables).
+bool launch_batch(fmn_server* s, Slot* sl, const std::vector<size_t>& idx, std::unique_lock<std::mutex>& lk) {
     fmn::NvtxRange nvtx("fmn server batch launch");
     const clk::time_point t0 = clk::now();
-    const bool ok = launch_batch_timed(s, sl, idx);
-    s->launch_ms += std::chrono::duration<double, std::milli>(clk::now() - t0).count();
-    return ok;
-}
-
-bool launch_batch_timed(fmn_server* s, Slot* sl, const std::vector<size_t>& idx) {
     const bool reuse = s->batching != 0;
+    std::vector<fmn_request> rq(idx.size());
     std::vector<fmn::Job> jobs(idx.size());
     size_t out_bytes = 0;
     for (size_t k = 0; k < idx.size(); ++k) {
-        const fmn_request& r = s->log[idx[k]].r;
-        if (!r.out) out_bytes += align256(out_len_of(r) * sizeof(u64));
-        jobs[k] = to_job(r, reuse, r.out);
+        rq[k] = s->log[idx[k]].r;
+        if (!rq[k].out) out_bytes += align256(out_len_of(rq[k]) * sizeof(u64));
+        jobs[k] = to_job(rq[k], reuse, rq[k].out);
     }
     // outputs owned by the server live after the batch workspace
     const bool single = jobs.size() == 1;
     size_t ws_bytes = single ? fmn::job_workspace_bytes(jobs[0]) : fmn::batch_workspace_bytes(jobs.data(), (int)jobs.size());
     ws_bytes = align256(ws_bytes);
     const size_t total = ws_bytes + out_bytes;
+    sl->busy = true;
+    sl->reqs = idx;
+    sl->bytes = total;
+    s->in_use += total;
+    if (s->in_use > s->peak) s->peak = s->in_use;
+    lk.unlock();
+    double alloc_ms = 0.0;
+    std::string err;
+    const bool ok = launch_unlocked(s, sl, rq, jobs, ws_bytes, total, &alloc_ms, &err);
+    lk.lock();
+    s->alloc_ms += alloc_ms;
+    if (ok) {
+        ++s->batches;
+    } else {
+        if (!err.empty()) s->error = err;
+        s->in_use -= total;
+        sl->busy = false;
+        sl->reqs.clear();
+        sl->bytes = 0;
+    }
+    s->launch_ms += std::chrono::duration<double, std::milli>(clk::now() - t0).count();
+    return ok;
+}
+
+bool launch_unlocked(fmn_server* s, Slot* sl, const std::vector<fmn_request>& rq, std::vector<fmn::Job>& jobs,
+                     size_t ws_bytes, size_t total, double* alloc_ms, std::string* err) {
+    const bool single = jobs.size() == 1;
     void* mem = nullptr;
     const clk::time_point ta = clk::now();
     const cudaError_t ea = cudaMallocFromPoolAsync(&mem, total, s->pool, sl->stream);
-    s->alloc_ms += std::chrono::duration<double, std::milli>(clk::now() - ta).count();
+    *alloc_ms = std::chrono::duration<double, std::milli>(clk::now() - ta).count();
     if (ea != cudaSuccess) {
         cudaGetLastError();
         return false;
     }
     char* ob = (char*)mem + ws_bytes;
-    for (size_t k = 0; k < idx.size(); ++k) {
-        const fmn_request& r = s->log[idx[k]].r;
+    for (size_t k = 0; k < rq.size(); ++k) {
+        const fmn_request& r = rq[k];
         if (!r.out) {
             jobs[k].out = (u64*)ob;
             ob += align256(out_len_of(r) * sizeof(u64));
@@ -263,8 +287,8 @@ bool launch_batch_timed(fmn_server* s, Slot* sl, const std::vector<size_t>& idx)
             e = fmn::enqueue_job(jobs[0], mem, ws_bytes, sl->stream, server_twiddles(s, n));
         }
     }
-    for (size_t k = 0; k < idx.size() && e == cudaSuccess; ++k) {
-        const fmn_request& r = s->log[idx[k]].r;
+    for (size_t k = 0; k < rq.size() && e == cudaSuccess; ++k) {
+        const fmn_request& r = rq[k];
         if (r.check) {
             k_compare<<<148, 256, 0, sl->stream>>>(jobs[k].out, r.check, out_len_of(r), s->d_mismatch);
             e = cudaGetLastError();
@@ -274,27 +298,20 @@ bool launch_batch_timed(fmn_server* s, Slot* sl, const std::vector<size_t>& idx)
         k_fold_status<<<1, 32, 0, sl->stream>>>((const unsigned*)mem, s->d_mismatch + 1);
         e = cudaGetLastError();
     }
-    if (e == cudaSuccess) e = cudaLaunchHostFunc(sl->stream, slot_done, sl);
+    if (e == cudaSuccess) e = cudaEventRecord(sl->done, sl->stream);
     if (e != cudaSuccess) {
         cudaGetLastError();
-        s->error = cudaGetErrorString(e);
+        *err = cudaGetErrorString(e);
         cudaFreeAsync(mem, sl->stream);
         return false;
     }
     sl->mem = mem;
-    sl->bytes = total;
-    sl->reqs = idx;
-    sl->busy = true;
-    sl->finished.store(false, std::memory_order_relaxed);
-    s->in_use += total;
-    if (s->in_use > s->peak) s->peak = s->in_use;
-    ++s->batches;
     return true;
 }
 
-void retire(fmn_server* s, Slot* sl) {
+void retire(fmn_server* s, Slot* sl, clk::time_point done_at) {
     for (size_t i : sl->reqs) {
-        s->log[i].done = sl->done_at;
+        s->log[i].done = done_at;
         s->completed_order.push_back(i);
     }
     cudaFreeAsync(sl->mem, sl->stream);
@@ -311,15 +328,30 @@ void dispatcher(fmn_server* s) {
     while (true) {
         bool progress = false;
         const size_t done_before = s->completed_order.size();
-        for (Slot* sl : s->slots)
-            if (sl->busy && sl->finished.load(std::memory_order_acquire)) {
-                retire(s, sl);
+        // finished batches: plain mode in launch order (one stream), batching mode any slot
+        auto finished = [](Slot* sl) {
+            const cudaError_t q = cudaEventQuery(sl->done);
+            if (q == cudaErrorNotReady) cudaGetLastError();
+            return q != cudaErrorNotReady;
+        };
+        if (!s->batching) {
+            while (!s->fifo.empty() && finished(s->fifo.front())) {
+                retire(s, s->fifo.front(), clk::now());
+                s->fifo.pop_front();
                 progress = true;
             }
+        } else {
+            for (Slot* sl : s->slots)
+                if (sl->busy && finished(sl)) {
+                    retire(s, sl, clk::now());
+                    progress = true;
+                }
+        }
         if (progress) s->cv.notify_all();
         // admission, each queue in arrival order, while budget and a slot allow.  Batching
-        // mode: slot 0 takes large products one at a time (each fills the GPU), the other
-        // slots take batches of small ones, so small requests never queue behind large ones.
+        // mode: the first kBigSlots slots take large products one per slot (each nearly fills
+        // the GPU; two let the next one queue behind the running one), the other slots take
+        // batches of small ones, so small requests never queue behind large ones.
         auto reject_if_too_big = [&](std::deque<size_t>& q) {
             while (!q.empty() && request_bytes(s->log[q.front()].r, s->batching != 0) > s->budget) {
                 const size_t i = q.front();
@@ -330,29 +362,32 @@ void dispatcher(fmn_server* s) {
             }
         };
         auto launch_or_fail = [&](Slot* sl, const std::vector<size_t>& take) {
-            if (!launch_batch(s, sl, take))
+            if (launch_batch(s, sl, take, lk)) {
+                if (!s->batching) s->fifo.push_back(sl);
+            } else {
                 for (size_t i : take) {                // could not launch: fail these requests
                     s->log[i].done = clk::now();
                     ++s->failures;
                     s->completed_order.push_back(i);
                 }
+            }
             progress = true;
         };
         if (s->batching && !s->paused) {
             reject_if_too_big(s->big);
-            if (!s->big.empty() && !s->slots[0]->busy) {
+            for (int k = 0; k < kBigSlots && !s->big.empty(); ++k) {
+                if (s->slots[k]->busy) continue;
                 const size_t i = s->big.front();
-                if (s->in_use + request_bytes(s->log[i].r, true) <= s->budget) {
-                    s->big.pop_front();
-                    launch_or_fail(s->slots[0], std::vector<size_t>{i});
-                }
+                if (s->in_use + request_bytes(s->log[i].r, true) > s->budget) break;
+                s->big.pop_front();
+                launch_or_fail(s->slots[k], std::vector<size_t>{i});
             }
         }
         while (!s->paused) {
             reject_if_too_big(s->pending);
             if (s->pending.empty()) break;
             Slot* free_slot = nullptr;
-            for (size_t k = s->batching ? 1 : 0; k < s->slots.size(); ++k)
+            for (size_t k = s->batching ? kBigSlots : 0; k < s->slots.size(); ++k)
                 if (!s->slots[k]->busy) {
                     free_slot = s->slots[k];
                     break;
@@ -489,7 +524,7 @@ int fmn_server_create(int device, size_t hbm_budget, int max_batch, int batching
     s->budget = hbm_budget;
     s->max_batch = batching ? max_batch : 1;
     s->batching = batching;
-    s->nslots = batching ? 4 : 64;          // plain mode: many products queued on one stream
+    s->nslots = batching ? kBigSlots + 3 : 64;   // plain mode: many products queued on one stream
     cudaStream_t plain = nullptr;
     if (!batching && (e = cudaStreamCreateWithFlags(&plain, cudaStreamNonBlocking)) != cudaSuccess) {
         delete s;
@@ -497,12 +532,13 @@ int fmn_server_create(int device, size_t hbm_budget, int max_batch, int batching
     }
     for (int k = 0; k < s->nslots; ++k) {
         Slot* sl = new Slot();
+        s->slots.push_back(sl);
+        if ((e = cudaEventCreateWithFlags(&sl->done, cudaEventDisableTiming)) != cudaSuccess) break;
         if (batching) {
             if ((e = cudaStreamCreateWithFlags(&sl->stream, cudaStreamNonBlocking)) != cudaSuccess) break;
         } else {
             sl->stream = plain;            // one in-order stream: the plain per-call path
         }
-        s->slots.push_back(sl);
     }
     cudaMemPoolProps props;
     memset(&props, 0, sizeof(props));
@@ -681,6 +717,7 @@ void fmn_server_destroy(fmn_server* s) {
     bool plain_freed = false;
     for (Slot* sl : s->slots) {
         if (sl->stage) cudaFreeHost(sl->stage);
+        if (sl->done) cudaEventDestroy(sl->done);
         if (sl->stream && (s->batching || !plain_freed)) {
             cudaStreamDestroy(sl->stream);
             plain_freed = true;
