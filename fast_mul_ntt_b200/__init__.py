@@ -36,7 +36,7 @@ EXPORTS = ["abs_mul64", "abs_sqr64", "fmn_init", "fmn_shutdown", "fmn_last_error
            "fmn_set_engine", "fmn_get_engine", "fmn_engine_for", "fmn_pieces_for",
            "fmn_force_pieces", "fmn_bench_bfly32", "fmn_get_plan_engine", "fmn_set_plan_engine",
            "fmn_test_fail_allocs", "fmn_test_carry_timeout", "fmn_server_cancel", "fmn_server_pause",
-           "fmn_wrap_for", "fmn_force_wrap"]
+           "fmn_wrap_for", "fmn_twist_for", "fmn_force_wrap"]
 
 ENGINE_AUTO, ENGINE_64, ENGINE_32 = 0, 1, 2
 
@@ -130,6 +130,8 @@ def load_library(path=None):
     lib.fmn_bench_bfly32.restype = ctypes.c_int
     lib.fmn_wrap_for.argtypes = [_u64, _u64, ctypes.c_int]
     lib.fmn_wrap_for.restype = _u64
+    lib.fmn_twist_for.argtypes = [_u64, _u64, ctypes.c_int]
+    lib.fmn_twist_for.restype = _u64
     lib.fmn_force_wrap.argtypes = [ctypes.c_int]
     lib.fmn_force_wrap.restype = ctypes.c_int
     lib.fmn_test_fail_allocs.argtypes = [ctypes.c_int]
@@ -531,9 +533,15 @@ def wrap_for(len1, len2, sqr=False):
     return int(load_library().fmn_wrap_for(len1, len2, 1 if sqr else 0))
 
 
-def force_wrap(on=True):
-    """Tests: wrap every product that allows it (False: cost model)."""
-    _check(load_library().fmn_force_wrap(1 if on else 0))
+def twist_for(len1, len2, sqr=False):
+    """Twisted length M of a wrapped product computed modulo X^M - c (0: not twisted)."""
+    return int(load_library().fmn_twist_for(len1, len2, 1 if sqr else 0))
+
+
+def force_wrap(mode=1):
+    """Tests: wrap every product that allows it -- 1 with the low product, 2 twisted; 0 or
+    False restores the cost model."""
+    _check(load_library().fmn_force_wrap(int(mode)))
 
 
 def autotune(n_lo=10, n_hi=27, save_path=None):

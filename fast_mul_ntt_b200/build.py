@@ -15,7 +15,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIBDIR, "libfastmul_b200.so")
 SOURCES = ["fmn_ntt.cu", "fmn_ntt32.cu", "fmn_api.cu", "fmn_noalloc.cu", "fmn_server.cu", "fmn_tune.cu"]
-HEADERS = ["fmn_arith.cuh", "fmn_arith32.cuh", "fmn_carry.cuh", "fmn_rounds.cuh", "fmn_tma.cuh", "fmn_internal.h"]
+HEADERS = ["fmn_arith.cuh", "fmn_arith32.cuh", "fmn_carry.cuh", "fmn_rounds.cuh", "fmn_internal.h"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
          "-Xcompiler", "-fPIC", "-Xcompiler", "-O2", "--expt-relaxed-constexpr",

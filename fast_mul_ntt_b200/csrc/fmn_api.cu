@@ -714,9 +714,20 @@ int fmn_pieces_for(u64 len1, u64 len2, int sqr) {
     return fmn::job_engine(j) == fmn::ENGINE_32 ? fmn::q32_pieces(len1, len2, sqr ? 1 : 0) : 1;
 }
 
-int fmn_force_wrap(int on) {
-    fmn::q32_force_wrap(on);
+int fmn_force_wrap(int mode) {
+    if (mode < 0 || mode > 2) return set_err(FMN_ERR_ARG, "wrap mode must be 0, 1 or 2");
+    fmn::q32_force_wrap(mode);
     return FMN_OK;
+}
+
+u64 fmn_twist_for(u64 len1, u64 len2, int sqr) {
+    fmn::Job j;
+    j.a = j.b = nullptr;
+    j.out = nullptr;
+    j.la = len1;
+    j.lb = len2;
+    j.sqr = sqr ? 1 : 0;
+    return fmn::job_engine(j) == fmn::ENGINE_32 ? fmn::q32_twisted(len1, len2, sqr ? 1 : 0) : 0;
 }
 
 u64 fmn_wrap_for(u64 len1, u64 len2, int sqr) {

@@ -88,7 +88,10 @@ void q32_release_tables(int dev);
 // Forward transform of `len` limbs into a 32-bit resident spectrum (3 * 2^log_n u32).
 cudaError_t q32_spectrum_enqueue(const u64* src, u64 len, int log_n, void* spec, cudaStream_t s, const Plan& plan);
 void q32_force_pieces(int m);                  // tests: split into m pieces where possible (0: model)
-void q32_force_wrap(int on);                   // tests: wrap every product that allows it (0: model)
+// tests: every product that allows it wrapped with the low product (1) or twisted (2); 0: model
+void q32_force_wrap(int mode);
+// Twisted length M of a wrapped product computed modulo X^M - c (0: not twisted).
+u64 q32_twisted(u64 la, u64 lb, int sqr);
 // Coefficients of the product that wrap around its transform length (0: not a wrapped product).
 u64 q32_wrapped(u64 la, u64 lb, int sqr);
 // Tests: the CRT + carry kernel with one look-back tile withheld (see fmn_ntt32.cu).

@@ -24,8 +24,7 @@
 // (j << 4) | (c ^ (j & 15)); the XOR swizzle keeps both the row-wise (16 columns of a row) and
 // the column-wise (consecutive rows of one column) access patterns free of bank conflicts.
 // Strided passes, whose rounds only ever read whole rows, use a dense tile (row pitch 16) that
-// arrives by bulk copies (one 128-byte cp.async.bulk per row, completing on an mbarrier;
-// fmn_tma.cuh) while the CTA prepares its twiddle factors.
+// arrives by asynchronous 16-byte copies while the CTA prepares its twiddle factors.
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <stdio.h>
@@ -38,7 +37,6 @@
 #include "fmn_arith.cuh"
 #include "fmn_carry.cuh"
 #include "fmn_internal.h"
-#include "fmn_tma.cuh"
 #include "fmn_rounds.cuh"
 
 namespace fmn {
@@ -66,27 +64,22 @@ __device__ __forceinline__ int sw(int j, int c) { return (j << 4) | (c ^ (j & 15
 // is a 128-byte copy target.
 __device__ __forceinline__ int dix(int j, int c) { return (j << 4) | c; }
 
-// Rows 0 .. L-1 of a strided tile (16 u64 each, row r at g + r * 2^logS) into a dense tile:
-// one 128-byte bulk copy per row, issued by the lanes of warp 0, completing on `bar`.  Every
-// thread calls it (it initialises the barrier and synchronises the CTA once).
-template <int L>
-__device__ __forceinline__ void stage_tile(u64* sm, const u64* __restrict__ g, int logS, uint64_t* bar) {
-    if (threadIdx.x == 0) {
-        mbar_init(bar, 1);
-        mbar_fence_init();
-    }
-    __syncthreads();
-    if (threadIdx.x < 32) {
-        if (threadIdx.x == 0) mbar_arrive_expect_tx(bar, L * 16 * (unsigned)sizeof(u64));
-        __syncwarp();
-#pragma unroll 4
-        for (int r = threadIdx.x; r < L; r += 32) bulk_copy_g2s(sm + r * 16, g + ((u64)r << logS), 16 * sizeof(u64), bar);
-    }
+// 16-byte asynchronous copy global -> shared.
+__device__ __forceinline__ void cp_async16(u64* sdst, const u64* gsrc) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gsrc) : "memory");
 }
-// Waits for a staged tile; false (in every thread) if the copy did not complete, which the
-// status word records.  Also the CTA barrier after the tile's arrival.
-__device__ __forceinline__ bool tile_arrived(uint64_t* bar, u32* err) {
-    return __syncthreads_and(mbar_wait_bounded(bar, err)) != 0;
+__device__ __forceinline__ void cp_async_commit_wait() {
+    asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;\n" ::: "memory");
+}
+// Rows 0 .. L-1 of a strided tile (16 u64 each, row r at g + r * 2^logS) into a dense tile.
+template <int L>
+__device__ __forceinline__ void stage_tile(u64* sm, const u64* __restrict__ g, int logS) {
+#pragma unroll 4
+    for (int e = threadIdx.x; e < L * 8; e += NT) {
+        const int r = e >> 3, k = e & 7;
+        cp_async16(sm + r * 16 + 2 * k, g + ((u64)r << logS) + 2 * k);
+    }
 }
 
 // ------------------------------------------------------------------ kernel arguments
@@ -105,7 +98,6 @@ struct PassArgs {
                       // generate them on the fly
     u64* dst;         // M_FUSED: where the product goes when `other` must stay intact
                       // (a resident spectrum); null writes it over `other`
-    u32* err;         // the product's status word (a tile copy that never completed is recorded here)
 };
 
 // ------------------------------------------------------------------ one round
@@ -266,15 +258,15 @@ __device__ __forceinline__ void body_fwd(u64* sm, const PassArgs& a, u64 tile, i
     const u64 len = a.len;
     const int shift = MAX_LOG_N - a.logB;
     u64* beta = sm + TC * L;
-    uint64_t* bar = reinterpret_cast<uint64_t*>(beta + TC * 16);
     const u64* __restrict__ tw = a.tw ? a.tw + ((u64)pi << a.logB) + col0 : nullptr;
-    // residue tiles arrive by bulk copies while the twiddle factors are prepared; the entry
-    // pass reads the caller's limbs directly
+    // residue tiles arrive by asynchronous copies while the twiddle factors are prepared; the
+    // entry pass reads the caller's limbs directly
     constexpr bool STAGED = !ENTRY;
-    if constexpr (STAGED) stage_tile<L>(sm, d + gbase, logS, bar);
+    if constexpr (STAGED) stage_tile<L>(sm, d + gbase, logS);
     if (!tw) fill_beta<LOGL, false>(beta, col0, shift, pi, q);     // read after the first round's barrier
     if constexpr (STAGED) {
-        if (!tile_arrived(bar, a.err)) return;
+        cp_async_commit_wait();
+        __syncthreads();
     }
     auto ld0 = [=](int j, int c) -> u64 {
         if constexpr (STAGED) return sm[dix(j, c)];
@@ -315,11 +307,11 @@ __device__ __forceinline__ void body_inv(u64* sm, const PassArgs& a, u64 tile, i
     u64* __restrict__ d = a.data + (u64)pi * a.N;
     const int shift = MAX_LOG_N - a.logB;
     u64* beta = sm + TC * L;
-    uint64_t* bar = reinterpret_cast<uint64_t*>(beta + TC * 16);
     const u64* __restrict__ tw = a.tw ? a.tw + ((u64)pi << a.logB) + col0 : nullptr;
-    stage_tile<L>(sm, d + gbase, logS, bar);              // in flight while the twiddles are prepared
+    stage_tile<L>(sm, d + gbase, logS);                   // in flight while the twiddles are prepared
     if (!tw) fill_beta<LOGL, true>(beta, col0, shift, pi, q);
-    if (!tile_arrived(bar, a.err)) return;
+    cp_async_commit_wait();
+    __syncthreads();
     auto ld0 = [=](int row0, int c, auto& x) {
 #pragma unroll
         for (int t = 0; t < R; ++t) x[t] = sm[dix(row0 + t, c)];
@@ -875,7 +867,7 @@ static const KernelTable& ktab() {
 // tile + the 16 x 16 four-step twiddle factors of strided passes; two tiles for V_FUSED2
 static size_t pass_smem(int logl, int variant = -1) {
     const size_t tile = (size_t)TC * ((size_t)1 << logl);
-    return (variant == V_FUSED2 ? 2 * tile : tile + TC * 16 + 1) * sizeof(u64);   // + the staging barrier
+    return (variant == V_FUSED2 ? 2 * tile : tile + TC * 16) * sizeof(u64);
 }
 
 cudaError_t ensure_tables() {
@@ -1295,7 +1287,6 @@ static void plan_job(const Job& j, const JobScratch& sc, const TwiddleSet* tws, 
     memset(&pa, 0, sizeof(pa));
     pa.N = N;
     pa.ncols = TC;
-    pa.err = sc.err;
     int logB[MAX_PASSES];
     logB[0] = w.n;
     for (int p = 1; p < P; ++p) logB[p] = logB[p - 1] - pl.bits[p - 1];

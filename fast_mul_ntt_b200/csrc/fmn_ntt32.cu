@@ -13,9 +13,9 @@
 // Data layout: per operand three residue arrays of N u32 (prime-major).  A strided pass
 // views a block of B = 2^logB digits as a [2^m][B / 2^m] row-major matrix; a CTA takes 32
 // adjacent columns (a 128-byte stretch of each row) and transforms every column in shared
-// memory.  Its tile is dense (row pitch 32 words) and arrives by bulk copies (one 128-byte
-// cp.async.bulk per row, completing on an mbarrier; fmn_tma.cuh) while the CTA computes its
-// four-step twiddle factors, so no thread waits on a global load inside the rounds.  Contiguous passes (32 blocks of 2^m digits, one per tile column) store
+// memory.  Its tile is dense (row pitch 32 words) and arrives by asynchronous 16-byte copies
+// while the CTA computes its four-step twiddle factors, so no thread waits on a global load
+// inside the rounds.  Contiguous passes (32 blocks of 2^m digits, one per tile column) store
 // element (row j, column c) at j * 33 + c: the padding word keeps both the row-wise and the
 // column-wise rounds free of bank conflicts.  Their results leave through the tile, row by
 // row, as 128-byte stores, and the fused pass copies the other operand's tile in while its
@@ -34,7 +34,6 @@
 #include "fmn_carry.cuh"
 #include "fmn_internal.h"
 #include "fmn_rounds.cuh"
-#include "fmn_tma.cuh"
 
 namespace fmn {
 namespace q32 {
@@ -89,31 +88,28 @@ __device__ __forceinline__ int tix(int j, int c) {
 // padding, and each row is a 128-byte copy target.
 __device__ __forceinline__ int dix(int j, int c) { return j * TC + c; }
 
-// Rows 0 .. L-1 of a strided tile (32 words each, row r at g + r * 2^logS) into a dense tile:
-// one 128-byte bulk copy per row, issued by the lanes of warp 0, completing on `bar`.  Every
-// thread calls it (it initialises the barrier and synchronises the CTA once).
-template <int L>
-__device__ __forceinline__ void stage_tile(u32* sm, const u32* __restrict__ g, int logS, uint64_t* bar) {
-    if (threadIdx.x == 0) {
-        mbar_init(bar, 1);
-        mbar_fence_init();
-    }
-    __syncthreads();
-    if (threadIdx.x < 32) {
-        if (threadIdx.x == 0) mbar_arrive_expect_tx(bar, L * TC * (unsigned)sizeof(u32));
-        __syncwarp();
-#pragma unroll 4
-        for (int r = threadIdx.x; r < L; r += 32)
-            bulk_copy_g2s(sm + r * TC, g + ((u32)r << logS), TC * (unsigned)sizeof(u32), bar);
-    }
+// 16-byte asynchronous copy global -> shared (no registers held while it is in flight).
+__device__ __forceinline__ void cp_async16(u32* sdst, const u32* gsrc) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gsrc) : "memory");
 }
-// Waits for a staged tile; false (in every thread) if the copy did not complete, which the
-// status word records.  Also the CTA barrier after the tile's arrival.
-__device__ __forceinline__ bool tile_arrived(uint64_t* bar, u32* err) {
-    return __syncthreads_and(mbar_wait_bounded(bar, err)) != 0;
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_commit_wait() {
+    asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;\n" ::: "memory");
+}
+// Rows 0 .. L-1 of a strided tile (32 words each, row r at g + r * 2^logS) into a dense tile,
+// by 16-byte asynchronous copies from every thread.
+template <int L>
+__device__ __forceinline__ void stage_tile(u32* sm, const u32* __restrict__ g, int logS) {
+#pragma unroll 4
+    for (int e = threadIdx.x; e < L * (TC / 4); e += NT) {
+        const int r = e / (TC / 4), k = e % (TC / 4);
+        cp_async16(sm + r * TC + 4 * k, g + ((u32)r << logS) + 4 * k);
+    }
 }
 
-enum { M_FWD = 0, M_FWD_LAST = 1, M_FUSED = 2, M_INV = 3, M_FUSED2 = 4, M_INV_ACC = 5 };
+enum { M_FWD = 0, M_FWD_LAST = 1, M_FUSED = 2, M_INV = 3, M_FUSED2 = 4, M_INV_ACC = 5, M_FWD_TW = 6 };
 
 struct QArgs {
     const u64* src;   // ENTRY: limbs of the operand being transformed
@@ -135,7 +131,11 @@ struct QArgs {
     // 2^logB entries per prime (frequency k of the column transform, column i), or null to
     // compute them from the root tables
     const uint2* tw;
-    u32* err;         // the product's status word (a tile copy that never completed is recorded here)
+    // M_FWD_TW (the first pass of a twisted product modulo X^M - c, M = 2^logB): digit g of the
+    // input is gamma^g * sum_{j < 2^fold_log} c^j a_{g + j M}, gamma = w^(2^tw_log) (w of order
+    // 2^26), c = gamma^M
+    int fold_log;
+    int tw_log;
 };
 
 // ------------------------------------------------------------------ one round
@@ -290,8 +290,30 @@ __device__ __forceinline__ const uint2* tw_group(const uint2* tw, u32 col, int r
     return tw + ((kq << logS) + col);
 }
 
-// Forward strided pass (pass p < P-1 of a multi-pass transform).
-template <int LOGL, bool ENTRY>
+// Twisted, folded entry (M_FWD_TW, see QArgs): c^j for j < 2^fold_log in Montgomery form, one
+// prime per CTA, in shared memory (`cp`, written before the first barrier of the pass).
+__device__ __forceinline__ void fill_cpow(u32* cp, const QArgs& a, int pi, const PrimeQ& q) {
+    if ((int)threadIdx.x < (1 << a.fold_log)) {
+        const u32 e = ((u32)threadIdx.x << (a.logB + a.tw_log)) & MASK_N;   // c^j = w^(j M 2^tw_log)
+        cp[threadIdx.x] = qroot(e, pi, q);
+    }
+}
+__device__ __forceinline__ u32 entry_val_tw(const u64* __restrict__ src, u64 len, u32 g, int logB, int fold_log,
+                                            int tw_log, const u32* cp, int pi, const PrimeQ& q) {
+    const u32* __restrict__ dig = reinterpret_cast<const u32*>(src);
+    const u64 nd = 2 * len;
+    u32 acc = 0;
+    for (int j = 0; j < (1 << fold_log); ++j) {
+        const u64 i = (u64)g + ((u64)j << logB);
+        if (i >= nd) break;
+        acc = qadd(acc, qmont(__ldg(dig + i), cp[j], q), q);
+    }
+    return qmont(acc, qroot(((u32)g << tw_log) & MASK_N, pi, q), q);
+}
+
+// Forward strided pass (pass p < P-1 of a multi-pass transform).  TWIST: the entry pass of a
+// twisted product (M_FWD_TW).
+template <int LOGL, bool ENTRY, bool TWIST = false>
 __device__ __forceinline__ void body_fwd(u32* sm, const QArgs& a, u64 tile, int pi, const PrimeQ& q) {
     constexpr int L = 1 << LOGL;
     constexpr int RB = round_bits(LOGL, rounds_count(LOGL) - 1), R = 1 << RB;
@@ -304,21 +326,28 @@ __device__ __forceinline__ void body_fwd(u32* sm, const QArgs& a, u64 tile, int 
     const u64* __restrict__ src = a.src;
     const u64 len = a.len;
     const int shift = Q32_MAX_LOG_N - a.logB;
-    // Residue tiles arrive by bulk copies while the twiddle factors are computed; the
+    // Residue tiles are copied in asynchronously while the twiddle factors are computed; the
     // entry pass reads the caller's limbs directly (8-byte alignment only, zero past the end).
     constexpr bool STAGED = !ENTRY;
     u32* beta = sm + (STAGED ? TC : TP) * L;
-    uint64_t* bar = reinterpret_cast<uint64_t*>(beta + TC * 16);
     const uint2* __restrict__ tw = a.tw ? a.tw + ((u64)pi << a.logB) : nullptr;
-    if constexpr (STAGED) stage_tile<L>(sm, d + gbase, logS, bar);
+    u32* cp = beta + TC * 16;                                 // TWIST: c^j
+    if constexpr (STAGED) stage_tile<L>(sm, d + gbase, logS);
     if (!tw) fill_beta<LOGL, false>(beta, col0, shift, pi, q);   // read after the first round's barrier
     if constexpr (STAGED) {
-        if (!tile_arrived(bar, a.err)) return;
+        cp_async_commit_wait();
+        __syncthreads();
     }
+    if constexpr (TWIST) {
+        fill_cpow(cp, a, pi, q);
+        __syncthreads();
+    }
+    const int fold_log = a.fold_log, tw_log = a.tw_log, logB = a.logB;
     auto ld0 = [=](int j, int c) -> u32 {
         if constexpr (STAGED) return sm[dix(j, c)];
         const u32 g = gbase + c + ((u32)j << logS);
-        if constexpr (ENTRY) return entry_val(src, len, g, q);
+        if constexpr (TWIST) return entry_val_tw(src, len, g, logB, fold_log, tw_log, cp, pi, q);
+        else if constexpr (ENTRY) return entry_val(src, len, g, q);
         else return d[g];
     };
     auto stl = [=](int row0, int c, const auto& x) {
@@ -359,11 +388,11 @@ __device__ __forceinline__ void body_inv(u32* sm, const QArgs& a, u64 tile, int 
     u32* __restrict__ d = a.data + (u64)pi * a.N;
     const int shift = Q32_MAX_LOG_N - a.logB;
     u32* beta = sm + TC * L;
-    uint64_t* bar = reinterpret_cast<uint64_t*>(beta + TC * 16);
     const uint2* __restrict__ tw = a.tw ? a.tw + ((u64)pi << a.logB) : nullptr;
-    stage_tile<L>(sm, d + gbase, logS, bar);              // in flight during fill_beta
+    stage_tile<L>(sm, d + gbase, logS);                   // in flight during fill_beta
     if (!tw) fill_beta<LOGL, true>(beta, col0, shift, pi, q);
-    if (!tile_arrived(bar, a.err)) return;
+    cp_async_commit_wait();
+    __syncthreads();
     auto ld0 = [=](int row0, int c, auto& x) {
 #pragma unroll
         for (int t = 0; t < R; ++t) x[t] = sm[dix(row0 + t, c)];
@@ -558,23 +587,15 @@ __device__ __forceinline__ void body_fused(u32* sm, const QArgs& a, u64 tile, in
         fused_lowest<LOGL, SQR>(ldg, stg, o, gbase, ncols, pi, q);
     } else {
         // the other operand's tile, column by column, is copied in while the forward rounds run
-        // (one bulk copy of L words per column, issued by the lanes of warp 0)
         constexpr bool OS = !SQR && LOGL <= 8;           // 9-bit tiles: no room for a second one
         u32* oth_s = sm + TP * L;
-        uint64_t* bar = reinterpret_cast<uint64_t*>(oth_s + TC * (L + 4));
         if constexpr (OS) {
-            if (threadIdx.x == 0) {
-                mbar_init(bar, 1);
-                mbar_fence_init();
+#pragma unroll 4
+            for (int e = threadIdx.x; e < TC * (L / 4); e += NT) {
+                const int c = e / (L / 4), k = e % (L / 4);
+                if (c < ncols) cp_async16(oth_s + c * (L + 4) + 4 * k, o + gbase + (u32)c * L + 4 * k);
             }
-            __syncthreads();
-            if (threadIdx.x < 32) {
-                if (threadIdx.x == 0) mbar_arrive_expect_tx(bar, (unsigned)ncols * L * (unsigned)sizeof(u32));
-                __syncwarp();
-                if ((int)threadIdx.x < ncols)
-                    bulk_copy_g2s(oth_s + threadIdx.x * (L + 4), o + gbase + threadIdx.x * L, L * (unsigned)sizeof(u32),
-                                  bar);
-            }
+            cp_async_commit();
         }
         constexpr int RB0 = round_bits(LOGL, 0);
         run_round<LOGL, RB0, LOGL - 1, false, true>(ldg, sts, pi, q);
@@ -583,11 +604,8 @@ __device__ __forceinline__ void body_fused(u32* sm, const QArgs& a, u64 tile, in
             constexpr int RB1 = round_bits(LOGL, 1), T1 = round_top(LOGL, 1);
             run_round<LOGL, RB1, T1, false, false>(lds, sts, pi, q);
         }
-        if constexpr (OS) {
-            if (!tile_arrived(bar, a.err)) return;
-        } else {
-            __syncthreads();
-        }
+        if constexpr (OS) cp_async_wait_all();
+        __syncthreads();
         fused_lowest<LOGL, SQR, OS ? 2 : 0>(lds, sts, OS ? oth_s : o, gbase, ncols, pi, q);
         __syncthreads();
         if constexpr (NR == 3) {
@@ -641,7 +659,8 @@ __device__ __forceinline__ void body_fused2(u32* sm, const QArgs& a, u64 tile, i
 // strided passes fit 64 registers without spills and run at 4 (1% faster than at 3).
 template <int MODE, int LOGL>
 constexpr int min_ctas() {
-    return ((MODE == M_FWD || MODE == M_INV || MODE == M_INV_ACC) && LOGL >= 9) || MODE == M_FUSED2 ||
+    return ((MODE == M_FWD || MODE == M_FWD_TW || MODE == M_INV || MODE == M_INV_ACC) && LOGL >= 9) ||
+                   MODE == M_FUSED2 ||
                    (MODE == M_FUSED && LOGL == 8)
                ? 3
                : 4;
@@ -654,6 +673,7 @@ __global__ void __launch_bounds__(NT, (min_ctas<MODE, LOGL>())) k_qpass(QArgs a)
     const u64 tile = blockIdx.x / 3;
     const PrimeQ q = c_q[pi];
     if constexpr (MODE == M_FWD) body_fwd<LOGL, ENTRY>(qsm, a, tile, pi, q);
+    else if constexpr (MODE == M_FWD_TW) body_fwd<LOGL, true, true>(qsm, a, tile, pi, q);
     else if constexpr (MODE == M_INV) body_inv<LOGL, false>(qsm, a, tile, pi, q);
     else if constexpr (MODE == M_INV_ACC) body_inv<LOGL, true>(qsm, a, tile, pi, q);
     else if constexpr (MODE == M_FWD_LAST) body_fwd_last<LOGL, ENTRY>(qsm, a, tile, pi, q);
@@ -708,6 +728,9 @@ struct QCrtArgs {
     u64 low_N;
     u64 wrap;           // K: coefficients that wrapped (0: none)
     u32 low_cst[3];     // the low product's scale constants (low_N^-1 * 2^64 mod q_i)
+    // twisted: `low` holds W (plain, reduced; low_cst = 2^32 mod q_i) with the wrapped
+    // coefficients c_{N+k} = W_k and c_k = res_k - W_k for k < K (see k_qtwist_w)
+    int twisted;
 };
 
 typedef unsigned __int128 u128;
@@ -745,10 +768,12 @@ __device__ __forceinline__ int qsource(const QCrtArgs& a, u64 k) {
     return k < a.wrap ? 1 : (k >= a.N && a.wrap ? 2 : 0);
 }
 // c_k mod q_i (reduced) of one prime, by source.
+// (a wrapped product's sources 1 and 2 swap formulas when it is twisted: res - low at k < K,
+// low alone at N + k)
 __device__ __forceinline__ u32 qscaled(const QCrtArgs& a, int src, u64 k, int i, const PrimeQ& q) {
     if (src == 0) return qmont(a.res[i * a.N + k], a.cst[i], q);
-    if (src == 1) return qmont(a.low[i * a.low_N + k], a.low_cst[i], q);
-    const u64 kk = k - a.N;
+    const u64 kk = src == 2 ? k - a.N : k;
+    if ((src == 2) == (a.twisted != 0)) return qmont(a.low[i * a.low_N + kk], a.low_cst[i], q);
     return qsub(qmont(a.res[i * a.N + kk], a.cst[i], q), qmont(a.low[i * a.low_N + kk], a.low_cst[i], q), q);
 }
 template <bool WRAP>
@@ -781,7 +806,7 @@ __device__ __forceinline__ void qcrt_carry_body(const QCrtArgs& a, u32 ncta) {
         u32 y0[4], y1[4], y2[4];                       // c_k mod q_i
         if (full) {
             const u64 k = kb + 2 * e2;
-            if (src == 1) {
+            if (src != 0 && (src == 2) == (a.twisted != 0)) {   // low alone
                 ld4(a.low + k, y0);
                 ld4(a.low + a.low_N + k, y1);
                 ld4(a.low + 2 * a.low_N + k, y2);
@@ -801,7 +826,7 @@ __device__ __forceinline__ void qcrt_carry_body(const QCrtArgs& a, u32 ncta) {
                     y1[t] = qmont(y1[t], a.cst[1], q1);
                     y2[t] = qmont(y2[t], a.cst[2], q2);
                 }
-                if (src == 2) {
+                if (src != 0) {                                  // res - low
                     u32 l0[4], l1[4], l2[4];
                     ld4(a.low + k, l0);
                     ld4(a.low + a.low_N + k, l1);
@@ -874,6 +899,40 @@ __global__ void __launch_bounds__(CNT) k_qcrt_carry_batch(const QCrtArgs* __rest
     qcrt_carry_body<false>(args[job], ncta[job]);
 }
 
+// ------------------------------------------------------------------ twisted products
+// A wrapped product computed as U = C mod (X^N - 1) (the cyclic transform of length N) and
+// V = C mod (X^M - c) (a cyclic transform of length M = N / 2^s of the operands folded modulo
+// X^M - c and twisted by gamma^i, gamma of order 2N, c = gamma^M, so c^(2^s) = -1).  With
+// C = U + (X^N - 1) W, deg W < K <= M, and X^N = -1 mod (X^M - c):
+//     W = (U mod (X^M - c) - V) / 2,   U mod (X^M - c) = sum_j c^j U_{k + j M}.
+// The kernel writes W_k (plain, reduced) over V_k for k < K; the CRT then takes c_{N+k} = W_k
+// and c_k = U_k - W_k.  Each residue array is scaled by its own length (and V untwisted).
+struct QTwistArgs {
+    const u32* U;       // cyclic product's residues (prime i at U + i N), raw
+    u32* V;             // twisted product's residues (prime i at V + i M), raw; W on return
+    u64 N, K;
+    int logM, fold_log, tw_log;
+    u32 cstN[3], cstM[3];
+};
+__global__ void __launch_bounds__(256) k_qtwist_w(QTwistArgs t) {
+    const int pi = blockIdx.y;
+    const PrimeQ q = c_q[pi];
+    __shared__ u32 cp[8];
+    if ((int)threadIdx.x < (1 << t.fold_log)) cp[threadIdx.x] = qroot(((u32)threadIdx.x << (t.logM + t.tw_log)) & MASK_N, pi, q);
+    __syncthreads();
+    const u32* __restrict__ U = t.U + (u64)pi * t.N;
+    u32* __restrict__ V = t.V + ((u64)pi << t.logM);
+    for (u64 k = (u64)blockIdx.x * blockDim.x + threadIdx.x; k < t.K; k += (u64)gridDim.x * blockDim.x) {
+        u32 ub = 0;
+        for (int j = 0; j < (1 << t.fold_log); ++j) ub = qadd(ub, qmont(U[k + ((u64)j << t.logM)], cp[j], q), q);
+        ub = qmont(ub, t.cstN[pi], q);
+        u32 v = qmont(V[k], t.cstM[pi], q);
+        v = qmont(v, qroot((0u - ((u32)k << t.tw_log)) & MASK_N, pi, q), q);   // times gamma^-k
+        const u32 d = qsub(ub, v, q);
+        V[k] = (d + ((d & 1u) ? q.p : 0u)) >> 1;
+    }
+}
+
 // ------------------------------------------------------------------ host: tables
 static u64 h_mulmod(u64 a, u64 b, u64 m) { return (u64)(((u128)a * b) % m); }
 static u64 h_pow(u64 b, u64 e, u64 m) {
@@ -887,6 +946,7 @@ static u64 h_pow(u64 b, u64 e, u64 m) {
     return r;
 }
 static const u32 kQ[3] = {Q32_P0, Q32_P1, Q32_P2};
+static u32 c_host_r1(int i) { return (u32)((1ull << 32) % kQ[i]); }   // Montgomery form of 1
 
 // Smallest primitive root of p (trial factorisation of p - 1).
 static u64 primitive_root(u64 p) {
@@ -967,7 +1027,7 @@ static const HostTables& host_tables() {
 
 // ------------------------------------------------------------------ host: kernels
 typedef void (*QKernel)(QArgs);
-enum { V_FWD, V_FWD_E, V_LAST, V_LAST_E, V_FUSED, V_FUSED_E, V_SQR, V_SQR_E, V_INV, V_FUSED2, V_INV_ACC, NV };
+enum { V_FWD, V_FWD_E, V_LAST, V_LAST_E, V_FUSED, V_FUSED_E, V_SQR, V_SQR_E, V_INV, V_FUSED2, V_INV_ACC, V_FWD_T, NV };
 
 template <int LOGL>
 static void fill_row(QKernel (&t)[NV][MAX_PASS_BITS + 1]) {
@@ -975,6 +1035,7 @@ static void fill_row(QKernel (&t)[NV][MAX_PASS_BITS + 1]) {
     constexpr int LM = (LOGL >= 5 && LOGL <= 8) ? LOGL : 5;       // merged pass: two tiles
     t[V_FWD][LOGL] = LOGL >= 5 ? k_qpass<M_FWD, LS, false, false> : nullptr;
     t[V_FWD_E][LOGL] = LOGL >= 5 ? k_qpass<M_FWD, LS, true, false> : nullptr;
+    t[V_FWD_T][LOGL] = LOGL >= 5 ? k_qpass<M_FWD_TW, LS, true, false> : nullptr;
     t[V_INV][LOGL] = LOGL >= 5 ? k_qpass<M_INV, LS, false, false> : nullptr;
     t[V_INV_ACC][LOGL] = LOGL >= 5 ? k_qpass<M_INV_ACC, LS, false, false> : nullptr;
     t[V_FUSED2][LOGL] = (LOGL >= 5 && LOGL <= 8) ? k_qpass<M_FUSED2, LM, false, false> : nullptr;
@@ -1047,7 +1108,7 @@ static const BatchKernelTable& bktab() {
 // tile + the 16 x 32 four-step twiddle factors of strided passes; two tiles when merged
 static size_t pass_smem(int logl, int variant) {
     const size_t L = (size_t)1 << logl, tile = (size_t)TP * L;
-    size_t w = variant == V_FUSED2 ? 2 * tile : tile + TC * 16 + 4;   // + the staging barrier (8 B)
+    size_t w = variant == V_FUSED2 ? 2 * tile : tile + TC * 16 + 8;   // + c^j of a twisted entry
     // staging buffer of the other operand's tile (body_fused, multi-round tiles of <= 8 bits)
     if ((variant == V_FUSED || variant == V_FUSED_E) && logl >= 5 && logl <= 8) w += TC * (L + 4);
     return w * sizeof(u32);
@@ -1181,6 +1242,9 @@ struct QJob {
     int nl;
     u64 NL;
     size_t la_off, lb_off;
+    // twisted (wrap > 0): instead of the low product, the product modulo X^NL - c of both whole
+    // operands (folded and twisted in its first pass), 2^(n - nl) <= 8 folds; see k_qtwist_w
+    bool twist;
 };
 
 constexpr int kMinSplitLog = 12;           // pieces transform at least 2^12 digits (>= 2 passes)
@@ -1213,6 +1277,34 @@ static double plan_wrap(u64 la, u64 lb, int sqr, QJob* W) {
     W->N = N;
     const double t = sqr ? 2.0 : 3.0;
     return t * (double)N * (n + 1) + t * (double)W->NL * (nl + 1) + kPieceCost;
+}
+
+// The twisted plan (see QJob and k_qtwist_w): the cyclic product of length N = 2^n and the
+// product modulo X^M - c, M = 2^m >= K, N / M <= 8, gamma of order 2N within the primes'
+// 2^26-th roots (n <= 25), and a twisted transform of at least two passes.
+constexpr int kMinTwistLog = 12;
+static double plan_twist(u64 la, u64 lb, int sqr, QJob* W) {
+    const u64 dc = 2 * (la + lb) - 1;
+    const int n = ilog2(dc) - 1;
+    if (n < kMinTwistLog || n > Q32_MAX_LOG_N - 1) return -1.0;
+    const u64 N = 1ull << n;
+    if (2 * la > N || 2 * lb > N) return -1.0;
+    const u64 K = dc - N;
+    int m = ilog2(K);
+    if (m < n - 3) m = n - 3;
+    if (m < kMinTwistLog) m = kMinTwistLog;
+    if (m > n) return -1.0;
+    W->wrap = K;
+    W->twist = true;
+    W->nl = m;
+    W->NL = 1ull << m;
+    W->n = n;
+    W->N = N;
+    const double t = sqr ? 2.0 : 3.0, F = (double)(1 << (n - m));
+    // the folded entry reads up to F digits per point (about two butterfly levels each), the
+    // W kernel F residues per wrapped coefficient
+    return t * (double)N * (n + 1) + t * (double)W->NL * (m + 1) + (sqr ? 1.0 : 2.0) * (double)W->NL * 2.0 * F +
+           (double)K * F + kPieceCost;
 }
 
 static QJob plan_job(u64 la, u64 lb, int sqr) {
@@ -1271,11 +1363,13 @@ static QJob plan_job(u64 la, u64 lb, int sqr) {
             }
         }
     }
-    if (best >= 0.0) {
+    // wrapped plans: the low product (force 1) or the twisted product (force 2)
+    const int fw = g_force_wrap.load();
+    for (int kind = 1; kind <= 2 && best >= 0.0; ++kind) {
         QJob W;
         memset(&W, 0, sizeof(W));
-        const double cw = plan_wrap(la, lb, sqr, &W);
-        if (cw >= 0.0 && (cw < best || g_force_wrap.load())) {
+        const double cw = kind == 1 ? plan_wrap(la, lb, sqr, &W) : plan_twist(la, lb, sqr, &W);
+        if (cw >= 0.0 && (fw ? fw == kind : cw < best)) {
             best = cw;
             J = W;
             J.ok = true;
@@ -1346,10 +1440,11 @@ struct Launcher {
         if (!k) return cudaErrorInvalidValue;
         cudaError_t e;
         const double vec = 3.0 * (double)N * 4.0, bfly = 3.0 * ((double)N / 2.0) * logl;
-        const bool entry = (variant == V_FWD_E || variant == V_LAST_E || variant == V_FUSED_E || variant == V_SQR_E);
+        const bool entry = (variant == V_FWD_E || variant == V_FWD_T || variant == V_LAST_E || variant == V_FUSED_E ||
+                            variant == V_SQR_E);
         double bytes = entry ? (double)a.len * 8.0 + vec : 2.0 * vec, mm = bfly + (entry ? 6.0 * (double)a.len : 0.0);
         int kind = K_FUSED;
-        if (variant == V_FWD || variant == V_FWD_E) kind = K_FWD;
+        if (variant == V_FWD || variant == V_FWD_E || variant == V_FWD_T) kind = K_FWD;
         else if (variant == V_LAST || variant == V_LAST_E) kind = K_FWD_LAST;
         else if (variant == V_INV || variant == V_INV_ACC) kind = K_INV;
         if (variant == V_FUSED2) {
@@ -1468,8 +1563,9 @@ static TwPass tw_tables(int logB, int logl, cudaStream_t s) {
 // the GPU together, the default (even) plans are faster (4096 products of 1k-100k limbs:
 // 137k against 104k products/s on B200).
 // `tws`: per pass, its twiddle tables (null: computed in the kernels).
-static void plan_whole(const Job& j, int n, u32* A, u32* B, QWhole* out, u32* err, bool batched = false,
-                       const TwPass* tws = nullptr) {
+// fold_log >= 0: a twisted product (the first pass of each operand is M_FWD_TW; see QArgs).
+static void plan_whole(const Job& j, int n, u32* A, u32* B, QWhole* out, bool batched = false,
+                       const TwPass* tws = nullptr, int fold_log = -1, int tw_log = 0) {
     const int sqr = j.sqr ? 1 : 0;
     if (sqr || j.spectrum) B = A;
     const Plan pl = j.spectrum && j.splan.passes ? j.splan                 // a spectrum keeps its plan
@@ -1489,7 +1585,8 @@ static void plan_whole(const Job& j, int n, u32* A, u32* B, QWhole* out, u32* er
     memset(&pa, 0, sizeof(pa));
     pa.N = N;
     pa.ncols = TC;
-    pa.err = err;
+    pa.fold_log = fold_log;
+    pa.tw_log = tw_log;
     auto add = [&](int variant, int logl, u64 tiles) {
         QRec& r = out->rec[out->count++];
         r.variant = variant;
@@ -1504,7 +1601,7 @@ static void plan_whole(const Job& j, int n, u32* A, u32* B, QWhole* out, u32* er
             pa.data = data;
             pa.logB = logB[p];
             pa.tw = tws ? tws[p].fwd : nullptr;
-            add(p == 0 ? V_FWD_E : V_FWD, pl.bits[p], N >> (pl.bits[p] + LOG_TC));
+            add(p == 0 ? (fold_log >= 0 ? V_FWD_T : V_FWD_E) : V_FWD, pl.bits[p], N >> (pl.bits[p] + LOG_TC));
         }
         pa.tw = nullptr;
     };
@@ -1729,10 +1826,15 @@ int q32_launches(u64 la, u64 lb, int sqr) {
         const int P = q32::qplan(J.n).passes;
         return P + J.m * ((P - 1) + 1 + (P - 1)) + 1;
     }
-    return whole(J.n) + (J.wrap ? whole(J.nl) : 0) + 1;
+    return whole(J.n) + (J.wrap ? whole(J.nl) + (J.twist ? 1 : 0) : 0) + 1;
 }
 
-void q32_force_wrap(int on) { q32::g_force_wrap.store(on ? 1 : 0); }
+void q32_force_wrap(int mode) { q32::g_force_wrap.store(mode == 1 || mode == 2 ? mode : 0); }
+
+u64 q32_twisted(u64 la, u64 lb, int sqr) {
+    const q32::QJob J = q32::plan_job(la, lb, sqr);
+    return J.ok && J.twist ? J.NL : 0;
+}
 
 u64 q32_wrapped(u64 la, u64 lb, int sqr) {
     const q32::QJob J = q32::plan_job(la, lb, sqr);
@@ -1798,7 +1900,7 @@ cudaError_t q32_batch_plan(const Job* jobs, const int* idx, int m, char* res, si
         }
         u32* ticket = (u32*)(st + *soff);
         *soff += q32_batch_state_bytes(j);
-        plan_whole(j, n, A, B, &W[t], err, true);
+        plan_whole(j, n, A, B, &W[t], true);
         QCrtArgs& ca = C[t];
         ca = proto;
         ca.res = A;
@@ -2000,7 +2102,6 @@ cudaError_t q32_enqueue(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s,
     memset(&pa, 0, sizeof(pa));
     pa.N = N;
     pa.ncols = TC;
-    pa.err = (u32*)base;
     auto fwd_strided = [&](const u64* src, u64 len, u32* data) -> cudaError_t {
         for (int p = 0; p + 1 < P; ++p) {
             pa.src = src;
@@ -2039,7 +2140,30 @@ cudaError_t q32_enqueue(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s,
         u32* A = (u32*)(base + J.a);
         u32* B = sqr ? A : (u32*)(base + J.b);
         u64 b_ready = sqr ? j.lb : 0;                          // limbs of the second operand requested so far
-        if (J.wrap) {
+        if (J.wrap && J.twist) {
+            // the product modulo X^M - c first (it reads both operands whole, folded)
+            const int tw_log = Q32_MAX_LOG_N - 1 - J.n;        // gamma = w^(2^tw_log), of order 2N
+            u32* TA = (u32*)(base + J.la_off);
+            u32* TB = sqr ? TA : (u32*)(base + J.lb_off);
+            const Plan plt = qplan(J.nl);
+            TwPass twt[MAX_PASSES];
+            for (int p = 0, lg = J.nl; p + 1 < plt.passes; lg -= plt.bits[p], ++p) twt[p] = tw_tables(lg, plt.bits[p], s);
+            QWhole WT;
+            plan_whole(j, J.nl, TA, TB, &WT, false, twt, J.n - J.nl, tw_log);
+            for (int k = 0; k < WT.count; ++k) {
+                if (b_ready < j.lb && WT.rec[k].a.src == j.b) {
+                    if ((e = launch.need(0, j.lb)) != cudaSuccess) return e;
+                    b_ready = j.lb;
+                }
+                if ((e = launch(WT.rec[k].variant, WT.rec[k].logl, WT.rec[k].a, WT.rec[k].tiles)) != cudaSuccess)
+                    return e;
+            }
+            ca.low = TA;
+            ca.low_N = J.NL;
+            ca.wrap = J.wrap;
+            ca.twisted = 1;
+            for (int i = 0; i < 3; ++i) ca.low_cst[i] = c_host_r1(i);
+        } else if (J.wrap) {
             // the product of the lowest digits first (it reads the second operand's first lpb
             // limbs): its coefficients below `wrap` are the product's c_0 .. c_{wrap-1}
             Job jl = j;
@@ -2051,7 +2175,7 @@ cudaError_t q32_enqueue(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s,
             TwPass twl[MAX_PASSES];
             for (int p = 0, lg = J.nl; p + 1 < pll.passes; lg -= pll.bits[p], ++p) twl[p] = tw_tables(lg, pll.bits[p], s);
             QWhole WL;
-            plan_whole(jl, J.nl, LA, LB, &WL, (u32*)base, false, twl);
+            plan_whole(jl, J.nl, LA, LB, &WL, false, twl);
             for (int k = 0; k < WL.count; ++k) {
                 if (b_ready == 0 && WL.rec[k].a.src == j.b) {
                     if ((e = launch.need(0, J.lpb)) != cudaSuccess) return e;
@@ -2069,7 +2193,7 @@ cudaError_t q32_enqueue(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s,
             for (int i = 0; i < 3; ++i) ca.low_cst[i] = cl.cst[i];
         }
         QWhole W;
-        plan_whole(j, J.n, A, B, &W, (u32*)base, false, tws);
+        plan_whole(j, J.n, A, B, &W, false, tws);
         bool have_b = sqr != 0;
         for (int k = 0; k < W.count; ++k) {
             if (!have_b && W.rec[k].a.src == j.b) {            // the second operand's first reader
@@ -2080,6 +2204,31 @@ cudaError_t q32_enqueue(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s,
         }
         ca.res = A;
         ca.N = N;
+        if (J.wrap && J.twist) {                               // W over the twisted product's residues
+            QTwistArgs ta;
+            memset(&ta, 0, sizeof(ta));
+            ta.U = A;
+            ta.V = (u32*)(base + J.la_off);
+            ta.N = N;
+            ta.K = J.wrap;
+            ta.logM = J.nl;
+            ta.fold_log = J.n - J.nl;
+            ta.tw_log = Q32_MAX_LOG_N - 1 - J.n;
+            QCrtArgs cm;
+            memset(&cm, 0, sizeof(cm));
+            crt_constants(J.NL, &cm);
+            for (int i = 0; i < 3; ++i) {
+                ta.cstN[i] = ca.cst[i];
+                ta.cstM[i] = cm.cst[i];
+            }
+            const u64 blocks = (J.wrap + 255) / 256 < 2048 ? (J.wrap + 255) / 256 : 2048;
+            const ProfMark m = prof_begin(K_CRT, 3.0 * (double)J.wrap * 4.0 * (2.0 + (double)(1 << ta.fold_log)),
+                                          3.0 * (double)J.wrap * (3.0 + (double)(1 << ta.fold_log)), s);
+            k_qtwist_w<<<dim3((unsigned)blocks, 3), 256, 0, s>>>(ta);
+            e = cudaGetLastError();
+            prof_end(m, s);
+            if (e != cudaSuccess) return e;
+        }
     } else {
         // split: S's spectrum once, then every piece of the long operand against it
         u32* R = (u32*)(base + J.a);

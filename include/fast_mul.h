@@ -232,12 +232,18 @@ int fmn_force_pieces(int pieces);
  * transform of 2^n digits (its first K coefficients then hold c_k + c_{k+2^n}) plus the
  * product of the operands' lowest ceil(K / 2) limbs, which gives c_0 .. c_{K-1}; the CRT
  * separates the two.  This replaces a transform of twice the length by one of the same length
- * and a small one: the padding a product just above a power of two would pay.  Chosen by the
- * cost model beside whole and split products.  fmn_wrap_for returns K for a product that runs
- * wrapped (0 otherwise); fmn_force_wrap(1) wraps every product that allows it (tests),
+ * and a small one: the padding a product just above a power of two would pay.  The twisted
+ * form replaces the low product by the product modulo X^M - c (M = 2^m >= K, 2^n / M <= 8,
+ * c^(2^n / M) = -1): one cyclic transform of M digits of both operands folded modulo X^M - c
+ * and twisted, half the size of the low product; then c_{2^n + k} = W_k and c_k = U_k - W_k
+ * with W = (U mod (X^M - c) - V) / 2.  The cost model chooses among whole, split, wrapped and
+ * twisted plans.  fmn_wrap_for returns K for a product that runs wrapped (0 otherwise),
+ * fmn_twist_for its twisted length M (0 when not twisted); fmn_force_wrap(1) wraps every
+ * product that allows it with the low product, fmn_force_wrap(2) twisted (tests),
  * fmn_force_wrap(0) restores the model.  No counterpart in the reference. */
 u64 fmn_wrap_for(u64 len1, u64 len2, int sqr);
-int fmn_force_wrap(int on);
+u64 fmn_twist_for(u64 len1, u64 len2, int sqr);
+int fmn_force_wrap(int mode);
 
 /* ----------------------------------------------------------------- pass plans and tuning
  * A 2^n-point transform runs as passes of <= 9 index bits each; the split is a plan (e.g.

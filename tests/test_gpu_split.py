@@ -66,7 +66,7 @@ def test_split_pinned_host_buffers(fmn, oracle, forced):
         assert np.array_equal(ho, oracle.mul(a, b)), (la, lb)
 
 
-@pytest.mark.parametrize("la,lb", [(5_000_000, 100_000), (300_000, 2_000_000)])
+@pytest.mark.parametrize("la,lb", [(5_000_000, 100_000), (200_000, 3_000_000)])
 def test_model_split_vs_oracle(fmn, oracle, la, lb):
     """Products the cost model splits by itself."""
     assert fmn.pieces_for(la, lb) > 1

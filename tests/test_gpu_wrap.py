@@ -1,8 +1,10 @@
 """Wrapped products on the 32-bit engine: a cyclic transform of 2^n digits whose first K
-coefficients hold c_k + c_{k+2^n}, plus the product of the operands' lowest digits, separated
-again in the CRT.  Every product must equal the reference's digest and the oracle bit for bit,
-whether the cost model picks the wrapped plan (10M x 10M) or it is forced (all shapes that
-allow one, including lengths just above a power of two, squares and unbalanced operands)."""
+coefficients hold c_k + c_{k+2^n}, separated again in the CRT with the help of either the
+product of the operands' lowest digits (mode 1) or the twisted product modulo X^M - c
+(mode 2).  Every product must equal the reference's digest and the oracle bit for bit,
+whether the cost model picks the plan (10M x 10M: twisted, M = 2^23) or it is forced (all
+shapes that allow one, including lengths just above a power of two, squares, unbalanced
+operands and the negacyclic case M = 2^n)."""
 import numpy as np
 import pytest
 
@@ -12,13 +14,18 @@ from tests.helpers import digest, operands_for
 pytestmark = pytest.mark.gpu
 
 
-@pytest.fixture
-def forced_wrap(fmn):
+@pytest.fixture(params=[1, 2], ids=["low", "twisted"])
+def forced_wrap(fmn, request):
     fmn.set_engine(fmn.ENGINE_32)
-    fmn.force_wrap(True)
-    yield
-    fmn.force_wrap(False)
+    fmn.force_wrap(request.param)
+    yield request.param
+    fmn.force_wrap(0)
     fmn.set_engine(fmn.ENGINE_AUTO)
+
+
+def _wrapped(fmn, mode, la, lb, sqr=False):
+    """Whether the forced plan applies to this shape (the twisted one needs 2^n >= 2^12)."""
+    return fmn.wrap_for(la, lb, sqr) > 0 and (mode == 1 or fmn.twist_for(la, lb, sqr) > 0)
 
 
 def test_golden_small_and_medium_wrapped(fmn, golden, forced_wrap):
@@ -29,8 +36,8 @@ def test_golden_small_and_medium_wrapped(fmn, golden, forced_wrap):
         a, b = operands_for(c)
         out = fmn.abs_sqr64(a) if c["op"] == "sqr" else fmn.abs_mul64(a, b)
         assert digest(out) == c["sha256"], (c["op"], c["kind"], c["len1"], c["len2"])
-        n_wrapped += fmn.wrap_for(c["len1"], c["len2"], c["op"] == "sqr") > 0
-    assert n_wrapped > 300
+        n_wrapped += _wrapped(fmn, forced_wrap, c["len1"], c["len2"], c["op"] == "sqr")
+    assert n_wrapped > (300 if forced_wrap == 1 else 5)
 
 
 def test_lengths_just_above_powers_of_two(fmn, oracle, forced_wrap):
@@ -63,7 +70,7 @@ def test_device_and_host_paths_wrapped(fmn, oracle, forced_wrap):
     import torch
     la, lb = 300001, 270000
     a, b = synth.operands("uniform", la, lb, 3)
-    assert fmn.wrap_for(la, lb) > 0
+    assert _wrapped(fmn, forced_wrap, la, lb)
     want = oracle.mul(a, b)
     da = torch.from_numpy(a.view(np.int64)).cuda()
     db = torch.from_numpy(b.view(np.int64)).cuda()
@@ -77,11 +84,31 @@ def test_device_and_host_paths_wrapped(fmn, oracle, forced_wrap):
     assert np.array_equal(fmn.abs_mul64(pa, pb, out=po), want)
 
 
+def test_twisted_folds_and_negacyclic(fmn, oracle, forced_wrap):
+    """Twisted products with 1, 2, 4 and 8 folds of the operands modulo X^M - c (M = 2^n down
+    to 2^(n-3)), all-ones carries, squares."""
+    if forced_wrap != 2:
+        pytest.skip("twisted plan only")
+    n = 16
+    N = 1 << n
+    for K in (N, N // 2 + 5, N // 4 + 1, N // 8, 3):          # wrapped coefficients
+        dc = N + K
+        la = (dc + 1) // 4
+        lb = (dc + 1) // 2 - la
+        for kind in ("uniform", "ones"):
+            a, b = synth.operands(kind, la, lb, K)
+            assert fmn.twist_for(la, lb) > 0, (la, lb)
+            assert np.array_equal(fmn.abs_mul64(a, b), oracle.mul(a, b)), (kind, la, lb, fmn.twist_for(la, lb))
+    a = synth.limbs("ones", N // 2, 7)
+    assert np.array_equal(fmn.abs_sqr64(a), oracle.sqr(a))
+
+
 def test_cost_model_wraps_10M_and_matches_reference(fmn, golden):
-    """The bench configuration: the cost model picks the wrapped plan (2^25-digit cyclic
-    transform + a 3.2M x 3.2M-limb low product) and the result is the reference's."""
+    """The bench configuration: the cost model picks the twisted plan (a 2^25-digit cyclic
+    transform + a 2^23-digit twisted one) and the result is the reference's."""
     assert fmn.engine_for(10_000_000, 10_000_000) == fmn.ENGINE_32
     assert fmn.wrap_for(10_000_000, 10_000_000) > 0
+    assert fmn.twist_for(10_000_000, 10_000_000) == 1 << 23
     for op, kind in (("mul", "uniform"), ("mul", "ones"), ("sqr", "uniform")):
         c = next(c for c in golden if (c["op"], c["kind"], c["len1"], c["len2"]) == (op, kind, 10_000_000, 10_000_000))
         a, b = operands_for(c)

@@ -133,9 +133,13 @@ def test_engine_selection_rules():
     assert fmn.wrap_for(1 << 24, (1 << 24) + 1) == 1
     assert fmn.engine_for(1000, 1000, sqr=True) == fmn.ENGINE_32
     # 10M x 10M: 40M - 1 digit coefficients, a 2^25-digit cyclic transform whose first
-    # 6,445,567 coefficients wrap, plus the 3.2M x 3.2M-limb product of the low limbs
+    # 6,445,567 coefficients wrap, plus the twisted product modulo X^(2^23) - c
     assert fmn.pieces_for(10_000_000, 10_000_000) == 1
     assert fmn.wrap_for(10_000_000, 10_000_000) == 2 * 20_000_000 - 1 - (1 << 25)
+    assert fmn.twist_for(10_000_000, 10_000_000) == 1 << 23
+    # 20M x 20M: the cyclic length would be 2^26, too long for a twist of order 2^27: low product
+    assert fmn.engine_for(20_000_000, 20_000_000) == fmn.ENGINE_32
+    assert fmn.wrap_for(20_000_000, 20_000_000) > 0 and fmn.twist_for(20_000_000, 20_000_000) == 0
     assert fmn.wrap_for(1_000_000, 1_000_000) == 0                        # whole at 2^22 is cheaper
     # split products: unbalanced products above 2^25 limbs reach the 32-bit engine only split
     assert fmn.engine_for(64_000_000, 250_000) == fmn.ENGINE_32
