@@ -72,7 +72,7 @@ def parse():
     ap.add_argument("--no-serve", action="store_true", help="skip the served-stream comparison")
     ap.add_argument("--serve-only", action="store_true", help="only the served-stream comparison")
     ap.add_argument("--serve-requests", type=int, default=100_000)
-    ap.add_argument("--serve-rates", default="1000,4000",
+    ap.add_argument("--serve-rates", default="2000,8000",
                     help="offered requests per second: one below the per-call path's capacity, one above")
     ap.add_argument("--no-extra", action="store_true", help="skip the other configurations")
     ap.add_argument("--extra-only", action="store_true", help="only the other configurations")

@@ -290,6 +290,7 @@ __device__ __forceinline__ const uint2* tw_group(const uint2* tw, u32 col, int r
     return tw + ((kq << logS) + col);
 }
 
+constexpr int kMaxFolds = 4;            // twisted products: N / M <= 4
 // Twisted, folded entry (M_FWD_TW, see QArgs): c^j for j < 2^fold_log in Montgomery form, one
 // prime per CTA, in shared memory (`cp`, written before the first barrier of the pass).
 __device__ __forceinline__ void fill_cpow(u32* cp, const QArgs& a, int pi, const PrimeQ& q) {
@@ -302,12 +303,17 @@ __device__ __forceinline__ u32 entry_val_tw(const u64* __restrict__ src, u64 len
                                             int tw_log, const u32* cp, int pi, const PrimeQ& q) {
     const u32* __restrict__ dig = reinterpret_cast<const u32*>(src);
     const u64 nd = 2 * len;
-    u32 acc = 0;
-    for (int j = 0; j < (1 << fold_log); ++j) {
+    // all folds' loads are issued before any is used (predicated, no early exit)
+    u32 x[kMaxFolds];
+#pragma unroll
+    for (int j = 0; j < kMaxFolds; ++j) {
         const u64 i = (u64)g + ((u64)j << logB);
-        if (i >= nd) break;
-        acc = qadd(acc, qmont(__ldg(dig + i), cp[j], q), q);
+        x[j] = (j < (1 << fold_log) && i < nd) ? __ldg(dig + i) : 0u;
     }
+    u32 acc = 0;
+#pragma unroll
+    for (int j = 0; j < kMaxFolds; ++j)
+        if (j < (1 << fold_log)) acc = qadd(acc, qmont(x[j], cp[j], q), q);
     return qmont(acc, qroot(((u32)g << tw_log) & MASK_N, pi, q), q);
 }
 
@@ -660,7 +666,7 @@ __device__ __forceinline__ void body_fused2(u32* sm, const QArgs& a, u64 tile, i
 template <int MODE, int LOGL>
 constexpr int min_ctas() {
     return ((MODE == M_FWD || MODE == M_FWD_TW || MODE == M_INV || MODE == M_INV_ACC) && LOGL >= 9) ||
-                   MODE == M_FUSED2 ||
+                   (MODE == M_FWD_TW && LOGL >= 7) || MODE == M_FUSED2 ||
                    (MODE == M_FUSED && LOGL == 8)
                ? 3
                : 4;
@@ -917,14 +923,19 @@ struct QTwistArgs {
 __global__ void __launch_bounds__(256) k_qtwist_w(QTwistArgs t) {
     const int pi = blockIdx.y;
     const PrimeQ q = c_q[pi];
-    __shared__ u32 cp[8];
+    __shared__ u32 cp[kMaxFolds];
     if ((int)threadIdx.x < (1 << t.fold_log)) cp[threadIdx.x] = qroot(((u32)threadIdx.x << (t.logM + t.tw_log)) & MASK_N, pi, q);
     __syncthreads();
     const u32* __restrict__ U = t.U + (u64)pi * t.N;
     u32* __restrict__ V = t.V + ((u64)pi << t.logM);
     for (u64 k = (u64)blockIdx.x * blockDim.x + threadIdx.x; k < t.K; k += (u64)gridDim.x * blockDim.x) {
+        u32 x[kMaxFolds];
+#pragma unroll
+        for (int j = 0; j < kMaxFolds; ++j) x[j] = j < (1 << t.fold_log) ? U[k + ((u64)j << t.logM)] : 0u;
         u32 ub = 0;
-        for (int j = 0; j < (1 << t.fold_log); ++j) ub = qadd(ub, qmont(U[k + ((u64)j << t.logM)], cp[j], q), q);
+#pragma unroll
+        for (int j = 0; j < kMaxFolds; ++j)
+            if (j < (1 << t.fold_log)) ub = qadd(ub, qmont(x[j], cp[j], q), q);
         ub = qmont(ub, t.cstN[pi], q);
         u32 v = qmont(V[k], t.cstM[pi], q);
         v = qmont(v, qroot((0u - ((u32)k << t.tw_log)) & MASK_N, pi, q), q);   // times gamma^-k
@@ -1243,7 +1254,7 @@ struct QJob {
     u64 NL;
     size_t la_off, lb_off;
     // twisted (wrap > 0): instead of the low product, the product modulo X^NL - c of both whole
-    // operands (folded and twisted in its first pass), 2^(n - nl) <= 8 folds; see k_qtwist_w
+    // operands (folded and twisted in its first pass), 2^(n - nl) <= 4 folds; see k_qtwist_w
     bool twist;
 };
 
@@ -1280,7 +1291,7 @@ static double plan_wrap(u64 la, u64 lb, int sqr, QJob* W) {
 }
 
 // The twisted plan (see QJob and k_qtwist_w): the cyclic product of length N = 2^n and the
-// product modulo X^M - c, M = 2^m >= K, N / M <= 8, gamma of order 2N within the primes'
+// product modulo X^M - c, M = 2^m >= K, N / M <= 4, gamma of order 2N within the primes'
 // 2^26-th roots (n <= 25), and a twisted transform of at least two passes.
 constexpr int kMinTwistLog = 12;
 static double plan_twist(u64 la, u64 lb, int sqr, QJob* W) {
@@ -1291,7 +1302,7 @@ static double plan_twist(u64 la, u64 lb, int sqr, QJob* W) {
     if (2 * la > N || 2 * lb > N) return -1.0;
     const u64 K = dc - N;
     int m = ilog2(K);
-    if (m < n - 3) m = n - 3;
+    if (m < n - 2) m = n - 2;                                   // at most kMaxFolds folds
     if (m < kMinTwistLog) m = kMinTwistLog;
     if (m > n) return -1.0;
     W->wrap = K;

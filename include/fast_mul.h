@@ -233,7 +233,7 @@ int fmn_force_pieces(int pieces);
  * product of the operands' lowest ceil(K / 2) limbs, which gives c_0 .. c_{K-1}; the CRT
  * separates the two.  This replaces a transform of twice the length by one of the same length
  * and a small one: the padding a product just above a power of two would pay.  The twisted
- * form replaces the low product by the product modulo X^M - c (M = 2^m >= K, 2^n / M <= 8,
+ * form replaces the low product by the product modulo X^M - c (M = 2^m >= K, 2^n / M <= 4,
  * c^(2^n / M) = -1): one cyclic transform of M digits of both operands folded modulo X^M - c
  * and twisted, half the size of the low product; then c_{2^n + k} = W_k and c_k = U_k - W_k
  * with W = (U mod (X^M - c) - V) / 2.  The cost model chooses among whole, split, wrapped and

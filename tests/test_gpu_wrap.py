@@ -85,8 +85,8 @@ def test_device_and_host_paths_wrapped(fmn, oracle, forced_wrap):
 
 
 def test_twisted_folds_and_negacyclic(fmn, oracle, forced_wrap):
-    """Twisted products with 1, 2, 4 and 8 folds of the operands modulo X^M - c (M = 2^n down
-    to 2^(n-3)), all-ones carries, squares."""
+    """Twisted products with 1, 2 and 4 folds of the operands modulo X^M - c (M = 2^n down
+    to 2^(n-2)), all-ones carries, squares."""
     if forced_wrap != 2:
         pytest.skip("twisted plan only")
     n = 16
