@@ -433,6 +433,10 @@ def serve_compare(fmn, torch, dev, n_requests, rates, seed=0, templates=256, res
         reqs.append(r)
     gaps = rng.exponential(1.0, n_requests)
     ops = [tmpl[t].op for t in pick]
+    # product length of each request (for latency by size class)
+    tlen = [(r.len1 + r.len2) if r.op == fmn.FMN_OP_MUL else 2 * r.len1 if r.op == fmn.FMN_OP_SQR
+            else res_ops[t % residents].len + r.len2 for t, r in enumerate(tmpl)]
+    big = np.array([tlen[t] > (1 << 20) for t in pick])
     gpu_work_s = float(sum(alone_ms[t] for t in pick)) * 1e-3
     out = {"workload": f"{n_requests} requests, open-loop Poisson; 70% multiply / 30% square, 25% of the "
                        f"multiplies by one of {residents} resident operands; lengths log-uniform in [{lo}, {hi}] "
@@ -440,6 +444,7 @@ def serve_compare(fmn, torch, dev, n_requests, rates, seed=0, templates=256, res
            "requests": n_requests,
            "mix": {"mul": ops.count(fmn.FMN_OP_MUL), "sqr": ops.count(fmn.FMN_OP_SQR),
                    "mul_resident": ops.count(fmn.FMN_OP_MUL_OPERAND)},
+           "large_requests": int(big.sum()),
            "gpu_work_alone_s": gpu_work_s,
            "per_call_device_bound_products_per_s": n_requests / gpu_work_s,
            "rates": {}}
@@ -455,8 +460,13 @@ def serve_compare(fmn, torch, dev, n_requests, rates, seed=0, templates=256, res
                 st = srv.stats()
             finally:
                 srv.close()
-            lat = np.sort(np.array(lat))
+            lat_all = np.array(lat)
+            pct = lambda x, p: float(np.percentile(x, p)) if len(x) else None
+            lat = np.sort(lat_all)
             res[name] = {"products_per_s": st["completed"] / wall, "wall_s": wall,
+                         "p90_ms": pct(lat_all, 90), "p999_ms": pct(lat_all, 99.9), "max_ms": float(lat.max()),
+                         "large_p50_ms": pct(lat_all[big], 50), "large_p99_ms": pct(lat_all[big], 99),
+                         "small_p50_ms": pct(lat_all[~big], 50), "small_p99_ms": pct(lat_all[~big], 99),
                          "p50_ms": float(lat[len(lat) // 2]),
                          "p99_ms": float(lat[min(len(lat) - 1, int(0.99 * len(lat)))]),
                          "mean_ms": float(lat.mean()), "batches": st["batches"],

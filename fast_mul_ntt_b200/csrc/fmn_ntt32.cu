@@ -109,7 +109,7 @@ __device__ __forceinline__ void stage_tile(u32* sm, const u32* __restrict__ g, i
     }
 }
 
-enum { M_FWD = 0, M_FWD_LAST = 1, M_FUSED = 2, M_INV = 3, M_FUSED2 = 4, M_INV_ACC = 5, M_FWD_TW = 6 };
+enum { M_FWD = 0, M_FWD_LAST = 1, M_FUSED = 2, M_INV = 3, M_FUSED2 = 4, M_INV_ACC = 5 };
 
 struct QArgs {
     const u64* src;   // ENTRY: limbs of the operand being transformed
@@ -131,11 +131,6 @@ struct QArgs {
     // 2^logB entries per prime (frequency k of the column transform, column i), or null to
     // compute them from the root tables
     const uint2* tw;
-    // M_FWD_TW (the first pass of a twisted product modulo X^M - c, M = 2^logB): digit g of the
-    // input is gamma^g * sum_{j < 2^fold_log} c^j a_{g + j M}, gamma = w^(2^tw_log) (w of order
-    // 2^26), c = gamma^M
-    int fold_log;
-    int tw_log;
 };
 
 // ------------------------------------------------------------------ one round
@@ -291,35 +286,9 @@ __device__ __forceinline__ const uint2* tw_group(const uint2* tw, u32 col, int r
 }
 
 constexpr int kMaxFolds = 4;            // twisted products: N / M <= 4
-// Twisted, folded entry (M_FWD_TW, see QArgs): c^j for j < 2^fold_log in Montgomery form, one
-// prime per CTA, in shared memory (`cp`, written before the first barrier of the pass).
-__device__ __forceinline__ void fill_cpow(u32* cp, const QArgs& a, int pi, const PrimeQ& q) {
-    if ((int)threadIdx.x < (1 << a.fold_log)) {
-        const u32 e = ((u32)threadIdx.x << (a.logB + a.tw_log)) & MASK_N;   // c^j = w^(j M 2^tw_log)
-        cp[threadIdx.x] = qroot(e, pi, q);
-    }
-}
-__device__ __forceinline__ u32 entry_val_tw(const u64* __restrict__ src, u64 len, u32 g, int logB, int fold_log,
-                                            int tw_log, const u32* cp, int pi, const PrimeQ& q) {
-    const u32* __restrict__ dig = reinterpret_cast<const u32*>(src);
-    const u64 nd = 2 * len;
-    // all folds' loads are issued before any is used (predicated, no early exit)
-    u32 x[kMaxFolds];
-#pragma unroll
-    for (int j = 0; j < kMaxFolds; ++j) {
-        const u64 i = (u64)g + ((u64)j << logB);
-        x[j] = (j < (1 << fold_log) && i < nd) ? __ldg(dig + i) : 0u;
-    }
-    u32 acc = 0;
-#pragma unroll
-    for (int j = 0; j < kMaxFolds; ++j)
-        if (j < (1 << fold_log)) acc = qadd(acc, qmont(x[j], cp[j], q), q);
-    return qmont(acc, qroot(((u32)g << tw_log) & MASK_N, pi, q), q);
-}
 
-// Forward strided pass (pass p < P-1 of a multi-pass transform).  TWIST: the entry pass of a
-// twisted product (M_FWD_TW).
-template <int LOGL, bool ENTRY, bool TWIST = false>
+// Forward strided pass (pass p < P-1 of a multi-pass transform).
+template <int LOGL, bool ENTRY>
 __device__ __forceinline__ void body_fwd(u32* sm, const QArgs& a, u64 tile, int pi, const PrimeQ& q) {
     constexpr int L = 1 << LOGL;
     constexpr int RB = round_bits(LOGL, rounds_count(LOGL) - 1), R = 1 << RB;
@@ -337,23 +306,16 @@ __device__ __forceinline__ void body_fwd(u32* sm, const QArgs& a, u64 tile, int 
     constexpr bool STAGED = !ENTRY;
     u32* beta = sm + (STAGED ? TC : TP) * L;
     const uint2* __restrict__ tw = a.tw ? a.tw + ((u64)pi << a.logB) : nullptr;
-    u32* cp = beta + TC * 16;                                 // TWIST: c^j
     if constexpr (STAGED) stage_tile<L>(sm, d + gbase, logS);
     if (!tw) fill_beta<LOGL, false>(beta, col0, shift, pi, q);   // read after the first round's barrier
     if constexpr (STAGED) {
         cp_async_commit_wait();
         __syncthreads();
     }
-    if constexpr (TWIST) {
-        fill_cpow(cp, a, pi, q);
-        __syncthreads();
-    }
-    const int fold_log = a.fold_log, tw_log = a.tw_log, logB = a.logB;
     auto ld0 = [=](int j, int c) -> u32 {
         if constexpr (STAGED) return sm[dix(j, c)];
         const u32 g = gbase + c + ((u32)j << logS);
-        if constexpr (TWIST) return entry_val_tw(src, len, g, logB, fold_log, tw_log, cp, pi, q);
-        else if constexpr (ENTRY) return entry_val(src, len, g, q);
+        if constexpr (ENTRY) return entry_val(src, len, g, q);
         else return d[g];
     };
     auto stl = [=](int row0, int c, const auto& x) {
@@ -665,8 +627,7 @@ __device__ __forceinline__ void body_fused2(u32* sm, const QArgs& a, u64 tile, i
 // strided passes fit 64 registers without spills and run at 4 (1% faster than at 3).
 template <int MODE, int LOGL>
 constexpr int min_ctas() {
-    return ((MODE == M_FWD || MODE == M_FWD_TW || MODE == M_INV || MODE == M_INV_ACC) && LOGL >= 9) ||
-                   (MODE == M_FWD_TW && LOGL >= 7) || MODE == M_FUSED2 ||
+    return ((MODE == M_FWD || MODE == M_INV || MODE == M_INV_ACC) && LOGL >= 9) || MODE == M_FUSED2 ||
                    (MODE == M_FUSED && LOGL == 8)
                ? 3
                : 4;
@@ -679,7 +640,6 @@ __global__ void __launch_bounds__(NT, (min_ctas<MODE, LOGL>())) k_qpass(QArgs a)
     const u64 tile = blockIdx.x / 3;
     const PrimeQ q = c_q[pi];
     if constexpr (MODE == M_FWD) body_fwd<LOGL, ENTRY>(qsm, a, tile, pi, q);
-    else if constexpr (MODE == M_FWD_TW) body_fwd<LOGL, true, true>(qsm, a, tile, pi, q);
     else if constexpr (MODE == M_INV) body_inv<LOGL, false>(qsm, a, tile, pi, q);
     else if constexpr (MODE == M_INV_ACC) body_inv<LOGL, true>(qsm, a, tile, pi, q);
     else if constexpr (MODE == M_FWD_LAST) body_fwd_last<LOGL, ENTRY>(qsm, a, tile, pi, q);
@@ -913,6 +873,46 @@ __global__ void __launch_bounds__(CNT) k_qcrt_carry_batch(const QCrtArgs* __rest
 //     W = (U mod (X^M - c) - V) / 2,   U mod (X^M - c) = sum_j c^j U_{k + j M}.
 // The kernel writes W_k (plain, reduced) over V_k for k < K; the CRT then takes c_{N+k} = W_k
 // and c_k = U_k - W_k.  Each residue array is scaled by its own length (and V untwisted).
+// The operand folded modulo X^M - c and twisted, as residues: entry g (< M) of prime i is
+// gamma^g sum_{j < 2^fold_log} c^j a_{g + jM} mod q_i (a the operand's 32-bit digits, zero past
+// its end), written to T + i M + g.  One thread per g: the fold's digits are loaded once for
+// all three primes, each load coalesced across the warp.
+struct QFoldArgs {
+    const u64* src;
+    u64 len;            // limbs (2 len digits)
+    u32* T;
+    int logM, fold_log, tw_log;
+};
+__global__ void __launch_bounds__(256) k_qtwist_fold(QFoldArgs f) {
+    __shared__ u32 cp[3][kMaxFolds];
+    const int F = 1 << f.fold_log;
+    if ((int)threadIdx.x < 3 * F) {
+        const int pi = threadIdx.x / F, j = threadIdx.x % F;
+        cp[pi][j] = qroot(((u32)j << (f.logM + f.tw_log)) & MASK_N, pi, c_q[pi]);   // c^j, Montgomery form
+    }
+    __syncthreads();
+    const u32* __restrict__ dig = reinterpret_cast<const u32*>(f.src);
+    const u64 nd = 2 * f.len, M = 1ull << f.logM;
+    for (u64 g = (u64)blockIdx.x * blockDim.x + threadIdx.x; g < M; g += (u64)gridDim.x * blockDim.x) {
+        u32 x[kMaxFolds];
+#pragma unroll
+        for (int j = 0; j < kMaxFolds; ++j) {
+            const u64 i = g + ((u64)j << f.logM);
+            x[j] = (j < F && i < nd) ? __ldg(dig + i) : 0u;
+        }
+        const u32 e = ((u32)g << f.tw_log) & MASK_N;              // gamma^g
+#pragma unroll
+        for (int pi = 0; pi < 3; ++pi) {
+            const PrimeQ q = c_q[pi];
+            u32 acc = 0;
+#pragma unroll
+            for (int j = 0; j < kMaxFolds; ++j)
+                if (j < F) acc = qadd(acc, qmont(x[j], cp[pi][j], q), q);
+            f.T[(u64)pi * M + g] = qmont(acc, qroot(e, pi, q), q);
+        }
+    }
+}
+
 struct QTwistArgs {
     const u32* U;       // cyclic product's residues (prime i at U + i N), raw
     u32* V;             // twisted product's residues (prime i at V + i M), raw; W on return
@@ -1038,7 +1038,7 @@ static const HostTables& host_tables() {
 
 // ------------------------------------------------------------------ host: kernels
 typedef void (*QKernel)(QArgs);
-enum { V_FWD, V_FWD_E, V_LAST, V_LAST_E, V_FUSED, V_FUSED_E, V_SQR, V_SQR_E, V_INV, V_FUSED2, V_INV_ACC, V_FWD_T, NV };
+enum { V_FWD, V_FWD_E, V_LAST, V_LAST_E, V_FUSED, V_FUSED_E, V_SQR, V_SQR_E, V_INV, V_FUSED2, V_INV_ACC, NV };
 
 template <int LOGL>
 static void fill_row(QKernel (&t)[NV][MAX_PASS_BITS + 1]) {
@@ -1046,7 +1046,6 @@ static void fill_row(QKernel (&t)[NV][MAX_PASS_BITS + 1]) {
     constexpr int LM = (LOGL >= 5 && LOGL <= 8) ? LOGL : 5;       // merged pass: two tiles
     t[V_FWD][LOGL] = LOGL >= 5 ? k_qpass<M_FWD, LS, false, false> : nullptr;
     t[V_FWD_E][LOGL] = LOGL >= 5 ? k_qpass<M_FWD, LS, true, false> : nullptr;
-    t[V_FWD_T][LOGL] = LOGL >= 5 ? k_qpass<M_FWD_TW, LS, true, false> : nullptr;
     t[V_INV][LOGL] = LOGL >= 5 ? k_qpass<M_INV, LS, false, false> : nullptr;
     t[V_INV_ACC][LOGL] = LOGL >= 5 ? k_qpass<M_INV_ACC, LS, false, false> : nullptr;
     t[V_FUSED2][LOGL] = (LOGL >= 5 && LOGL <= 8) ? k_qpass<M_FUSED2, LM, false, false> : nullptr;
@@ -1119,7 +1118,7 @@ static const BatchKernelTable& bktab() {
 // tile + the 16 x 32 four-step twiddle factors of strided passes; two tiles when merged
 static size_t pass_smem(int logl, int variant) {
     const size_t L = (size_t)1 << logl, tile = (size_t)TP * L;
-    size_t w = variant == V_FUSED2 ? 2 * tile : tile + TC * 16 + 8;   // + c^j of a twisted entry
+    size_t w = variant == V_FUSED2 ? 2 * tile : tile + TC * 16;
     // staging buffer of the other operand's tile (body_fused, multi-round tiles of <= 8 bits)
     if ((variant == V_FUSED || variant == V_FUSED_E) && logl >= 5 && logl <= 8) w += TC * (L + 4);
     return w * sizeof(u32);
@@ -1254,7 +1253,7 @@ struct QJob {
     u64 NL;
     size_t la_off, lb_off;
     // twisted (wrap > 0): instead of the low product, the product modulo X^NL - c of both whole
-    // operands (folded and twisted in its first pass), 2^(n - nl) <= 4 folds; see k_qtwist_w
+    // operands (folded and twisted by k_qtwist_fold), 2^(n - nl) <= 4 folds; see k_qtwist_w
     bool twist;
 };
 
@@ -1312,9 +1311,9 @@ static double plan_twist(u64 la, u64 lb, int sqr, QJob* W) {
     W->n = n;
     W->N = N;
     const double t = sqr ? 2.0 : 3.0, F = (double)(1 << (n - m));
-    // the folded entry reads up to F digits per point (about two butterfly levels each), the
-    // W kernel F residues per wrapped coefficient
-    return t * (double)N * (n + 1) + t * (double)W->NL * (m + 1) + (sqr ? 1.0 : 2.0) * (double)W->NL * 2.0 * F +
+    // the fold kernels and the W kernel: memory passes over F digits / residues per point,
+    // about one butterfly level each
+    return t * (double)N * (n + 1) + t * (double)W->NL * (m + 1) + (sqr ? 1.0 : 2.0) * (double)W->NL * F +
            (double)K * F + kPieceCost;
 }
 
@@ -1451,11 +1450,10 @@ struct Launcher {
         if (!k) return cudaErrorInvalidValue;
         cudaError_t e;
         const double vec = 3.0 * (double)N * 4.0, bfly = 3.0 * ((double)N / 2.0) * logl;
-        const bool entry = (variant == V_FWD_E || variant == V_FWD_T || variant == V_LAST_E || variant == V_FUSED_E ||
-                            variant == V_SQR_E);
+        const bool entry = (variant == V_FWD_E || variant == V_LAST_E || variant == V_FUSED_E || variant == V_SQR_E);
         double bytes = entry ? (double)a.len * 8.0 + vec : 2.0 * vec, mm = bfly + (entry ? 6.0 * (double)a.len : 0.0);
         int kind = K_FUSED;
-        if (variant == V_FWD || variant == V_FWD_E || variant == V_FWD_T) kind = K_FWD;
+        if (variant == V_FWD || variant == V_FWD_E) kind = K_FWD;
         else if (variant == V_LAST || variant == V_LAST_E) kind = K_FWD_LAST;
         else if (variant == V_INV || variant == V_INV_ACC) kind = K_INV;
         if (variant == V_FUSED2) {
@@ -1574,9 +1572,10 @@ static TwPass tw_tables(int logB, int logl, cudaStream_t s) {
 // the GPU together, the default (even) plans are faster (4096 products of 1k-100k limbs:
 // 137k against 104k products/s on B200).
 // `tws`: per pass, its twiddle tables (null: computed in the kernels).
-// fold_log >= 0: a twisted product (the first pass of each operand is M_FWD_TW; see QArgs).
+// prefolded: the operands' residues are already in A and B (a twisted product, written by
+// k_qtwist_fold), so the first pass reads them instead of the limbs.
 static void plan_whole(const Job& j, int n, u32* A, u32* B, QWhole* out, bool batched = false,
-                       const TwPass* tws = nullptr, int fold_log = -1, int tw_log = 0) {
+                       const TwPass* tws = nullptr, bool prefolded = false) {
     const int sqr = j.sqr ? 1 : 0;
     if (sqr || j.spectrum) B = A;
     const Plan pl = j.spectrum && j.splan.passes ? j.splan                 // a spectrum keeps its plan
@@ -1596,8 +1595,6 @@ static void plan_whole(const Job& j, int n, u32* A, u32* B, QWhole* out, bool ba
     memset(&pa, 0, sizeof(pa));
     pa.N = N;
     pa.ncols = TC;
-    pa.fold_log = fold_log;
-    pa.tw_log = tw_log;
     auto add = [&](int variant, int logl, u64 tiles) {
         QRec& r = out->rec[out->count++];
         r.variant = variant;
@@ -1612,7 +1609,7 @@ static void plan_whole(const Job& j, int n, u32* A, u32* B, QWhole* out, bool ba
             pa.data = data;
             pa.logB = logB[p];
             pa.tw = tws ? tws[p].fwd : nullptr;
-            add(p == 0 ? (fold_log >= 0 ? V_FWD_T : V_FWD_E) : V_FWD, pl.bits[p], N >> (pl.bits[p] + LOG_TC));
+            add(p == 0 && !prefolded ? V_FWD_E : V_FWD, pl.bits[p], N >> (pl.bits[p] + LOG_TC));
         }
         pa.tw = nullptr;
     };
@@ -1837,7 +1834,7 @@ int q32_launches(u64 la, u64 lb, int sqr) {
         const int P = q32::qplan(J.n).passes;
         return P + J.m * ((P - 1) + 1 + (P - 1)) + 1;
     }
-    return whole(J.n) + (J.wrap ? whole(J.nl) + (J.twist ? 1 : 0) : 0) + 1;
+    return whole(J.n) + (J.wrap ? whole(J.nl) + (J.twist ? (sqr ? 2 : 3) : 0) : 0) + 1;   // + folds and W
 }
 
 void q32_force_wrap(int mode) { q32::g_force_wrap.store(mode == 1 || mode == 2 ? mode : 0); }
@@ -2159,16 +2156,30 @@ cudaError_t q32_enqueue(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s,
             const Plan plt = qplan(J.nl);
             TwPass twt[MAX_PASSES];
             for (int p = 0, lg = J.nl; p + 1 < plt.passes; lg -= plt.bits[p], ++p) twt[p] = tw_tables(lg, plt.bits[p], s);
+            // both operands folded and twisted into TA / TB, then an ordinary transform of them
+            const u64 fblocks = (J.NL + 255) / 256 < 1184 ? (J.NL + 255) / 256 : 1184;
+            for (int op = 0; op < (sqr ? 1 : 2); ++op) {
+                if (op == 1 && (e = launch.need(0, j.lb)) != cudaSuccess) return e;
+                QFoldArgs fa;
+                fa.src = op ? j.b : j.a;
+                fa.len = op ? j.lb : j.la;
+                fa.T = op ? TB : TA;
+                fa.logM = J.nl;
+                fa.fold_log = J.n - J.nl;
+                fa.tw_log = tw_log;
+                const ProfMark m = prof_begin(K_FWD, (double)fa.len * 8.0 + 3.0 * (double)J.NL * 4.0,
+                                              3.0 * (double)J.NL * (2.0 + (double)(1 << fa.fold_log)), s);
+                k_qtwist_fold<<<(unsigned)fblocks, 256, 0, s>>>(fa);
+                e = cudaGetLastError();
+                prof_end(m, s);
+                if (e != cudaSuccess) return e;
+            }
+            b_ready = j.lb;
             QWhole WT;
-            plan_whole(j, J.nl, TA, TB, &WT, false, twt, J.n - J.nl, tw_log);
-            for (int k = 0; k < WT.count; ++k) {
-                if (b_ready < j.lb && WT.rec[k].a.src == j.b) {
-                    if ((e = launch.need(0, j.lb)) != cudaSuccess) return e;
-                    b_ready = j.lb;
-                }
+            plan_whole(j, J.nl, TA, TB, &WT, false, twt, true);
+            for (int k = 0; k < WT.count; ++k)
                 if ((e = launch(WT.rec[k].variant, WT.rec[k].logl, WT.rec[k].a, WT.rec[k].tiles)) != cudaSuccess)
                     return e;
-            }
             ca.low = TA;
             ca.low_N = J.NL;
             ca.wrap = J.wrap;

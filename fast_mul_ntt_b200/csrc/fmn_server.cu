@@ -21,6 +21,7 @@
 #include <string.h>
 
 #include <atomic>
+#include <cmath>
 #include <chrono>
 #include <condition_variable>
 #include <deque>
@@ -137,6 +138,24 @@ void ensure_server_twiddles(fmn_server* s, int log_n, cudaStream_t st) {
     s->tw.push_back({buf, ts});
 }
 
+// Whether a product with a resident operand should use its spectrum.  The spectrum has the
+// transform length of the operand's longest partner, so a product with a short partner can be
+// much cheaper from scratch.  Modelled costs (points x bits of the spectrum's engine): reuse
+// transforms the partner and inverts at the spectrum's length; a fresh product costs whatever
+// that engine's planner picks for the two lengths.
+bool spectrum_pays(const fmn_request& r) {
+    const fmn_operand* o = r.operand;
+    const double reuse = 2.0 * std::ldexp(1.0, o->log_n) * (o->log_n + 1);
+    double fresh;
+    if (o->engine == fmn::ENGINE_32) {
+        fresh = fmn::q32_cost(o->len, r.len2, 0);
+    } else {
+        const int n = ilog2c(o->len + r.len2 - 1);
+        fresh = 3.0 * std::ldexp(1.0, n) * (n + 1);
+    }
+    return reuse <= fresh;
+}
+
 fmn::Job to_job(const fmn_request& r, bool reuse, u64* out) {
     fmn::Job j;
     j.out = out;
@@ -146,7 +165,7 @@ fmn::Job to_job(const fmn_request& r, bool reuse, u64* out) {
         j.b = r.in2;
         j.lb = r.len2;
         j.sqr = 0;
-        if (reuse) {
+        if (reuse && spectrum_pays(r)) {
             j.a = nullptr;
             j.spectrum = o->spec;
             j.log_n = o->log_n;
@@ -176,7 +195,7 @@ size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 // Transform length (log2) of a request's product.
 int request_log_n(const fmn_request& r, bool reuse) {
     // in 64-bit points (a 32-bit spectrum has two digits per limb)
-    if (r.op == FMN_OP_MUL_OPERAND && reuse)
+    if (r.op == FMN_OP_MUL_OPERAND && reuse && spectrum_pays(r))
         return r.operand->engine == fmn::ENGINE_32 ? r.operand->log_n - 1 : r.operand->log_n;
     const u64 ol = out_len_of(r);
     return ol > 1 ? ilog2c(ol - 1) : 0;

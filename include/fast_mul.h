@@ -146,9 +146,13 @@ int fmn_mul_operand_ws(const fmn_operand* op, const u64* d_in2, u64 len2, u64* d
  * Continuous batching: requests submitted from any thread are admitted in arrival order
  * while their scratch fits the HBM budget and a slot (CUDA stream) is free; admitted
  * requests run as one batch, batches overlap on the device, and requests arriving meanwhile
- * join the next batch as slots and memory free up.  With batching = 0 the server is the
- * plain per-call path: one product per launch sequence, in arrival order, on one stream,
- * without resident-operand reuse.  No counterpart in the reference. */
+ * join the next batch as slots and memory free up.  Large products (above 2^20 limbs) run
+ * one per slot on two dedicated slots, so small requests never queue behind them.  A product
+ * with a resident operand uses the operand's spectrum when that is modelled cheaper than
+ * computing it from scratch (the spectrum has the length of the longest partner it was sized
+ * for).  With batching = 0 the server is the plain per-call path: one product per launch
+ * sequence, in arrival order, on one stream, without resident-operand reuse.  No counterpart
+ * in the reference. */
 enum { FMN_OP_MUL = 0, FMN_OP_SQR = 1, FMN_OP_MUL_OPERAND = 2 };
 typedef struct {
     int op;                      /* FMN_OP_* */
