@@ -724,10 +724,16 @@ __device__ __forceinline__ u128 qgarner(u32 x0, u32 y1, u32 y2, const QCrtArgs& 
     hi += (lo < ml) + (mid >> 32);
     return ((u128)hi << 64) | lo;
 }
-// Residue vectors of 4 consecutive coefficients from one array of one prime.
-__device__ __forceinline__ void ld4(const u32* p, u32 (&r)[4]) {
-    const uint4 v = *reinterpret_cast<const uint4*>(p);
-    r[0] = v.x, r[1] = v.y, r[2] = v.z, r[3] = v.w;
+// Residue vectors of VW (2 or 4) consecutive coefficients from one array of one prime.
+template <int VW>
+__device__ __forceinline__ void ldv(const u32* p, u32 (&r)[VW]) {
+    if constexpr (VW == 4) {
+        const uint4 v = *reinterpret_cast<const uint4*>(p);
+        r[0] = v.x, r[1] = v.y, r[2] = v.z, r[3] = v.w;
+    } else {
+        const uint2 v = *reinterpret_cast<const uint2*>(p);
+        r[0] = v.x, r[1] = v.y;
+    }
 }
 // Where coefficient k comes from (see QCrtArgs): 0 res_k, 1 low_k, 2 res_{k-N} - low_{k-N}.
 __device__ __forceinline__ int qsource(const QCrtArgs& a, u64 k) {
@@ -767,38 +773,41 @@ __device__ __forceinline__ void qcrt_carry_body(const QCrtArgs& a, u32 ncta) {
     const int src = WRAP ? qsource(a, k0) : 0;
     const bool full = k0 + 2 * QCE <= a.nvalid && (src != 1 || k0 + 2 * QCE <= a.wrap);
     const u64 kb = src == 2 ? k0 - a.N : k0;
+    // VW coefficients (VW / 2 limbs) at a time: four for plain products, two for wrapped ones,
+    // whose two sources would otherwise hold too many registers for 4 CTAs per SM
+    constexpr int VW = WRAP ? 2 : 4;
 #pragma unroll
-    for (int e2 = 0; e2 < QCE; e2 += 2) {             // two limbs = four coefficients at a time
-        u32 y0[4], y1[4], y2[4];                       // c_k mod q_i
+    for (int e2 = 0; e2 < QCE; e2 += VW / 2) {
+        u32 y0[VW], y1[VW], y2[VW];                    // c_k mod q_i
         if (full) {
             const u64 k = kb + 2 * e2;
             if (src != 0 && (src == 2) == (a.twisted != 0)) {   // low alone
-                ld4(a.low + k, y0);
-                ld4(a.low + a.low_N + k, y1);
-                ld4(a.low + 2 * a.low_N + k, y2);
+                ldv<VW>(a.low + k, y0);
+                ldv<VW>(a.low + a.low_N + k, y1);
+                ldv<VW>(a.low + 2 * a.low_N + k, y2);
 #pragma unroll
-                for (int t = 0; t < 4; ++t) {
+                for (int t = 0; t < VW; ++t) {
                     y0[t] = qmont(y0[t], a.low_cst[0], q0);
                     y1[t] = qmont(y1[t], a.low_cst[1], q1);
                     y2[t] = qmont(y2[t], a.low_cst[2], q2);
                 }
             } else {
-                ld4(a.res + k, y0);
-                ld4(a.res + a.N + k, y1);
-                ld4(a.res + 2 * a.N + k, y2);
+                ldv<VW>(a.res + k, y0);
+                ldv<VW>(a.res + a.N + k, y1);
+                ldv<VW>(a.res + 2 * a.N + k, y2);
 #pragma unroll
-                for (int t = 0; t < 4; ++t) {
+                for (int t = 0; t < VW; ++t) {
                     y0[t] = qmont(y0[t], a.cst[0], q0);
                     y1[t] = qmont(y1[t], a.cst[1], q1);
                     y2[t] = qmont(y2[t], a.cst[2], q2);
                 }
                 if (src != 0) {                                  // res - low
-                    u32 l0[4], l1[4], l2[4];
-                    ld4(a.low + k, l0);
-                    ld4(a.low + a.low_N + k, l1);
-                    ld4(a.low + 2 * a.low_N + k, l2);
+                    u32 l0[VW], l1[VW], l2[VW];
+                    ldv<VW>(a.low + k, l0);
+                    ldv<VW>(a.low + a.low_N + k, l1);
+                    ldv<VW>(a.low + 2 * a.low_N + k, l2);
 #pragma unroll
-                    for (int t = 0; t < 4; ++t) {
+                    for (int t = 0; t < VW; ++t) {
                         y0[t] = qsub(y0[t], qmont(l0[t], a.low_cst[0], q0), q0);
                         y1[t] = qsub(y1[t], qmont(l1[t], a.low_cst[1], q1), q1);
                         y2[t] = qsub(y2[t], qmont(l2[t], a.low_cst[2], q2), q2);
@@ -807,7 +816,7 @@ __device__ __forceinline__ void qcrt_carry_body(const QCrtArgs& a, u32 ncta) {
             }
         }
 #pragma unroll
-        for (int u = 0; u < 2; ++u) {
+        for (int u = 0; u < VW / 2; ++u) {
             const int e = e2 + u;
             u128 cl, ch;
             if (full) {
@@ -847,9 +856,8 @@ __device__ __forceinline__ void qcrt_carry_body(const QCrtArgs& a, u32 ncta) {
 __global__ void __launch_bounds__(CNT, QCE <= 8 ? 4 : 3) k_qcrt_carry(QCrtArgs a) {
     qcrt_carry_body<false>(a, 0xffffffffu);
 }
-// Wrapped products: two residue sources and a second set of scale constants take more
-// registers than 4 CTAs per SM allow without spills.
-__global__ void __launch_bounds__(CNT, 3) k_qcrt_carry_wrap(QCrtArgs a) { qcrt_carry_body<true>(a, 0xffffffffu); }
+// Wrapped products (two residue sources, two sets of scale constants).
+__global__ void __launch_bounds__(CNT, 4) k_qcrt_carry_wrap(QCrtArgs a) { qcrt_carry_body<true>(a, 0xffffffffu); }
 
 // The plain kernel with a look-back limit of 2^12 polls (milliseconds instead of seconds), for
 // the test that withholds a tile and checks that the wait expires into the status word.
