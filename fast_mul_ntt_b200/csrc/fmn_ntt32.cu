@@ -901,22 +901,31 @@ __global__ void __launch_bounds__(256) k_qtwist_fold(QFoldArgs f) {
     __syncthreads();
     const u32* __restrict__ dig = reinterpret_cast<const u32*>(f.src);
     const u64 nd = 2 * f.len, M = 1ull << f.logM;
-    for (u64 g = (u64)blockIdx.x * blockDim.x + threadIdx.x; g < M; g += (u64)gridDim.x * blockDim.x) {
+    const u64 g0 = (u64)blockIdx.x * blockDim.x + threadIdx.x, S = (u64)gridDim.x * blockDim.x;
+    // gamma^g in Montgomery form, stepped by gamma^S along the grid-stride loop
+    u32 gm[3], gs[3];
+#pragma unroll
+    for (int pi = 0; pi < 3; ++pi) {
+        gm[pi] = qroot(((u32)g0 << f.tw_log) & MASK_N, pi, c_q[pi]);
+        gs[pi] = qroot(((u32)S << f.tw_log) & MASK_N, pi, c_q[pi]);
+    }
+    for (u64 g = g0; g < M; g += S) {
         u32 x[kMaxFolds];
 #pragma unroll
         for (int j = 0; j < kMaxFolds; ++j) {
             const u64 i = g + ((u64)j << f.logM);
             x[j] = (j < F && i < nd) ? __ldg(dig + i) : 0u;
         }
-        const u32 e = ((u32)g << f.tw_log) & MASK_N;              // gamma^g
+        const u64 top = nd > g ? (nd - g + M - 1) >> f.logM : 0;   // folds holding digits at g
 #pragma unroll
         for (int pi = 0; pi < 3; ++pi) {
             const PrimeQ q = c_q[pi];
             u32 acc = 0;
 #pragma unroll
             for (int j = 0; j < kMaxFolds; ++j)
-                if (j < F) acc = qadd(acc, qmont(x[j], cp[pi][j], q), q);
-            f.T[(u64)pi * M + g] = qmont(acc, qroot(e, pi, q), q);
+                if (j < F && (u64)j < top) acc = qadd(acc, qmont(x[j], cp[pi][j], q), q);
+            f.T[(u64)pi * M + g] = qmont(acc, gm[pi], q);
+            gm[pi] = qmont(gm[pi], gs[pi], q);
         }
     }
 }
@@ -936,19 +945,24 @@ __global__ void __launch_bounds__(256) k_qtwist_w(QTwistArgs t) {
     __syncthreads();
     const u32* __restrict__ U = t.U + (u64)pi * t.N;
     u32* __restrict__ V = t.V + ((u64)pi << t.logM);
-    for (u64 k = (u64)blockIdx.x * blockDim.x + threadIdx.x; k < t.K; k += (u64)gridDim.x * blockDim.x) {
+    const u64 k0 = (u64)blockIdx.x * blockDim.x + threadIdx.x, S = (u64)gridDim.x * blockDim.x;
+    // gamma^-k in Montgomery form, stepped by gamma^-S along the grid-stride loop
+    u32 gm = qroot((0u - ((u32)k0 << t.tw_log)) & MASK_N, pi, q);
+    const u32 gs = qroot((0u - ((u32)S << t.tw_log)) & MASK_N, pi, q);
+    for (u64 k = k0; k < t.K; k += S) {
         u32 x[kMaxFolds];
 #pragma unroll
         for (int j = 0; j < kMaxFolds; ++j) x[j] = j < (1 << t.fold_log) ? U[k + ((u64)j << t.logM)] : 0u;
+        const u32 vr = V[k];
         u32 ub = 0;
 #pragma unroll
         for (int j = 0; j < kMaxFolds; ++j)
             if (j < (1 << t.fold_log)) ub = qadd(ub, qmont(x[j], cp[j], q), q);
         ub = qmont(ub, t.cstN[pi], q);
-        u32 v = qmont(V[k], t.cstM[pi], q);
-        v = qmont(v, qroot((0u - ((u32)k << t.tw_log)) & MASK_N, pi, q), q);   // times gamma^-k
+        const u32 v = qmont(qmont(vr, t.cstM[pi], q), gm, q);   // V_k, untwisted
         const u32 d = qsub(ub, v, q);
         V[k] = (d + ((d & 1u) ? q.p : 0u)) >> 1;
+        gm = qmont(gm, gs, q);
     }
 }
 
