@@ -62,7 +62,7 @@ class FmnJob(ctypes.Structure):
     """fmn_job of include/fast_mul.h (device pointers)."""
     _fields_ = [("in1", ctypes.c_void_p), ("len1", ctypes.c_uint64), ("in2", ctypes.c_void_p),
                 ("len2", ctypes.c_uint64), ("out", ctypes.c_void_p)]
-KERNEL_KINDS = 5
+KERNEL_KINDS = 6
 
 _u64 = ctypes.c_uint64
 _u64p = ctypes.POINTER(ctypes.c_uint64)

@@ -197,7 +197,8 @@ const char* launch_diag();
 
 // ---- optional per-kernel timing (used by bench.py; off by default)
 // Kernel kinds of the pipeline.
-enum KernelKind { K_FWD = 0, K_FWD_LAST, K_FUSED, K_INV, K_CRT, K_KINDS };
+// K_WRAP: the fold and W kernels of twisted wrapped products.
+enum KernelKind { K_FWD = 0, K_FWD_LAST, K_FUSED, K_INV, K_CRT, K_WRAP, K_KINDS };
 const char* kernel_kind_name(int k);
 struct KindStats {
     double ms;          // summed CUDA-event time

@@ -1117,7 +1117,7 @@ cudaError_t spectrum_enqueue(const u64* src, u64 len, int log_n, u64* spec, cuda
 // ------------------------------------------------------------------ host: profiling
 const char* kernel_kind_name(int k) {
     static const char* names[K_KINDS] = {"fwd_pass", "fwd_last_pass", "fused_pointwise_pass", "inv_pass",
-                                         "crt_carry"};
+                                         "crt_carry", "wrap_fold_w"};
     return (k >= 0 && k < K_KINDS) ? names[k] : "?";
 }
 

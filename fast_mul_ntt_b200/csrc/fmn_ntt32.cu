@@ -2189,7 +2189,7 @@ cudaError_t q32_enqueue(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s,
                 fa.logM = J.nl;
                 fa.fold_log = J.n - J.nl;
                 fa.tw_log = tw_log;
-                const ProfMark m = prof_begin(K_FWD, (double)fa.len * 8.0 + 3.0 * (double)J.NL * 4.0,
+                const ProfMark m = prof_begin(K_WRAP, (double)fa.len * 8.0 + 3.0 * (double)J.NL * 4.0,
                                               3.0 * (double)J.NL * (2.0 + (double)(1 << fa.fold_log)), s);
                 k_qtwist_fold<<<(unsigned)fblocks, 256, 0, s>>>(fa);
                 e = cudaGetLastError();
@@ -2266,7 +2266,7 @@ cudaError_t q32_enqueue(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s,
                 ta.cstM[i] = cm.cst[i];
             }
             const u64 blocks = (J.wrap + 255) / 256 < 2048 ? (J.wrap + 255) / 256 : 2048;
-            const ProfMark m = prof_begin(K_CRT, 3.0 * (double)J.wrap * 4.0 * (2.0 + (double)(1 << ta.fold_log)),
+            const ProfMark m = prof_begin(K_WRAP, 3.0 * (double)J.wrap * 4.0 * (2.0 + (double)(1 << ta.fold_log)),
                                           3.0 * (double)J.wrap * (3.0 + (double)(1 << ta.fold_log)), s);
             k_qtwist_w<<<dim3((unsigned)blocks, 3), 256, 0, s>>>(ta);
             e = cudaGetLastError();

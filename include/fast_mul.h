@@ -276,8 +276,9 @@ int fmn_load_default_plans(void);
  * (no counterpart in the reference; used by bench.py) */
 
 /* Kernel kinds of the pipeline, in this order: forward pass, forward last pass, fused
- * pointwise pass, inverse pass, CRT + carry. */
-#define FMN_KERNEL_KINDS 5
+ * pointwise pass, inverse pass, CRT + carry, and the fold / W kernels of twisted wrapped
+ * products. */
+#define FMN_KERNEL_KINDS 6
 const char* fmn_kernel_kind_name(int kind);
 /* Record CUDA events around every kernel launch of the calling thread (on = 1) or stop. */
 int fmn_profile_enable(int on);
