@@ -694,8 +694,8 @@ struct QCrtArgs {
     u64 low_N;
     u64 wrap;           // K: coefficients that wrapped (0: none)
     u32 low_cst[3];     // the low product's scale constants (low_N^-1 * 2^64 mod q_i)
-    // twisted: `low` holds W (plain, reduced; low_cst = 2^32 mod q_i) with the wrapped
-    // coefficients c_{N+k} = W_k and c_k = res_k - W_k for k < K (see k_qtwist_w)
+    // twisted: `low` holds W (plain, reduced; low_cst = 2^32 mod q_i), the wrapped
+    // coefficients c_{N+k} = W_k, and res_k already holds c_k for k < K (see k_qtwist_w)
     int twisted;
 };
 
@@ -735,9 +735,10 @@ __device__ __forceinline__ void ldv(const u32* p, u32 (&r)[VW]) {
         r[0] = v.x, r[1] = v.y;
     }
 }
-// Where coefficient k comes from (see QCrtArgs): 0 res_k, 1 low_k, 2 res_{k-N} - low_{k-N}.
+// Where coefficient k comes from (see QCrtArgs): 0 res_k, 1 low_k, 2 res_{k-N} - low_{k-N}
+// (twisted: k_qtwist_w has already written c_k into res below N, so only 0 and 2, low alone).
 __device__ __forceinline__ int qsource(const QCrtArgs& a, u64 k) {
-    return k < a.wrap ? 1 : (k >= a.N && a.wrap ? 2 : 0);
+    return k >= a.N && a.wrap ? 2 : (k < a.wrap && !a.twisted ? 1 : 0);
 }
 // c_k mod q_i (reduced) of one prime, by source.
 // (a wrapped product's sources 1 and 2 swap formulas when it is twisted: res - low at k < K,
@@ -879,8 +880,11 @@ __global__ void __launch_bounds__(CNT) k_qcrt_carry_batch(const QCrtArgs* __rest
 // X^M - c and twisted by gamma^i, gamma of order 2N, c = gamma^M, so c^(2^s) = -1).  With
 // C = U + (X^N - 1) W, deg W < K <= M, and X^N = -1 mod (X^M - c):
 //     W = (U mod (X^M - c) - V) / 2,   U mod (X^M - c) = sum_j c^j U_{k + j M}.
-// The kernel writes W_k (plain, reduced) over V_k for k < K; the CRT then takes c_{N+k} = W_k
-// and c_k = U_k - W_k.  Each residue array is scaled by its own length (and V untwisted).
+// The kernel writes W_k (plain, reduced) over V_k and c_k = U_k - W_k over U_k (in U's raw
+// form, times N 2^-32, as the CRT reads it) for k < K; the CRT then takes c_{N+k} = W_k and
+// c_k from U.  Each residue array is scaled by its own length (and V untwisted).  Updating U_k
+// in place is safe: the other residues read for a k, U_{k+jM} with j >= 1, lie at or above
+// M >= K.
 // The operand folded modulo X^M - c and twisted, as residues: entry g (< M) of prime i is
 // gamma^g sum_{j < 2^fold_log} c^j a_{g + jM} mod q_i (a the operand's 32-bit digits, zero past
 // its end), written to T + i M + g.  One thread per g: the fold's digits are loaded once for
@@ -931,11 +935,12 @@ __global__ void __launch_bounds__(256) k_qtwist_fold(QFoldArgs f) {
 }
 
 struct QTwistArgs {
-    const u32* U;       // cyclic product's residues (prime i at U + i N), raw
+    u32* U;             // cyclic product's residues (prime i at U + i N), raw; c_k below K on return
     u32* V;             // twisted product's residues (prime i at V + i M), raw; W on return
     u64 N, K;
     int logM, fold_log, tw_log;
     u32 cstN[3], cstM[3];
+    u32 nmod[3];        // N mod q_i: qmont(c, N) is c in U's raw form
 };
 __global__ void __launch_bounds__(256) k_qtwist_w(QTwistArgs t) {
     const int pi = blockIdx.y;
@@ -943,7 +948,7 @@ __global__ void __launch_bounds__(256) k_qtwist_w(QTwistArgs t) {
     __shared__ u32 cp[kMaxFolds];
     if ((int)threadIdx.x < (1 << t.fold_log)) cp[threadIdx.x] = qroot(((u32)threadIdx.x << (t.logM + t.tw_log)) & MASK_N, pi, q);
     __syncthreads();
-    const u32* __restrict__ U = t.U + (u64)pi * t.N;
+    u32* __restrict__ U = t.U + (u64)pi * t.N;
     u32* __restrict__ V = t.V + ((u64)pi << t.logM);
     const u64 k0 = (u64)blockIdx.x * blockDim.x + threadIdx.x, S = (u64)gridDim.x * blockDim.x;
     // gamma^-k in Montgomery form, stepped by gamma^-S along the grid-stride loop
@@ -961,7 +966,9 @@ __global__ void __launch_bounds__(256) k_qtwist_w(QTwistArgs t) {
         ub = qmont(ub, t.cstN[pi], q);
         const u32 v = qmont(qmont(vr, t.cstM[pi], q), gm, q);   // V_k, untwisted
         const u32 d = qsub(ub, v, q);
-        V[k] = (d + ((d & 1u) ? q.p : 0u)) >> 1;
+        const u32 w = (d + ((d & 1u) ? q.p : 0u)) >> 1;
+        V[k] = w;
+        U[k] = qmont(qsub(qmont(x[0], t.cstN[pi], q), w, q), t.nmod[pi], q);   // c_k = U_k - W_k
         gm = qmont(gm, gs, q);
     }
 }
@@ -2264,6 +2271,7 @@ cudaError_t q32_enqueue(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s,
             for (int i = 0; i < 3; ++i) {
                 ta.cstN[i] = ca.cst[i];
                 ta.cstM[i] = cm.cst[i];
+                ta.nmod[i] = (u32)(N % kQ[i]);
             }
             const u64 blocks = (J.wrap + 255) / 256 < 2048 ? (J.wrap + 255) / 256 : 2048;
             const ProfMark m = prof_begin(K_WRAP, 3.0 * (double)J.wrap * 4.0 * (2.0 + (double)(1 << ta.fold_log)),
