@@ -263,10 +263,36 @@ def _stream_ptr(stream):
     return getattr(stream, "cuda_stream", stream)
 
 
+_LIMB_DTYPES = None
+
+
+def _dev_limbs(t, what, need=None):
+    """A CUDA tensor of 64-bit limbs, contiguous, with at least ``need`` elements (outputs):
+    checked before any launch, since the C ABI takes plain pointers and sizes and a short
+    output buffer would be written past its end."""
+    global _LIMB_DTYPES
+    if _LIMB_DTYPES is None:
+        import torch
+        _LIMB_DTYPES = frozenset(d for d in (torch.int64, getattr(torch, "uint64", None)) if d is not None)
+    if (getattr(t, "is_cuda", False) and t.dtype in _LIMB_DTYPES and t.is_contiguous()
+            and (need is None or t.numel() >= need)):
+        return t
+    if not getattr(t, "is_cuda", False):
+        raise ValueError(f"{what}: expected a CUDA tensor")
+    if t.element_size() != 8 or t.dtype.is_floating_point or t.dtype.is_complex:
+        raise ValueError(f"{what}: expected 64-bit integer limbs, got {t.dtype}")
+    if not t.is_contiguous():
+        raise ValueError(f"{what}: expected a contiguous tensor")
+    if need is not None and t.numel() < need:
+        raise ValueError(f"{what}: holds {t.numel()} limbs, needs {need}")
+    return t
+
+
 def mul_device(a, b, out, stream=None):
     """Device product of int64/uint64 CUDA tensors holding limbs; asynchronous on ``stream``
     (default: torch's current stream).  ``out`` must hold len(a) + len(b) limbs."""
     lib = load_library()
+    _dev_limbs(a, "a"), _dev_limbs(b, "b"), _dev_limbs(out, "out", a.numel() + b.numel())
     _check(lib.fmn_mul_device(a.data_ptr(), a.numel(), b.data_ptr(), b.numel(), out.data_ptr(),
                               _stream_ptr(stream)))
     return out
@@ -275,6 +301,7 @@ def mul_device(a, b, out, stream=None):
 def sqr_device(a, out, stream=None):
     """Device square of a CUDA limb tensor into ``out`` (2 * len(a) limbs)."""
     lib = load_library()
+    _dev_limbs(a, "a"), _dev_limbs(out, "out", 2 * a.numel())
     _check(lib.fmn_sqr_device(a.data_ptr(), a.numel(), out.data_ptr(), _stream_ptr(stream)))
     return out
 
@@ -293,6 +320,7 @@ def mul_device_ws(a, b, out, ws, stream=None):
     """Device product with caller-provided scratch ``ws`` (a CUDA tensor of at least
     workspace_size bytes, 256-byte aligned)."""
     lib = load_library()
+    _dev_limbs(a, "a"), _dev_limbs(b, "b"), _dev_limbs(out, "out", a.numel() + b.numel())
     _check(lib.fmn_mul_device_ws(a.data_ptr(), a.numel(), b.data_ptr(), b.numel(), out.data_ptr(),
                                  ws.data_ptr(), ws.numel() * ws.element_size(), _stream_ptr(stream)))
     return out
@@ -308,6 +336,7 @@ def mul_device_noalloc(a, b, out, stream=None):
     <= 65537).  For callers that cannot allocate device memory while they run; waits for
     ``stream``.  Calls overlapping on the GPU share the array and race."""
     lib = load_library()
+    _dev_limbs(a, "a"), _dev_limbs(b, "b"), _dev_limbs(out, "out", a.numel() + b.numel())
     _check(lib.fmn_mul_device_noalloc(a.data_ptr(), a.numel(), b.data_ptr(), b.numel(), out.data_ptr(),
                                       _stream_ptr(stream)))
     return out
@@ -351,18 +380,33 @@ def _job_array(jobs):
     """[(a, b, out), ...] of CUDA tensors -> ctypes array of FmnJob (a is b: square)."""
     arr = (FmnJob * len(jobs))()
     for i, (a, b, out) in enumerate(jobs):
+        _dev_limbs(a, f"jobs[{i}] a"), _dev_limbs(b, f"jobs[{i}] b")
+        _dev_limbs(out, f"jobs[{i}] out", a.numel() + (a.numel() if a is b else b.numel()))
         arr[i].in1, arr[i].len1 = a.data_ptr(), a.numel()
         arr[i].in2, arr[i].len2 = b.data_ptr(), b.numel()
         arr[i].out = out.data_ptr()
     return arr
 
 
+class BatchJobs:
+    """A job list for mul_batch_device checked and marshalled once, for a batch that is
+    launched again and again on the same tensors (the tensors must outlive it)."""
+
+    def __init__(self, jobs):
+        self._jobs = jobs
+        self.arr = _job_array(jobs)
+        self.n = len(jobs)
+
+
 def mul_batch_device(jobs, stream=None):
-    """All products of ``jobs`` ([(a, b, out)], CUDA limb tensors; ``a is b`` squares) in
-    batched launches, asynchronously on ``stream``."""
+    """All products of ``jobs`` ([(a, b, out)], CUDA limb tensors; ``a is b`` squares; or a
+    BatchJobs) in batched launches, asynchronously on ``stream``."""
     lib = load_library()
-    arr = _job_array(jobs)
-    _check(lib.fmn_mul_batch_device(arr, len(jobs), _stream_ptr(stream)))
+    if isinstance(jobs, BatchJobs):
+        arr, n = jobs.arr, jobs.n
+    else:
+        arr, n = _job_array(jobs), len(jobs)
+    _check(lib.fmn_mul_batch_device(arr, n, _stream_ptr(stream)))
 
 
 class BatchGraph:
@@ -401,7 +445,7 @@ class Operand:
 
     def __init__(self, limbs, max_partner_len, stream=None):
         lib = load_library()
-        self.limbs = limbs
+        self.limbs = _dev_limbs(limbs, "limbs")
         h = ctypes.c_void_p()
         _check(lib.fmn_operand_create(limbs.data_ptr(), limbs.numel(), max_partner_len, _stream_ptr(stream),
                                       ctypes.byref(h)))
@@ -409,6 +453,7 @@ class Operand:
         self.len = limbs.numel()
 
     def mul(self, b, out, stream=None):
+        _dev_limbs(b, "b"), _dev_limbs(out, "out", self.len + b.numel())
         _check(load_library().fmn_mul_operand_device(self.handle, b.data_ptr(), b.numel(), out.data_ptr(),
                                                       _stream_ptr(stream)))
         return out

@@ -17,6 +17,10 @@
 
 #include <atomic>
 #include <condition_variable>
+#include <algorithm>
+#include <thread>
+#include <functional>
+#include <deque>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -53,6 +57,84 @@ struct HostLane {
     size_t io_cap = 0;
     unsigned* h_err = nullptr;             // pinned word for reading the device error flag
     bool busy = false;
+    // pageable host buffers: pinned staging slots (kStageSlots x kStageChunk bytes, allocated
+    // on first use) and the event of each slot's last transfer
+    char* stage = nullptr;
+    cudaEvent_t stage_ev[4] = {nullptr};
+    bool stage_used[4] = {false};
+};
+
+constexpr size_t kStageChunk = 8u << 20;   // bytes per staging slot
+constexpr int kStageSlots = 4;
+
+// A few host threads that copy between pageable and pinned memory in parallel: one thread's
+// memcpy reaches a fraction of the host's memory bandwidth.  FMN_COPY_THREADS (1 .. 32,
+// default min(8, hardware threads / 2)) sets their number, counting the calling thread (on a
+// 16-thread host, 8 copied faster than 16 or 24 at 10M x 10M limbs).
+class CopyPool {
+  public:
+    static CopyPool& get() {
+        static CopyPool* p = new CopyPool();      // never destroyed: threads outlive static teardown
+        return *p;
+    }
+    // dst[0, n) = src[0, n), split across the pool and the calling thread.
+    void copy(void* dst, const void* src, size_t n) {
+        const size_t parts = n < (1u << 20) ? 1 : std::min<size_t>(workers_ + 1, n >> 20);
+        if (parts <= 1) {
+            memcpy(dst, src, n);
+            return;
+        }
+        const size_t per = ((n + parts - 1) / parts + 63) & ~(size_t)63;
+        // the count is changed and read only under m, so the caller cannot return (and free
+        // m and cv) before the last worker has let go of m
+        int left = 0;
+        std::mutex m;
+        std::condition_variable cv;
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            for (size_t k = 1; k < parts; ++k) {
+                const size_t off = k * per;
+                if (off >= n) break;
+                const size_t len = std::min(per, n - off);
+                ++left;
+                tasks_.push_back([=, &left, &m, &cv] {
+                    memcpy((char*)dst + off, (const char*)src + off, len);
+                    std::lock_guard<std::mutex> g(m);
+                    if (--left == 0) cv.notify_one();
+                });
+            }
+        }
+        cv_.notify_all();
+        memcpy(dst, src, std::min(per, n));
+        std::unique_lock<std::mutex> lk(m);
+        cv.wait(lk, [&] { return left == 0; });
+    }
+
+  private:
+    CopyPool() {
+        const char* v = getenv("FMN_COPY_THREADS");
+        unsigned hw = std::thread::hardware_concurrency();
+        int n = v ? atoi(v) : (int)std::min(8u, hw > 1 ? hw / 2 : 1u);
+        n = n < 1 ? 1 : (n > 32 ? 32 : n);
+        workers_ = (size_t)n - 1;
+        for (size_t k = 0; k < workers_; ++k) std::thread([this] { run(); }).detach();
+    }
+    void run() {
+        for (;;) {
+            std::function<void()> t;
+            {
+                std::unique_lock<std::mutex> lk(mu_);
+                cv_.wait(lk, [&] { return !tasks_.empty(); });
+                t = std::move(tasks_.front());
+                tasks_.pop_front();
+            }
+            t();
+        }
+    }
+    size_t workers_ = 0;
+    std::mutex mu_;
+    std::condition_variable cv_;
+    std::deque<std::function<void()>> tasks_;
 };
 
 struct DevCtx {
@@ -190,6 +272,9 @@ void destroy_lane(HostLane* L) {
         if (ev) cudaEventDestroy(ev);
     for (cudaEvent_t ev : L->ci_event)
         if (ev) cudaEventDestroy(ev);
+    for (cudaEvent_t ev : L->stage_ev)
+        if (ev) cudaEventDestroy(ev);
+    if (L->stage) cudaFreeHost(L->stage);
     delete L;
 }
 
@@ -215,6 +300,8 @@ int acquire_lane(DevCtx* c, HostLane** out) {
     for (cudaEvent_t& ev : L->cb_event)
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
     for (cudaEvent_t& ev : L->ci_event)
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+    for (cudaEvent_t& ev : L->stage_ev)
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaMallocHost((void**)&L->h_err, sizeof(unsigned));
     if (e != cudaSuccess) {
@@ -453,6 +540,57 @@ int host_product_pinned(DevCtx* c, HostLane* L, const u64* in1, u64 len1, const 
     return take_device_error(L->ws, L->h_err, L->s);
 }
 
+// Pageable source -> device, through the lane's pinned slots: each chunk is copied into a free
+// slot by the copy pool, then sent by DMA on the copy-in stream while the next chunk is
+// copied.  Returns once every chunk is in flight (the caller orders its kernels after them).
+int stage_in(HostLane* L, char* d_dst, const char* h_src, size_t bytes) {
+    cudaError_t e;
+    int slot = 0;
+    for (size_t off = 0; off < bytes; off += kStageChunk, slot = (slot + 1) % kStageSlots) {
+        const size_t n = std::min(kStageChunk, bytes - off);
+        if (L->stage_used[slot] && (e = cudaEventSynchronize(L->stage_ev[slot])) != cudaSuccess)
+            return set_err(FMN_ERR_CUDA, "waiting for a staging slot", e);
+        char* pin = L->stage + (size_t)slot * kStageChunk;
+        CopyPool::get().copy(pin, h_src + off, n);
+        if ((e = cudaMemcpyAsync(d_dst + off, pin, n, cudaMemcpyHostToDevice, L->cs)) != cudaSuccess ||
+            (e = cudaEventRecord(L->stage_ev[slot], L->cs)) != cudaSuccess)
+            return set_err(FMN_ERR_CUDA, "copying an operand to the device", e);
+        L->stage_used[slot] = true;
+    }
+    return FMN_OK;
+}
+
+// Device -> pageable destination after the lane's stream: up to kStageSlots chunks in flight by
+// DMA into the slots; each is copied out by the copy pool as soon as it lands, and its slot
+// takes the next chunk.
+int stage_out(HostLane* L, char* h_dst, const char* d_src, size_t bytes) {
+    cudaError_t e;
+    const size_t nch = (bytes + kStageChunk - 1) / kStageChunk;
+    auto issue = [&](size_t k) -> cudaError_t {
+        const int slot = (int)(k % kStageSlots);
+        const size_t off = k * kStageChunk, n = std::min(kStageChunk, bytes - off);
+        // the slot's previous transfer (an input chunk on the copy-in stream) must be done
+        if (L->stage_used[slot] && (e = cudaStreamWaitEvent(L->s, L->stage_ev[slot], 0)) != cudaSuccess) return e;
+        if ((e = cudaMemcpyAsync(L->stage + (size_t)slot * kStageChunk, d_src + off, n, cudaMemcpyDeviceToHost, L->s)) !=
+            cudaSuccess)
+            return e;
+        L->stage_used[slot] = true;
+        return cudaEventRecord(L->stage_ev[slot], L->s);
+    };
+    for (size_t k = 0; k < nch && k < (size_t)kStageSlots; ++k)
+        if ((e = issue(k)) != cudaSuccess) return set_err(FMN_ERR_CUDA, "copying the product to the host", e);
+    for (size_t k = 0; k < nch; ++k) {
+        const int slot = (int)(k % kStageSlots);
+        const size_t off = k * kStageChunk, n = std::min(kStageChunk, bytes - off);
+        if ((e = cudaEventSynchronize(L->stage_ev[slot])) != cudaSuccess)
+            return set_err(FMN_ERR_CUDA, "copying the product to the host", e);
+        CopyPool::get().copy(h_dst + off, L->stage + (size_t)slot * kStageChunk, n);
+        if (k + kStageSlots < nch && (e = issue(k + kStageSlots)) != cudaSuccess)
+            return set_err(FMN_ERR_CUDA, "copying the product to the host", e);
+    }
+    return FMN_OK;
+}
+
 int host_product(const u64* in1, u64 len1, const u64* in2, u64 len2, u64* out, int sqr) {
     fmn::NvtxRange nvtx("fmn host product");
     const u64 out_len = len1 + len2;
@@ -474,14 +612,20 @@ int host_product(const u64* in1, u64 len1, const u64* in2, u64 len2, u64* out, i
         ((const char*)out + (len1 + len2) * 8 <= (const char*)in1 || (const char*)out >= (const char*)(in1 + len1)) &&
         (sqr || (const char*)out + (len1 + len2) * 8 <= (const char*)in2 || (const char*)out >= (const char*)(in2 + len2)))
         return host_product_pinned(c, L, in1, len1, in2, len2, out, sqr);
-    // pageable buffers: copies through the driver's staging (they may block the calling
-    // thread, so they are issued outside the device lock); device layout [in1][in2][out]
+    // pageable buffers: staged through the lane's pinned slots (copies issued outside the
+    // device lock); device layout [in1][in2][out]
     const size_t o1 = 0, o2 = round256(len1 * 8), oo = o2 + (sqr ? 0 : round256(len2 * 8));
     fmn::Job j;
     cudaError_t e;
     {
         std::lock_guard<std::mutex> lk(c->mu);
         if ((rc = ensure_buf((void**)&L->io, &L->io_cap, oo + round256(out_len * 8), false))) return rc;
+    }
+    if (!L->stage) {
+        if ((e = cudaMallocHost((void**)&L->stage, kStageSlots * kStageChunk)) != cudaSuccess) {
+            L->stage = nullptr;
+            return set_err(FMN_ERR_NOMEM, "pinned staging buffers", e);
+        }
     }
     char* io = (char*)L->io;
     j.a = (const u64*)(io + o1);
@@ -490,12 +634,13 @@ int host_product(const u64* in1, u64 len1, const u64* in2, u64 len2, u64* out, i
     j.lb = len2;
     j.out = (u64*)(io + oo);
     j.sqr = sqr;
-    if (L->done_valid && (e = cudaStreamWaitEvent(L->s, L->done, 0)) != cudaSuccess)
+    // the copy-in stream may not overwrite the operands before the lane's previous product is done
+    if (L->done_valid && (e = cudaStreamWaitEvent(L->cs, L->done, 0)) != cudaSuccess)
         return set_err(FMN_ERR_CUDA, "cudaStreamWaitEvent", e);
-    if ((e = cudaMemcpyAsync(io + o1, in1, len1 * 8, cudaMemcpyHostToDevice, L->s)) != cudaSuccess)
-        return set_err(FMN_ERR_CUDA, "copying in1 to the device", e);
-    if (!sqr && (e = cudaMemcpyAsync(io + o2, in2, len2 * 8, cudaMemcpyHostToDevice, L->s)) != cudaSuccess)
-        return set_err(FMN_ERR_CUDA, "copying in2 to the device", e);
+    if ((rc = stage_in(L, io + o1, (const char*)in1, len1 * 8))) return rc;
+    if (!sqr && (rc = stage_in(L, io + o2, (const char*)in2, len2 * 8))) return rc;
+    if ((e = cudaEventRecord(L->join[0], L->cs)) != cudaSuccess || (e = cudaStreamWaitEvent(L->s, L->join[0], 0)) != cudaSuccess)
+        return set_err(FMN_ERR_CUDA, "ordering the product after its copies", e);
     {
         std::lock_guard<std::mutex> lk(c->mu);
         if ((rc = ensure_buf(&L->ws, &L->ws_cap, fmn::job_workspace_bytes(j), true))) return rc;
@@ -508,8 +653,7 @@ int host_product(const u64* in1, u64 len1, const u64* in2, u64 len2, u64* out, i
         if ((e = cudaEventRecord(L->done, L->s)) != cudaSuccess) return set_err(FMN_ERR_CUDA, "cudaEventRecord", e);
         L->done_valid = true;
     }
-    if ((e = cudaMemcpyAsync(out, io + oo, out_len * 8, cudaMemcpyDeviceToHost, L->s)) != cudaSuccess)
-        return set_err(FMN_ERR_CUDA, "copying the product to the host", e);
+    if ((rc = stage_out(L, (char*)out, io + oo, out_len * 8))) return rc;
     return take_device_error(L->ws, L->h_err, L->s);
 }
 

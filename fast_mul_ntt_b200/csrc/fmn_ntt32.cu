@@ -756,9 +756,12 @@ __device__ __forceinline__ u128 qcoef(const QCrtArgs& a, u64 k, const PrimeQ& q0
     return qgarner(qscaled(a, src, k, 0, q0), qscaled(a, src, k, 1, q1), qscaled(a, src, k, 2, q2), a, q1, q2);
 }
 
-// WRAP: the product is wrapped (see QCrtArgs); its kernel holds more registers per thread.
-template <bool WRAP, long LIMIT = SPIN_LIMIT>
+// MODE 0: a plain product; 1: wrapped with a low product (see QCrtArgs), whose threads may
+// read two sources at once and so hold more registers; 2: twisted, whose threads read one
+// source each (the cyclic residues below N, W above).
+template <int MODE, long LIMIT = SPIN_LIMIT>
 __device__ __forceinline__ void qcrt_carry_body(const QCrtArgs& a, u32 ncta) {
+    constexpr bool WRAP = MODE != 0;
     __shared__ u64 s_hw[CNT / 32];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const PrimeQ q0 = c_q[0], q1 = c_q[1], q2 = c_q[2];
@@ -774,9 +777,9 @@ __device__ __forceinline__ void qcrt_carry_body(const QCrtArgs& a, u32 ncta) {
     const int src = WRAP ? qsource(a, k0) : 0;
     const bool full = k0 + 2 * QCE <= a.nvalid && (src != 1 || k0 + 2 * QCE <= a.wrap);
     const u64 kb = src == 2 ? k0 - a.N : k0;
-    // VW coefficients (VW / 2 limbs) at a time: four for plain products, two for wrapped ones,
-    // whose two sources would otherwise hold too many registers for 4 CTAs per SM
-    constexpr int VW = WRAP ? 2 : 4;
+    // VW coefficients (VW / 2 limbs) at a time: four, or two for wrapped products with a low
+    // product, whose two sources would otherwise hold too many registers for 4 CTAs per SM
+    constexpr int VW = MODE == 1 ? 2 : 4;
 #pragma unroll
     for (int e2 = 0; e2 < QCE; e2 += VW / 2) {
         u32 y0[VW], y1[VW], y2[VW];                    // c_k mod q_i
@@ -802,7 +805,7 @@ __device__ __forceinline__ void qcrt_carry_body(const QCrtArgs& a, u32 ncta) {
                     y1[t] = qmont(y1[t], a.cst[1], q1);
                     y2[t] = qmont(y2[t], a.cst[2], q2);
                 }
-                if (src != 0) {                                  // res - low
+                if (MODE == 1 && src != 0) {                     // res - low
                     u32 l0[VW], l1[VW], l2[VW];
                     ldv<VW>(a.low + k, l0);
                     ldv<VW>(a.low + a.low_N + k, l1);
@@ -855,15 +858,17 @@ __device__ __forceinline__ void qcrt_carry_body(const QCrtArgs& a, u32 ncta) {
 }
 
 __global__ void __launch_bounds__(CNT, QCE <= 8 ? 4 : 3) k_qcrt_carry(QCrtArgs a) {
-    qcrt_carry_body<false>(a, 0xffffffffu);
+    qcrt_carry_body<0>(a, 0xffffffffu);
 }
-// Wrapped products (two residue sources, two sets of scale constants).
-__global__ void __launch_bounds__(CNT, 4) k_qcrt_carry_wrap(QCrtArgs a) { qcrt_carry_body<true>(a, 0xffffffffu); }
+// Wrapped products with a low product (two residue sources, two sets of scale constants).
+__global__ void __launch_bounds__(CNT, 4) k_qcrt_carry_wrap(QCrtArgs a) { qcrt_carry_body<1>(a, 0xffffffffu); }
+// Twisted wrapped products (a CTA tile lies wholly below or above N: one source per tile).
+__global__ void __launch_bounds__(CNT, 4) k_qcrt_carry_twist(QCrtArgs a) { qcrt_carry_body<2>(a, 0xffffffffu); }
 
 // The plain kernel with a look-back limit of 2^12 polls (milliseconds instead of seconds), for
 // the test that withholds a tile and checks that the wait expires into the status word.
 __global__ void __launch_bounds__(CNT, 4) k_qcrt_carry_short_wait(QCrtArgs a) {
-    qcrt_carry_body<false, (1l << 12)>(a, 0xffffffffu);
+    qcrt_carry_body<0, (1l << 12)>(a, 0xffffffffu);
 }
 
 // CRT + carry of many products: CTAs take per-product tickets; tickets beyond a product's
@@ -871,7 +876,7 @@ __global__ void __launch_bounds__(CNT, 4) k_qcrt_carry_short_wait(QCrtArgs a) {
 __global__ void __launch_bounds__(CNT) k_qcrt_carry_batch(const QCrtArgs* __restrict__ args, u32 ctas_per_job,
                                                           const u32* __restrict__ ncta) {
     const u32 job = blockIdx.x / ctas_per_job;
-    qcrt_carry_body<false>(args[job], ncta[job]);
+    qcrt_carry_body<0>(args[job], ncta[job]);
 }
 
 // ------------------------------------------------------------------ twisted products
@@ -1471,14 +1476,15 @@ struct Launcher {
     cudaStream_t s;
     NeedLimbs need_b;
     void* need_ctx;
-    u64 N;
 
     cudaError_t need(u64 first, u64 end) { return need_b ? need_b(need_ctx, first, end, s) : cudaSuccess; }
     cudaError_t operator()(int variant, int logl, const QArgs& a, u64 tiles) {
         QKernel k = ktab().k[variant][logl];
         if (!k) return cudaErrorInvalidValue;
         cudaError_t e;
-        const double vec = 3.0 * (double)N * 4.0, bfly = 3.0 * ((double)N / 2.0) * logl;
+        // work of this launch's own transform (a.N: the twisted or low sub-product of a wrapped
+        // product is shorter than the product's main transform)
+        const double Nl = (double)a.N, vec = 3.0 * Nl * 4.0, bfly = 3.0 * (Nl / 2.0) * logl;
         const bool entry = (variant == V_FWD_E || variant == V_LAST_E || variant == V_FUSED_E || variant == V_SQR_E);
         double bytes = entry ? (double)a.len * 8.0 + vec : 2.0 * vec, mm = bfly + (entry ? 6.0 * (double)a.len : 0.0);
         int kind = K_FUSED;
@@ -1487,10 +1493,10 @@ struct Launcher {
         else if (variant == V_INV || variant == V_INV_ACC) kind = K_INV;
         if (variant == V_FUSED2) {
             bytes += vec;
-            mm = 3.0 * bfly + 3.0 * (double)N;
+            mm = 3.0 * bfly + 3.0 * Nl;
         } else if (kind == K_FUSED) {
             if (variant == V_FUSED || variant == V_FUSED_E) bytes += vec;
-            mm = 2.0 * bfly + 3.0 * (double)N + (entry ? 6.0 * (double)a.len : 0.0);
+            mm = 2.0 * bfly + 3.0 * Nl + (entry ? 6.0 * (double)a.len : 0.0);
         }
         const ProfMark m = prof_begin(kind, bytes, mm, s);
         k<<<(unsigned)(tiles * 3), NT, pass_smem(logl, variant), s>>>(a);
@@ -1817,7 +1823,7 @@ cudaError_t q32_spectrum_enqueue(const u64* src, u64 len, int log_n, void* spec,
     const int P = pl.passes;
     const u64 N = 1ull << log_n;
     const Job j{};
-    Launcher launch{j, s, nullptr, nullptr, N};
+    Launcher launch{j, s, nullptr, nullptr};
     QArgs pa;
     memset(&pa, 0, sizeof(pa));
     pa.N = N;
@@ -2058,7 +2064,8 @@ static cudaError_t crt_launch(const QCrtArgs& ca, u64 ncta, u64 t0, u64 t1, cuda
     const u64 n = t1 - t0;
     const double crt_bytes = 3.0 * (double)ca.nvalid * 4.0 + (double)ca.out_len * 8.0;
     const ProfMark m = prof_begin(K_CRT, crt_bytes * (double)n / (double)ncta, 3.0 * (double)ca.nvalid * (double)n / (double)ncta, s);
-    if (ca.wrap) k_qcrt_carry_wrap<<<(unsigned)n, CNT, 0, s>>>(ca);
+    if (ca.wrap && ca.twisted) k_qcrt_carry_twist<<<(unsigned)n, CNT, 0, s>>>(ca);
+    else if (ca.wrap) k_qcrt_carry_wrap<<<(unsigned)n, CNT, 0, s>>>(ca);
     else k_qcrt_carry<<<(unsigned)n, CNT, 0, s>>>(ca);
     cudaError_t e = cudaGetLastError();
     prof_end(m, s);
@@ -2131,7 +2138,7 @@ cudaError_t q32_enqueue(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s,
     const u64 nblk_last = N >> lastl;
     const u64 tiles_last = (nblk_last + TC - 1) / TC;
     const int ncols_last = nblk_last < (u64)TC ? (int)nblk_last : TC;
-    Launcher launch{j, s, need_b, need_ctx, N};
+    Launcher launch{j, s, need_b, need_ctx};
     TwPass tws[MAX_PASSES];
     for (int p = 0; p + 1 < P; ++p) tws[p] = tw_tables(logB[p], pl.bits[p], s);
 

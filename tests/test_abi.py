@@ -61,3 +61,46 @@ def test_too_large_is_rejected_before_any_device_call():
     rc = lib.fmn_mul_device(ctypes.c_void_p(16), 1 << 30, ctypes.c_void_p(32), 1 << 30, ctypes.c_void_p(64), None)
     assert rc == 5       # FMN_ERR_TOO_LARGE
     assert b"2^30" in lib.fmn_last_error()
+
+
+class _FakeDeviceLimbs:
+    """Stands in for a CUDA tensor of int64 limbs (only what the wrapper's checks read)."""
+
+    def __init__(self, n, cuda=True, contiguous=True, dtype=None):
+        import torch
+        self.n, self.is_cuda, self.contig = n, cuda, contiguous
+        self.dtype = dtype or torch.int64
+
+    def numel(self):
+        return self.n
+
+    def element_size(self):
+        return self.dtype.itemsize
+
+    def is_contiguous(self):
+        return self.contig
+
+
+def test_device_wrappers_check_buffers_before_any_launch():
+    """The C ABI takes plain pointers and sizes, so the Python wrappers check every device
+    tensor first: a short output (which the kernels would write past) and non-CUDA or
+    strided tensors raise ValueError before the library is called."""
+    import pytest
+    import torch
+    a, b = _FakeDeviceLimbs(600), _FakeDeviceLimbs(500)
+    with pytest.raises(ValueError, match="needs 1100"):
+        fmn.mul_device(a, b, _FakeDeviceLimbs(1099))
+    with pytest.raises(ValueError, match="needs 1200"):
+        fmn.sqr_device(a, _FakeDeviceLimbs(1100))
+    with pytest.raises(ValueError, match="needs 1100"):
+        fmn.mul_batch_device([(a, b, _FakeDeviceLimbs(1000))])
+    with pytest.raises(ValueError, match="needs 1200"):
+        fmn.mul_batch_device([(a, a, _FakeDeviceLimbs(1100))])
+    with pytest.raises(ValueError, match="CUDA"):
+        fmn.mul_device(torch.zeros(4, dtype=torch.int64), b, _FakeDeviceLimbs(504))
+    with pytest.raises(ValueError, match="contiguous"):
+        fmn.sqr_device(_FakeDeviceLimbs(4, contiguous=False), _FakeDeviceLimbs(8))
+    with pytest.raises(ValueError, match="64-bit"):
+        fmn.mul_device(_FakeDeviceLimbs(4, dtype=torch.int32), b, _FakeDeviceLimbs(504))
+    with pytest.raises(ValueError, match="64-bit"):
+        fmn.mul_device(_FakeDeviceLimbs(4, dtype=torch.float64), b, _FakeDeviceLimbs(504))

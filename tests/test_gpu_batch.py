@@ -78,6 +78,15 @@ def test_batch_equals_per_call_on_the_mixed_size_stream(fmn, engine):
     fmn.sync()
     for (_, _, out), r in zip(jobs, ref):
         assert torch.equal(out, r)
+    # the same jobs checked and marshalled once, launched twice
+    prepared = fmn.BatchJobs(jobs)
+    for _ in range(2):
+        for _, _, out in jobs:
+            out.fill_(-1)
+        fmn.mul_batch_device(prepared)
+        fmn.sync()
+        for (_, _, out), r in zip(jobs, ref):
+            assert torch.equal(out, r)
 
 
 def test_batch_graph_recomputes_updated_inputs(fmn, oracle):

@@ -124,6 +124,48 @@ def test_pinned_host_buffers(fmn, oracle, engine):
         assert np.array_equal(hs, oracle.sqr(a)), la
 
 
+def test_pageable_staging_many_chunks(fmn, oracle, engine):
+    """Pageable buffers go through the lane's 4 x 8 MiB pinned slots: operands and product
+    several times larger than all slots together (slot reuse in both directions), the output
+    aliasing the first operand, and a square, equal to the device path's product."""
+    import torch
+    lib = fmn.load_library()
+    P = ctypes.POINTER(ctypes.c_uint64)
+    la, lb = 3_000_003, 2_500_001           # 24 + 20 MB in, 44 MB out: 3 + 3 and 6 chunks
+    a, b = synth.operands("uniform", la, lb, 41)
+    da = torch.from_numpy(a.view(np.int64)).cuda()
+    db = torch.from_numpy(b.view(np.int64)).cuda()
+    dout = torch.empty(la + lb, dtype=torch.int64, device="cuda")
+    fmn.mul_device(da, db, dout)
+    fmn.sync()
+    want = dout.cpu().numpy().view(np.uint64)
+    assert residue_check(oracle, a, b, want)
+    got = fmn.abs_mul64(a, b)
+    assert np.array_equal(got, want)
+    buf = np.zeros(la + lb, np.uint64)
+    buf[:la] = a
+    p = buf.ctypes.data_as(P)
+    lib.abs_mul64(p, la, b.ctypes.data_as(P), lb, p)     # void, aborts on failure
+    assert np.array_equal(buf, want)
+    dsq = torch.empty(2 * la, dtype=torch.int64, device="cuda")
+    fmn.sqr_device(da, dsq)
+    fmn.sync()
+    assert np.array_equal(fmn.abs_sqr64(a), dsq.cpu().numpy().view(np.uint64))
+
+
+def test_pageable_staging_threads(fmn, oracle):
+    """Several host threads on pageable buffers at once: each takes its own lane and its
+    own staging slots."""
+    from concurrent.futures import ThreadPoolExecutor
+    shapes = [(1_200_000 + 7 * i, 900_000 + 3 * i) for i in range(6)]
+    ops = [synth.operands("uniform", la, lb, 50 + i) for i, (la, lb) in enumerate(shapes)]
+    with ThreadPoolExecutor(4) as ex:
+        outs = list(ex.map(lambda ab: fmn.abs_mul64(*ab), ops))
+    for (a, b), out in zip(ops, outs):
+        assert residue_check(oracle, a, b, out)
+    assert np.array_equal(outs[0], fmn.abs_mul64(*ops[0]))
+
+
 def test_device_api_and_caller_workspace(fmn, oracle, engine):
     import torch
     a, b = synth.operands("uniform", 70000, 50000, 21)
