@@ -893,47 +893,43 @@ __global__ void __launch_bounds__(CNT) k_qcrt_carry_batch(const QCrtArgs* __rest
 // The operand folded modulo X^M - c and twisted, as residues: entry g (< M) of prime i is
 // gamma^g sum_{j < 2^fold_log} c^j a_{g + jM} mod q_i (a the operand's 32-bit digits, zero past
 // its end), written to T + i M + g.  One thread per g: the fold's digits are loaded once for
-// all three primes, each load coalesced across the warp.
+// all three primes, each load coalesced across the warp; c^j multiplies as a Shoup constant
+// (host-computed), gamma^g as a Montgomery factor stepped along the grid-stride loop.
+// Indices are 32-bit: a twisted product has N <= 2^25 digits and both operands fit N.
 struct QFoldArgs {
     const u64* src;
     u64 len;            // limbs (2 len digits)
     u32* T;
     int logM, fold_log, tw_log;
+    uint2 cpow[3][kMaxFolds];   // c^j mod q_i, plain, with Shoup companion floor(c^j 2^32 / q_i)
 };
 __global__ void __launch_bounds__(256) k_qtwist_fold(QFoldArgs f) {
-    __shared__ u32 cp[3][kMaxFolds];
-    const int F = 1 << f.fold_log;
-    if ((int)threadIdx.x < 3 * F) {
-        const int pi = threadIdx.x / F, j = threadIdx.x % F;
-        cp[pi][j] = qroot(((u32)j << (f.logM + f.tw_log)) & MASK_N, pi, c_q[pi]);   // c^j, Montgomery form
-    }
-    __syncthreads();
     const u32* __restrict__ dig = reinterpret_cast<const u32*>(f.src);
-    const u64 nd = 2 * f.len, M = 1ull << f.logM;
-    const u64 g0 = (u64)blockIdx.x * blockDim.x + threadIdx.x, S = (u64)gridDim.x * blockDim.x;
+    const u32 nd = (u32)(2 * f.len), M = 1u << f.logM;
+    const int F = 1 << f.fold_log;
+    const u32 g0 = blockIdx.x * blockDim.x + threadIdx.x, S = gridDim.x * blockDim.x;
     // gamma^g in Montgomery form, stepped by gamma^S along the grid-stride loop
     u32 gm[3], gs[3];
 #pragma unroll
     for (int pi = 0; pi < 3; ++pi) {
-        gm[pi] = qroot(((u32)g0 << f.tw_log) & MASK_N, pi, c_q[pi]);
-        gs[pi] = qroot(((u32)S << f.tw_log) & MASK_N, pi, c_q[pi]);
+        gm[pi] = qroot((g0 << f.tw_log) & MASK_N, pi, c_q[pi]);
+        gs[pi] = qroot((S << f.tw_log) & MASK_N, pi, c_q[pi]);
     }
-    for (u64 g = g0; g < M; g += S) {
+    for (u32 g = g0; g < M; g += S) {
+        // folds holding digits at g: a_{g + jM} for j < nf (all zero past the operand)
+        const u32 left = nd > g ? (nd - g + M - 1) >> f.logM : 0u;
+        const int nf = left < (u32)F ? (int)left : F;
         u32 x[kMaxFolds];
 #pragma unroll
-        for (int j = 0; j < kMaxFolds; ++j) {
-            const u64 i = g + ((u64)j << f.logM);
-            x[j] = (j < F && i < nd) ? __ldg(dig + i) : 0u;
-        }
-        const u64 top = nd > g ? (nd - g + M - 1) >> f.logM : 0;   // folds holding digits at g
+        for (int j = 0; j < kMaxFolds; ++j) x[j] = j < nf ? __ldg(dig + g + ((u32)j << f.logM)) : 0u;
 #pragma unroll
         for (int pi = 0; pi < 3; ++pi) {
             const PrimeQ q = c_q[pi];
-            u32 acc = 0;
+            u32 acc = qsmul(x[0], f.cpow[pi][0].x, f.cpow[pi][0].y, q);
 #pragma unroll
-            for (int j = 0; j < kMaxFolds; ++j)
-                if (j < F && (u64)j < top) acc = qadd(acc, qmont(x[j], cp[pi][j], q), q);
-            f.T[(u64)pi * M + g] = qmont(acc, gm[pi], q);
+            for (int j = 1; j < kMaxFolds; ++j)
+                if (j < nf) acc = qadd(acc, qsmul(x[j], f.cpow[pi][j].x, f.cpow[pi][j].y, q), q);
+            f.T[pi * M + g] = qmont(acc, gm[pi], q);
             gm[pi] = qmont(gm[pi], gs[pi], q);
         }
     }
@@ -942,38 +938,36 @@ __global__ void __launch_bounds__(256) k_qtwist_fold(QFoldArgs f) {
 struct QTwistArgs {
     u32* U;             // cyclic product's residues (prime i at U + i N), raw; c_k below K on return
     u32* V;             // twisted product's residues (prime i at V + i M), raw; W on return
-    u64 N, K;
+    u32 N, K;
     int logM, fold_log, tw_log;
-    u32 cstN[3], cstM[3];
-    u32 nmod[3];        // N mod q_i: qmont(c, N) is c in U's raw form
+    u32 cstM[3];        // M^-1 2^64 mod q_i: with gamma^-k in Montgomery form, V raw -> V untwisted
+    uint2 ucj[3][kMaxFolds];   // c^j N^-1 2^32 mod q_i (Shoup pairs): U raw -> c^j U
+    uint2 nraw[3];      // N 2^-32 mod q_i (Shoup pair): a coefficient -> U's raw form
 };
 __global__ void __launch_bounds__(256) k_qtwist_w(QTwistArgs t) {
     const int pi = blockIdx.y;
     const PrimeQ q = c_q[pi];
-    __shared__ u32 cp[kMaxFolds];
-    if ((int)threadIdx.x < (1 << t.fold_log)) cp[threadIdx.x] = qroot(((u32)threadIdx.x << (t.logM + t.tw_log)) & MASK_N, pi, q);
-    __syncthreads();
-    u32* __restrict__ U = t.U + (u64)pi * t.N;
-    u32* __restrict__ V = t.V + ((u64)pi << t.logM);
-    const u64 k0 = (u64)blockIdx.x * blockDim.x + threadIdx.x, S = (u64)gridDim.x * blockDim.x;
-    // gamma^-k in Montgomery form, stepped by gamma^-S along the grid-stride loop
-    u32 gm = qroot((0u - ((u32)k0 << t.tw_log)) & MASK_N, pi, q);
-    const u32 gs = qroot((0u - ((u32)S << t.tw_log)) & MASK_N, pi, q);
-    for (u64 k = k0; k < t.K; k += S) {
+    const int F = 1 << t.fold_log;
+    u32* __restrict__ U = t.U + pi * t.N;
+    u32* __restrict__ V = t.V + (pi << t.logM);
+    const u32 k0 = blockIdx.x * blockDim.x + threadIdx.x, S = gridDim.x * blockDim.x;
+    // gamma^-k M^-1 2^32 (the Montgomery form of gamma^-k times cstM 2^-32), stepped by gamma^-S
+    u32 gm = qmont(qroot((0u - (k0 << t.tw_log)) & MASK_N, pi, q), t.cstM[pi], q);
+    const u32 gs = qroot((0u - (S << t.tw_log)) & MASK_N, pi, q);
+    for (u32 k = k0; k < t.K; k += S) {
         u32 x[kMaxFolds];
 #pragma unroll
-        for (int j = 0; j < kMaxFolds; ++j) x[j] = j < (1 << t.fold_log) ? U[k + ((u64)j << t.logM)] : 0u;
+        for (int j = 0; j < kMaxFolds; ++j) x[j] = j < F ? U[k + ((u32)j << t.logM)] : 0u;
         const u32 vr = V[k];
-        u32 ub = 0;
+        const u32 u0 = qsmul(x[0], t.ucj[pi][0].x, t.ucj[pi][0].y, q);    // U_k
+        u32 ub = u0;
 #pragma unroll
-        for (int j = 0; j < kMaxFolds; ++j)
-            if (j < (1 << t.fold_log)) ub = qadd(ub, qmont(x[j], cp[j], q), q);
-        ub = qmont(ub, t.cstN[pi], q);
-        const u32 v = qmont(qmont(vr, t.cstM[pi], q), gm, q);   // V_k, untwisted
-        const u32 d = qsub(ub, v, q);
+        for (int j = 1; j < kMaxFolds; ++j)
+            if (j < F) ub = qadd(ub, qsmul(x[j], t.ucj[pi][j].x, t.ucj[pi][j].y, q), q);
+        const u32 d = qsub(ub, qmont(vr, gm, q), q);                      // U mod (X^M - c) - V
         const u32 w = (d + ((d & 1u) ? q.p : 0u)) >> 1;
         V[k] = w;
-        U[k] = qmont(qsub(qmont(x[0], t.cstN[pi], q), w, q), t.nmod[pi], q);   // c_k = U_k - W_k
+        U[k] = qsmul(qsub(u0, w, q), t.nraw[pi].x, t.nraw[pi].y, q);     // c_k = U_k - W_k, raw
         gm = qmont(gm, gs, q);
     }
 }
@@ -1017,6 +1011,7 @@ static u64 primitive_root(u64 p) {
 struct HostTables {
     std::vector<u32> rt;   // [2][3][RT_SIZE][2]: (w, floor(w 2^32 / q)) Shoup pairs
     std::vector<u32> tw;   // [2][3][1 << QTWB]: Montgomery form
+    u64 w26[3];            // the root of order 2^26 of each prime that all tables use
 };
 
 static const HostTables& host_tables() {
@@ -1028,6 +1023,7 @@ static const HostTables& host_tables() {
         for (int i = 0; i < 3; ++i) {
             const u64 p = kQ[i];
             const u64 w = h_pow(primitive_root(p), (p - 1) >> Q32_MAX_LOG_N, p);   // order 2^26
+            T.w26[i] = w;
             std::vector<u64> lo(1u << QTWB), hi(1u << QTWB);
             const u64 whi = h_pow(w, 1ull << QTWB, p);
             u64 cl = 1, ch = 1;
@@ -1157,6 +1153,11 @@ static size_t pass_smem(int logl, int variant) {
     if ((variant == V_FUSED || variant == V_FUSED_E) && logl >= 5 && logl <= 8) w += TC * (L + 4);
     return w * sizeof(u32);
 }
+
+// w^e mod q_i (plain form) for the tables' root w of order 2^26, e taken mod 2^26.
+static u64 h_root(int i, u64 e) { return h_pow(host_tables().w26[i], e & MASK_N, kQ[i]); }
+// (w, floor(w 2^32 / q_i)): w as a Shoup constant.
+static uint2 h_shoup(u64 w, int i) { return make_uint2((u32)w, (u32)((w << 32) / kQ[i])); }
 
 static cudaError_t ensure_tables() {
     int dev = 0;
@@ -2184,8 +2185,17 @@ cudaError_t q32_enqueue(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s,
         u32* A = (u32*)(base + J.a);
         u32* B = sqr ? A : (u32*)(base + J.b);
         u64 b_ready = sqr ? j.lb : 0;                          // limbs of the second operand requested so far
+        QWhole W;
+        plan_whole(j, J.n, A, B, &W, false, tws);
+        int k_main = 0;                                        // main launches issued so far
         if (J.wrap && J.twist) {
-            // the product modulo X^M - c first (it reads both operands whole, folded)
+            // the main transform's passes over the first operand alone go first, so that a host
+            // caller's copy of the second operand overlaps them; then the product modulo
+            // X^M - c (it reads both operands whole, folded)
+            for (; k_main < W.count && (sqr || W.rec[k_main].a.src != j.b); ++k_main)
+                if ((e = launch(W.rec[k_main].variant, W.rec[k_main].logl, W.rec[k_main].a, W.rec[k_main].tiles)) !=
+                    cudaSuccess)
+                    return e;
             const int tw_log = Q32_MAX_LOG_N - 1 - J.n;        // gamma = w^(2^tw_log), of order 2N
             u32* TA = (u32*)(base + J.la_off);
             u32* TB = sqr ? TA : (u32*)(base + J.lb_off);
@@ -2203,6 +2213,9 @@ cudaError_t q32_enqueue(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s,
                 fa.logM = J.nl;
                 fa.fold_log = J.n - J.nl;
                 fa.tw_log = tw_log;
+                for (int i = 0; i < 3; ++i)                    // c^j = gamma^(jM)
+                    for (int jj = 0; jj < kMaxFolds; ++jj)
+                        fa.cpow[i][jj] = h_shoup(h_root(i, (u64)jj << (fa.logM + tw_log)), i);
                 const ProfMark m = prof_begin(K_WRAP, (double)fa.len * 8.0 + 3.0 * (double)J.NL * 4.0,
                                               3.0 * (double)J.NL * (2.0 + (double)(1 << fa.fold_log)), s);
                 k_qtwist_fold<<<(unsigned)fblocks, 256, 0, s>>>(fa);
@@ -2250,10 +2263,8 @@ cudaError_t q32_enqueue(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s,
             ca.wrap = J.wrap;
             for (int i = 0; i < 3; ++i) ca.low_cst[i] = cl.cst[i];
         }
-        QWhole W;
-        plan_whole(j, J.n, A, B, &W, false, tws);
         bool have_b = sqr != 0;
-        for (int k = 0; k < W.count; ++k) {
+        for (int k = k_main; k < W.count; ++k) {
             if (!have_b && W.rec[k].a.src == j.b) {            // the second operand's first reader
                 if (b_ready < j.lb && (e = launch.need(b_ready, j.lb)) != cudaSuccess) return e;
                 have_b = true;
@@ -2267,8 +2278,8 @@ cudaError_t q32_enqueue(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s,
             memset(&ta, 0, sizeof(ta));
             ta.U = A;
             ta.V = (u32*)(base + J.la_off);
-            ta.N = N;
-            ta.K = J.wrap;
+            ta.N = (u32)N;
+            ta.K = (u32)J.wrap;
             ta.logM = J.nl;
             ta.fold_log = J.n - J.nl;
             ta.tw_log = Q32_MAX_LOG_N - 1 - J.n;
@@ -2276,9 +2287,12 @@ cudaError_t q32_enqueue(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s,
             memset(&cm, 0, sizeof(cm));
             crt_constants(J.NL, &cm);
             for (int i = 0; i < 3; ++i) {
-                ta.cstN[i] = ca.cst[i];
+                const u64 p = kQ[i];
+                const u64 r32 = h_pow(2, 32, p), ninv = h_pow(N % p, p - 2, p);
                 ta.cstM[i] = cm.cst[i];
-                ta.nmod[i] = (u32)(N % kQ[i]);
+                for (int jj = 0; jj < kMaxFolds; ++jj)   // c^j N^-1 2^32
+                    ta.ucj[i][jj] = h_shoup(h_mulmod(h_mulmod(h_root(i, (u64)jj << (ta.logM + ta.tw_log)), ninv, p), r32, p), i);
+                ta.nraw[i] = h_shoup(h_mulmod(N % p, h_pow(r32, p - 2, p), p), i);   // N 2^-32
             }
             const u64 blocks = (J.wrap + 255) / 256 < 2048 ? (J.wrap + 255) / 256 : 2048;
             const ProfMark m = prof_begin(K_WRAP, 3.0 * (double)J.wrap * 4.0 * (2.0 + (double)(1 << ta.fold_log)),
