@@ -480,6 +480,7 @@ def serve_compare(fmn, torch, dev, n_requests, rates, seed=0, templates=256, res
                          "gpu_work_over_wall": gpu_work_s / wall,
                          "host_launch_ms_per_request": st["launch_ms"] / max(1, st["completed"]),
                          "host_alloc_ms_per_request": st["alloc_ms"] / max(1, st["completed"]),
+                         "host_launch_ms_max": st["max_launch_ms"], "host_alloc_ms_max": st["max_alloc_ms"],
                          "mismatches": st["mismatches"], "rejected": st["rejected"],
                          "device_errors": st["device_errors"],
                          "bit_exact": st["mismatches"] == 0 and st["device_errors"] == 0 and st["rejected"] == 0}

@@ -36,7 +36,7 @@ EXPORTS = ["abs_mul64", "abs_sqr64", "fmn_init", "fmn_shutdown", "fmn_last_error
            "fmn_set_engine", "fmn_get_engine", "fmn_engine_for", "fmn_pieces_for",
            "fmn_force_pieces", "fmn_bench_bfly32", "fmn_get_plan_engine", "fmn_set_plan_engine",
            "fmn_test_fail_allocs", "fmn_test_carry_timeout", "fmn_server_cancel", "fmn_server_pause",
-           "fmn_wrap_for", "fmn_twist_for", "fmn_force_wrap"]
+           "fmn_wrap_for", "fmn_twist_for", "fmn_batch_twist_for", "fmn_force_wrap"]
 
 ENGINE_AUTO, ENGINE_64, ENGINE_32 = 0, 1, 2
 
@@ -55,7 +55,8 @@ class FmnServerStats(ctypes.Structure):
     _fields_ = [("submitted", ctypes.c_uint64), ("completed", ctypes.c_uint64), ("rejected", ctypes.c_uint64),
                 ("failed", ctypes.c_uint64), ("batches", ctypes.c_uint64), ("mismatches", ctypes.c_uint64),
                 ("device_errors", ctypes.c_uint64), ("peak_bytes", ctypes.c_size_t), ("cancelled", ctypes.c_uint64),
-                ("launch_ms", ctypes.c_double), ("alloc_ms", ctypes.c_double)]
+                ("launch_ms", ctypes.c_double), ("alloc_ms", ctypes.c_double),
+                ("max_launch_ms", ctypes.c_double), ("max_alloc_ms", ctypes.c_double)]
 
 
 class FmnJob(ctypes.Structure):
@@ -132,6 +133,8 @@ def load_library(path=None):
     lib.fmn_wrap_for.restype = _u64
     lib.fmn_twist_for.argtypes = [_u64, _u64, ctypes.c_int]
     lib.fmn_twist_for.restype = _u64
+    lib.fmn_batch_twist_for.argtypes = [_u64, _u64, ctypes.c_int]
+    lib.fmn_batch_twist_for.restype = _u64
     lib.fmn_force_wrap.argtypes = [ctypes.c_int]
     lib.fmn_force_wrap.restype = ctypes.c_int
     lib.fmn_test_fail_allocs.argtypes = [ctypes.c_int]
@@ -581,6 +584,11 @@ def wrap_for(len1, len2, sqr=False):
 def twist_for(len1, len2, sqr=False):
     """Twisted length M of a wrapped product computed modulo X^M - c (0: not twisted)."""
     return int(load_library().fmn_twist_for(len1, len2, 1 if sqr else 0))
+
+
+def batch_twist_for(len1, len2, sqr=False):
+    """Twisted length M of a product run twisted inside a batch (0: whole)."""
+    return int(load_library().fmn_batch_twist_for(len1, len2, 1 if sqr else 0))
 
 
 def force_wrap(mode=1):

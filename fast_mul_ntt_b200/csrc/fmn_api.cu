@@ -874,6 +874,16 @@ u64 fmn_twist_for(u64 len1, u64 len2, int sqr) {
     return fmn::job_engine(j) == fmn::ENGINE_32 ? fmn::q32_twisted(len1, len2, sqr ? 1 : 0) : 0;
 }
 
+u64 fmn_batch_twist_for(u64 len1, u64 len2, int sqr) {
+    fmn::Job j;
+    j.a = j.b = nullptr;
+    j.out = nullptr;
+    j.la = len1;
+    j.lb = len2;
+    j.sqr = sqr ? 1 : 0;
+    return fmn::batch_twist_for(j);
+}
+
 u64 fmn_wrap_for(u64 len1, u64 len2, int sqr) {
     fmn::Job j;
     j.a = j.b = nullptr;

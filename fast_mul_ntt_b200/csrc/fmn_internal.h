@@ -154,16 +154,23 @@ cudaError_t enqueue_job(const Job& job, void* ws, size_t ws_bytes, cudaStream_t 
 cudaError_t enqueue_job_overlapped(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s, const TwiddleSet* tw,
                                    NeedLimbs need_b, void* need_ctx, int crt_chunks, ChunkDone after_chunk, void* ctx);
 
-// ---- 32-bit engine batches (whole products; see enqueue_batch)
+// ---- 32-bit engine batches (whole and twisted wrapped products; see enqueue_batch)
+constexpr int Q32_MAX_REC = 2 * (3 * MAX_PASSES + 2);   // pass launches of a twisted product
 struct Q32Group {
-    int m, count;                           // products, launches per product
-    int variant[3 * MAX_PASSES + 2], logl[3 * MAX_PASSES + 2];
-    u64 tiles[3 * MAX_PASSES + 2];
-    size_t args_off[3 * MAX_PASSES + 2];    // descriptor offsets: m launch-argument records each
+    int m, count;                           // products, pass launches per product
+    int variant[Q32_MAX_REC], logl[Q32_MAX_REC];
+    u64 tiles[Q32_MAX_REC];
+    size_t args_off[Q32_MAX_REC];           // descriptor offsets: m launch-argument records each
     size_t crt_off, ncta_off;
     unsigned max_ncta;
+    // twisted wrapped products (twist = log2 M > 0): the operands' folds (nfold of them), the
+    // pass launches (twisted transform, then the cyclic one), the W kernel, the twisted CRT
+    int twist, nfold;
+    size_t fold_off[2], w_off;
+    unsigned fold_bpj, w_bpj;
 };
-int q32_batch_log_n(const Job& j);          // transform log length, < 0 if not a 32-bit batch product
+int q32_batch_log_n(const Job& j);          // (cyclic) transform log length, < 0 if not a 32-bit batch product
+int q32_batch_twist_log(const Job& j);      // log2 M of a batched product run twisted, 0 for a whole product
 size_t q32_batch_res_bytes(const Job& j);   // residue arrays of one product
 size_t q32_batch_state_bytes(const Job& j); // carry-scan ticket + state of one product
 size_t q32_batch_desc_bytes_per_job();      // descriptor bytes one product needs (upper bound)
@@ -177,6 +184,7 @@ cudaError_t q32_batch_launch(const Q32Group& g, const char* d_desc, cudaStream_t
 cudaError_t q32_prepare();                  // tables + kernel attributes on the current device
 
 // ---- batches of products
+u64 batch_twist_for(const Job& j);          // M of a batched product run twisted, 0 if whole
 // Workspace bytes for a batch (device) and host staging bytes for its launch descriptors.
 size_t batch_workspace_bytes(const Job* jobs, int count);
 size_t batch_stage_bytes(const Job* jobs, int count);

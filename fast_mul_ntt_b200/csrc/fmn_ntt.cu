@@ -1550,6 +1550,7 @@ static cudaError_t set_batch_attrs() {
 // the streams in `streams` (round robin), forked from and joined back into `s`.
 struct BatchGroup {
     int engine, n, kind;  // kind: 0 multiply, 1 square, 2 resident first operand
+    int twist;            // 32-bit engine: log2 M of twisted wrapped products, 0 for whole ones
     std::vector<int> idx;
 };
 static int job_kind(const Job& j) { return j.spectrum ? 2 : (j.sqr ? 1 : 0); }
@@ -1561,6 +1562,12 @@ static int batch_engine(const Job& j) {
     const int e = j.engine ? j.engine : default_engine();
     if (e == ENGINE_64) return ENGINE_64;
     return q32_batch_log_n(j) >= 0 ? ENGINE_32 : ENGINE_64;
+}
+
+u64 batch_twist_for(const Job& j) {
+    if (j.la == 0 || j.lb == 0 || batch_engine(j) != ENGINE_32) return 0;
+    const int m = q32_batch_twist_log(j);
+    return m ? 1ull << m : 0;
 }
 
 static void batch_sizes(const Job& j, size_t* res, size_t* st) {
@@ -1582,11 +1589,12 @@ static void batch_groups(const Job* jobs, int count, std::vector<BatchGroup>& gr
         const int eng = batch_engine(j);
         const int n = eng == ENGINE_32 ? q32_batch_log_n(j) : ws_layout(j.la, j.lb, j.sqr, j.spectrum ? j.log_n : 0).n;
         const int sq = job_kind(j);
+        const int tw = eng == ENGINE_32 ? q32_batch_twist_log(j) : 0;
         BatchGroup* g = nullptr;
         for (auto& x : groups)
-            if (x.engine == eng && x.n == n && x.kind == sq) g = &x;
+            if (x.engine == eng && x.n == n && x.kind == sq && x.twist == tw) g = &x;
         if (!g) {
-            groups.push_back(BatchGroup{eng, n, sq, {}});
+            groups.push_back(BatchGroup{eng, n, sq, tw, {}});
             g = &groups.back();
         }
         g->idx.push_back(i);

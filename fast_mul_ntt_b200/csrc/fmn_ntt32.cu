@@ -26,6 +26,7 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <algorithm>
 #include <atomic>
 #include <mutex>
 #include <vector>
@@ -878,6 +879,12 @@ __global__ void __launch_bounds__(CNT) k_qcrt_carry_batch(const QCrtArgs* __rest
     const u32 job = blockIdx.x / ctas_per_job;
     qcrt_carry_body<0>(args[job], ncta[job]);
 }
+// The same for twisted wrapped products.
+__global__ void __launch_bounds__(CNT, 4) k_qcrt_carry_twist_batch(const QCrtArgs* __restrict__ args, u32 ctas_per_job,
+                                                                   const u32* __restrict__ ncta) {
+    const u32 job = blockIdx.x / ctas_per_job;
+    qcrt_carry_body<2>(args[job], ncta[job]);
+}
 
 // ------------------------------------------------------------------ twisted products
 // A wrapped product computed as U = C mod (X^N - 1) (the cyclic transform of length N) and
@@ -903,11 +910,12 @@ struct QFoldArgs {
     int logM, fold_log, tw_log;
     uint2 cpow[3][kMaxFolds];   // c^j mod q_i, plain, with Shoup companion floor(c^j 2^32 / q_i)
 };
-__global__ void __launch_bounds__(256) k_qtwist_fold(QFoldArgs f) {
+// Blocks blk of nblk (256 threads each) cover one operand.
+__device__ __forceinline__ void qtwist_fold_body(const QFoldArgs& f, u32 blk, u32 nblk) {
     const u32* __restrict__ dig = reinterpret_cast<const u32*>(f.src);
     const u32 nd = (u32)(2 * f.len), M = 1u << f.logM;
     const int F = 1 << f.fold_log;
-    const u32 g0 = blockIdx.x * blockDim.x + threadIdx.x, S = gridDim.x * blockDim.x;
+    const u32 g0 = blk * blockDim.x + threadIdx.x, S = nblk * blockDim.x;
     // gamma^g in Montgomery form, stepped by gamma^S along the grid-stride loop
     u32 gm[3], gs[3];
 #pragma unroll
@@ -934,6 +942,11 @@ __global__ void __launch_bounds__(256) k_qtwist_fold(QFoldArgs f) {
         }
     }
 }
+__global__ void __launch_bounds__(256) k_qtwist_fold(QFoldArgs f) { qtwist_fold_body(f, blockIdx.x, gridDim.x); }
+// Batches: bpj consecutive blocks per product.
+__global__ void __launch_bounds__(256) k_qtwist_fold_batch(const QFoldArgs* __restrict__ args, u32 bpj) {
+    qtwist_fold_body(args[blockIdx.x / bpj], blockIdx.x % bpj, bpj);
+}
 
 struct QTwistArgs {
     u32* U;             // cyclic product's residues (prime i at U + i N), raw; c_k below K on return
@@ -944,13 +957,13 @@ struct QTwistArgs {
     uint2 ucj[3][kMaxFolds];   // c^j N^-1 2^32 mod q_i (Shoup pairs): U raw -> c^j U
     uint2 nraw[3];      // N 2^-32 mod q_i (Shoup pair): a coefficient -> U's raw form
 };
-__global__ void __launch_bounds__(256) k_qtwist_w(QTwistArgs t) {
-    const int pi = blockIdx.y;
+// Prime pi; blocks blk of nblk cover the wrapped coefficients.
+__device__ __forceinline__ void qtwist_w_body(const QTwistArgs& t, int pi, u32 blk, u32 nblk) {
     const PrimeQ q = c_q[pi];
     const int F = 1 << t.fold_log;
     u32* __restrict__ U = t.U + pi * t.N;
     u32* __restrict__ V = t.V + (pi << t.logM);
-    const u32 k0 = blockIdx.x * blockDim.x + threadIdx.x, S = gridDim.x * blockDim.x;
+    const u32 k0 = blk * blockDim.x + threadIdx.x, S = nblk * blockDim.x;
     // gamma^-k M^-1 2^32 (the Montgomery form of gamma^-k times cstM 2^-32), stepped by gamma^-S
     u32 gm = qmont(qroot((0u - (k0 << t.tw_log)) & MASK_N, pi, q), t.cstM[pi], q);
     const u32 gs = qroot((0u - (S << t.tw_log)) & MASK_N, pi, q);
@@ -970,6 +983,10 @@ __global__ void __launch_bounds__(256) k_qtwist_w(QTwistArgs t) {
         U[k] = qsmul(qsub(u0, w, q), t.nraw[pi].x, t.nraw[pi].y, q);     // c_k = U_k - W_k, raw
         gm = qmont(gm, gs, q);
     }
+}
+__global__ void __launch_bounds__(256) k_qtwist_w(QTwistArgs t) { qtwist_w_body(t, blockIdx.y, blockIdx.x, gridDim.x); }
+__global__ void __launch_bounds__(256) k_qtwist_w_batch(const QTwistArgs* __restrict__ args, u32 bpj) {
+    qtwist_w_body(args[blockIdx.x / bpj], blockIdx.y, blockIdx.x % bpj, bpj);
 }
 
 // ------------------------------------------------------------------ host: tables
@@ -1890,16 +1907,44 @@ int q32_pieces(u64 la, u64 lb, int sqr) {
     return J.ok ? J.m : 0;
 }
 
-// ---- batches: whole products grouped by transform length and kind share every launch
+// ---- batches: products grouped by transform length(s) and kind share every launch
+namespace q32 {
+// A batched product runs twisted (see plan_twist) when that plan, without the per-sequence
+// launch cost (a batch shares its launches among its products), models at least 15% cheaper
+// than the whole product: a twisted group adds its fold, W and CRT launches, so a negacyclic
+// plan (M = 2^n, about the whole product's cost) stays whole.  Returns the twisted plan
+// (T->ok) or leaves T->ok false.
+static void batch_twist_plan(const Job& j, QJob* T) {
+    memset(T, 0, sizeof(*T));
+    if (j.spectrum || j.la == 0 || j.lb == 0) return;
+    const int fw = g_force_wrap.load();
+    if (fw == 1) return;                                         // tests: the low-product form (none in batches)
+    const int sqr = j.sqr ? 1 : 0, nw = whole_log_n(j.la, j.lb);
+    if (nw < 0) return;
+    const double ct = plan_twist(j.la, j.lb, sqr, T);
+    const double cw = (sqr ? 2.0 : 3.0) * (double)(1ull << nw) * (nw + 1);
+    T->ok = ct >= 0.0 && (fw == 2 || ct - kPieceCost < 0.85 * cw);
+}
+}  // namespace q32
+
+int q32_batch_twist_log(const Job& j) {
+    q32::QJob T;
+    q32::batch_twist_plan(j, &T);
+    return T.ok ? T.nl : 0;
+}
+
 int q32_batch_log_n(const Job& j) {
     if (j.spectrum) return j.engine == ENGINE_32 && q32::plan_resident(j).ok ? j.log_n : -1;
-    return q32::whole_log_n(j.la, j.lb);
+    q32::QJob T;
+    q32::batch_twist_plan(j, &T);
+    return T.ok ? T.n : q32::whole_log_n(j.la, j.lb);
 }
 
 size_t q32_batch_res_bytes(const Job& j) {
     const int n = q32_batch_log_n(j);
     if (n < 0) return 0;
-    return q32::align256(3 * (1ull << n) * sizeof(u32)) * (j.sqr || j.spectrum ? 1 : 2);
+    const int ops = j.sqr || j.spectrum ? 1 : 2, m = q32_batch_twist_log(j);
+    return (q32::align256(3 * (1ull << n) * sizeof(u32)) + (m ? q32::align256(3 * (1ull << m) * sizeof(u32)) : 0)) * ops;
 }
 
 size_t q32_batch_state_bytes(const Job& j) {
@@ -1908,7 +1953,8 @@ size_t q32_batch_state_bytes(const Job& j) {
 }
 
 size_t q32_batch_desc_bytes_per_job() {
-    return (3 * MAX_PASSES + 2) * (sizeof(q32::QArgs) + 16) + sizeof(q32::QCrtArgs) + sizeof(u32) + 32;
+    return Q32_MAX_REC * (sizeof(q32::QArgs) + 16) + 2 * (sizeof(q32::QFoldArgs) + 16) + sizeof(q32::QTwistArgs) +
+           sizeof(q32::QCrtArgs) + sizeof(u32) + 64;
 }
 
 cudaError_t q32_prepare() { return q32::ensure_tables(); }
@@ -1922,31 +1968,92 @@ cudaError_t q32_batch_plan(const Job* jobs, const int* idx, int m, char* res, si
         *hoff = (*hoff + bytes + 15) & ~(size_t)15;
         return o;
     };
-    std::vector<QWhole> W(m);
+    std::vector<QWhole> W(m), WT(m);
     std::vector<QCrtArgs> C(m);
+    std::vector<QFoldArgs> FA(m), FB(m);
+    std::vector<QTwistArgs> TW(m);
     std::vector<u32> nc(m);
     u32 maxc = 0;
     const int n = q32_batch_log_n(jobs[idx[0]]);
+    const int tm = q32_batch_twist_log(jobs[idx[0]]);            // 0: whole products
     if (n < 0) return cudaErrorInvalidValue;
+    const u64 N = 1ull << n, M = tm ? 1ull << tm : 0;
+    const int tw_log = Q32_MAX_LOG_N - 1 - n, fold_log = tm ? n - tm : 0;
     QCrtArgs proto;
     memset(&proto, 0, sizeof(proto));
-    crt_constants(1ull << n, &proto);
+    crt_constants(N, &proto);
+    // twisted: the constants of the folds and of the W kernel are the same for the whole group
+    QFoldArgs fproto;
+    QTwistArgs tproto;
+    memset(&fproto, 0, sizeof(fproto));
+    memset(&tproto, 0, sizeof(tproto));
+    u64 kmax = 0;
+    if (tm) {
+        fproto.logM = tproto.logM = tm;
+        fproto.fold_log = tproto.fold_log = fold_log;
+        fproto.tw_log = tproto.tw_log = tw_log;
+        QCrtArgs cm;
+        memset(&cm, 0, sizeof(cm));
+        crt_constants(M, &cm);
+        for (int i = 0; i < 3; ++i) {
+            const u64 p = kQ[i];
+            const u64 r32 = h_pow(2, 32, p), ninv = h_pow(N % p, p - 2, p);
+            tproto.cstM[i] = cm.cst[i];
+            for (int jj = 0; jj < kMaxFolds; ++jj) {
+                const u64 c = h_root(i, (u64)jj << (tm + tw_log));
+                fproto.cpow[i][jj] = h_shoup(c, i);
+                tproto.ucj[i][jj] = h_shoup(h_mulmod(h_mulmod(c, ninv, p), r32, p), i);
+            }
+            tproto.nraw[i] = h_shoup(h_mulmod(N % p, h_pow(r32, p - 2, p), p), i);
+        }
+        tproto.N = (u32)N;
+    }
     for (int t = 0; t < m; ++t) {
         const Job& j = jobs[idx[t]];
-        if (q32_batch_log_n(j) != n) return cudaErrorInvalidValue;
-        const u64 N = 1ull << n, out_len = j.la + j.lb;
+        if (q32_batch_log_n(j) != n || q32_batch_twist_log(j) != tm) return cudaErrorInvalidValue;
+        const u64 out_len = j.la + j.lb;
+        const bool one = j.sqr || j.spectrum;
         u32* A = (u32*)(res + *roff);
         *roff += align256(3 * N * sizeof(u32));
         u32* B = A;
-        if (!j.sqr && !j.spectrum) {
+        if (!one) {
             B = (u32*)(res + *roff);
             *roff += align256(3 * N * sizeof(u32));
         }
         u32* ticket = (u32*)(st + *soff);
         *soff += q32_batch_state_bytes(j);
-        plan_whole(j, n, A, B, &W[t], true);
         QCrtArgs& ca = C[t];
         ca = proto;
+        if (tm) {
+            u32* TA = (u32*)(res + *roff);
+            *roff += align256(3 * M * sizeof(u32));
+            u32* TB = TA;
+            if (!one) {
+                TB = (u32*)(res + *roff);
+                *roff += align256(3 * M * sizeof(u32));
+            }
+            FA[t] = fproto;
+            FA[t].src = j.a;
+            FA[t].len = j.la;
+            FA[t].T = TA;
+            FB[t] = fproto;
+            FB[t].src = j.b;
+            FB[t].len = j.lb;
+            FB[t].T = TB;
+            plan_whole(j, tm, TA, TB, &WT[t], true, nullptr, true);
+            const u64 K = 2 * out_len - 1 - N;
+            TW[t] = tproto;
+            TW[t].U = A;
+            TW[t].V = TA;
+            TW[t].K = (u32)K;
+            if (K > kmax) kmax = K;
+            ca.low = TA;
+            ca.low_N = M;
+            ca.wrap = K;
+            ca.twisted = 1;
+            for (int i = 0; i < 3; ++i) ca.low_cst[i] = c_host_r1(i);
+        }
+        plan_whole(j, n, A, B, &W[t], true);
         ca.res = A;
         ca.N = N;
         ca.nvalid = 2 * out_len - 1;
@@ -1957,19 +2064,37 @@ cudaError_t q32_batch_plan(const Job* jobs, const int* idx, int m, char* res, si
         ca.err = err;
         nc[t] = (u32)((out_len + QCTILE - 1) / QCTILE);
         if (nc[t] > maxc) maxc = nc[t];
-        if (W[t].count != W[0].count) return cudaErrorInvalidValue;
+        if (W[t].count != W[0].count || (tm && WT[t].count != WT[0].count)) return cudaErrorInvalidValue;
     }
+    const bool sq = jobs[idx[0]].sqr || jobs[idx[0]].spectrum;
     g->m = m;
-    g->count = W[0].count;
+    g->twist = tm;
+    g->nfold = tm ? (sq ? 1 : 2) : 0;
+    g->count = (tm ? WT[0].count : 0) + W[0].count;
+    if (g->count > Q32_MAX_REC) return cudaErrorInvalidValue;
     g->max_ncta = maxc;
     for (int k = 0; k < g->count; ++k) {
-        g->variant[k] = W[0].rec[k].variant;
-        g->logl[k] = W[0].rec[k].logl;
-        g->tiles[k] = W[0].rec[k].tiles;
+        const bool tk = tm && k < WT[0].count;                  // a launch of the twisted transform
+        const QWhole* src = tk ? WT.data() : W.data();
+        const int kk = tk ? k : k - (tm ? WT[0].count : 0);
+        g->variant[k] = src[0].rec[kk].variant;
+        g->logl[k] = src[0].rec[kk].logl;
+        g->tiles[k] = src[0].rec[kk].tiles;
         g->args_off[k] = reserve((size_t)m * sizeof(QArgs));
         if (*hoff > hcap) return cudaErrorInvalidValue;
         QArgs* d = (QArgs*)(h + g->args_off[k]);
-        for (int t = 0; t < m; ++t) d[t] = W[t].rec[k].a;
+        for (int t = 0; t < m; ++t) d[t] = src[t].rec[kk].a;
+    }
+    if (tm) {
+        g->fold_bpj = (unsigned)std::min<u64>((M + 255) / 256, 128);
+        g->w_bpj = (unsigned)std::min<u64>((kmax + 255) / 256, 128);
+        g->fold_off[0] = reserve((size_t)m * sizeof(QFoldArgs));
+        g->fold_off[1] = reserve((size_t)m * sizeof(QFoldArgs));
+        g->w_off = reserve((size_t)m * sizeof(QTwistArgs));
+        if (*hoff > hcap) return cudaErrorInvalidValue;
+        memcpy(h + g->fold_off[0], FA.data(), (size_t)m * sizeof(QFoldArgs));
+        memcpy(h + g->fold_off[1], FB.data(), (size_t)m * sizeof(QFoldArgs));
+        memcpy(h + g->w_off, TW.data(), (size_t)m * sizeof(QTwistArgs));
     }
     g->crt_off = reserve((size_t)m * sizeof(QCrtArgs));
     g->ncta_off = reserve((size_t)m * sizeof(u32));
@@ -1983,6 +2108,11 @@ cudaError_t q32_batch_launch(const Q32Group& g, const char* d_desc, cudaStream_t
     using namespace q32;
     const BatchKernelTable& BK = bktab();
     cudaError_t e;
+    for (int f = 0; f < g.nfold; ++f) {
+        k_qtwist_fold_batch<<<(unsigned)g.m * g.fold_bpj, 256, 0, s>>>((const QFoldArgs*)(d_desc + g.fold_off[f]),
+                                                                       g.fold_bpj);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
     for (int k = 0; k < g.count; ++k) {
         QBatchKernel kk = BK.k[g.variant[k]][g.logl[k]];
         if (!kk) return cudaErrorInvalidValue;
@@ -1990,6 +2120,13 @@ cudaError_t q32_batch_launch(const Q32Group& g, const char* d_desc, cudaStream_t
         kk<<<grid, NT, pass_smem(g.logl[k], g.variant[k]), s>>>((const QArgs*)(d_desc + g.args_off[k]),
                                                                 (u32)g.tiles[k]);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
+    if (g.twist) {
+        k_qtwist_w_batch<<<dim3((unsigned)g.m * g.w_bpj, 3), 256, 0, s>>>((const QTwistArgs*)(d_desc + g.w_off), g.w_bpj);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        k_qcrt_carry_twist_batch<<<(unsigned)(g.m * g.max_ncta), CNT, 0, s>>>(
+            (const QCrtArgs*)(d_desc + g.crt_off), g.max_ncta, (const u32*)(d_desc + g.ncta_off));
+        return cudaGetLastError();
     }
     k_qcrt_carry_batch<<<(unsigned)(g.m * g.max_ncta), CNT, 0, s>>>((const QCrtArgs*)(d_desc + g.crt_off), g.max_ncta,
                                                                     (const u32*)(d_desc + g.ncta_off));

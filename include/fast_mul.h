@@ -151,8 +151,10 @@ int fmn_mul_operand_ws(const fmn_operand* op, const u64* d_in2, u64 len2, u64* d
  * with a resident operand uses the operand's spectrum when that is modelled cheaper than
  * computing it from scratch (the spectrum has the length of the longest partner it was sized
  * for).  With batching = 0 the server is the plain per-call path: one product per launch
- * sequence, in arrival order, on one stream, without resident-operand reuse.  No counterpart
- * in the reference. */
+ * sequence, in arrival order, on one stream, without resident-operand reuse.  Scratch comes
+ * from the server's own stream-ordered memory pool, of which min(budget, 2 GiB) is mapped when
+ * the server is created (the first growth of a fresh pool stalled a running stream).  No
+ * counterpart in the reference. */
 enum { FMN_OP_MUL = 0, FMN_OP_SQR = 1, FMN_OP_MUL_OPERAND = 2 };
 typedef struct {
     int op;                      /* FMN_OP_* */
@@ -173,6 +175,8 @@ typedef struct {
     u64 cancelled;               /* requests withdrawn by fmn_server_cancel (also in completed) */
     double launch_ms;            /* host time the dispatcher spent launching batches */
     double alloc_ms;             /* of which: taking scratch from the server's memory pool */
+    double max_launch_ms;        /* the longest single batch launch */
+    double max_alloc_ms;         /* the longest single pool allocation */
 } fmn_server_stats;
 typedef struct fmn_server fmn_server;
 int fmn_server_create(int device, size_t hbm_budget_bytes, int max_batch, int batching, fmn_server** out);
@@ -244,9 +248,13 @@ int fmn_force_pieces(int pieces);
  * twisted plans.  fmn_wrap_for returns K for a product that runs wrapped (0 otherwise),
  * fmn_twist_for its twisted length M (0 when not twisted); fmn_force_wrap(1) wraps every
  * product that allows it with the low product, fmn_force_wrap(2) twisted (tests),
- * fmn_force_wrap(0) restores the model.  No counterpart in the reference. */
+ * fmn_force_wrap(0) restores the model.  Batched products (fmn_mul_batch_device, the
+ * server) run whole or twisted; fmn_batch_twist_for returns M for one that runs twisted in
+ * a batch (0 when whole): there the per-product launch cost does not count, since a batch
+ * shares its launches among its products.  No counterpart in the reference. */
 u64 fmn_wrap_for(u64 len1, u64 len2, int sqr);
 u64 fmn_twist_for(u64 len1, u64 len2, int sqr);
+u64 fmn_batch_twist_for(u64 len1, u64 len2, int sqr);
 int fmn_force_wrap(int mode);
 
 /* ----------------------------------------------------------------- pass plans and tuning

@@ -114,3 +114,36 @@ def test_batch_graph_recomputes_updated_inputs(fmn, oracle):
                 assert np.array_equal(_host(out), want)
     finally:
         g.close()
+
+
+def test_twisted_batched_products(fmn, oracle):
+    """Batched products whose coefficient count is just above a power of two run twisted (a
+    cyclic transform of 2^n digits plus the product modulo X^M - c), grouped by (2^n, M),
+    in the same batch as whole products and squares: by the cost model, and with every
+    product that allows it forced twisted.  Every output equals the oracle."""
+    import torch
+    shapes = []
+    for k in range(11, 17):
+        shapes += [(2 ** (k - 1) + 1, 2 ** (k - 1), False), (2 ** (k - 1) + 2 ** (k - 3), 2 ** (k - 1) - 5, False),
+                   (2 ** k - 3, 7 * 2 ** (k - 4), False), (2 ** (k - 1) + 3, 2 ** (k - 1) + 3, True)]
+    shapes += [(1000, 1200, False), (3000, 50, False), (777, 777, True)]
+    for mode in (0, 2):
+        fmn.force_wrap(mode)
+        try:
+            twisted = sum(fmn.batch_twist_for(la, lb, sq) > 0 for la, lb, sq in shapes)
+            assert twisted >= (12 if mode == 0 else 18), (mode, twisted)
+            jobs, cases = [], []
+            for i, (la, lb, sq) in enumerate(shapes):
+                a, b = synth.operands(("uniform", "ones")[i % 2], la, lb, 900 + i)
+                da = _dev(a)
+                db = da if sq else _dev(b)
+                out = torch.full((2 * la if sq else la + lb,), -1, dtype=torch.int64, device="cuda")
+                jobs.append((da, db, out))
+                cases.append((a, None if sq else b))
+            fmn.mul_batch_device(jobs)
+            fmn.sync()
+            for (a, b), (_, _, out) in zip(cases, jobs):
+                want = oracle.sqr(a) if b is None else oracle.mul(a, b)
+                assert np.array_equal(_host(out), want), (mode, len(a), None if b is None else len(b))
+        finally:
+            fmn.force_wrap(0)
