@@ -412,7 +412,7 @@ int run_job_ctx(DevCtx* c, const fmn::Job& j, cudaStream_t s) {
     if (c->done_valid && (e = cudaStreamWaitEvent(s, c->done, 0)) != cudaSuccess)
         return set_err(FMN_ERR_CUDA, "cudaStreamWaitEvent", e);
     const fmn::TwiddleSet* tws = fmn::job_engine(j) != fmn::ENGINE_64 ? nullptr
-                                 : get_twiddles(c, j.spectrum ? j.log_n : ilog2_ceil(j.la + j.lb - 1), s);
+                                 : get_twiddles(c, fmn::job_twiddle_log_n(j), s);
     if ((e = fmn::enqueue_job(j, c->ws, c->ws_cap, s, tws)) != cudaSuccess) {
         std::string m = std::string("kernel launch (") + fmn::launch_diag() + ")";
         return set_err(FMN_ERR_CUDA, m.c_str(), e);
@@ -510,7 +510,7 @@ int host_product_pinned(DevCtx* c, HostLane* L, const u64* in1, u64 len1, const 
                               (e = cudaStreamWaitEvent(co, L->done, 0)) != cudaSuccess))
             return set_err(FMN_ERR_CUDA, "cudaStreamWaitEvent", e);
         const fmn::TwiddleSet* tws =
-            fmn::job_engine(j) != fmn::ENGINE_64 ? nullptr : get_twiddles(c, ilog2_ceil(out_len - 1), s);
+            fmn::job_engine(j) != fmn::ENGINE_64 ? nullptr : get_twiddles(c, fmn::job_twiddle_log_n(j), s);
         if ((e = cudaMemcpyAsync(io + o1, in1, len1 * 8, cudaMemcpyHostToDevice, s)) != cudaSuccess)
             return set_err(FMN_ERR_CUDA, "copying in1 to the device", e);
         CopyIn ci;
@@ -645,7 +645,7 @@ int host_product(const u64* in1, u64 len1, const u64* in2, u64 len2, u64* out, i
         std::lock_guard<std::mutex> lk(c->mu);
         if ((rc = ensure_buf(&L->ws, &L->ws_cap, fmn::job_workspace_bytes(j), true))) return rc;
         const fmn::TwiddleSet* tws =
-            fmn::job_engine(j) != fmn::ENGINE_64 ? nullptr : get_twiddles(c, ilog2_ceil(out_len - 1), L->s);
+            fmn::job_engine(j) != fmn::ENGINE_64 ? nullptr : get_twiddles(c, fmn::job_twiddle_log_n(j), L->s);
         if ((e = fmn::enqueue_job(j, L->ws, L->ws_cap, L->s, tws)) != cudaSuccess) {
             std::string m = std::string("kernel launch (") + fmn::launch_diag() + ")";
             return set_err(FMN_ERR_CUDA, m.c_str(), e);
@@ -891,7 +891,7 @@ u64 fmn_wrap_for(u64 len1, u64 len2, int sqr) {
     j.la = len1;
     j.lb = len2;
     j.sqr = sqr ? 1 : 0;
-    return fmn::job_engine(j) == fmn::ENGINE_32 ? fmn::q32_wrapped(len1, len2, sqr ? 1 : 0) : 0;
+    return fmn::job_engine(j) == fmn::ENGINE_32 ? fmn::q32_wrapped(len1, len2, sqr ? 1 : 0) : fmn::wrap64_for(j);
 }
 
 int fmn_engine_for(u64 len1, u64 len2, int sqr) {

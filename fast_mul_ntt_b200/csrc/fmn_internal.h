@@ -56,6 +56,7 @@ struct Job {
     int engine = 0;    // ENGINE_*: 0 follows the process-wide default; with `spectrum`, the
                        // engine that spectrum belongs to (log_n in that engine's points)
     Plan splan = Plan{};   // with `spectrum`: the pass plan it was transformed with
+    bool no_wrap = false;  // 64-bit engine: never the wrapped plan (fixed-size scratch)
 };
 
 // Residue engines.  ENGINE_64 transforms 64-bit limbs modulo the reference's three 62-bit
@@ -169,6 +170,9 @@ struct Q32Group {
     size_t fold_off[2], w_off;
     unsigned fold_bpj, w_bpj;
 };
+int q32_forced_wrap();                      // fmn_force_wrap mode (0: the cost model decides)
+int job_twiddle_log_n(const Job& j);        // 64-bit engine: log2 of the main transform (twiddle tables)
+u64 wrap64_for(const Job& j);               // 64-bit engine: K of a wrapped product, 0 if whole
 int q32_batch_log_n(const Job& j);          // (cyclic) transform log length, < 0 if not a 32-bit batch product
 int q32_batch_twist_log(const Job& j);      // log2 M of a batched product run twisted, 0 for a whole product
 size_t q32_batch_res_bytes(const Job& j);   // residue arrays of one product

@@ -78,6 +78,7 @@ extern "C" int fmn_mul_device_noalloc(const u64* d_in1, u64 len1, const u64* d_i
     j.out = d_out;
     j.sqr = sq;
     j.engine = fmn::ENGINE_64;      // the scratch array is sized for this engine's layout
+    j.no_wrap = true;               // ... of a whole product
     if (out_len - 1 > kNoallocMaxNtt)
         return fmn::api_set_error(FMN_ERR_TOO_LARGE,
                                   "fmn_mul_device_noalloc: product needs a transform above 65536 points "

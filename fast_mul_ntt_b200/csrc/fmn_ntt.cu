@@ -598,13 +598,22 @@ cudaError_t build_twiddle_tables(int log_n, u64* buf, TwiddleSet* out, cudaStrea
 struct CrtArgs {
     const u64* res;     // three natural-order residue arrays (prime i at res + i*N), < 4p
     u64 N;
-    u64 nvalid;         // coefficients that may be nonzero: min(conv_len, N)
+    u64 nvalid;         // coefficients that may be nonzero: min(conv_len, N), or conv_len if wrapped
     u64* out;
     u64 out_len;
     u64 cst[3];         // M_i^-1 * N^-1 * 2^128 mod p_i (undoes the two Montgomery products)
     u32* state;         // per-CTA look-back words, zeroed before launch
     u32* ticket;        // zeroed before launch
     u32* err;
+    // wrapped products (wrap = K > 0): `res` holds the cyclic convolution of length N, whose
+    // entry k < K is c_k + c_{k+N}, and `low` the product of the operands' lowest K limbs
+    // (prime i at low + i*low_N), whose coefficients below K are c_0 .. c_{K-1}; each with its
+    // own scale constants.  c_k = low_k for k < K, res_k for K <= k < N, and
+    // res_{k-N} - low_{k-N} for N <= k < conv_len.
+    const u64* low;
+    u64 low_N;
+    u64 wrap;
+    u64 low_cst[3];
 };
 
 __host__ __device__ constexpr u64 m_lo(int i) {
@@ -634,12 +643,8 @@ __device__ __forceinline__ void acc_mul(u64 y, u64 ml, u64 mh, u64& w0, u64& w1,
     w2 = w2 + (u64)(hi >> 64) + (u64)(s1 >> 64);
 }
 
-// crt3 of one coefficient from its three residues r0, r1, r2 (< 4p_i).
-__device__ __forceinline__ void crt_of(u64 r0, u64 r1, u64 r2, const u64 (&cst)[3], u64& w0, u64& w1, u64& w2,
-                                       const PrimeRT& q0, const PrimeRT& q1, const PrimeRT& q2) {
-    const u64 y0 = red1(mmul(r0, cst[0], q0), q0);
-    const u64 y1 = red1(mmul(r1, cst[1], q1), q1);
-    const u64 y2 = red1(mmul(r2, cst[2], q2), q2);
+// crt3 of one coefficient from y_i = c mod p_i times M_i^-1 (each in [0, p_i)).
+__device__ __forceinline__ void crt_acc(u64 y0, u64 y1, u64 y2, u64& w0, u64& w1, u64& w2) {
     w0 = w1 = w2 = 0;
     acc_mul(y0, m_lo(0), m_hi(0), w0, w1, w2);
     acc_mul(y1, m_lo(1), m_hi(1), w0, w1, w2);
@@ -657,12 +662,38 @@ __device__ __forceinline__ void crt_of(u64 r0, u64 r1, u64 r2, const u64 (&cst)[
         }
     }
 }
+// crt3 of one coefficient from its three residues r0, r1, r2 (< 4p_i).
+__device__ __forceinline__ void crt_of(u64 r0, u64 r1, u64 r2, const u64 (&cst)[3], u64& w0, u64& w1, u64& w2,
+                                       const PrimeRT& q0, const PrimeRT& q1, const PrimeRT& q2) {
+    crt_acc(red1(mmul(r0, cst[0], q0), q0), red1(mmul(r1, cst[1], q1), q1), red1(mmul(r2, cst[2], q2), q2), w0, w1,
+            w2);
+}
 
+// Where coefficient j of a wrapped product comes from (see CrtArgs): 0 res_j, 1 low_j,
+// 2 res_{j-N} - low_{j-N}.
+template <bool WRAP>
+__device__ __forceinline__ int src64(const CrtArgs& a, u64 j) {
+    return !WRAP ? 0 : (j >= a.N ? 2 : (j < a.wrap ? 1 : 0));
+}
+// c_j mod p_i times M_i^-1, in [0, p_i), from source src.
+__device__ __forceinline__ u64 y_of(const CrtArgs& a, int src, u64 j, int i, const PrimeRT& q) {
+    if (src == 0) return red1(mmul(a.res[i * a.N + j], a.cst[i], q), q);
+    const u64 jj = src == 2 ? j - a.N : j;
+    const u64 yl = red1(mmul(a.low[i * a.low_N + jj], a.low_cst[i], q), q);
+    if (src == 1) return yl;
+    return red1(red1(mmul(a.res[i * a.N + jj], a.cst[i], q), q) + q.p - yl, q);
+}
+template <bool WRAP>
 __device__ __forceinline__ void crt_coef(const CrtArgs& a, u64 j, u64& w0, u64& w1, u64& w2,
                                          const PrimeRT& q0, const PrimeRT& q1, const PrimeRT& q2) {
     w0 = w1 = w2 = 0;
     if (j >= a.nvalid) return;
-    crt_of(a.res[j], a.res[a.N + j], a.res[2 * a.N + j], a.cst, w0, w1, w2, q0, q1, q2);
+    if (!WRAP) {
+        crt_of(a.res[j], a.res[a.N + j], a.res[2 * a.N + j], a.cst, w0, w1, w2, q0, q1, q2);
+        return;
+    }
+    const int src = src64<WRAP>(a, j);
+    crt_acc(y_of(a, src, j, 0, q0), y_of(a, src, j, 1, q1), y_of(a, src, j, 2, q2), w0, w1, w2);
 }
 
 // Output limbs per thread of the CRT + carry kernel: 8 keeps a thread's sums and 192-bit CRT
@@ -671,6 +702,7 @@ __device__ __forceinline__ void crt_coef(const CrtArgs& a, u64 j, u64& w0, u64& 
 constexpr int WCE = 8;
 constexpr u64 WCTILE = (u64)CNT * WCE;
 
+template <bool WRAP>
 __device__ __forceinline__ void crt_carry_body(const CrtArgs& a, u32 ncta) {
     __shared__ u64 s_hw[CNT / 32][3];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -684,7 +716,9 @@ __device__ __forceinline__ void crt_carry_body(const CrtArgs& a, u32 ncta) {
     u64 lo[WCE];
     u32 h[WCE];
     u64 pw1 = 0, pw2 = 0, ppw2 = 0;          // c_{j-1}[1], c_{j-1}[2], c_{j-2}[2]
-    const bool full = j0 + WCE <= a.nvalid;
+    // wrapped: the vector path takes threads whose coefficients all come from res; the few
+    // around and beyond the wrap boundaries go coefficient by coefficient
+    const bool full = j0 + WCE <= a.nvalid && (!WRAP || (src64<WRAP>(a, j0) == 0 && src64<WRAP>(a, j0 + WCE - 1) == 0));
 #pragma unroll
     for (int e2 = 0; e2 < WCE; e2 += 2) {
         u64 r0[2], r1[2], r2[2];
@@ -699,7 +733,7 @@ __device__ __forceinline__ void crt_carry_body(const CrtArgs& a, u32 ncta) {
             const int e = e2 + u;
             u64 w0, w1, w2;
             if (full) crt_of(r0[u], r1[u], r2[u], a.cst, w0, w1, w2, q0, q1, q2);
-            else crt_coef(a, j0 + e, w0, w1, w2, q0, q1, q2);
+            else crt_coef<WRAP>(a, j0 + e, w0, w1, w2, q0, q1, q2);
             u64 l = w0;
             u32 hh = 0;
             add_to(l, hh, pw1);
@@ -728,8 +762,8 @@ __device__ __forceinline__ void crt_carry_body(const CrtArgs& a, u32 ncta) {
             n3 = s_hw[warp - 1][2];
         } else {
             u64 u0, u1, u2, v0, v1, v2;
-            if (j0 >= 1) crt_coef(a, j0 - 1, u0, u1, u2, q0, q1, q2); else u0 = u1 = u2 = 0;
-            if (j0 >= 2) crt_coef(a, j0 - 2, v0, v1, v2, q0, q1, q2); else v0 = v1 = v2 = 0;
+            if (j0 >= 1) crt_coef<WRAP>(a, j0 - 1, u0, u1, u2, q0, q1, q2); else u0 = u1 = u2 = 0;
+            if (j0 >= 2) crt_coef<WRAP>(a, j0 - 2, v0, v1, v2, q0, q1, q2); else v0 = v1 = v2 = 0;
             n1 = u1;
             n2 = u2;
             n3 = v2;
@@ -742,7 +776,11 @@ __device__ __forceinline__ void crt_carry_body(const CrtArgs& a, u32 ncta) {
     carry_finish(lo, h, tile, j0, a.state, a.err, a.out, a.out_len);
 }
 
-__global__ void __launch_bounds__(CNT, 4) k_crt_carry(CrtArgs a) { crt_carry_body(a, 0xffffffffu); }
+// 5 CTAs per SM (48 registers, no spills): while one CTA's warps wait at the barrier of its
+// look-back, the others compute.
+__global__ void __launch_bounds__(CNT, 5) k_crt_carry(CrtArgs a) { crt_carry_body<false>(a, 0xffffffffu); }
+// Wrapped products (see CrtArgs): 62 registers, 4 CTAs (5 spilled).
+__global__ void __launch_bounds__(CNT, 4) k_crt_carry_wrap(CrtArgs a) { crt_carry_body<true>(a, 0xffffffffu); }
 
 // ------------------------------------------------------------------ host: tables
 static u64 h_mulmod(u64 a, u64 b, u64 m) { return (u64)(((unsigned __int128)a * b) % m); }
@@ -1022,14 +1060,56 @@ struct WsLayout {
     int n;
     size_t a, b, ticket, state, total;
     u64 ncta;
+    // wrapped (wrap = K > 0): the cyclic product at N plus the product of both operands'
+    // lowest K limbs, a whole product at NL points whose residues sit at la_off / lb_off
+    u64 wrap;
+    u64 NL;
+    size_t la_off, lb_off;
 };
-static WsLayout ws_layout(u64 la, u64 lb, int sqr, int force_n = 0) {
+
+// Wrapped plan of this engine (the 32-bit engine's plan_wrap, restated for limbs): a product
+// of dc = la + lb - 1 coefficients with 2^n < dc and both operands within N = 2^n limbs runs as
+// the cyclic convolution of length N (its entry k < K = dc - N holds c_k + c_{k+N}) plus the
+// whole product of the operands' lowest K limbs (K < min(la, lb), so it gives c_0 .. c_{K-1}
+// exactly), and the CRT + carry kernel separates the two (k_crt_carry_wrap).  Taken when its
+// modelled cost, (1 + 2) transforms of N and of NL = ceil_pow2(2K - 1) points x (log + 1)
+// plus one launch sequence, is below the whole product's at 2N, or when fmn_force_wrap asks.
+constexpr double kSeqCost64 = 1.25e7;      // launch overhead of one launch sequence, in (points x bits)
+static bool wrap64_plan(u64 la, u64 lb, int sqr, u64* N_out, u64* K_out, u64* NL_out) {
+    if (la == 0 || lb == 0) return false;
+    const u64 dc = la + lb - 1;
+    if (dc < 3) return false;
+    const int n = ilog2(dc) - 1;               // ilog2 rounds up: 2^n < dc <= 2^(n+1)
+    if (n < 12 || n + 1 > MAX_LOG_N) return false;
+    const u64 N = 1ull << n;
+    if (la > N || lb > N || dc <= N) return false;   // an operand would wrap onto itself
+    const u64 K = dc - N;                      // 1 <= K < min(la, lb)
+    const u64 NL = ceil_pow2(2 * K - 1);
+    const double t = sqr ? 2.0 : 3.0;
+    const double whole = t * (double)(2 * N) * (n + 2);
+    const double wrap = t * (double)N * (n + 1) + t * (double)NL * (ilog2(NL) + 1) + kSeqCost64;
+    if (!(q32_forced_wrap() ? true : wrap < whole)) return false;
+    *N_out = N;
+    *K_out = K;
+    *NL_out = NL;
+    return true;
+}
+
+// wrap_ok: the product may take the wrapped plan (single products; not batches, resident
+// spectra or the fixed-size scratch of fmn_mul_device_noalloc).
+static WsLayout ws_layout(u64 la, u64 lb, int sqr, int force_n = 0, bool wrap_ok = false) {
     WsLayout w;
     memset(&w, 0, sizeof(w));
     const u64 out_len = la + lb;
     if (la == 0 || lb == 0) return w;
     w.N = ceil_pow2(out_len - 1);
     if (force_n > 0 && (1ull << force_n) > w.N) w.N = 1ull << force_n;
+    u64 N = 0, K = 0, NL = 0;
+    if (wrap_ok && force_n <= 0 && wrap64_plan(la, lb, sqr, &N, &K, &NL)) {
+        w.N = N;
+        w.wrap = K;
+        w.NL = NL;
+    }
     w.n = ilog2(w.N);
     w.ncta = (out_len + WCTILE - 1) / WCTILE;
     size_t off = 256;
@@ -1037,6 +1117,12 @@ static WsLayout ws_layout(u64 la, u64 lb, int sqr, int force_n = 0) {
     off = align256(off + 3 * w.N * sizeof(u64));
     w.b = off;
     if (!sqr) off = align256(off + 3 * w.N * sizeof(u64));
+    if (w.wrap) {
+        w.la_off = off;
+        off = align256(off + 3 * w.NL * sizeof(u64));
+        w.lb_off = off;
+        if (!sqr) off = align256(off + 3 * w.NL * sizeof(u64));
+    }
     w.ticket = off;
     w.state = off + 16;
     off = align256(w.state + w.ncta * sizeof(u32));
@@ -1073,10 +1159,22 @@ static Job plain_job(u64 la, u64 lb, int sqr) {
     return j;
 }
 
+static bool wrap_ok(const Job& j) { return !j.spectrum && !j.no_wrap; }
+
 size_t job_workspace_bytes(const Job& j) {
     if (job_engine(j) == ENGINE_32) return q32_job_workspace_bytes(j);
-    const size_t t = ws_layout(j.la, j.lb, j.sqr, j.spectrum ? j.log_n : 0).total;
+    const size_t t = ws_layout(j.la, j.lb, j.sqr, j.spectrum ? j.log_n : 0, wrap_ok(j)).total;
     return t ? t : 256;
+}
+
+u64 wrap64_for(const Job& j) {
+    if (j.spectrum || j.la == 0 || j.lb == 0) return 0;
+    return ws_layout(j.la, j.lb, j.sqr, 0, wrap_ok(j)).wrap;
+}
+
+int job_twiddle_log_n(const Job& j) {
+    if (j.spectrum) return j.log_n;
+    return ws_layout(j.la, j.lb, j.sqr, 0, wrap_ok(j)).n;
 }
 
 size_t job_workspace_bytes(u64 la, u64 lb, int sqr) { return job_workspace_bytes(plain_job(la, lb, sqr)); }
@@ -1230,15 +1328,21 @@ static cudaError_t launch_pass(int variant, int logl, const PassArgs& a, u64 til
                         [&] { k<<<(unsigned)(tiles * 3), NT, pass_smem(logl, variant), s>>>(a); });
 }
 
-int job_launches(u64 la, u64 lb, int sqr) {
-    if (la == 0 || lb == 0) return 0;
-    if (job_engine(plain_job(la, lb, sqr)) == ENGINE_32) return q32_launches(la, lb, sqr);
-    const WsLayout w = ws_layout(la, lb, sqr);
-    const Plan pl = make_plan(w.n);
+// Launches of one 64-bit product of the given layout length (pass launches + the CRT).
+static int launches64(int n, int sqr) {
+    const Plan pl = make_plan(n);
     const int P = pl.passes;
     // forward strided passes (A, and B unless squaring) + A's last pass + fused + inverse + crt
     if (!sqr && P >= 2 && pl.bits[P - 1] >= 5 && pl.bits[P - 1] <= 8) return 2 * (P - 1) + 1 + (P - 1) + 1;   // merged
     return sqr ? (P - 1) + 1 + (P - 1) + 1 : 2 * (P - 1) + 1 + 1 + (P - 1) + 1;
+}
+
+int job_launches(u64 la, u64 lb, int sqr) {
+    if (la == 0 || lb == 0) return 0;
+    if (job_engine(plain_job(la, lb, sqr)) == ENGINE_32) return q32_launches(la, lb, sqr);
+    const WsLayout w = ws_layout(la, lb, sqr, 0, true);
+    // a wrapped product adds the low product's pass launches (its own CRT is not run)
+    return launches64(w.n, sqr) + (w.wrap ? launches64(ilog2(w.NL), sqr) - 1 : 0);
 }
 
 // Every launch one product needs, in order, with its arguments (no launch happens here).
@@ -1264,10 +1368,12 @@ struct JobScratch {
     u32* err;
 };
 
-static void plan_job(const Job& j, const JobScratch& sc, const TwiddleSet* tws, JobLaunches* out) {
+// wrap: the layout may take the wrapped plan (single products); the caller then plans and
+// launches the low product itself (enqueue_job) and fills the CRT's wrap fields.
+static void plan_job(const Job& j, const JobScratch& sc, const TwiddleSet* tws, JobLaunches* out, bool wrap = false) {
     const u64 out_len = j.la + j.lb;
     const int sqr = j.sqr ? 1 : 0;
-    const WsLayout w = ws_layout(j.la, j.lb, sqr, j.spectrum ? j.log_n : 0);
+    const WsLayout w = ws_layout(j.la, j.lb, sqr, j.spectrum ? j.log_n : 0, wrap && wrap_ok(j));
     u64* A = sc.A;
     u64* B = sqr ? A : sc.B;
     const Plan pl = j.spectrum && j.splan.passes ? j.splan : make_plan(w.n);   // a spectrum keeps its plan
@@ -1385,7 +1491,7 @@ static void plan_job(const Job& j, const JobScratch& sc, const TwiddleSet* tws, 
     }
     ca.res = A;
     ca.N = N;
-    ca.nvalid = (out_len - 1) < N ? (out_len - 1) : N;
+    ca.nvalid = w.wrap || (out_len - 1) < N ? (out_len - 1) : N;
     ca.out = j.out;
     ca.out_len = out_len;
     ca.state = sc.state;
@@ -1395,9 +1501,29 @@ static void plan_job(const Job& j, const JobScratch& sc, const TwiddleSet* tws, 
 }
 
 static cudaError_t launch_crt(const CrtArgs& ca, u64 ncta, cudaStream_t s) {
-    const double crt_bytes = 3.0 * (double)ca.nvalid * 8.0 + (double)ca.out_len * 8.0;
-    return timed_launch(K_CRT, crt_bytes, 3.0 * (double)ca.nvalid, s,
-                        [&] { k_crt_carry<<<(unsigned)ncta, CNT, 0, s>>>(ca); });
+    const double crt_bytes = 3.0 * (double)ca.nvalid * 8.0 + 3.0 * (double)ca.wrap * 16.0 + (double)ca.out_len * 8.0;
+    return timed_launch(K_CRT, crt_bytes, 3.0 * (double)ca.nvalid, s, [&] {
+        if (ca.wrap) k_crt_carry_wrap<<<(unsigned)ncta, CNT, 0, s>>>(ca);
+        else k_crt_carry<<<(unsigned)ncta, CNT, 0, s>>>(ca);
+    });
+}
+
+// The low product of a wrapped 64-bit product (see wrap64_plan): the operands' lowest K limbs
+// as an ordinary whole product into the layout's low arrays; its inverse spectrum is left in
+// place for the main CRT, whose wrap fields this fills.
+static void plan_low64(const Job& j, const WsLayout& w, char* base, const JobScratch& sc, JobLaunches* low,
+                       CrtArgs* ca) {
+    Job jl = j;
+    jl.la = w.wrap;
+    jl.lb = w.wrap;
+    jl.out = nullptr;
+    jl.no_wrap = true;
+    JobScratch scl{(u64*)(base + w.la_off), (u64*)(base + w.lb_off), sc.ticket, sc.state, sc.err};
+    plan_job(jl, scl, nullptr, low);
+    ca->low = scl.A;
+    ca->low_N = low->crt.N;
+    ca->wrap = w.wrap;
+    for (int i = 0; i < 3; ++i) ca->low_cst[i] = low->crt.cst[i];
 }
 
 cudaError_t enqueue_job(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s, const TwiddleSet* tws) {
@@ -1406,7 +1532,7 @@ cudaError_t enqueue_job(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s,
     if (j.la == 0 || j.lb == 0) return cudaMemsetAsync(j.out, 0, out_len * sizeof(u64), s);
     if (job_engine(j) == ENGINE_32) return q32_enqueue(j, ws, ws_bytes, s, nullptr, nullptr, 1, nullptr, nullptr);
     const int sqr = j.sqr ? 1 : 0;
-    const WsLayout w = ws_layout(j.la, j.lb, sqr, j.spectrum ? j.log_n : 0);
+    const WsLayout w = ws_layout(j.la, j.lb, sqr, j.spectrum ? j.log_n : 0, wrap_ok(j));
     if (ws_bytes < w.total || w.n > MAX_LOG_N) return cudaErrorInvalidValue;
     cudaError_t e = ensure_tables();
     if (e != cudaSuccess) return e;
@@ -1414,7 +1540,14 @@ cudaError_t enqueue_job(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s,
     JobScratch sc{(u64*)(base + w.a), (u64*)(base + w.b), (u32*)(base + w.ticket), (u32*)(base + w.state),
                   (u32*)base};
     JobLaunches L;
-    plan_job(j, sc, tws, &L);
+    plan_job(j, sc, tws, &L, true);
+    if (w.wrap) {
+        JobLaunches LL;
+        plan_low64(j, w, base, sc, &LL, &L.crt);
+        for (int k = 0; k < LL.count; ++k)
+            if ((e = launch_pass(LL.rec[k].variant, LL.rec[k].logl, LL.rec[k].pa, LL.rec[k].tiles, s)) != cudaSuccess)
+                return e;
+    }
     for (int k = 0; k < L.count; ++k) {
         const LaunchRec& r = L.rec[k];
         if ((e = launch_pass(r.variant, r.logl, r.pa, r.tiles, s)) != cudaSuccess) return e;
@@ -1430,23 +1563,40 @@ cudaError_t enqueue_job_overlapped(const Job& j, void* ws, size_t ws_bytes, cuda
     if (job_engine(j) == ENGINE_32)
         return q32_enqueue(j, ws, ws_bytes, s, need_b, need_ctx, crt_chunks, after_chunk, ctx);
     const int sqr = j.sqr ? 1 : 0;
-    const WsLayout w = ws_layout(j.la, j.lb, sqr, j.spectrum ? j.log_n : 0);
+    const WsLayout w = ws_layout(j.la, j.lb, sqr, j.spectrum ? j.log_n : 0, wrap_ok(j));
     if (ws_bytes < w.total || w.n > MAX_LOG_N) return cudaErrorInvalidValue;
     cudaError_t e = ensure_tables();
     if (e != cudaSuccess) return e;
     char* base = (char*)ws;
     JobScratch sc{(u64*)(base + w.a), (u64*)(base + w.b), (u32*)(base + w.ticket), (u32*)(base + w.state),
                   (u32*)base};
-    JobLaunches L;
-    plan_job(j, sc, tws, &L);
-    bool waited = false;
+    JobLaunches L, LL;
+    plan_job(j, sc, tws, &L, true);
+    LL.count = 0;
+    if (w.wrap) plan_low64(j, w, base, sc, &LL, &L.crt);
+    // the first operand's passes, then (once the second operand is copied) the low product,
+    // which reads both, and the rest
+    bool waited = false, low_done = LL.count == 0;
+    auto run_low = [&]() -> cudaError_t {
+        for (int k = 0; k < LL.count; ++k) {
+            const cudaError_t e2 = launch_pass(LL.rec[k].variant, LL.rec[k].logl, LL.rec[k].pa, LL.rec[k].tiles, s);
+            if (e2 != cudaSuccess) return e2;
+        }
+        low_done = true;
+        return cudaSuccess;
+    };
     for (int k = 0; k < L.count; ++k) {
         const LaunchRec& r = L.rec[k];
         if (r.needs_b && !waited && need_b) {           // second operand copied meanwhile
             if ((e = need_b(need_ctx, 0, j.lb, s)) != cudaSuccess) return e;
             waited = true;
         }
+        if ((r.needs_b || sqr) && !low_done && (e = run_low()) != cudaSuccess) return e;
         if ((e = launch_pass(r.variant, r.logl, r.pa, r.tiles, s)) != cudaSuccess) return e;
+    }
+    if (!low_done) {
+        if (!waited && need_b && !sqr && (e = need_b(need_ctx, 0, j.lb, s)) != cudaSuccess) return e;
+        if ((e = run_low()) != cudaSuccess) return e;
     }
     if ((e = cudaMemsetAsync(base + w.ticket, 0, w.total - w.ticket, s)) != cudaSuccess) return e;
     // carry scan in chunks of CTAs: tickets continue across launches, each chunk's limbs are
@@ -1486,7 +1636,7 @@ __global__ void __launch_bounds__(NT, (pass_min_ctas<MODE, LOGL>())) k_pass_batc
 __global__ void __launch_bounds__(CNT) k_crt_carry_batch(const CrtArgs* __restrict__ args, u32 ctas_per_job,
                                                          const u32* __restrict__ ncta) {
     const u32 job = blockIdx.x / ctas_per_job;
-    crt_carry_body(args[job], ncta[job]);
+    crt_carry_body<false>(args[job], ncta[job]);
 }
 
 typedef void (*BatchKernel)(const PassArgs*, u32);

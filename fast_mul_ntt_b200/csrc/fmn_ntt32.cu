@@ -858,13 +858,15 @@ __device__ __forceinline__ void qcrt_carry_body(const QCrtArgs& a, u32 ncta) {
     carry_finish<QCE, LIMIT>(lo, h, tile, j0, a.state, a.err, a.out, a.out_len);
 }
 
-__global__ void __launch_bounds__(CNT, QCE <= 8 ? 4 : 3) k_qcrt_carry(QCrtArgs a) {
+// 5 CTAs per SM (48 registers, no spills): while one CTA's warps wait at the barrier of its
+// look-back, the others compute (4 CTAs: 56-62 registers, barrier the top stall)
+__global__ void __launch_bounds__(CNT, 5) k_qcrt_carry(QCrtArgs a) {
     qcrt_carry_body<0>(a, 0xffffffffu);
 }
 // Wrapped products with a low product (two residue sources, two sets of scale constants).
 __global__ void __launch_bounds__(CNT, 4) k_qcrt_carry_wrap(QCrtArgs a) { qcrt_carry_body<1>(a, 0xffffffffu); }
 // Twisted wrapped products (a CTA tile lies wholly below or above N: one source per tile).
-__global__ void __launch_bounds__(CNT, 4) k_qcrt_carry_twist(QCrtArgs a) { qcrt_carry_body<2>(a, 0xffffffffu); }
+__global__ void __launch_bounds__(CNT, 5) k_qcrt_carry_twist(QCrtArgs a) { qcrt_carry_body<2>(a, 0xffffffffu); }
 
 // The plain kernel with a look-back limit of 2^12 polls (milliseconds instead of seconds), for
 // the test that withholds a tile and checks that the wait expires into the status word.
@@ -1926,6 +1928,8 @@ static void batch_twist_plan(const Job& j, QJob* T) {
     T->ok = ct >= 0.0 && (fw == 2 || ct - kPieceCost < 0.85 * cw);
 }
 }  // namespace q32
+
+int q32_forced_wrap() { return q32::g_force_wrap.load(); }
 
 int q32_batch_twist_log(const Job& j) {
     q32::QJob T;

@@ -289,7 +289,9 @@ bool launch_unlocked(fmn_server* s, Slot* sl, const std::vector<fmn_request>& rq
             ob += align256(out_len_of(r) * sizeof(u64));
         }
         if (jobs[k].la && jobs[k].lb && fmn::job_engine(jobs[k]) == fmn::ENGINE_64) {
-            const int n = jobs[k].spectrum ? jobs[k].log_n : ilog2c(jobs[k].la + jobs[k].lb - 1);
+            const int n = jobs[k].spectrum ? jobs[k].log_n
+                          : single      ? fmn::job_twiddle_log_n(jobs[k])    // a single product may be wrapped
+                                        : ilog2c(jobs[k].la + jobs[k].lb - 1);
             ensure_server_twiddles(s, n, sl->stream);
         }
     }
@@ -308,7 +310,7 @@ bool launch_unlocked(fmn_server* s, Slot* sl, const std::vector<fmn_request>& rq
                           : cudaErrorMemoryAllocation;
         } else {
             const int n = jobs[0].spectrum ? jobs[0].log_n
-                          : (jobs[0].la && jobs[0].lb ? ilog2c(jobs[0].la + jobs[0].lb - 1) : 0);
+                          : (jobs[0].la && jobs[0].lb ? fmn::job_twiddle_log_n(jobs[0]) : 0);
             e = fmn::enqueue_job(jobs[0], mem, ws_bytes, sl->stream, server_twiddles(s, n));
         }
     }

@@ -114,3 +114,62 @@ def test_cost_model_wraps_10M_and_matches_reference(fmn, golden):
         a, b = operands_for(c)
         out = fmn.abs_sqr64(a) if op == "sqr" else fmn.abs_mul64(a, b)
         assert digest(out) == c["sha256"], (op, kind)
+
+
+@pytest.fixture
+def engine64(fmn):
+    fmn.set_engine(fmn.ENGINE_64)
+    yield
+    fmn.force_wrap(0)
+    fmn.set_engine(fmn.ENGINE_AUTO)
+
+
+def test_engine64_wrapped_products(fmn, oracle, golden, engine64):
+    """The 64-bit engine (the reference's primes) wraps a product of dc = la + lb - 1 limb
+    coefficients just above 2^n around the cyclic length 2^n and recovers c_0 .. c_{K-1} from
+    the product of the operands' lowest K = dc - 2^n limbs: forced wherever it applies (small
+    shapes, multiplies and squares, one to 147k wrapped coefficients) and chosen by the cost
+    model (large shapes, where the saving outweighs a second launch sequence), against the
+    oracle and the reference's golden digests."""
+    forced = []
+    for k in range(13, 19):
+        forced += [(2 ** (k - 1) + 3, 2 ** (k - 1), False), (2 ** (k - 1) + 2 ** (k - 4), 2 ** (k - 1), False),
+                   (2 ** k - 5, 9 * 2 ** (k - 4), False), (2 ** (k - 1) + 7, 2 ** (k - 1) + 7, True)]
+    modelled = [(2 ** 19 + 3, 2 ** 19, False), (2 ** 19 + 2 ** 16, 2 ** 19, False), (600000, 700001, False),
+                (2 ** 20 + 7, 2 ** 20 + 7, True)]
+    for mode, shapes in ((1, forced), (0, modelled)):
+        fmn.force_wrap(mode)
+        for i, (la, lb, sq) in enumerate(shapes):
+            assert fmn.wrap_for(la, lb, sq) > 0, (mode, la, lb, sq)
+            a, b = synth.operands(("uniform", "ones", "sparse")[i % 3], la, lb, 300 + i)
+            if sq:
+                assert np.array_equal(fmn.abs_sqr64(a), oracle.sqr(a)), (mode, la)
+            else:
+                assert np.array_equal(fmn.abs_mul64(a, b), oracle.mul(a, b)), (mode, la, lb, fmn.wrap_for(la, lb))
+    fmn.force_wrap(1)
+    n = 0
+    for c in golden:
+        if c["len1"] + c["len2"] > 140000 or c["len1"] + c["len2"] < 4097:
+            continue
+        a, b = operands_for(c)
+        out = fmn.abs_sqr64(a) if c["op"] == "sqr" else fmn.abs_mul64(a, b)
+        assert digest(out) == c["sha256"], (c["op"], c["kind"], c["len1"], c["len2"])
+        n += fmn.wrap_for(c["len1"], c["len2"], c["op"] == "sqr") > 0
+    assert n >= 3
+
+
+def test_engine64_wrapped_10M_matches_reference(fmn, golden, engine64):
+    """10M x 10M on the 64-bit engine runs wrapped (cyclic 2^24 limbs + the 3.2M-limb low
+    product) and equals the reference's digest, on the device path and through abs_mul64."""
+    import torch
+    assert fmn.wrap_for(10_000_000, 10_000_000) == 3_222_783
+    c = next(c for c in golden if c["op"] == "mul" and c["kind"] == "uniform" and c["len1"] == 10_000_000
+             and c["len2"] == 10_000_000)
+    a, b = operands_for(c)
+    da = torch.from_numpy(a.view(np.int64)).cuda()
+    db = torch.from_numpy(b.view(np.int64)).cuda()
+    out = torch.empty(20_000_000, dtype=torch.int64, device="cuda")
+    fmn.mul_device(da, db, out)
+    fmn.sync()
+    assert digest(out.cpu().numpy().view(np.uint64)) == c["sha256"]
+    assert digest(fmn.abs_mul64(a, b)) == c["sha256"]
