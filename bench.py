@@ -768,7 +768,7 @@ def run_ours(args, ws, rank, local):
     # caller has its own output.
     lib = fmn.load_library()
     P = ctypes.POINTER(ctypes.c_uint64)
-    e2e_steps = max(3, min(args.steps, 10))
+    e2e_steps = max(3, min(2 * args.steps, 40))   # about 0.3-1.2 s per figure: PCIe and host noise averages out
     callers = args.e2e_callers
 
     def pinned(x):
