@@ -871,7 +871,7 @@ u64 fmn_twist_for(u64 len1, u64 len2, int sqr) {
     j.la = len1;
     j.lb = len2;
     j.sqr = sqr ? 1 : 0;
-    return fmn::job_engine(j) == fmn::ENGINE_32 ? fmn::q32_twisted(len1, len2, sqr ? 1 : 0) : 0;
+    return fmn::job_engine(j) == fmn::ENGINE_32 ? fmn::q32_twisted(len1, len2, sqr ? 1 : 0) : fmn::twist64_for(j);
 }
 
 u64 fmn_batch_twist_for(u64 len1, u64 len2, int sqr) {

@@ -173,6 +173,7 @@ struct Q32Group {
 int q32_forced_wrap();                      // fmn_force_wrap mode (0: the cost model decides)
 int job_twiddle_log_n(const Job& j);        // 64-bit engine: log2 of the main transform (twiddle tables)
 u64 wrap64_for(const Job& j);               // 64-bit engine: K of a wrapped product, 0 if whole
+u64 twist64_for(const Job& j);              // 64-bit engine: M of a twisted product, 0 otherwise
 int q32_batch_log_n(const Job& j);          // (cyclic) transform log length, < 0 if not a 32-bit batch product
 int q32_batch_twist_log(const Job& j);      // log2 M of a batched product run twisted, 0 for a whole product
 size_t q32_batch_res_bytes(const Job& j);   // residue arrays of one product

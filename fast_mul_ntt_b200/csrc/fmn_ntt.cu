@@ -614,6 +614,9 @@ struct CrtArgs {
     u64 low_N;
     u64 wrap;
     u64 low_cst[3];
+    // twisted (see k_twist_w64): `low` holds W (plain, reduced; low_cst = M_i^-1 2^64), res_k
+    // already holds c_k for k < K, and c_{N+k} = W_k
+    int twisted;
 };
 
 __host__ __device__ constexpr u64 m_lo(int i) {
@@ -670,29 +673,30 @@ __device__ __forceinline__ void crt_of(u64 r0, u64 r1, u64 r2, const u64 (&cst)[
 }
 
 // Where coefficient j of a wrapped product comes from (see CrtArgs): 0 res_j, 1 low_j,
-// 2 res_{j-N} - low_{j-N}.
-template <bool WRAP>
+// 2 res_{j-N} - low_{j-N}, 3 (twisted) W_{j-N}.  MODE 0 plain, 1 low product, 2 twisted.
+template <int MODE>
 __device__ __forceinline__ int src64(const CrtArgs& a, u64 j) {
-    return !WRAP ? 0 : (j >= a.N ? 2 : (j < a.wrap ? 1 : 0));
+    return MODE == 0 ? 0 : MODE == 2 ? (j >= a.N ? 3 : 0) : (j >= a.N ? 2 : (j < a.wrap ? 1 : 0));
 }
 // c_j mod p_i times M_i^-1, in [0, p_i), from source src.
 __device__ __forceinline__ u64 y_of(const CrtArgs& a, int src, u64 j, int i, const PrimeRT& q) {
     if (src == 0) return red1(mmul(a.res[i * a.N + j], a.cst[i], q), q);
-    const u64 jj = src == 2 ? j - a.N : j;
+    const u64 jj = src == 1 ? j : j - a.N;
     const u64 yl = red1(mmul(a.low[i * a.low_N + jj], a.low_cst[i], q), q);
-    if (src == 1) return yl;
+    if (src != 2) return yl;
     return red1(red1(mmul(a.res[i * a.N + jj], a.cst[i], q), q) + q.p - yl, q);
 }
-template <bool WRAP>
+template <int MODE>
 __device__ __forceinline__ void crt_coef(const CrtArgs& a, u64 j, u64& w0, u64& w1, u64& w2,
                                          const PrimeRT& q0, const PrimeRT& q1, const PrimeRT& q2) {
+    constexpr bool WRAP = MODE != 0;
     w0 = w1 = w2 = 0;
     if (j >= a.nvalid) return;
     if (!WRAP) {
         crt_of(a.res[j], a.res[a.N + j], a.res[2 * a.N + j], a.cst, w0, w1, w2, q0, q1, q2);
         return;
     }
-    const int src = src64<WRAP>(a, j);
+    const int src = src64<MODE>(a, j);
     crt_acc(y_of(a, src, j, 0, q0), y_of(a, src, j, 1, q1), y_of(a, src, j, 2, q2), w0, w1, w2);
 }
 
@@ -702,8 +706,9 @@ __device__ __forceinline__ void crt_coef(const CrtArgs& a, u64 j, u64& w0, u64& 
 constexpr int WCE = 8;
 constexpr u64 WCTILE = (u64)CNT * WCE;
 
-template <bool WRAP>
+template <int MODE>
 __device__ __forceinline__ void crt_carry_body(const CrtArgs& a, u32 ncta) {
+    constexpr bool WRAP = MODE != 0;
     __shared__ u64 s_hw[CNT / 32][3];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const PrimeRT q0 = c_prime[0], q1 = c_prime[1], q2 = c_prime[2];
@@ -718,7 +723,7 @@ __device__ __forceinline__ void crt_carry_body(const CrtArgs& a, u32 ncta) {
     u64 pw1 = 0, pw2 = 0, ppw2 = 0;          // c_{j-1}[1], c_{j-1}[2], c_{j-2}[2]
     // wrapped: the vector path takes threads whose coefficients all come from res; the few
     // around and beyond the wrap boundaries go coefficient by coefficient
-    const bool full = j0 + WCE <= a.nvalid && (!WRAP || (src64<WRAP>(a, j0) == 0 && src64<WRAP>(a, j0 + WCE - 1) == 0));
+    const bool full = j0 + WCE <= a.nvalid && (!WRAP || (src64<MODE>(a, j0) == 0 && src64<MODE>(a, j0 + WCE - 1) == 0));
 #pragma unroll
     for (int e2 = 0; e2 < WCE; e2 += 2) {
         u64 r0[2], r1[2], r2[2];
@@ -733,7 +738,7 @@ __device__ __forceinline__ void crt_carry_body(const CrtArgs& a, u32 ncta) {
             const int e = e2 + u;
             u64 w0, w1, w2;
             if (full) crt_of(r0[u], r1[u], r2[u], a.cst, w0, w1, w2, q0, q1, q2);
-            else crt_coef<WRAP>(a, j0 + e, w0, w1, w2, q0, q1, q2);
+            else crt_coef<MODE>(a, j0 + e, w0, w1, w2, q0, q1, q2);
             u64 l = w0;
             u32 hh = 0;
             add_to(l, hh, pw1);
@@ -762,8 +767,8 @@ __device__ __forceinline__ void crt_carry_body(const CrtArgs& a, u32 ncta) {
             n3 = s_hw[warp - 1][2];
         } else {
             u64 u0, u1, u2, v0, v1, v2;
-            if (j0 >= 1) crt_coef<WRAP>(a, j0 - 1, u0, u1, u2, q0, q1, q2); else u0 = u1 = u2 = 0;
-            if (j0 >= 2) crt_coef<WRAP>(a, j0 - 2, v0, v1, v2, q0, q1, q2); else v0 = v1 = v2 = 0;
+            if (j0 >= 1) crt_coef<MODE>(a, j0 - 1, u0, u1, u2, q0, q1, q2); else u0 = u1 = u2 = 0;
+            if (j0 >= 2) crt_coef<MODE>(a, j0 - 2, v0, v1, v2, q0, q1, q2); else v0 = v1 = v2 = 0;
             n1 = u1;
             n2 = u2;
             n3 = v2;
@@ -778,9 +783,101 @@ __device__ __forceinline__ void crt_carry_body(const CrtArgs& a, u32 ncta) {
 
 // 5 CTAs per SM (48 registers, no spills): while one CTA's warps wait at the barrier of its
 // look-back, the others compute.
-__global__ void __launch_bounds__(CNT, 5) k_crt_carry(CrtArgs a) { crt_carry_body<false>(a, 0xffffffffu); }
+__global__ void __launch_bounds__(CNT, 5) k_crt_carry(CrtArgs a) { crt_carry_body<0>(a, 0xffffffffu); }
 // Wrapped products (see CrtArgs): 62 registers, 4 CTAs (5 spilled).
-__global__ void __launch_bounds__(CNT, 4) k_crt_carry_wrap(CrtArgs a) { crt_carry_body<true>(a, 0xffffffffu); }
+__global__ void __launch_bounds__(CNT, 4) k_crt_carry_wrap(CrtArgs a) { crt_carry_body<1>(a, 0xffffffffu); }
+__global__ void __launch_bounds__(CNT, 4) k_crt_carry_twist(CrtArgs a) { crt_carry_body<2>(a, 0xffffffffu); }
+
+// ------------------------------------------------------------------ twisted products
+// The 32-bit engine's twisted form (fmn_ntt32.cu, k_qtwist_fold / k_qtwist_w) restated for
+// limbs: the product is U = C mod (X^N - 1) (the cyclic transform of length N) and
+// V = C mod (X^M - c), a cyclic transform of length M = N / 2^s of both operands folded modulo
+// X^M - c and twisted by gamma^g (gamma of order 2N, c = gamma^M, so c^(2^s) = -1); then
+// W = (sum_j c^j U_{k+jM} - V) / 2 gives c_{N+k} = W_k and c_k = U_k - W_k for k < K.
+// Residues are plain values below 2p, as the entry pass produces them.
+constexpr int kMaxFolds64 = 4;
+constexpr u32 MASK30 = (1u << MAX_LOG_N) - 1;
+struct FoldArgs64 {
+    const u64* src;
+    u64 len;                      // limbs
+    u64* T;                       // prime i at T + i M
+    int logM, fold_log, tw_log;   // gamma = w_{2^30}^(2^tw_log)
+    ulonglong2 cpow[3][kMaxFolds64];   // c^j mod p_i (plain) and floor(c^j 2^64 / p_i)
+};
+// Entry g (< M) of prime i: gamma^g sum_{j < 2^fold_log} c^j a_{g + jM} mod p_i, a the limbs
+// (zero past the end); one thread per g, the limbs loaded once for all three primes.
+__global__ void __launch_bounds__(256) k_twist_fold64(FoldArgs64 f) {
+    const u64 M = 1ull << f.logM;
+    const int F = 1 << f.fold_log;
+    const u64 g0 = blockIdx.x * (u64)blockDim.x + threadIdx.x, S = (u64)gridDim.x * blockDim.x;
+    // gamma^g in Montgomery form, stepped by gamma^S along the grid-stride loop
+    u64 gm[3], gs[3];
+#pragma unroll
+    for (int pi = 0; pi < 3; ++pi) {
+        gm[pi] = root30((u32)((g0 << f.tw_log) & MASK30), pi, c_prime[pi]);
+        gs[pi] = root30((u32)((S << f.tw_log) & MASK30), pi, c_prime[pi]);
+    }
+    for (u64 g = g0; g < M; g += S) {
+        const u64 left = f.len > g ? (f.len - g + M - 1) >> f.logM : 0;
+        const int nf = left < (u64)F ? (int)left : F;
+        u64 x[kMaxFolds64];
+#pragma unroll
+        for (int j = 0; j < kMaxFolds64; ++j) x[j] = j < nf ? __ldg(f.src + g + ((u64)j << f.logM)) : 0ull;
+#pragma unroll
+        for (int pi = 0; pi < 3; ++pi) {
+            const PrimeRT q = c_prime[pi];
+            u64 acc = smul(x[0], f.cpow[pi][0].x, f.cpow[pi][0].y, q);            // [0, 2p)
+#pragma unroll
+            for (int j = 1; j < kMaxFolds64; ++j)
+                if (j < nf) acc = red2(acc + smul(x[j], f.cpow[pi][j].x, f.cpow[pi][j].y, q), q);
+            f.T[(u64)pi * M + g] = mmul(acc, gm[pi], q);                           // (0, 2p)
+            gm[pi] = mmul(gm[pi], gs[pi], q);
+        }
+    }
+}
+
+struct TwistArgs64 {
+    u64* U;                       // cyclic product's residues (prime i at U + i N), raw
+    u64* V;                       // twisted product's residues (prime i at V + i M), raw; W on return
+    u64 N, K;
+    int logM, fold_log, tw_log;
+    u64 cstM[3];                  // M^-1 2^128 mod p_i
+    ulonglong2 ucj[3][kMaxFolds64];   // c^j N^-1 2^64 mod p_i (Shoup pairs): U raw -> c^j U
+    ulonglong2 nraw[3];           // N 2^-64 mod p_i (Shoup pair): a coefficient -> U's raw form
+};
+// Raw residues after the inverse transform are r = x N 2^-64 (x the convolution entry, see
+// the CRT constants), so x = r N^-1 2^64; V's entries also carry gamma^k.  For k < K the kernel
+// writes W_k (plain, reduced) over V_k and U_k - W_k (raw) over U_k; U_{k+jM} with j >= 1 lie
+// at or above M >= K, so updating U_k in place is safe.
+__global__ void __launch_bounds__(256) k_twist_w64(TwistArgs64 t) {
+    const int pi = blockIdx.y;
+    const PrimeRT q = c_prime[pi];
+    const int F = 1 << t.fold_log;
+    u64* __restrict__ U = t.U + (u64)pi * t.N;
+    u64* __restrict__ V = t.V + ((u64)pi << t.logM);
+    const u64 k0 = blockIdx.x * (u64)blockDim.x + threadIdx.x, S = (u64)gridDim.x * blockDim.x;
+    // gamma^-k M^-1 2^128 (Montgomery form of gamma^-k times cstM 2^-64), stepped by gamma^-S
+    u64 gm = mmul(root30((u32)((0ull - (k0 << t.tw_log)) & MASK30), pi, q), t.cstM[pi], q);
+    const u64 gs = root30((u32)((0ull - (S << t.tw_log)) & MASK30), pi, q);
+    for (u64 k = k0; k < t.K; k += S) {
+        u64 x[kMaxFolds64];
+#pragma unroll
+        for (int j = 0; j < kMaxFolds64; ++j) x[j] = j < F ? U[k + ((u64)j << t.logM)] : 0ull;
+        const u64 vr = V[k];
+        const u64 u0 = red1(smul(x[0], t.ucj[pi][0].x, t.ucj[pi][0].y, q), q);          // U_k
+        u64 ub = u0;
+#pragma unroll
+        for (int j = 1; j < kMaxFolds64; ++j)
+            if (j < F) ub = red1(ub + red1(smul(x[j], t.ucj[pi][j].x, t.ucj[pi][j].y, q), q), q);
+        // vr < 4p: its factor must be below p for vr * factor < p 2^64 (p2 > 2^61)
+        const u64 v = red1(mmul(vr, red1(gm, q), q), q);                                 // V_k, untwisted
+        const u64 d = red1(ub + q.p - v, q);                                             // U mod (X^M - c) - V
+        const u64 w = (d + ((d & 1) ? q.p : 0)) >> 1;
+        V[k] = w;
+        U[k] = smul(red1(u0 + q.p - w, q), t.nraw[pi].x, t.nraw[pi].y, q);              // c_k = U_k - W_k, raw
+        gm = mmul(gm, gs, q);
+    }
+}
 
 // ------------------------------------------------------------------ host: tables
 static u64 h_mulmod(u64 a, u64 b, u64 m) { return (u64)(((unsigned __int128)a * b) % m); }
@@ -800,6 +897,7 @@ static const u64 kG[3] = {5, 5, 3};   // primitive roots (src/data.h:69-71)
 struct HostTables {
     std::vector<u64> rt;   // [2][3][RT_SIZE][2]: (w, floor(w 2^64 / p)) plain Shoup pairs
     std::vector<u64> tw;   // [2][3][1 << TWB]
+    u64 w30[3];            // the root of order 2^30 of each prime that all tables use
 };
 
 static const HostTables& host_tables() {
@@ -812,6 +910,7 @@ static const HostTables& host_tables() {
             const u64 p = kP[i];
             const u64 r1 = (u64)((((unsigned __int128)1) << 64) % p);
             const u64 w = h_pow(kG[i], (p - 1) >> MAX_LOG_N, p);     // root of order 2^30
+            T.w30[i] = w;
             std::vector<u64> lo(1u << TWB), hi(1u << TWB);
             const u64 whi = h_pow(w, 1ull << TWB, p);
             u64 cl = 1, ch = 1;
@@ -1061,10 +1160,12 @@ struct WsLayout {
     size_t a, b, ticket, state, total;
     u64 ncta;
     // wrapped (wrap = K > 0): the cyclic product at N plus the product of both operands'
-    // lowest K limbs, a whole product at NL points whose residues sit at la_off / lb_off
+    // lowest K limbs, a whole product at NL points whose residues sit at la_off / lb_off; or,
+    // twisted, the product modulo X^NL - c of both operands folded (see k_twist_fold64)
     u64 wrap;
     u64 NL;
     size_t la_off, lb_off;
+    bool twist;
 };
 
 // Wrapped plan of this engine (the 32-bit engine's plan_wrap, restated for limbs): a product
@@ -1074,8 +1175,13 @@ struct WsLayout {
 // exactly), and the CRT + carry kernel separates the two (k_crt_carry_wrap).  Taken when its
 // modelled cost, (1 + 2) transforms of N and of NL = ceil_pow2(2K - 1) points x (log + 1)
 // plus one launch sequence, is below the whole product's at 2N, or when fmn_force_wrap asks.
+// The twisted form (k_twist_fold64, k_twist_w64) needs a product modulo X^M - c of only
+// M = 2^m >= K points (N / M <= 4, m >= 12) instead of the low product's 2K, at the price of the
+// folded entry and the W pass; the cheapest of the three plans is taken (fmn_force_wrap(1)
+// forces the low product, 2 the twisted form where it applies).
 constexpr double kSeqCost64 = 1.25e7;      // launch overhead of one launch sequence, in (points x bits)
-static bool wrap64_plan(u64 la, u64 lb, int sqr, u64* N_out, u64* K_out, u64* NL_out) {
+constexpr int kMinTwistLog64 = 12;
+static bool wrap64_plan(u64 la, u64 lb, int sqr, u64* N_out, u64* K_out, u64* NL_out, bool* twist_out) {
     if (la == 0 || lb == 0) return false;
     const u64 dc = la + lb - 1;
     if (dc < 3) return false;
@@ -1088,10 +1194,29 @@ static bool wrap64_plan(u64 la, u64 lb, int sqr, u64* N_out, u64* K_out, u64* NL
     const double t = sqr ? 2.0 : 3.0;
     const double whole = t * (double)(2 * N) * (n + 2);
     const double wrap = t * (double)N * (n + 1) + t * (double)NL * (ilog2(NL) + 1) + kSeqCost64;
-    if (!(q32_forced_wrap() ? true : wrap < whole)) return false;
+    int m = ilog2(K);                          // ilog2 rounds up: 2^m >= K
+    if (m < n - 2) m = n - 2;
+    if (m < kMinTwistLog64) m = kMinTwistLog64;
+    const bool tw_ok = m <= n;
+    const u64 M = 1ull << m;
+    const double F = tw_ok ? (double)(1ull << (n - m)) : 0.0;
+    // folds and W: elementwise passes over F limbs / residues per point, about half a butterfly level each
+    const double twist = t * (double)N * (n + 1) + t * (double)M * (m + 1) +
+                         0.5 * ((sqr ? 1.0 : 2.0) * (double)M * F + (double)K * (F + 3.0)) + kSeqCost64;
+    // the cost model must promise 15%: the second product computes its four-step twiddles
+    // (no tables) and a negacyclic M = N plan models within a few percent of the whole one
+    // but measured slower (64M x 64M: 31.8 against 27.6 ms)
+    const double limit = 0.85 * whole;
+    const int fw = q32_forced_wrap();
+    bool use_twist;
+    if (fw == 1) use_twist = false;
+    else if (fw == 2) use_twist = tw_ok;
+    else if (wrap >= limit && (!tw_ok || twist >= limit)) return false;
+    else use_twist = tw_ok && twist < wrap && twist < limit;
     *N_out = N;
     *K_out = K;
-    *NL_out = NL;
+    *NL_out = use_twist ? M : NL;
+    *twist_out = use_twist;
     return true;
 }
 
@@ -1105,10 +1230,12 @@ static WsLayout ws_layout(u64 la, u64 lb, int sqr, int force_n = 0, bool wrap_ok
     w.N = ceil_pow2(out_len - 1);
     if (force_n > 0 && (1ull << force_n) > w.N) w.N = 1ull << force_n;
     u64 N = 0, K = 0, NL = 0;
-    if (wrap_ok && force_n <= 0 && wrap64_plan(la, lb, sqr, &N, &K, &NL)) {
+    bool tw = false;
+    if (wrap_ok && force_n <= 0 && wrap64_plan(la, lb, sqr, &N, &K, &NL, &tw)) {
         w.N = N;
         w.wrap = K;
         w.NL = NL;
+        w.twist = tw;
     }
     w.n = ilog2(w.N);
     w.ncta = (out_len + WCTILE - 1) / WCTILE;
@@ -1170,6 +1297,12 @@ size_t job_workspace_bytes(const Job& j) {
 u64 wrap64_for(const Job& j) {
     if (j.spectrum || j.la == 0 || j.lb == 0) return 0;
     return ws_layout(j.la, j.lb, j.sqr, 0, wrap_ok(j)).wrap;
+}
+
+u64 twist64_for(const Job& j) {
+    if (j.spectrum || j.la == 0 || j.lb == 0) return 0;
+    const WsLayout w = ws_layout(j.la, j.lb, j.sqr, 0, wrap_ok(j));
+    return w.twist ? w.NL : 0;
 }
 
 int job_twiddle_log_n(const Job& j) {
@@ -1341,8 +1474,9 @@ int job_launches(u64 la, u64 lb, int sqr) {
     if (la == 0 || lb == 0) return 0;
     if (job_engine(plain_job(la, lb, sqr)) == ENGINE_32) return q32_launches(la, lb, sqr);
     const WsLayout w = ws_layout(la, lb, sqr, 0, true);
-    // a wrapped product adds the low product's pass launches (its own CRT is not run)
-    return launches64(w.n, sqr) + (w.wrap ? launches64(ilog2(w.NL), sqr) - 1 : 0);
+    // a wrapped product adds the second product's pass launches (its own CRT is not run) and,
+    // twisted, the folds and the W kernel
+    return launches64(w.n, sqr) + (w.wrap ? launches64(ilog2(w.NL), sqr) - 1 : 0) + (w.twist ? (sqr ? 2 : 3) : 0);
 }
 
 // Every launch one product needs, in order, with its arguments (no launch happens here).
@@ -1370,7 +1504,10 @@ struct JobScratch {
 
 // wrap: the layout may take the wrapped plan (single products); the caller then plans and
 // launches the low product itself (enqueue_job) and fills the CRT's wrap fields.
-static void plan_job(const Job& j, const JobScratch& sc, const TwiddleSet* tws, JobLaunches* out, bool wrap = false) {
+// prefolded: the operands' residues are already in the scratch arrays (a twisted product's
+// folded operands), so the first pass reads them instead of the limbs.
+static void plan_job(const Job& j, const JobScratch& sc, const TwiddleSet* tws, JobLaunches* out, bool wrap = false,
+                     bool prefolded = false) {
     const u64 out_len = j.la + j.lb;
     const int sqr = j.sqr ? 1 : 0;
     const WsLayout w = ws_layout(j.la, j.lb, sqr, j.spectrum ? j.log_n : 0, wrap && wrap_ok(j));
@@ -1407,7 +1544,7 @@ static void plan_job(const Job& j, const JobScratch& sc, const TwiddleSet* tws, 
             pa.data = data;
             pa.logB = logB[p];
             pa.tw = tws ? tws->fwd[p] : nullptr;
-            add(p == 0 ? V_FWD_E : V_FWD, pl.bits[p], pa, N >> (pl.bits[p] + 4));
+            add(p == 0 && !prefolded ? V_FWD_E : V_FWD, pl.bits[p], pa, N >> (pl.bits[p] + 4));
         }
     };
     const bool merged = !sqr && !j.spectrum && P >= 2 && lastl >= 5 && lastl <= 8;   // two tiles fit
@@ -1503,27 +1640,113 @@ static void plan_job(const Job& j, const JobScratch& sc, const TwiddleSet* tws, 
 static cudaError_t launch_crt(const CrtArgs& ca, u64 ncta, cudaStream_t s) {
     const double crt_bytes = 3.0 * (double)ca.nvalid * 8.0 + 3.0 * (double)ca.wrap * 16.0 + (double)ca.out_len * 8.0;
     return timed_launch(K_CRT, crt_bytes, 3.0 * (double)ca.nvalid, s, [&] {
-        if (ca.wrap) k_crt_carry_wrap<<<(unsigned)ncta, CNT, 0, s>>>(ca);
+        if (ca.twisted) k_crt_carry_twist<<<(unsigned)ncta, CNT, 0, s>>>(ca);
+        else if (ca.wrap) k_crt_carry_wrap<<<(unsigned)ncta, CNT, 0, s>>>(ca);
         else k_crt_carry<<<(unsigned)ncta, CNT, 0, s>>>(ca);
     });
 }
 
-// The low product of a wrapped 64-bit product (see wrap64_plan): the operands' lowest K limbs
-// as an ordinary whole product into the layout's low arrays; its inverse spectrum is left in
-// place for the main CRT, whose wrap fields this fills.
-static void plan_low64(const Job& j, const WsLayout& w, char* base, const JobScratch& sc, JobLaunches* low,
-                       CrtArgs* ca) {
+// w^e mod p_i (plain form) for the tables' root w of order 2^30, e taken mod 2^30.
+static u64 h_root64(int i, u64 e) { return h_pow(host_tables().w30[i], e & MASK30, kP[i]); }
+// (w, floor(w 2^64 / p_i)): w as a Shoup constant.
+static ulonglong2 h_shoup64(u64 w, int i) {
+    return make_ulonglong2(w, (u64)(((unsigned __int128)w << 64) / kP[i]));
+}
+
+// The second product of a wrapped 64-bit product (see wrap64_plan) and what the main CRT takes
+// from it: the low product (an ordinary whole product of the operands' lowest K limbs) or,
+// twisted, the folds of both operands, the transform of the folded operands and the W kernel.
+struct Side64 {
+    JobLaunches rec;              // pass launches of the second product
+    bool twist;
+    int nfold;
+    FoldArgs64 fold[2];
+    u64 fold_blocks, w_blocks;
+    TwistArgs64 tw;
+};
+static void plan_side64(const Job& j, const WsLayout& w, char* base, const JobScratch& sc, Side64* sd, CrtArgs* ca) {
+    const int sqr = j.sqr ? 1 : 0;
     Job jl = j;
-    jl.la = w.wrap;
-    jl.lb = w.wrap;
     jl.out = nullptr;
     jl.no_wrap = true;
     JobScratch scl{(u64*)(base + w.la_off), (u64*)(base + w.lb_off), sc.ticket, sc.state, sc.err};
-    plan_job(jl, scl, nullptr, low);
+    sd->twist = w.twist;
+    sd->nfold = 0;
     ca->low = scl.A;
-    ca->low_N = low->crt.N;
     ca->wrap = w.wrap;
-    for (int i = 0; i < 3; ++i) ca->low_cst[i] = low->crt.cst[i];
+    if (!w.twist) {
+        jl.la = w.wrap;
+        jl.lb = w.wrap;
+        plan_job(jl, scl, nullptr, &sd->rec);
+        ca->low_N = sd->rec.crt.N;
+        for (int i = 0; i < 3; ++i) ca->low_cst[i] = sd->rec.crt.cst[i];
+        return;
+    }
+    const u64 N = w.N, M = w.NL;
+    const int n = w.n, m = ilog2(M), tw_log = MAX_LOG_N - 1 - n;   // gamma of order 2N
+    jl.la = jl.lb = M / 2;                                       // a transform of M points
+    plan_job(jl, scl, nullptr, &sd->rec, false, true);
+    for (int op = 0; op < (sqr ? 1 : 2); ++op) {
+        FoldArgs64& f = sd->fold[sd->nfold++];
+        memset(&f, 0, sizeof(f));
+        f.src = op ? j.b : j.a;
+        f.len = op ? j.lb : j.la;
+        f.T = op ? scl.B : scl.A;
+        f.logM = m;
+        f.fold_log = n - m;
+        f.tw_log = tw_log;
+        for (int i = 0; i < 3; ++i)
+            for (int jj = 0; jj < kMaxFolds64; ++jj) f.cpow[i][jj] = h_shoup64(h_root64(i, (u64)jj << (m + tw_log)), i);
+    }
+    sd->fold_blocks = (M + 255) / 256 < 1184 ? (M + 255) / 256 : 1184;
+    TwistArgs64& t = sd->tw;
+    memset(&t, 0, sizeof(t));
+    t.U = sc.A;
+    t.V = scl.A;
+    t.N = N;
+    t.K = w.wrap;
+    t.logM = m;
+    t.fold_log = n - m;
+    t.tw_log = tw_log;
+    for (int i = 0; i < 3; ++i) {
+        const u64 p = kP[i];
+        const u64 r64 = (u64)((((unsigned __int128)1) << 64) % p), r128 = h_mulmod(r64, r64, p);
+        const u64 ninv = h_pow(N % p, p - 2, p), inv_r64 = h_pow(r64, p - 2, p);
+        t.cstM[i] = h_mulmod(h_pow(M % p, p - 2, p), r128, p);
+        for (int jj = 0; jj < kMaxFolds64; ++jj)   // c^j N^-1 2^64
+            t.ucj[i][jj] = h_shoup64(h_mulmod(h_mulmod(h_root64(i, (u64)jj << (m + tw_log)), ninv, p), r64, p), i);
+        t.nraw[i] = h_shoup64(h_mulmod(N % p, inv_r64, p), i);   // N 2^-64
+        // W is plain: y = W M_i^-1 (M_i the product of the other two primes)
+        const unsigned __int128 Mi = (unsigned __int128)kP[(i + 1) % 3] * kP[(i + 2) % 3];
+        ca->low_cst[i] = h_mulmod(h_pow((u64)(Mi % p), p - 2, p), r64, p);
+    }
+    sd->w_blocks = (w.wrap + 255) / 256 < 2048 ? (w.wrap + 255) / 256 : 2048;
+    ca->low_N = M;
+    ca->twisted = 1;
+}
+// The folds and the second product's passes (they read both operands).
+static cudaError_t run_side64(const Side64& sd, cudaStream_t s) {
+    cudaError_t e;
+    for (int f = 0; f < sd.nfold; ++f) {
+        const FoldArgs64& fa = sd.fold[f];
+        const double M = (double)(1ull << fa.logM);
+        e = timed_launch(K_WRAP, (double)fa.len * 8.0 + 3.0 * M * 8.0, 3.0 * M * (2.0 + (double)(1 << fa.fold_log)), s,
+                         [&] { k_twist_fold64<<<(unsigned)sd.fold_blocks, 256, 0, s>>>(fa); });
+        if (e != cudaSuccess) return e;
+    }
+    for (int k = 0; k < sd.rec.count; ++k)
+        if ((e = launch_pass(sd.rec.rec[k].variant, sd.rec.rec[k].logl, sd.rec.rec[k].pa, sd.rec.rec[k].tiles, s)) !=
+            cudaSuccess)
+            return e;
+    return cudaSuccess;
+}
+// Twisted: the W kernel, after the cyclic product's inverse passes.
+static cudaError_t run_side64_w(const Side64& sd, cudaStream_t s) {
+    if (!sd.twist) return cudaSuccess;
+    const TwistArgs64& t = sd.tw;
+    const double F = (double)(1 << t.fold_log);
+    return timed_launch(K_WRAP, 3.0 * (double)t.K * 8.0 * (F + 3.0), 3.0 * (double)t.K * (F + 3.0), s,
+                        [&] { k_twist_w64<<<dim3((unsigned)sd.w_blocks, 3), 256, 0, s>>>(t); });
 }
 
 cudaError_t enqueue_job(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s, const TwiddleSet* tws) {
@@ -1541,17 +1764,19 @@ cudaError_t enqueue_job(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s,
                   (u32*)base};
     JobLaunches L;
     plan_job(j, sc, tws, &L, true);
+    Side64 sd;
+    sd.rec.count = 0;
+    sd.twist = false;
+    sd.nfold = 0;
     if (w.wrap) {
-        JobLaunches LL;
-        plan_low64(j, w, base, sc, &LL, &L.crt);
-        for (int k = 0; k < LL.count; ++k)
-            if ((e = launch_pass(LL.rec[k].variant, LL.rec[k].logl, LL.rec[k].pa, LL.rec[k].tiles, s)) != cudaSuccess)
-                return e;
+        plan_side64(j, w, base, sc, &sd, &L.crt);
+        if ((e = run_side64(sd, s)) != cudaSuccess) return e;
     }
     for (int k = 0; k < L.count; ++k) {
         const LaunchRec& r = L.rec[k];
         if ((e = launch_pass(r.variant, r.logl, r.pa, r.tiles, s)) != cudaSuccess) return e;
     }
+    if ((e = run_side64_w(sd, s)) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(base + w.ticket, 0, w.total - w.ticket, s)) != cudaSuccess) return e;
     return launch_crt(L.crt, L.ncta, s);
 }
@@ -1570,20 +1795,19 @@ cudaError_t enqueue_job_overlapped(const Job& j, void* ws, size_t ws_bytes, cuda
     char* base = (char*)ws;
     JobScratch sc{(u64*)(base + w.a), (u64*)(base + w.b), (u32*)(base + w.ticket), (u32*)(base + w.state),
                   (u32*)base};
-    JobLaunches L, LL;
+    JobLaunches L;
     plan_job(j, sc, tws, &L, true);
-    LL.count = 0;
-    if (w.wrap) plan_low64(j, w, base, sc, &LL, &L.crt);
-    // the first operand's passes, then (once the second operand is copied) the low product,
+    Side64 sd;
+    sd.rec.count = 0;
+    sd.twist = false;
+    sd.nfold = 0;
+    if (w.wrap) plan_side64(j, w, base, sc, &sd, &L.crt);
+    // the first operand's passes, then (once the second operand is copied) the second product,
     // which reads both, and the rest
-    bool waited = false, low_done = LL.count == 0;
+    bool waited = false, low_done = w.wrap == 0;
     auto run_low = [&]() -> cudaError_t {
-        for (int k = 0; k < LL.count; ++k) {
-            const cudaError_t e2 = launch_pass(LL.rec[k].variant, LL.rec[k].logl, LL.rec[k].pa, LL.rec[k].tiles, s);
-            if (e2 != cudaSuccess) return e2;
-        }
         low_done = true;
-        return cudaSuccess;
+        return run_side64(sd, s);
     };
     for (int k = 0; k < L.count; ++k) {
         const LaunchRec& r = L.rec[k];
@@ -1598,6 +1822,7 @@ cudaError_t enqueue_job_overlapped(const Job& j, void* ws, size_t ws_bytes, cuda
         if (!waited && need_b && !sqr && (e = need_b(need_ctx, 0, j.lb, s)) != cudaSuccess) return e;
         if ((e = run_low()) != cudaSuccess) return e;
     }
+    if ((e = run_side64_w(sd, s)) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(base + w.ticket, 0, w.total - w.ticket, s)) != cudaSuccess) return e;
     // carry scan in chunks of CTAs: tickets continue across launches, each chunk's limbs are
     // final once its launch completes
@@ -1636,7 +1861,7 @@ __global__ void __launch_bounds__(NT, (pass_min_ctas<MODE, LOGL>())) k_pass_batc
 __global__ void __launch_bounds__(CNT) k_crt_carry_batch(const CrtArgs* __restrict__ args, u32 ctas_per_job,
                                                          const u32* __restrict__ ncta) {
     const u32 job = blockIdx.x / ctas_per_job;
-    crt_carry_body<false>(args[job], ncta[job]);
+    crt_carry_body<0>(args[job], ncta[job]);
 }
 
 typedef void (*BatchKernel)(const PassArgs*, u32);

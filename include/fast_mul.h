@@ -245,8 +245,9 @@ int fmn_force_pieces(int pieces);
  * c^(2^n / M) = -1): one cyclic transform of M digits of both operands folded modulo X^M - c
  * and twisted, half the size of the low product; then c_{2^n + k} = W_k and c_k = U_k - W_k
  * with W = (U mod (X^M - c) - V) / 2.  The cost model chooses among whole, split, wrapped and
- * twisted plans; the 64-bit engine (the reference's primes) wraps with the low product of the
- * operands' lowest K limbs.  fmn_wrap_for returns K for a product that runs wrapped (0 otherwise),
+ * twisted plans; the 64-bit engine (the reference's primes) wraps too, with the low product
+ * of the operands' lowest K limbs or the twisted form.  fmn_wrap_for returns K for a product
+ * that runs wrapped (0 otherwise),
  * fmn_twist_for its twisted length M (0 when not twisted); fmn_force_wrap(1) wraps every
  * product that allows it with the low product, fmn_force_wrap(2) twisted (tests),
  * fmn_force_wrap(0) restores the model.  Batched products (fmn_mul_batch_device, the

@@ -137,10 +137,11 @@ def test_engine64_wrapped_products(fmn, oracle, golden, engine64):
                    (2 ** k - 5, 9 * 2 ** (k - 4), False), (2 ** (k - 1) + 7, 2 ** (k - 1) + 7, True)]
     modelled = [(2 ** 19 + 3, 2 ** 19, False), (2 ** 19 + 2 ** 16, 2 ** 19, False), (600000, 700001, False),
                 (2 ** 20 + 7, 2 ** 20 + 7, True)]
-    for mode, shapes in ((1, forced), (0, modelled)):
+    for mode, shapes in ((1, forced), (2, forced), (0, modelled)):
         fmn.force_wrap(mode)
         for i, (la, lb, sq) in enumerate(shapes):
             assert fmn.wrap_for(la, lb, sq) > 0, (mode, la, lb, sq)
+            assert (fmn.twist_for(la, lb, sq) > 0) == (mode == 2) or mode == 0, (mode, la, lb, sq)
             a, b = synth.operands(("uniform", "ones", "sparse")[i % 3], la, lb, 300 + i)
             if sq:
                 assert np.array_equal(fmn.abs_sqr64(a), oracle.sqr(a)), (mode, la)
@@ -158,11 +159,28 @@ def test_engine64_wrapped_products(fmn, oracle, golden, engine64):
     assert n >= 3
 
 
+def test_engine64_twisted_folds(fmn, oracle, engine64):
+    """The 64-bit engine's twisted form with one to four folds (M = 2^n .. 2^(n-2)), squares
+    and operands of unequal length, against the oracle."""
+    fmn.force_wrap(2)
+    n = 14
+    for la, lb, sq in [(2 ** (n - 1) + 5, 2 ** (n - 1), False), (2 ** n - 1, 2 ** (n - 2) + 3, False),
+                       (2 ** n - 1, 2 ** n - 3, False), (2 ** (n - 1) + 9, 2 ** (n - 1) + 9, True),
+                       (2 ** n - 2, 2 ** n - 2, True), (3 * 2 ** (n - 2), 2 ** (n - 1) + 2 ** (n - 3), False)]:
+        assert fmn.twist_for(la, lb, sq) > 0, (la, lb, sq)
+        a, b = synth.operands("ones" if la % 2 else "uniform", la, lb, la + lb)
+        want = oracle.sqr(a) if sq else oracle.mul(a, b)
+        got = fmn.abs_sqr64(a) if sq else fmn.abs_mul64(a, b)
+        assert np.array_equal(got, want), (la, lb, sq, fmn.twist_for(la, lb, sq))
+
+
 def test_engine64_wrapped_10M_matches_reference(fmn, golden, engine64):
-    """10M x 10M on the 64-bit engine runs wrapped (cyclic 2^24 limbs + the 3.2M-limb low
-    product) and equals the reference's digest, on the device path and through abs_mul64."""
+    """10M x 10M on the 64-bit engine runs wrapped (cyclic 2^24 limbs + the twisted product
+    modulo X^(2^22) - c) and equals the reference's digest, on the device path and through
+    abs_mul64."""
     import torch
     assert fmn.wrap_for(10_000_000, 10_000_000) == 3_222_783
+    assert fmn.twist_for(10_000_000, 10_000_000) == 1 << 22
     c = next(c for c in golden if c["op"] == "mul" and c["kind"] == "uniform" and c["len1"] == 10_000_000
              and c["len2"] == 10_000_000)
     a, b = operands_for(c)
