@@ -559,6 +559,20 @@ def rooflines(fmn, prof, steps, engine, peaks, traffic_key):
     return hbm, integer, kernels
 
 
+def plan_label(fmn, l1, l2, sqr=False):
+    """How the library runs this product (whole, split, wrapped or twisted)."""
+    pieces = fmn.pieces_for(l1, l2, sqr)
+    if pieces > 1:
+        return ("the longer operand in %d pieces, each multiplied with the other's resident spectrum" % pieces)
+    k, m = fmn.wrap_for(l1, l2, sqr), fmn.twist_for(l1, l2, sqr)
+    if m:
+        return ("wrapped: the cyclic transform plus the twisted product modulo X^%d - c "
+                "(%d coefficients wrapped)" % (m, k))
+    if k:
+        return "wrapped: the cyclic transform plus the product of the lowest limbs (%d coefficients wrapped)" % k
+    return "one transform of the whole product"
+
+
 def engine_label(fmn, engine):
     return ("32-bit digits mod three 31-bit primes" if engine == fmn.ENGINE_32
             else "64-bit limbs mod the reference's three 62-bit primes")
@@ -630,7 +644,8 @@ def time_config(fmn, torch, dev, op, kind, l1, l2, steps, warmup, peaks):
     hbm, integer, kernels = rooflines(fmn, prof, steps, engine, peaks, key)
     us = 1e3 * total / steps
     res = {"op": op, "kind": kind, "len1": l1, "len2": l2, "engine": engine_label(fmn, engine),
-           "pieces": fmn.pieces_for(l1, l2, op == "sqr"), "steps": steps, "warmup": warmup,
+           "pieces": fmn.pieces_for(l1, l2, op == "sqr"), "plan": plan_label(fmn, l1, l2, op == "sqr"),
+           "steps": steps, "warmup": warmup,
            "us_per_product": us, "products_per_s": 1e6 / us, "limbs_per_s": (l1 + l2) * 1e6 / us,
            "bit_exact": (got_digest == want) if want else None,
            "l2_policy": "256 MB L2 flush before every timed product",
@@ -806,8 +821,7 @@ def run_ours(args, ws, rank, local):
             "data": DATA,
             "config": {"workload": WORKLOAD if (l1, l2) == (LEN1, LEN2) else f"abs_mul64 {l1} x {l2} limbs",
                        "len1": l1, "len2": l2, "engine": engine_label(fmn, engine), "pieces": pieces,
-                       "plan": ("the longer operand in %d pieces, each multiplied with the other's resident "
-                                "spectrum" % pieces if pieces > 1 else "one transform of the whole product"),
+                       "plan": plan_label(fmn, l1, l2),
                        "reference_ntt_len": fmn.ntt_len(l1, l2),
                        "parallelism": "replicas: one independent product per GPU" if ws > 1 else "single GPU",
                        "l2_policy": "no flush: operands (%d MB) and scratch (%d MB) per product exceed the 126 MB L2"
