@@ -49,6 +49,7 @@ struct HostLane {
     cudaEvent_t done = nullptr;                              // the lane's last product
     bool done_valid = false;
     cudaEvent_t join[2] = {nullptr, nullptr};
+    cudaEvent_t a_in = nullptr;            // the first operand's copy (shared copy streams)
     cudaEvent_t cb_event[4] = {nullptr};   // chunked copy-back
     cudaEvent_t ci_event[8] = {nullptr};   // piecewise copy-in of the second operand
     void* ws = nullptr;
@@ -163,6 +164,9 @@ struct DevCtx {
     size_t stage_cap = 0;
     cudaEvent_t stage_free = nullptr;   // the last batch's descriptor copy has completed
     bool stage_pending = false;
+    // pinned host products with FMN_COPY_ORDER=fifo: one copy-in and one copy-back stream shared
+    // by all lanes, so copies run in the order the calls enqueued them (created on first use)
+    cudaStream_t cin = nullptr, cout = nullptr;
     // host lanes: created on demand up to host_lanes(), handed out under lane_mu
     std::vector<HostLane*> lanes;
     std::mutex lane_mu;
@@ -260,13 +264,26 @@ int host_lanes() {
     return n;
 }
 
+// Copies of pinned host products: "lane" (default) gives every host lane its own copy streams,
+// so concurrent callers share PCIe between them; "fifo" (FMN_COPY_ORDER=fifo) puts every
+// lane's copies on two streams shared per device, in the order the calls were enqueued, so
+// each call's operands arrive whole before the next call's.  At 10M x 10M on B200: 256-277
+// products/s by lane against 223/s in fifo order from 4 callers; 181-184 against 216 from 6.
+bool copy_fifo() {
+    static const bool f = [] {
+        const char* v = getenv("FMN_COPY_ORDER");
+        return v && strcmp(v, "fifo") == 0;
+    }();
+    return f;
+}
+
 void destroy_lane(HostLane* L) {
     if (L->ws) cudaFree(L->ws);
     if (L->io) cudaFree(L->io);
     if (L->h_err) cudaFreeHost(L->h_err);
     for (cudaStream_t st : {L->s, L->cs, L->co})
         if (st) cudaStreamDestroy(st);
-    for (cudaEvent_t ev : {L->done, L->join[0], L->join[1]})
+    for (cudaEvent_t ev : {L->done, L->join[0], L->join[1], L->a_in})
         if (ev) cudaEventDestroy(ev);
     for (cudaEvent_t ev : L->cb_event)
         if (ev) cudaEventDestroy(ev);
@@ -295,7 +312,7 @@ int acquire_lane(DevCtx* c, HostLane** out) {
     cudaError_t e = cudaSuccess;
     for (cudaStream_t* st : {&L->s, &L->cs, &L->co})
         if (e == cudaSuccess) e = cudaStreamCreateWithFlags(st, cudaStreamNonBlocking);
-    for (cudaEvent_t* ev : {&L->done, &L->join[0], &L->join[1]})
+    for (cudaEvent_t* ev : {&L->done, &L->join[0], &L->join[1], &L->a_in})
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming);
     for (cudaEvent_t& ev : L->cb_event)
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
@@ -495,8 +512,14 @@ int host_product_pinned(DevCtx* c, HostLane* L, const u64* in1, u64 len1, const 
         std::lock_guard<std::mutex> lk(c->mu);
         if ((rc = ensure_buf((void**)&L->io, &L->io_cap, oo + round256(out_len * 8), false))) return rc;
         char* io = (char*)L->io;
-        cudaStream_t s = L->s, cs = L->cs, co = L->co;
         cudaError_t e;
+        const bool fifo = copy_fifo();
+        if (fifo && !c->cin) {
+            if ((e = cudaStreamCreateWithFlags(&c->cin, cudaStreamNonBlocking)) != cudaSuccess ||
+                (e = cudaStreamCreateWithFlags(&c->cout, cudaStreamNonBlocking)) != cudaSuccess)
+                return set_err(FMN_ERR_CUDA, "creating the copy streams", e);
+        }
+        cudaStream_t s = L->s, cs = fifo ? c->cin : L->cs, co = fifo ? c->cout : L->co;
         fmn::Job j;
         j.a = (const u64*)(io + o1);
         j.la = len1;
@@ -505,14 +528,17 @@ int host_product_pinned(DevCtx* c, HostLane* L, const u64* in1, u64 len1, const 
         j.out = (u64*)(io + oo);
         j.sqr = sqr;
         if ((rc = ensure_buf(&L->ws, &L->ws_cap, fmn::job_workspace_bytes(j), true))) return rc;
+        // (the shared streams need no such wait: a call returns only after its own copies)
         if (L->done_valid && ((e = cudaStreamWaitEvent(s, L->done, 0)) != cudaSuccess ||
-                              (e = cudaStreamWaitEvent(cs, L->done, 0)) != cudaSuccess ||
-                              (e = cudaStreamWaitEvent(co, L->done, 0)) != cudaSuccess))
+                              (!fifo && (e = cudaStreamWaitEvent(cs, L->done, 0)) != cudaSuccess) ||
+                              (!fifo && (e = cudaStreamWaitEvent(co, L->done, 0)) != cudaSuccess)))
             return set_err(FMN_ERR_CUDA, "cudaStreamWaitEvent", e);
         const fmn::TwiddleSet* tws =
             fmn::job_engine(j) != fmn::ENGINE_64 ? nullptr : get_twiddles(c, fmn::job_twiddle_log_n(j), s);
-        if ((e = cudaMemcpyAsync(io + o1, in1, len1 * 8, cudaMemcpyHostToDevice, s)) != cudaSuccess)
+        if ((e = cudaMemcpyAsync(io + o1, in1, len1 * 8, cudaMemcpyHostToDevice, fifo ? cs : s)) != cudaSuccess)
             return set_err(FMN_ERR_CUDA, "copying in1 to the device", e);
+        if (fifo && ((e = cudaEventRecord(L->a_in, cs)) != cudaSuccess || (e = cudaStreamWaitEvent(s, L->a_in, 0)) != cudaSuccess))
+            return set_err(FMN_ERR_CUDA, "ordering the product after its first operand", e);
         CopyIn ci;
         ci.copy = cs;
         ci.used = 0;
@@ -781,6 +807,8 @@ void fmn_shutdown(void) {
         if (c->stage_free) cudaEventDestroy(c->stage_free);
         if (c->done) cudaEventDestroy(c->done);
         if (c->stream) cudaStreamDestroy(c->stream);
+        if (c->cin) cudaStreamDestroy(c->cin);
+        if (c->cout) cudaStreamDestroy(c->cout);
         delete c;
         g_ctx[d] = nullptr;
     }
