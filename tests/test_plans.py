@@ -172,6 +172,35 @@ def test_engine_selection_rules():
         fmn.set_engine(7)
 
 
+def test_engine64_wrapped_plans():
+    """The 64-bit engine's wrapped plans (the reference's primes): twisted where the second
+    product's transform is a quarter of the cyclic one (10M x 10M: 2^24 + 2^22 limbs), the low
+    product where K is tiny, the whole transform at exact powers of two (64M x 64M) and for
+    small products (a second launch sequence does not pay), with the 15% margin keeping
+    negacyclic plans whole; batches, spectra and the no-allocation path never wrap, and the
+    scratch follows the plan."""
+    fmn.set_engine(fmn.ENGINE_64)
+    try:
+        assert fmn.wrap_for(10_000_000, 10_000_000) == 20_000_000 - 1 - (1 << 24)
+        assert fmn.twist_for(10_000_000, 10_000_000) == 1 << 22
+        assert fmn.workspace_size(10_000_000, 10_000_000) < 3 * (1 << 25) * 8 * 2     # below the whole plan
+        assert fmn.wrap_for(64_000_000, 64_000_000) == 0                              # 2^27 exactly
+        assert fmn.wrap_for(2 ** 19 + 3, 2 ** 19) == 2 and fmn.twist_for(2 ** 19 + 3, 2 ** 19) == 0
+        assert fmn.wrap_for(5000, 4000) == 0                                          # small: whole
+        # K close to N: the twisted plan would be negacyclic (M = N), the low product as long as
+        # the whole transform; neither is 15% cheaper
+        assert fmn.wrap_for((1 << 20) - 5, (1 << 20) - 7) == 0
+        fmn.force_wrap(2)
+        assert fmn.twist_for(2 ** 13 + 5, 2 ** 13) == 1 << 12                       # four folds
+        assert fmn.twist_for((1 << 14) - 1, (1 << 14) - 3) == 1 << 14                # negacyclic, forced
+        fmn.force_wrap(1)
+        assert fmn.wrap_for(2 ** 13 + 5, 2 ** 13) == 4 and fmn.twist_for(2 ** 13 + 5, 2 ** 13) == 0
+        assert fmn.batch_twist_for(2 ** 13 + 5, 2 ** 13) == 0                        # 64-bit batches stay whole
+    finally:
+        fmn.force_wrap(0)
+        fmn.set_engine(fmn.ENGINE_AUTO)
+
+
 @pytest.mark.gpu
 def test_products_under_engine32_plans(fmn, oracle):
     """32-bit engine: whole products (2^n digits, operands of 2^(n-2) limbs) and a split product
