@@ -358,7 +358,10 @@ size_t round256(size_t x) { return (x + 255) & ~(size_t)255; }
 // Twiddle tables for transforms of 2^log_n points, built on stream s on first use (caller
 // holds c->mu and has ordered s after the context's previous work).  Returns null when the
 // transform has one pass or memory is short; the kernels then generate the twiddles.
-const fmn::TwiddleSet* get_twiddles(DevCtx* c, int log_n, cudaStream_t s) {
+// The cached twiddle tables of length 2^log_n (built on s the first time), or null.  The
+// pointer is into the cache and valid only until the next call; `keep` (a log length, or -1)
+// is never evicted, so a caller that copied one set can look up a second one.
+const fmn::TwiddleSet* get_twiddles(DevCtx* c, int log_n, cudaStream_t s, int keep = -1) {
     const size_t bytes = fmn::twiddle_table_bytes(log_n);
     if (bytes == 0) return nullptr;
     const fmn::Plan cur = fmn::make_plan(log_n);
@@ -382,9 +385,11 @@ const fmn::TwiddleSet* get_twiddles(DevCtx* c, int log_n, cudaStream_t s) {
     size_t held = 0;
     for (auto& t : c->tw) held += t.bytes;
     while (!c->tw.empty() && (held + bytes > cap || c->tw.size() >= 8)) {
-        size_t lru = 0;
-        for (size_t k = 1; k < c->tw.size(); ++k)
-            if (c->tw[k].last_use < c->tw[lru].last_use) lru = k;
+        size_t lru = c->tw.size();
+        for (size_t k = 0; k < c->tw.size(); ++k)
+            if (c->tw[k].set.log_n != keep && (lru == c->tw.size() || c->tw[k].last_use < c->tw[lru].last_use)) lru = k;
+        if (lru == c->tw.size()) break;       // only the kept set is left
+
         cudaFree(c->tw[lru].buf);             // synchronises the device: no job still reads it
         held -= c->tw[lru].bytes;
         c->tw.erase(c->tw.begin() + lru);
@@ -409,6 +414,32 @@ const fmn::TwiddleSet* get_twiddles(DevCtx* c, int log_n, cudaStream_t s) {
     return &c->tw.back().set;
 }
 
+// A 64-bit product's twiddle tables, copied out of the cache: the main transform's and, for a
+// wrapped product, its second transform's (looked up without evicting the first set).
+struct JobTwiddles {
+    fmn::TwiddleSet main, side;
+    bool has_main = false, has_side = false;
+    const fmn::TwiddleSet* main_ptr() const { return has_main ? &main : nullptr; }
+    const fmn::TwiddleSet* side_ptr() const { return has_side ? &side : nullptr; }
+};
+JobTwiddles job_twiddles(DevCtx* c, const fmn::Job& j, cudaStream_t s) {
+    JobTwiddles t;
+    if (fmn::job_engine(j) != fmn::ENGINE_64) return t;
+    const int n = fmn::job_twiddle_log_n(j);
+    if (const fmn::TwiddleSet* p = get_twiddles(c, n, s)) {
+        t.main = *p;
+        t.has_main = true;
+    }
+    const int m = fmn::job_side_log_n(j);
+    if (m > 0 && m != n) {
+        if (const fmn::TwiddleSet* p = get_twiddles(c, m, s, n)) {
+            t.side = *p;
+            t.has_side = true;
+        }
+    }
+    return t;
+}
+
 const fmn::TwiddleSet* ctx_twiddles(void* ctx, int log_n) {
     DevCtx* c = (DevCtx*)ctx;
     return get_twiddles(c, log_n, c->stream);
@@ -428,9 +459,8 @@ int run_job_ctx(DevCtx* c, const fmn::Job& j, cudaStream_t s) {
     cudaError_t e;
     if (c->done_valid && (e = cudaStreamWaitEvent(s, c->done, 0)) != cudaSuccess)
         return set_err(FMN_ERR_CUDA, "cudaStreamWaitEvent", e);
-    const fmn::TwiddleSet* tws = fmn::job_engine(j) != fmn::ENGINE_64 ? nullptr
-                                 : get_twiddles(c, fmn::job_twiddle_log_n(j), s);
-    if ((e = fmn::enqueue_job(j, c->ws, c->ws_cap, s, tws)) != cudaSuccess) {
+    const JobTwiddles tw = job_twiddles(c, j, s);
+    if ((e = fmn::enqueue_job(j, c->ws, c->ws_cap, s, tw.main_ptr(), tw.side_ptr())) != cudaSuccess) {
         std::string m = std::string("kernel launch (") + fmn::launch_diag() + ")";
         return set_err(FMN_ERR_CUDA, m.c_str(), e);
     }
@@ -533,8 +563,7 @@ int host_product_pinned(DevCtx* c, HostLane* L, const u64* in1, u64 len1, const 
                               (!fifo && (e = cudaStreamWaitEvent(cs, L->done, 0)) != cudaSuccess) ||
                               (!fifo && (e = cudaStreamWaitEvent(co, L->done, 0)) != cudaSuccess)))
             return set_err(FMN_ERR_CUDA, "cudaStreamWaitEvent", e);
-        const fmn::TwiddleSet* tws =
-            fmn::job_engine(j) != fmn::ENGINE_64 ? nullptr : get_twiddles(c, fmn::job_twiddle_log_n(j), s);
+        const JobTwiddles tw = job_twiddles(c, j, s);
         if ((e = cudaMemcpyAsync(io + o1, in1, len1 * 8, cudaMemcpyHostToDevice, fifo ? cs : s)) != cudaSuccess)
             return set_err(FMN_ERR_CUDA, "copying in1 to the device", e);
         if (fifo && ((e = cudaEventRecord(L->a_in, cs)) != cudaSuccess || (e = cudaStreamWaitEvent(s, L->a_in, 0)) != cudaSuccess))
@@ -553,8 +582,8 @@ int host_product_pinned(DevCtx* c, HostLane* L, const u64* in1, u64 len1, const 
         cb.src = j.out;
         for (int k = 0; k < 4; ++k) cb.ev[k] = L->cb_event[k];
         const int chunks = out_len >= (1u << 20) ? 4 : 1;
-        if ((e = fmn::enqueue_job_overlapped(j, L->ws, L->ws_cap, s, tws, sqr ? nullptr : copy_in_range, &ci, chunks,
-                                             copy_back_chunk, &cb)) != cudaSuccess)
+        if ((e = fmn::enqueue_job_overlapped(j, L->ws, L->ws_cap, s, tw.main_ptr(), sqr ? nullptr : copy_in_range, &ci,
+                                             chunks, copy_back_chunk, &cb, tw.side_ptr())) != cudaSuccess)
             return set_err(FMN_ERR_CUDA, "kernel launch", e);
         // the copy streams end after the last chunk; order the main stream (and later jobs) after them
         if ((e = cudaEventRecord(L->join[0], co)) != cudaSuccess || (e = cudaStreamWaitEvent(s, L->join[0], 0)) != cudaSuccess ||
@@ -670,9 +699,8 @@ int host_product(const u64* in1, u64 len1, const u64* in2, u64 len2, u64* out, i
     {
         std::lock_guard<std::mutex> lk(c->mu);
         if ((rc = ensure_buf(&L->ws, &L->ws_cap, fmn::job_workspace_bytes(j), true))) return rc;
-        const fmn::TwiddleSet* tws =
-            fmn::job_engine(j) != fmn::ENGINE_64 ? nullptr : get_twiddles(c, fmn::job_twiddle_log_n(j), L->s);
-        if ((e = fmn::enqueue_job(j, L->ws, L->ws_cap, L->s, tws)) != cudaSuccess) {
+        const JobTwiddles tw = job_twiddles(c, j, L->s);
+        if ((e = fmn::enqueue_job(j, L->ws, L->ws_cap, L->s, tw.main_ptr(), tw.side_ptr())) != cudaSuccess) {
             std::string m = std::string("kernel launch (") + fmn::launch_diag() + ")";
             return set_err(FMN_ERR_CUDA, m.c_str(), e);
         }

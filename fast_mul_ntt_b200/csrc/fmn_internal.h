@@ -143,8 +143,9 @@ cudaError_t build_twiddle_tables(int log_n, u64* buf, TwiddleSet* out, cudaStrea
 // when a bounded wait gives up; callers zero it once and read it after the stream is done.
 // `tw` (optional) holds precomputed four-step twiddles for this transform length; without
 // it the kernels generate them.
+// tw_side: a wrapped 64-bit product's second product's tables (job_side_log_n), or null.
 cudaError_t enqueue_job(const Job& job, void* ws, size_t ws_bytes, cudaStream_t stream,
-                        const TwiddleSet* tw = nullptr);
+                        const TwiddleSet* tw = nullptr, const TwiddleSet* tw_side = nullptr);
 
 // A product with copy overlap: before the first launch that reads a range of the second
 // operand's limbs, `need_b(need_ctx, first, end, s)` is called (the caller copies that range
@@ -153,7 +154,8 @@ cudaError_t enqueue_job(const Job& job, void* ws, size_t ws_bytes, cudaStream_t 
 // so the caller can copy those final limbs back while the rest computes.  A split product
 // scans the limbs that a piece completes right after that piece.
 cudaError_t enqueue_job_overlapped(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s, const TwiddleSet* tw,
-                                   NeedLimbs need_b, void* need_ctx, int crt_chunks, ChunkDone after_chunk, void* ctx);
+                                   NeedLimbs need_b, void* need_ctx, int crt_chunks, ChunkDone after_chunk, void* ctx,
+                                   const TwiddleSet* tw_side = nullptr);
 
 // ---- 32-bit engine batches (whole and twisted wrapped products; see enqueue_batch)
 constexpr int Q32_MAX_REC = 2 * (3 * MAX_PASSES + 2);   // pass launches of a twisted product
@@ -174,6 +176,7 @@ int q32_forced_wrap();                      // fmn_force_wrap mode (0: the cost 
 int job_twiddle_log_n(const Job& j);        // 64-bit engine: log2 of the main transform (twiddle tables)
 u64 wrap64_for(const Job& j);               // 64-bit engine: K of a wrapped product, 0 if whole
 u64 twist64_for(const Job& j);              // 64-bit engine: M of a twisted product, 0 otherwise
+int job_side_log_n(const Job& j);           // 64-bit engine: log2 of a wrapped product's second transform, 0 if whole
 int q32_batch_log_n(const Job& j);          // (cyclic) transform log length, < 0 if not a 32-bit batch product
 int q32_batch_twist_log(const Job& j);      // log2 M of a batched product run twisted, 0 for a whole product
 size_t q32_batch_res_bytes(const Job& j);   // residue arrays of one product

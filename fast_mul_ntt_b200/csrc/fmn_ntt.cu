@@ -1299,6 +1299,12 @@ u64 wrap64_for(const Job& j) {
     return ws_layout(j.la, j.lb, j.sqr, 0, wrap_ok(j)).wrap;
 }
 
+int job_side_log_n(const Job& j) {
+    if (j.spectrum || j.la == 0 || j.lb == 0 || job_engine(j) != ENGINE_64) return 0;
+    const WsLayout w = ws_layout(j.la, j.lb, j.sqr, 0, wrap_ok(j));
+    return w.wrap ? ilog2(w.NL) : 0;
+}
+
 u64 twist64_for(const Job& j) {
     if (j.spectrum || j.la == 0 || j.lb == 0) return 0;
     const WsLayout w = ws_layout(j.la, j.lb, j.sqr, 0, wrap_ok(j));
@@ -1664,7 +1670,8 @@ struct Side64 {
     u64 fold_blocks, w_blocks;
     TwistArgs64 tw;
 };
-static void plan_side64(const Job& j, const WsLayout& w, char* base, const JobScratch& sc, Side64* sd, CrtArgs* ca) {
+static void plan_side64(const Job& j, const WsLayout& w, char* base, const JobScratch& sc, Side64* sd, CrtArgs* ca,
+                        const TwiddleSet* tws_side) {
     const int sqr = j.sqr ? 1 : 0;
     Job jl = j;
     jl.out = nullptr;
@@ -1677,7 +1684,7 @@ static void plan_side64(const Job& j, const WsLayout& w, char* base, const JobSc
     if (!w.twist) {
         jl.la = w.wrap;
         jl.lb = w.wrap;
-        plan_job(jl, scl, nullptr, &sd->rec);
+        plan_job(jl, scl, tws_side, &sd->rec);
         ca->low_N = sd->rec.crt.N;
         for (int i = 0; i < 3; ++i) ca->low_cst[i] = sd->rec.crt.cst[i];
         return;
@@ -1685,7 +1692,7 @@ static void plan_side64(const Job& j, const WsLayout& w, char* base, const JobSc
     const u64 N = w.N, M = w.NL;
     const int n = w.n, m = ilog2(M), tw_log = MAX_LOG_N - 1 - n;   // gamma of order 2N
     jl.la = jl.lb = M / 2;                                       // a transform of M points
-    plan_job(jl, scl, nullptr, &sd->rec, false, true);
+    plan_job(jl, scl, tws_side, &sd->rec, false, true);
     for (int op = 0; op < (sqr ? 1 : 2); ++op) {
         FoldArgs64& f = sd->fold[sd->nfold++];
         memset(&f, 0, sizeof(f));
@@ -1749,7 +1756,8 @@ static cudaError_t run_side64_w(const Side64& sd, cudaStream_t s) {
                         [&] { k_twist_w64<<<dim3((unsigned)sd.w_blocks, 3), 256, 0, s>>>(t); });
 }
 
-cudaError_t enqueue_job(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s, const TwiddleSet* tws) {
+cudaError_t enqueue_job(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s, const TwiddleSet* tws,
+                        const TwiddleSet* tws_side) {
     const u64 out_len = j.la + j.lb;
     if (out_len == 0) return cudaSuccess;
     if (j.la == 0 || j.lb == 0) return cudaMemsetAsync(j.out, 0, out_len * sizeof(u64), s);
@@ -1769,7 +1777,7 @@ cudaError_t enqueue_job(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s,
     sd.twist = false;
     sd.nfold = 0;
     if (w.wrap) {
-        plan_side64(j, w, base, sc, &sd, &L.crt);
+        plan_side64(j, w, base, sc, &sd, &L.crt, tws_side);
         if ((e = run_side64(sd, s)) != cudaSuccess) return e;
     }
     for (int k = 0; k < L.count; ++k) {
@@ -1782,7 +1790,8 @@ cudaError_t enqueue_job(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s,
 }
 
 cudaError_t enqueue_job_overlapped(const Job& j, void* ws, size_t ws_bytes, cudaStream_t s, const TwiddleSet* tws,
-                                   NeedLimbs need_b, void* need_ctx, int crt_chunks, ChunkDone after_chunk, void* ctx) {
+                                   NeedLimbs need_b, void* need_ctx, int crt_chunks, ChunkDone after_chunk, void* ctx,
+                                   const TwiddleSet* tws_side) {
     const u64 out_len = j.la + j.lb;
     if (j.la == 0 || j.lb == 0 || out_len == 0) return cudaErrorInvalidValue;
     if (job_engine(j) == ENGINE_32)
@@ -1801,7 +1810,7 @@ cudaError_t enqueue_job_overlapped(const Job& j, void* ws, size_t ws_bytes, cuda
     sd.rec.count = 0;
     sd.twist = false;
     sd.nfold = 0;
-    if (w.wrap) plan_side64(j, w, base, sc, &sd, &L.crt);
+    if (w.wrap) plan_side64(j, w, base, sc, &sd, &L.crt, tws_side);
     // the first operand's passes, then (once the second operand is copied) the second product,
     // which reads both, and the rest
     bool waited = false, low_done = w.wrap == 0;
