@@ -1017,9 +1017,13 @@ int fmn_mul_batch_device(const fmn_job* jobs, int count, void* stream) {
     cudaError_t e;
     if (c->done_valid && (e = cudaStreamWaitEvent(s, c->done, 0)) != cudaSuccess)
         return set_err(FMN_ERR_CUDA, "cudaStreamWaitEvent", e);
-    // twiddle tables are built on the context stream: order s after it
+    // the 64-bit engine's twiddle tables (one lookup per transform length its products use)
+    // are built on the context stream: order s after it
+    u64 lengths = 0;
     for (const auto& j : v)
-        if (j.la && j.lb) ctx_twiddles(c, ilog2_ceil(j.la + j.lb - 1));
+        if (fmn::batch_on_engine64(j)) lengths |= 1ull << ilog2_ceil(j.la + j.lb - 1);
+    for (int n = 0; n < 64; ++n)
+        if (lengths >> n & 1) ctx_twiddles(c, n);
     if ((e = cudaEventRecord(c->wevent[0], c->stream)) != cudaSuccess ||
         (e = cudaStreamWaitEvent(s, c->wevent[0], 0)) != cudaSuccess)
         return set_err(FMN_ERR_CUDA, "ordering after twiddle tables", e);
@@ -1109,7 +1113,7 @@ int fmn_batch_graph_create(const fmn_job* jobs, int count, fmn_batch_graph** out
             return fail(FMN_ERR_CUDA, "event", e);
     // the graph's own twiddle tables, one set per transform length in the batch
     for (const auto& j : v) {
-        if (!j.la || !j.lb) continue;
+        if (!fmn::batch_on_engine64(j)) continue;       // 32-bit batches compute their twiddles
         const int n = ilog2_ceil(j.la + j.lb - 1);
         const size_t bytes = fmn::twiddle_table_bytes(n);
         bool have = false;

@@ -193,6 +193,7 @@ cudaError_t q32_prepare();                  // tables + kernel attributes on the
 
 // ---- batches of products
 u64 batch_twist_for(const Job& j);          // M of a batched product run twisted, 0 if whole
+bool batch_on_engine64(const Job& j);       // a batched product that runs on the 64-bit engine
 // Workspace bytes for a batch (device) and host staging bytes for its launch descriptors.
 size_t batch_workspace_bytes(const Job* jobs, int count);
 size_t batch_stage_bytes(const Job* jobs, int count);

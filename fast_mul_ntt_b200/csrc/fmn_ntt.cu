@@ -1948,6 +1948,8 @@ static int batch_engine(const Job& j) {
     return q32_batch_log_n(j) >= 0 ? ENGINE_32 : ENGINE_64;
 }
 
+bool batch_on_engine64(const Job& j) { return j.la && j.lb && batch_engine(j) == ENGINE_64; }
+
 u64 batch_twist_for(const Job& j) {
     if (j.la == 0 || j.lb == 0 || batch_engine(j) != ENGINE_32) return 0;
     const int m = q32_batch_twist_log(j);
