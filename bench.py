@@ -11,7 +11,9 @@ length taken as the max over ranks.
   e2e     the same metric through the C ABI abs_mul64 with pinned host buffers: each call
           copies both operands host->device and the product device->host.  --e2e-callers
           host threads (default 4) call at once, as the reference arm runs its products on
-          parallel host threads; the one-thread figure is reported beside it;
+          parallel host threads; the one-thread figure is reported beside it, and e2e.link
+          the GPU's host link measured in the same run (pinned copies each way alone and
+          both at once) with the products/s it allows and e2e's fraction of that;
   roofline / roofline_int
           the dominant kernel, timed live with CUDA events inside the timed region, against
           the measured HBM copy bandwidth (MEASURED_PEAKS.json) and against the measured
@@ -695,6 +697,35 @@ def e2e_rate(lib, pa, l1, pb, l2, outs, steps, barrier, dev):
     return max_over_ranks(time.perf_counter() - t0, dev)
 
 
+def link_rates(dev, nbytes=160 << 20, reps=8):
+    """This GPU's host link, pinned buffers: GB/s host->device alone, device->host alone, and
+    each way with both directions busy at once (the end-to-end path's bound)."""
+    import torch
+    h_in = torch.empty(nbytes, dtype=torch.uint8).pin_memory()
+    h_out = torch.empty(nbytes, dtype=torch.uint8).pin_memory()
+    d_in = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+    d_out = torch.zeros(nbytes, dtype=torch.uint8, device=dev)
+    s_in, s_out = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
+
+    def run(h2d, d2h):
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            if h2d:
+                with torch.cuda.stream(s_in):
+                    d_in.copy_(h_in, non_blocking=True)
+            if d2h:
+                with torch.cuda.stream(s_out):
+                    h_out.copy_(d_out, non_blocking=True)
+        torch.cuda.synchronize(dev)
+        return reps * nbytes / (time.perf_counter() - t0) / 1e9
+
+    run(True, True)                                   # warm-up
+    rates = {"h2d_gbs": run(True, False), "d2h_gbs": run(False, True), "both_each_gbs": run(True, True)}
+    del h_in, h_out, d_in, d_out
+    return rates
+
+
 # ----------------------------------------------------------------------------- ours
 def run_ours(args, ws, rank, local):
     import torch
@@ -805,6 +836,7 @@ def run_ours(args, ws, rank, local):
     pg_s = e2e_rate(lib, pg_pa, l1, pg_pb, l2, ppos, e2e_steps, barrier, dev)
     pg_exact = all(bool(np.array_equal(h, got)) for h in pouts)
     del pouts
+    link = link_rates(dev)
 
     result = None
     if rank == 0:
@@ -837,6 +869,9 @@ def run_ours(args, ws, rank, local):
             "e2e": {"value": ws * callers * e2e_steps / e2e_s, "unit": UNIT,
                     "h2d_bytes_per_step": io * callers, "d2h_bytes_per_step": io * callers,
                     "steps": e2e_steps, "bit_exact": e2e_exact, "callers": callers,
+                    # the host link bounds this figure: io bytes each way per product
+                    "link": dict(link, bound_products_per_s=ws * link["both_each_gbs"] * 1e9 / io,
+                                 frac=(ws * callers * e2e_steps / e2e_s) / (ws * link["both_each_gbs"] * 1e9 / io)),
                     "path": ("abs_mul64 (C ABI) on pinned host buffers from %d host threads at once, one "
                              "synchronous call each per step (host wall clock)" % callers),
                     "single_caller": {"value": ws * e2e_steps / e2e1_s, "unit": UNIT,
