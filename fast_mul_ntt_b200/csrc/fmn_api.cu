@@ -267,8 +267,8 @@ int host_lanes() {
 // Copies of pinned host products: "lane" (default) gives every host lane its own copy streams,
 // so concurrent callers share PCIe between them; "fifo" (FMN_COPY_ORDER=fifo) puts every
 // lane's copies on two streams shared per device, in the order the calls were enqueued, so
-// each call's operands arrive whole before the next call's.  At 10M x 10M on B200: 256-277
-// products/s by lane against 223/s in fifo order from 4 callers; 181-184 against 216 from 6.
+// each call's operands arrive whole before the next call's.  At 10M x 10M on B200: 274-280
+// products/s by lane against 224/s in fifo order from 4 callers; 240 against 223 from 6.
 bool copy_fifo() {
     static const bool f = [] {
         const char* v = getenv("FMN_COPY_ORDER");
